@@ -1,0 +1,29 @@
+// Per-alignment control kernels (see align.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "ndt_types.h"
+
+namespace ndt {
+
+constexpr int NDT_ST_WATCHDOG_DEV = 1;
+
+struct StepParams {
+    int compat;
+    int max_iterations;
+    double eps;        // transformation_epsilon: |step| < eps stop test
+    double step_max;   // step_size
+    double step_min;   // eps / 2
+    int watchdog_evals;
+};
+
+int launch_tiles(const int *d_offsets, int B, int *d_tile_begin, Tile *d_tiles, int *d_num_tiles, cudaStream_t st);
+int launch_init(AlignState *d_states, const float *d_guesses, const int *d_offsets, int B, const StepParams &P,
+                double *d_exc, cudaStream_t st);
+int launch_step(AlignState *d_states, const double *d_partials, const int *d_tile_begin, double *d_exc, int B,
+                const StepParams &P, int *d_active, Counters *d_counters, cudaStream_t st);
+int launch_prepare_eval(AlignState *d_state, const double *d_p6, int n, double *d_exc, cudaStream_t st);
+int launch_finalize(const AlignState *d_states, int B, float *d_out, int *d_conv, double *d_fit, int *d_status,
+                    cudaStream_t st);
+
+}  // namespace ndt

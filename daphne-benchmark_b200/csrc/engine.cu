@@ -1,0 +1,561 @@
+// C ABI of the library (include/ndt_b200.h): context, device memory, the
+// per-batch launch sequence and the host-buffer entry points.
+//
+// Device memory is owned by the context and grows on demand (never shrinks),
+// so steady-state calls allocate nothing.  All work of a context is ordered on
+// its own non-blocking stream.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ndt_b200.h"
+#include "align.h"
+#include "derivatives.h"
+#include "grid_build.h"
+#include "ndt_types.h"
+
+using namespace ndt;
+
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= cap && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = bytes < 256 ? 256 : bytes;
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <class T>
+    T *as() const {
+        return (T *)p;
+    }
+};
+
+struct HostBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= cap && p) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = bytes < 256 ? 256 : bytes;
+        cudaError_t e = cudaMallocHost(&p, want);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <class T>
+    T *as() const {
+        return (T *)p;
+    }
+};
+
+}  // namespace
+
+struct ndt_ctx {
+    ndt_params prm{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int num_sms = 148;
+    std::string err;
+    double d1 = 0, d2 = 0;
+    // grid
+    DevBuf map, index, mean, icov32, icov64, count, cell, seg_start, seg_cell, scratch, meta;
+    GridMeta meta_host{};
+    bool have_map = false;
+    int map_points = 0;
+    // batch
+    DevBuf points, offsets, guesses, states, tiles, tile_begin, num_tiles, partials, exc, out_T, out_conv, out_fit,
+        out_status, active, counters, p6, trans;
+    HostBuf h_offsets, h_active, h_counters, h_out;
+    ndt_counters last{};
+    long long launches = 0;
+};
+
+namespace {
+
+int fail(ndt_ctx *c, int code, const std::string &msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(ndt_ctx *c, cudaError_t e, const char *what) {
+    return fail(c, NDT_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                             \
+    do {                                                     \
+        cudaError_t e_ = (call);                             \
+        if (e_ != cudaSuccess) return cuda_fail(c, e_, #call); \
+    } while (0)
+
+// Gauss fitting constants, with the reference's host arithmetic
+// (computeTransformation, kernel.cpp:1181-1185).
+void gauss_constants(const ndt_params &p, double &d1, double &d2) {
+    double outlier = p.outlier_ratio;
+    float res = p.resolution;
+    double c1 = 10 * (1 - outlier);
+    double c2 = outlier / std::pow((double)res, 3.0);
+    double d3 = -std::log(c2);
+    d1 = -std::log(c1 + c2) - d3;
+    d2 = -2 * std::log((-std::log(c1 * std::exp(-0.5) + c2) - d3) / d1);
+}
+
+StepParams step_params(const ndt_params &p) {
+    StepParams s;
+    s.compat = p.compat;
+    s.max_iterations = p.max_iterations;
+    s.eps = p.transformation_epsilon;
+    s.step_max = p.step_size;
+    s.step_min = p.transformation_epsilon / 2;
+    s.watchdog_evals = p.watchdog_evals > 0 ? p.watchdog_evals : 1024;
+    return s;
+}
+
+GridBuffers grid_buffers(ndt_ctx *c) {
+    GridBuffers b;
+    b.index = c->index.as<int32_t>();
+    b.mean = c->mean.as<double4>();
+    b.icov32 = c->icov32.as<float4>();
+    b.icov64 = c->icov64.as<double>();
+    b.count = c->count.as<int32_t>();
+    b.cell = c->cell.as<int32_t>();
+    b.seg_start = c->seg_start.as<int32_t>();
+    b.seg_cell = c->seg_cell.as<uint32_t>();
+    return b;
+}
+
+GridDev grid_dev(ndt_ctx *c) {
+    GridDev g;
+    g.meta = c->meta_host;
+    g.index = c->index.as<int32_t>();
+    g.mean = c->mean.as<double4>();
+    g.icov32 = c->icov32.as<float4>();
+    g.icov64 = c->icov64.as<double>();
+    return g;
+}
+
+int set_device(ndt_ctx *c) {
+    CK(cudaSetDevice(c->device));
+    return NDT_OK;
+}
+
+// Grid build from a device-resident map (any device pointer valid on the
+// context's stream for the duration of the call).
+int build_grid(ndt_ctx *c, const float4 *d_map, int m) {
+    if (m <= 0) return fail(c, NDT_E_ARG, "map must have at least one point");
+    // voxel slots travel in 26 bits of a packed pair code (slot << 6 | flag << 5 | lane)
+    if (m >= (1 << 25)) return fail(c, NDT_E_CAPACITY, "map larger than 2^25 points");
+    c->have_map = false;
+    CK(c->scratch.ensure(ndt::grid_scratch_bytes(m)));
+    CK(c->meta.ensure(sizeof(GridMeta)));
+    int rc = grid_bbox(d_map, m, c->prm.resolution, c->meta.as<GridMeta>(), c->scratch.p, c->stream);
+    if (rc) return cuda_fail(c, (cudaError_t)rc, "grid_bbox");
+    c->launches += 2;
+    CK(cudaMemcpyAsync(&c->meta_host, c->meta.p, sizeof(GridMeta), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (c->meta_host.error == 2) return fail(c, NDT_E_ARG, "map has non-finite coordinates");
+    if (c->meta_host.error) return fail(c, NDT_E_GRID, "voxel grid does not fit 32-bit cell indices");
+    const size_t G = (size_t)c->meta_host.G;
+    CK(c->index.ensure(sizeof(int32_t) * G));
+    CK(c->mean.ensure(sizeof(double4) * (size_t)m));
+    CK(c->icov32.ensure(2 * sizeof(float4) * (size_t)m));
+    CK(c->icov64.ensure(9 * sizeof(double) * (size_t)m));
+    CK(c->count.ensure(sizeof(int32_t) * (size_t)m));
+    CK(c->cell.ensure(sizeof(int32_t) * (size_t)m));
+    CK(c->seg_start.ensure(sizeof(int32_t) * (size_t)m));
+    CK(c->seg_cell.ensure(sizeof(uint32_t) * (size_t)m));
+    NdtGridOptions opt;
+    opt.compat = c->prm.compat;
+    opt.min_points = c->prm.min_points_per_voxel;
+    opt.eigen_ratio = c->prm.eigen_ratio;
+    int nl = 0;
+    rc = grid_build(d_map, m, c->meta_host, c->meta.as<GridMeta>(), opt, grid_buffers(c), c->scratch.p, c->stream, &nl);
+    if (rc) return cuda_fail(c, (cudaError_t)rc, "grid_build");
+    c->launches += nl;
+    c->have_map = true;
+    c->map_points = m;
+    return NDT_OK;
+}
+
+// Device-side batch: everything already on the device.
+int run_batch(ndt_ctx *c, int B, const float4 *d_points, const int *d_offsets, int total, const float *d_guesses,
+              float *d_out, int *d_conv, double *d_fit, int *d_status) {
+    if (!c->have_map) return fail(c, NDT_E_NOMAP, "no map set");
+    if (B <= 0 || total < 0) return fail(c, NDT_E_ARG, "empty batch");
+    const int max_tiles = total / kTile + B + 1;
+    CK(c->states.ensure(sizeof(AlignState) * (size_t)B));
+    CK(c->tile_begin.ensure(sizeof(int) * (size_t)(B + 1)));
+    CK(c->tiles.ensure(sizeof(Tile) * (size_t)max_tiles));
+    CK(c->num_tiles.ensure(sizeof(int)));
+    CK(c->partials.ensure(sizeof(double) * kPartial * (size_t)max_tiles));
+    CK(c->exc.ensure(sizeof(double) * kPartial * (size_t)B));
+    CK(c->active.ensure(sizeof(int)));
+    CK(c->counters.ensure(sizeof(Counters)));
+    CK(c->h_active.ensure(sizeof(int)));
+    cudaStream_t st = c->stream;
+    CK(cudaMemsetAsync(c->counters.p, 0, sizeof(Counters), st));
+    long long nl = 0;
+    int rc = launch_tiles(d_offsets, B, c->tile_begin.as<int>(), c->tiles.as<Tile>(), c->num_tiles.as<int>(), st);
+    if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_tiles");
+    nl += 3;
+    const StepParams P = step_params(c->prm);
+    rc = launch_init(c->states.as<AlignState>(), d_guesses, d_offsets, B, P, c->exc.as<double>(), st);
+    if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_init");
+    nl += 1;
+    EvalArgs ea;
+    ea.grid = grid_dev(c);
+    ea.points = d_points;
+    ea.trans = nullptr;
+    ea.tiles = c->tiles.as<Tile>();
+    ea.num_tiles = c->num_tiles.as<int>();
+    ea.max_tiles = max_tiles;
+    ea.states = c->states.as<AlignState>();
+    ea.partials = c->partials.as<double>();
+    ea.exc = c->exc.as<double>();
+    ea.d1 = c->d1;
+    ea.d2 = c->d2;
+    ea.compat = c->prm.compat;
+    ea.counters = c->counters.as<Counters>();
+    const int per_sm = c->prm.precision == 1 ? 1 : 2;
+    const int grid_blocks = c->num_sms * per_sm;
+    // With the reference's line-search test (compat, step_max > step_min)
+    // every Newton iteration takes at most one evaluation, so the round count
+    // is fixed and no host polling is needed.
+    const bool fixed = P.compat && (P.step_max - P.step_min) > 0;
+    const int max_rounds = fixed ? P.max_iterations + 3 : P.watchdog_evals + 1;
+    const int poll_every = 4;
+    int rounds = 0;
+    for (int r = 0; r < max_rounds; ++r) {
+        rc = launch_derivatives(ea, c->prm.precision, grid_blocks, st);
+        if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_derivatives");
+        CK(cudaMemsetAsync(c->active.p, 0, sizeof(int), st));
+        rc = launch_step(c->states.as<AlignState>(), c->partials.as<double>(), c->tile_begin.as<int>(),
+                         c->exc.as<double>(), B, P, c->active.as<int>(), c->counters.as<Counters>(), st);
+        if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_step");
+        nl += 2;
+        ++rounds;
+        if (!fixed && (r + 1) % poll_every == 0) {
+            CK(cudaMemcpyAsync(c->h_active.p, c->active.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if (*c->h_active.as<int>() == 0) break;
+        }
+    }
+    rc = launch_finalize(c->states.as<AlignState>(), B, d_out, d_conv, d_fit, d_status, st);
+    if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_finalize");
+    nl += 1;
+    c->launches += nl;
+    c->last.launches = nl;
+    c->last.evaluations = rounds;
+    return NDT_OK;
+}
+
+int read_counters(ndt_ctx *c) {
+    CK(c->h_counters.ensure(sizeof(Counters)));
+    CK(cudaMemcpyAsync(c->h_counters.p, c->counters.p, sizeof(Counters), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const Counters *k = c->h_counters.as<Counters>();
+    c->last.points = (int64_t)k->points;
+    c->last.probes = (int64_t)k->probes;
+    c->last.pairs = (int64_t)k->pairs;
+    c->last.evaluations = (int64_t)k->evaluations;
+    return NDT_OK;
+}
+
+// Host batch: stage scans and guesses into the context's device buffers.
+int host_batch(ndt_ctx *c, int B, const float *const *scans, const int *ns, const float *guesses, float *out,
+               int *conv, double *fit, int *status) {
+    if (B <= 0 || !scans || !ns || !guesses || !out || !conv || !fit) return fail(c, NDT_E_ARG, "null argument");
+    CK(c->h_offsets.ensure(sizeof(int) * (size_t)(B + 1)));
+    int *off = c->h_offsets.as<int>();
+    long long total = 0;
+    off[0] = 0;
+    for (int b = 0; b < B; ++b) {
+        if (ns[b] < 0 || (ns[b] > 0 && !scans[b])) return fail(c, NDT_E_ARG, "bad scan");
+        total += ns[b];
+        if (total > (1LL << 31) - 1) return fail(c, NDT_E_CAPACITY, "batch larger than 2^31 points");
+        off[b + 1] = (int)total;
+    }
+    cudaStream_t st = c->stream;
+    CK(c->points.ensure(sizeof(float4) * (size_t)(total > 0 ? total : 1)));
+    CK(c->offsets.ensure(sizeof(int) * (size_t)(B + 1)));
+    CK(c->guesses.ensure(sizeof(float) * 16 * (size_t)B));
+    CK(c->out_T.ensure(sizeof(float) * 16 * (size_t)B));
+    CK(c->out_conv.ensure(sizeof(int) * (size_t)B));
+    CK(c->out_fit.ensure(sizeof(double) * (size_t)B));
+    CK(c->out_status.ensure(sizeof(int) * (size_t)B));
+    for (int b = 0; b < B; ++b)
+        if (ns[b] > 0)
+            CK(cudaMemcpyAsync(c->points.as<float4>() + off[b], scans[b], sizeof(float4) * (size_t)ns[b],
+                               cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->offsets.p, off, sizeof(int) * (size_t)(B + 1), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->guesses.p, guesses, sizeof(float) * 16 * (size_t)B, cudaMemcpyHostToDevice, st));
+    int rc = run_batch(c, B, c->points.as<float4>(), c->offsets.as<int>(), (int)total, c->guesses.as<float>(),
+                       c->out_T.as<float>(), c->out_conv.as<int>(), c->out_fit.as<double>(), c->out_status.as<int>());
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(out, c->out_T.p, sizeof(float) * 16 * (size_t)B, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(conv, c->out_conv.p, sizeof(int) * (size_t)B, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(fit, c->out_fit.p, sizeof(double) * (size_t)B, cudaMemcpyDeviceToHost, st));
+    if (status) CK(cudaMemcpyAsync(status, c->out_status.p, sizeof(int) * (size_t)B, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return NDT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void ndt_params_reference(ndt_params *p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->resolution = 1.0f;
+    p->outlier_ratio = 0.55;
+    p->step_size = 0.1;
+    p->transformation_epsilon = 0.1;
+    p->max_iterations = 0;
+    p->compat = 1;
+    p->min_points_per_voxel = 0;
+    p->precision = 0;
+    p->eigen_ratio = 0.0;
+    p->watchdog_evals = 0;
+}
+
+void ndt_params_corrected(ndt_params *p) {
+    if (!p) return;
+    ndt_params_reference(p);
+    p->transformation_epsilon = 0.01;
+    p->max_iterations = 30;
+    p->compat = 0;
+    p->min_points_per_voxel = 6;
+    p->eigen_ratio = 0.01;
+}
+
+int ndt_create(const ndt_params *params, int device, ndt_ctx **out) {
+    if (!out) return NDT_E_ARG;
+    *out = nullptr;
+    if (!params) return NDT_E_ARG;
+    if (!(params->resolution > 0.0f) || !std::isfinite(params->resolution)) return NDT_E_ARG;
+    if (params->precision != 0 && params->precision != 1) return NDT_E_ARG;
+    if (params->outlier_ratio <= 0.0 || params->outlier_ratio >= 1.0) return NDT_E_ARG;
+    ndt_ctx *c = new ndt_ctx();
+    c->prm = *params;
+    c->device = device;
+    gauss_constants(c->prm, c->d1, c->d2);
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) {
+        delete c;
+        return NDT_E_CUDA;
+    }
+    *out = c;
+    return NDT_OK;
+}
+
+void ndt_destroy(ndt_ctx *c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    DevBuf *bufs[] = {&c->map, &c->index, &c->mean, &c->icov32, &c->icov64, &c->count, &c->cell, &c->seg_start,
+                      &c->seg_cell, &c->scratch, &c->meta, &c->points, &c->offsets, &c->guesses, &c->states,
+                      &c->tiles, &c->tile_begin, &c->num_tiles, &c->partials, &c->exc, &c->out_T, &c->out_conv,
+                      &c->out_fit, &c->out_status, &c->active, &c->counters, &c->p6, &c->trans};
+    for (DevBuf *b : bufs) b->release();
+    HostBuf *hb[] = {&c->h_offsets, &c->h_active, &c->h_counters, &c->h_out};
+    for (HostBuf *b : hb) b->release();
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char *ndt_last_error(const ndt_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+void *ndt_stream(ndt_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int ndt_synchronize(ndt_ctx *c) {
+    if (!c) return NDT_E_ARG;
+    CK(cudaStreamSynchronize(c->stream));
+    return NDT_OK;
+}
+
+int ndt_set_map(ndt_ctx *c, const float *map, int m) {
+    if (!c || !map || m <= 0) return fail(c, NDT_E_ARG, "null map or empty map");
+    if (int rc = set_device(c)) return rc;
+    CK(c->map.ensure(sizeof(float4) * (size_t)m));
+    CK(cudaMemcpyAsync(c->map.p, map, sizeof(float4) * (size_t)m, cudaMemcpyHostToDevice, c->stream));
+    return build_grid(c, c->map.as<float4>(), m);
+}
+
+int ndt_set_map_device(ndt_ctx *c, const float *d_map, int m) {
+    if (!c || !d_map || m <= 0) return fail(c, NDT_E_ARG, "null map or empty map");
+    if (int rc = set_device(c)) return rc;
+    return build_grid(c, (const float4 *)d_map, m);
+}
+
+int ndt_align(ndt_ctx *c, const float *scan, int n, const float guess16[16], float out16[16], int *converged,
+              double *fitness) {
+    if (!c || !guess16 || !out16 || !converged || !fitness || n < 0 || (n > 0 && !scan))
+        return fail(c, NDT_E_ARG, "null argument");
+    if (int rc = set_device(c)) return rc;
+    const float *scans[1] = {scan};
+    int ns[1] = {n};
+    return host_batch(c, 1, scans, ns, guess16, out16, converged, fitness, nullptr);
+}
+
+int ndt_align_with_map(ndt_ctx *c, const float *scan, int n, const float guess16[16], const float *map, int m,
+                       float out16[16], int *converged, double *fitness) {
+    if (int rc = ndt_set_map(c, map, m)) return rc;
+    return ndt_align(c, scan, n, guess16, out16, converged, fitness);
+}
+
+int ndt_align_batch(ndt_ctx *c, int B, const float *const *scans, const int *ns, const float *guesses, float *out,
+                    int *converged, double *fitness, int *status) {
+    if (!c) return NDT_E_ARG;
+    if (int rc = set_device(c)) return rc;
+    return host_batch(c, B, scans, ns, guesses, out, converged, fitness, status);
+}
+
+int ndt_align_batch_device(ndt_ctx *c, int B, const float *d_points, const int *d_offsets, int total_points,
+                           const float *d_guesses, float *d_out, int *d_conv, double *d_fit, int *d_status) {
+    if (!c || !d_points || !d_offsets || !d_guesses || !d_out || !d_conv || !d_fit)
+        return fail(c, NDT_E_ARG, "null argument");
+    if (int rc = set_device(c)) return rc;
+    return run_batch(c, B, (const float4 *)d_points, d_offsets, total_points, d_guesses, d_out, d_conv, d_fit,
+                     d_status);
+}
+
+int ndt_get_counters(ndt_ctx *c, ndt_counters *out) {
+    if (!c || !out) return NDT_E_ARG;
+    if (!c->counters.p) {
+        std::memset(out, 0, sizeof(*out));
+        return NDT_OK;
+    }
+    if (int rc = read_counters(c)) return rc;
+    *out = c->last;
+    return NDT_OK;
+}
+
+int ndt_grid_info(ndt_ctx *c, float *bbox6, int *dims3, int *occupied) {
+    if (!c) return NDT_E_ARG;
+    if (!c->have_map) return fail(c, NDT_E_NOMAP, "no map set");
+    CK(cudaMemcpyAsync(&c->meta_host, c->meta.p, sizeof(GridMeta), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int e = 0; e < 3; ++e) {
+        if (bbox6) {
+            bbox6[e] = c->meta_host.minv[e];
+            bbox6[3 + e] = c->meta_host.maxv[e];
+        }
+        if (dims3) dims3[e] = c->meta_host.dim[e];
+    }
+    if (occupied) *occupied = c->meta_host.occupied;
+    return NDT_OK;
+}
+
+int ndt_grid_cells(ndt_ctx *c, int cap, int *cell_index, int *count, double *mean3, double *icov9) {
+    int K = 0;
+    if (int rc = ndt_grid_info(c, nullptr, nullptr, &K)) return rc;
+    if (cap < K) return fail(c, NDT_E_CAPACITY, "cell arrays too small");
+    std::vector<double4> mean(K);
+    cudaStream_t st = c->stream;
+    if (K) {
+        if (cell_index) CK(cudaMemcpyAsync(cell_index, c->cell.p, sizeof(int) * (size_t)K, cudaMemcpyDeviceToHost, st));
+        if (count) CK(cudaMemcpyAsync(count, c->count.p, sizeof(int) * (size_t)K, cudaMemcpyDeviceToHost, st));
+        if (mean3) CK(cudaMemcpyAsync(mean.data(), c->mean.p, sizeof(double4) * (size_t)K, cudaMemcpyDeviceToHost, st));
+        if (icov9)
+            CK(cudaMemcpyAsync(icov9, c->icov64.p, sizeof(double) * 9 * (size_t)K, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    if (mean3)
+        for (int k = 0; k < K; ++k) {
+            mean3[3 * k] = mean[k].x;
+            mean3[3 * k + 1] = mean[k].y;
+            mean3[3 * k + 2] = mean[k].z;
+        }
+    return K;
+}
+
+int ndt_derivatives(ndt_ctx *c, const float *scan, const float *trans, int n, const double p6[6], double *score,
+                    double g6[6], double H36[36]) {
+    if (!c || !scan || !trans || n <= 0 || !p6 || !score || !g6 || !H36) return fail(c, NDT_E_ARG, "null argument");
+    if (!c->have_map) return fail(c, NDT_E_NOMAP, "no map set");
+    if (int rc = set_device(c)) return rc;
+    cudaStream_t st = c->stream;
+    const int max_tiles = n / kTile + 2;
+    CK(c->points.ensure(sizeof(float4) * (size_t)n));
+    CK(c->trans.ensure(sizeof(float4) * (size_t)n));
+    CK(c->offsets.ensure(sizeof(int) * 2));
+    CK(c->states.ensure(sizeof(AlignState)));
+    CK(c->tile_begin.ensure(sizeof(int) * 2));
+    CK(c->tiles.ensure(sizeof(Tile) * (size_t)max_tiles));
+    CK(c->num_tiles.ensure(sizeof(int)));
+    CK(c->partials.ensure(sizeof(double) * kPartial * (size_t)max_tiles));
+    CK(c->exc.ensure(sizeof(double) * kPartial));
+    CK(c->p6.ensure(sizeof(double) * 6));
+    CK(c->counters.ensure(sizeof(Counters)));
+    CK(c->h_offsets.ensure(sizeof(int) * 2));
+    int *off = c->h_offsets.as<int>();
+    off[0] = 0;
+    off[1] = n;
+    CK(cudaMemcpyAsync(c->points.p, scan, sizeof(float4) * (size_t)n, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->trans.p, trans, sizeof(float4) * (size_t)n, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->offsets.p, off, sizeof(int) * 2, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->p6.p, p6, sizeof(double) * 6, cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(c->counters.p, 0, sizeof(Counters), st));
+    int rc = launch_tiles(c->offsets.as<int>(), 1, c->tile_begin.as<int>(), c->tiles.as<Tile>(),
+                          c->num_tiles.as<int>(), st);
+    if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_tiles");
+    rc = launch_prepare_eval(c->states.as<AlignState>(), c->p6.as<double>(), n, c->exc.as<double>(), st);
+    if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_prepare_eval");
+    EvalArgs ea;
+    ea.grid = grid_dev(c);
+    ea.points = c->points.as<float4>();
+    ea.trans = c->trans.as<float4>();
+    ea.tiles = c->tiles.as<Tile>();
+    ea.num_tiles = c->num_tiles.as<int>();
+    ea.max_tiles = max_tiles;
+    ea.states = c->states.as<AlignState>();
+    ea.partials = c->partials.as<double>();
+    ea.exc = c->exc.as<double>();
+    ea.d1 = c->d1;
+    ea.d2 = c->d2;
+    ea.compat = c->prm.compat;
+    ea.counters = c->counters.as<Counters>();
+    rc = launch_derivatives(ea, c->prm.precision, c->num_sms * 2, st);
+    if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_derivatives");
+    int nt = 0;
+    std::vector<double> part((size_t)max_tiles * kPartial), exc(kPartial);
+    CK(cudaMemcpyAsync(&nt, c->num_tiles.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    CK(cudaMemcpyAsync(part.data(), c->partials.p, sizeof(double) * kPartial * (size_t)nt, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(exc.data(), c->exc.p, sizeof(double) * kPartial, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    double v[kPartial] = {0};
+    for (int t = 0; t < nt; ++t)
+        for (int k = 0; k < kPartial; ++k) v[k] += part[(size_t)t * kPartial + k];
+    for (int k = 0; k < kPartial; ++k) v[k] += exc[k];
+    *score = v[0];
+    for (int i = 0; i < 6; ++i) g6[i] = v[1 + i];
+    for (int k = 0; k < 36; ++k) H36[k] = v[7 + k];
+    return read_counters(c);
+}
+
+}  // extern "C"

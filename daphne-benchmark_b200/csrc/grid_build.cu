@@ -1,0 +1,548 @@
+// Voxel-grid build on the device (replaces ndt_mapping::initCompute,
+// src/CPU/ndt_mapping/kernel.cpp:1302-1373).
+//
+// Pipeline (one map):
+//   bbox_partial / bbox_final   bounding box +-0.01, dims, G        (:1305-1322)
+//   cell_key                    dense cell id of every map point     (:1343, :236-244)
+//   radix_{upsweep,scan,down}   stable LSD sort of (cell, point index)
+//   seg_{count,write}           one segment per occupied cell
+//   cell_finalize_{compat,corrected}
+//                               per-cell sums in point order, covariance, inverse
+//
+// Because the sort is stable, every cell's points are visited in the map's
+// original order, so the FP64 sums of the compat finaliser are the reference's
+// sequential sums bit for bit (the reference adds points in index order,
+// :1341-1353).  No floating-point atomics are used anywhere.
+#include <cuda_runtime.h>
+#include <float.h>
+#include <stdint.h>
+
+#include "grid_build.h"
+#include "ndt_math.cuh"
+
+namespace ndt {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kItems = 8;                       // items per thread in the sort / segment tiles
+constexpr int kSortTile = kThreads * kItems;    // 2048
+constexpr int kWarps = kThreads / 32;
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// ---------------------------------------------------------------------------
+// Bounding box.  min/max are exact in any order; NaN/inf points are counted
+// and make the build fail (the reference's behaviour there is undefined).
+__global__ void bbox_partial_kernel(const float4 *__restrict__ map, int m, float *__restrict__ part,
+                                    int *__restrict__ nonfinite) {
+    float mn0 = FLT_MAX, mn1 = FLT_MAX, mn2 = FLT_MAX;
+    float mx0 = -FLT_MAX, mx1 = -FLT_MAX, mx2 = -FLT_MAX;
+    int bad = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        float4 p = map[i];
+        if (!isfinite(p.x) || !isfinite(p.y) || !isfinite(p.z)) {
+            bad = 1;
+            continue;
+        }
+        mn0 = fminf(mn0, p.x); mn1 = fminf(mn1, p.y); mn2 = fminf(mn2, p.z);
+        mx0 = fmaxf(mx0, p.x); mx1 = fmaxf(mx1, p.y); mx2 = fmaxf(mx2, p.z);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mn0 = fminf(mn0, __shfl_xor_sync(0xffffffffu, mn0, o));
+        mn1 = fminf(mn1, __shfl_xor_sync(0xffffffffu, mn1, o));
+        mn2 = fminf(mn2, __shfl_xor_sync(0xffffffffu, mn2, o));
+        mx0 = fmaxf(mx0, __shfl_xor_sync(0xffffffffu, mx0, o));
+        mx1 = fmaxf(mx1, __shfl_xor_sync(0xffffffffu, mx1, o));
+        mx2 = fmaxf(mx2, __shfl_xor_sync(0xffffffffu, mx2, o));
+    }
+    __shared__ float s[kWarps][6];
+    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        s[w][0] = mn0; s[w][1] = mn1; s[w][2] = mn2;
+        s[w][3] = mx0; s[w][4] = mx1; s[w][5] = mx2;
+    }
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(nonfinite, 1);
+    if (threadIdx.x < 6) {
+        float v = s[0][threadIdx.x];
+        for (int k = 1; k < kWarps; ++k)
+            v = threadIdx.x < 3 ? fminf(v, s[k][threadIdx.x]) : fmaxf(v, s[k][threadIdx.x]);
+        part[6 * blockIdx.x + threadIdx.x] = v;
+    }
+}
+
+// kernel.cpp:1318-1322: min -= 0.01f, max += 0.01f, dim = (max - min) / res + 1
+// (float arithmetic, truncated to int).
+__global__ void bbox_final_kernel(const float *__restrict__ part, int nblk, float res,
+                                  const int *__restrict__ nonfinite, GridMeta *__restrict__ meta) {
+    if (threadIdx.x != 0) return;
+    float v[6];
+    for (int k = 0; k < 6; ++k) v[k] = part[k];
+    for (int b = 1; b < nblk; ++b)
+        for (int k = 0; k < 6; ++k)
+            v[k] = k < 3 ? fminf(v[k], part[6 * b + k]) : fmaxf(v[k], part[6 * b + k]);
+    GridMeta g;
+    g.res = res;
+    g.occupied = 0;
+    g.error = *nonfinite ? 2 : 0;
+    long long G = 1;
+    for (int e = 0; e < 3; ++e) {
+        g.minv[e] = v[e] - 0.01f;
+        g.maxv[e] = v[3 + e] + 0.01f;
+        float d = (g.maxv[e] - g.minv[e]) / res + 1;
+        g.dim[e] = (d >= 1.0f && d < 2147483647.0f) ? (int)d : 0;
+        G *= (long long)g.dim[e];
+    }
+    if (G <= 0 || G > 2147483647LL) {
+        if (!g.error) g.error = 1;
+        G = 0;
+    }
+    g.G = G;
+    *meta = g;
+}
+
+// Dense cell id of each map point (linearizeCoord, kernel.cpp:236-244).
+__global__ void cell_key_kernel(const float4 *__restrict__ map, int m, const GridMeta *__restrict__ meta,
+                                uint32_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const GridMeta g = *meta;
+    if (g.error) return;
+    float4 p = map[i];
+    int ix = (int)((p.x - g.minv[0]) / g.res);
+    int iy = (int)((p.y - g.minv[1]) / g.res);
+    int iz = (int)((p.z - g.minv[2]) / g.res);
+    keys[i] = (uint32_t)(ix + g.dim[0] * (iy + g.dim[1] * iz));
+    vals[i] = (uint32_t)i;
+}
+
+// ---------------------------------------------------------------------------
+// Stable LSD radix sort of (key, value) pairs, `bits`-wide digit per pass.
+// hist layout: digit-major, hist[d * nblk + block].
+__global__ void radix_upsweep_kernel(const uint32_t *__restrict__ keys, int n, int shift, int bits,
+                                     int *__restrict__ hist) {
+    extern __shared__ int s_hist[];
+    const int nb = 1 << bits;
+    for (int d = threadIdx.x; d < nb; d += blockDim.x) s_hist[d] = 0;
+    __syncthreads();
+    const int base = blockIdx.x * kSortTile;
+    const uint32_t mask = (uint32_t)nb - 1u;
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+        int i = base + k * kThreads + threadIdx.x;
+        if (i < n) atomicAdd(&s_hist[(keys[i] >> shift) & mask], 1);
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < nb; d += blockDim.x) hist[d * gridDim.x + blockIdx.x] = s_hist[d];
+}
+
+// Exclusive scan of n ints in place with one block of 1024 threads; each
+// thread owns a contiguous chunk.  *total (optional) receives the sum.
+__global__ void scan_single_block_kernel(int *__restrict__ data, int n, int *__restrict__ total) {
+    __shared__ int s_warp[32];
+    const int t = threadIdx.x, nt = blockDim.x;
+    const int chunk = (n + nt - 1) / nt;
+    const int lo = min(n, t * chunk), hi = min(n, lo + chunk);
+    int sum = 0;
+    for (int i = lo; i < hi; ++i) sum += data[i];
+    int lane = t & 31, w = t >> 5;
+    int incl = sum;
+    for (int o = 1; o < 32; o <<= 1) {
+        int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) s_warp[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        int v = (lane < (nt >> 5)) ? s_warp[lane] : 0;
+        int inc2 = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            int u = __shfl_up_sync(0xffffffffu, inc2, o);
+            if (lane >= o) inc2 += u;
+        }
+        s_warp[lane] = inc2 - v;
+    }
+    __syncthreads();
+    int run = s_warp[w] + incl - sum;
+    for (int i = lo; i < hi; ++i) {
+        int v = data[i];
+        data[i] = run;
+        run += v;
+    }
+    if (total && t == nt - 1) *total = run;
+}
+
+// Stable scatter: warp w of a block owns items [base + w*256, base + w*256 + 256)
+// in 8 chunks of 32 consecutive items; ranks inside a chunk come from
+// __match_any_sync peer masks, so equal digits keep their input order.
+__global__ void radix_downsweep_kernel(const uint32_t *__restrict__ kin, const uint32_t *__restrict__ vin,
+                                       uint32_t *__restrict__ kout, uint32_t *__restrict__ vout, int n,
+                                       int shift, int bits, const int *__restrict__ hist) {
+    extern __shared__ int s_cnt[];  // [kWarps][nb]
+    const int nb = 1 << bits;
+    const uint32_t mask = (uint32_t)nb - 1u;
+    for (int d = threadIdx.x; d < kWarps * nb; d += blockDim.x) s_cnt[d] = 0;
+    __syncthreads();
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wbase = blockIdx.x * kSortTile + w * (32 * kItems);
+    int *cnt = s_cnt + w * nb;
+    uint32_t key[kItems], val[kItems];
+    int rank[kItems];
+    const unsigned lt = lanemask_lt();
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+        int i = wbase + k * 32 + lane;
+        bool valid = i < n;
+        key[k] = valid ? kin[i] : 0u;
+        val[k] = valid ? vin[i] : 0u;
+        uint32_t d = valid ? ((key[k] >> shift) & mask) : (uint32_t)nb;  // sentinel group
+        unsigned peers = __match_any_sync(0xffffffffu, d);
+        int before = valid ? cnt[d] : 0;
+        __syncwarp();
+        rank[k] = before + __popc(peers & lt);
+        int leader = __ffs(peers) - 1;
+        if (valid && lane == leader) cnt[d] = before + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    // exclusive prefix over warps, per digit
+    for (int d = threadIdx.x; d < nb; d += blockDim.x) {
+        int run = 0;
+        for (int ww = 0; ww < kWarps; ++ww) {
+            int c = s_cnt[ww * nb + d];
+            s_cnt[ww * nb + d] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+        int i = wbase + k * 32 + lane;
+        if (i < n) {
+            uint32_t d = (key[k] >> shift) & mask;
+            int pos = hist[d * gridDim.x + blockIdx.x] + cnt[d] + rank[k];
+            kout[pos] = key[k];
+            vout[pos] = val[k];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Segments of equal keys in the sorted order = occupied cells.
+__device__ __forceinline__ bool is_head(const uint32_t *k, int i) { return i == 0 || k[i] != k[i - 1]; }
+
+__global__ void seg_count_kernel(const uint32_t *__restrict__ keys, int n, int *__restrict__ counts) {
+    int c = 0;
+    const int base = blockIdx.x * kSortTile;
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+        int i = base + k * kThreads + threadIdx.x;
+        if (i < n && is_head(keys, i)) ++c;
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    __shared__ int s[kWarps];
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int k = 0; k < kWarps; ++k) t += s[k];
+        counts[blockIdx.x] = t;
+    }
+}
+
+// Writes seg_start[s] and seg_cell[s] for every segment head, s in sorted order.
+__global__ void seg_write_kernel(const uint32_t *__restrict__ keys, int n, const int *__restrict__ offsets,
+                                 int *__restrict__ seg_start, uint32_t *__restrict__ seg_cell) {
+    __shared__ int s_warp[kWarps];
+    __shared__ int s_run;
+    if (threadIdx.x == 0) s_run = offsets[blockIdx.x];
+    const int base = blockIdx.x * kSortTile;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int k = 0; k < kItems; ++k) {
+        int i = base + k * kThreads + threadIdx.x;
+        bool h = i < n && is_head(keys, i);
+        unsigned b = __ballot_sync(0xffffffffu, h);
+        if (lane == 0) s_warp[w] = __popc(b);
+        __syncthreads();
+        int before = 0, total = 0;
+        for (int ww = 0; ww < kWarps; ++ww) {
+            int c = s_warp[ww];
+            if (ww < w) before += c;
+            total += c;
+        }
+        int run = s_run;
+        if (h) {
+            int s = run + before + __popc(b & lanemask_lt());
+            seg_start[s] = i;
+            seg_cell[s] = keys[i];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_run = run + total;
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Voxel records.
+__device__ void write_records(int s, const double *mu, const double *C, GridBuffers buf) {
+    bool bad = false;
+    for (int k = 0; k < 9; ++k) {
+        double v = C[k];
+        if (!(fabs(v) <= 1e30)) bad = true;  // also catches NaN
+    }
+    for (int k = 0; k < 3; ++k)
+        if (!isfinite(mu[k])) bad = true;
+    buf.mean[s] = make_double4(mu[0], mu[1], mu[2], bad ? 1.0 : 0.0);
+    float c00 = (float)C[0], c11 = (float)C[4], c22 = (float)C[8];
+    float c01 = (float)((C[1] + C[3]) * 0.5), c02 = (float)((C[2] + C[6]) * 0.5), c12 = (float)((C[5] + C[7]) * 0.5);
+    buf.icov32[2 * s] = make_float4(c00, c01, c02, c11);
+    buf.icov32[2 * s + 1] = make_float4(c12, c22, 0.0f, 0.0f);
+    for (int k = 0; k < 9; ++k) buf.icov64[9 * (size_t)s + k] = C[k];
+}
+
+// Reference voxel (kernel.cpp:1324-1372): sums start at mean = 0 and
+// invCovariance = anti-diagonal identity; every point adds its float xyz and
+// the float products x_r * x_c; then mean = sum / N and
+//   S_rc = ((S_rc - 2 (sum_r mean_c)) / G + mean_r mean_c) * ((G - 1) / N)
+// (G = dense cell count), inverted by adjugate (invertMatrix, :1277-1300).
+__global__ void cell_finalize_compat_kernel(const float4 *__restrict__ map, const uint32_t *__restrict__ order,
+                                            const int *__restrict__ seg_start, const uint32_t *__restrict__ seg_cell,
+                                            const int *__restrict__ nseg, int n, const GridMeta *__restrict__ meta,
+                                            GridBuffers buf) {
+    const int K = *nseg;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= K) return;
+    const int lo = seg_start[s], hi = (s + 1 < K) ? seg_start[s + 1] : n;
+    double sum[3] = {0.0, 0.0, 0.0};
+    double S[9] = {0.0, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0, 0.0, 0.0};
+    int cnt = 0;
+    for (int j = lo; j < hi; ++j) {
+        float4 p = map[order[j]];
+        const float v[3] = {p.x, p.y, p.z};
+        sum[0] += v[0];
+        sum[1] += v[1];
+        sum[2] += v[2];
+        ++cnt;
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) S[3 * r + c] += (double)(v[r] * v[c]);
+    }
+    const double Gd = (double)meta->G;
+    double mu[3];
+    for (int e = 0; e < 3; ++e) mu[e] = sum[e] / cnt;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            double v = (S[3 * r + c] - 2 * (sum[r] * mu[c])) / Gd + mu[r] * mu[c];
+            S[3 * r + c] = v * ((Gd - 1.0) / cnt);
+        }
+    // adjugate / determinant
+    const double *m = S;
+    double det = m[0] * (m[8] * m[4] - m[7] * m[5]) - m[3] * (m[8] * m[1] - m[7] * m[2]) +
+                 m[6] * (m[5] * m[1] - m[4] * m[2]);
+    double inv_det = 1.0 / det;
+    double t[9];
+    t[0] = m[8] * m[4] - m[7] * m[5];
+    t[1] = -(m[8] * m[1] - m[7] * m[2]);
+    t[2] = m[5] * m[1] - m[4] * m[2];
+    t[3] = -(m[8] * m[1] - m[6] * m[5]);
+    t[4] = m[8] * m[0] - m[7] * m[2];
+    t[5] = -(m[5] * m[0] - m[3] * m[2]);
+    t[6] = m[7] * m[3] - m[6] * m[4];
+    t[7] = -(m[7] * m[0] - m[6] * m[1]);
+    t[8] = m[4] * m[0] - m[3] * m[1];
+    double C[9];
+    for (int k = 0; k < 9; ++k) C[k] = t[k] * inv_det;
+    write_records(s, mu, C, buf);
+    buf.count[s] = cnt;
+    buf.cell[s] = (int)seg_cell[s];
+    buf.index[seg_cell[s]] = s;
+}
+
+// Symmetric 3x3 eigen-decomposition by cyclic Jacobi rotations (V columns =
+// eigenvectors); the same algorithm as the FP64 oracle's.
+__device__ void jacobi3(double A[3][3], double V[3][3], double w[3]) {
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) V[i][j] = (i == j) ? 1.0 : 0.0;
+    for (int sweep = 0; sweep < 16; ++sweep) {
+        double off = A[0][1] * A[0][1] + A[0][2] * A[0][2] + A[1][2] * A[1][2];
+        double diag = A[0][0] * A[0][0] + A[1][1] * A[1][1] + A[2][2] * A[2][2];
+        if (off <= 1e-30 * diag || off == 0.0) break;
+        for (int p = 0; p < 2; ++p)
+            for (int q = p + 1; q < 3; ++q) {
+                double apq = A[p][q];
+                if (apq == 0.0) continue;
+                double theta = (A[q][q] - A[p][p]) / (2.0 * apq);
+                double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+                for (int k = 0; k < 3; ++k) {
+                    double akp = A[k][p], akq = A[k][q];
+                    A[k][p] = c * akp - s * akq;
+                    A[k][q] = s * akp + c * akq;
+                }
+                for (int k = 0; k < 3; ++k) {
+                    double apk = A[p][k], aqk = A[q][k];
+                    A[p][k] = c * apk - s * aqk;
+                    A[q][k] = s * apk + c * aqk;
+                }
+                for (int k = 0; k < 3; ++k) {
+                    double vkp = V[k][p], vkq = V[k][q];
+                    V[k][p] = c * vkp - s * vkq;
+                    V[k][q] = s * vkp + c * vkq;
+                }
+            }
+    }
+    for (int i = 0; i < 3; ++i) w[i] = A[i][i];
+}
+
+// Corrected voxel: mean, centred covariance / (N - 1), usable only with at
+// least min_points points, eigenvalues floored at eig_ratio * max, inverse
+// as V diag(1 / w) V^T.
+__global__ void cell_finalize_corrected_kernel(const float4 *__restrict__ map, const uint32_t *__restrict__ order,
+                                               const int *__restrict__ seg_start,
+                                               const uint32_t *__restrict__ seg_cell, const int *__restrict__ nseg,
+                                               int n, int min_points, double eig_ratio, GridBuffers buf) {
+    const int K = *nseg;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= K) return;
+    const int lo = seg_start[s], hi = (s + 1 < K) ? seg_start[s + 1] : n;
+    const int cnt = hi - lo;
+    buf.count[s] = cnt;
+    buf.cell[s] = (int)seg_cell[s];
+    if (cnt < min_points || cnt < 2) return;
+    double sum[3] = {0.0, 0.0, 0.0};
+    for (int j = lo; j < hi; ++j) {
+        float4 p = map[order[j]];
+        sum[0] += (double)p.x;
+        sum[1] += (double)p.y;
+        sum[2] += (double)p.z;
+    }
+    double mu[3];
+    for (int e = 0; e < 3; ++e) mu[e] = sum[e] / cnt;
+    double m2[6] = {0, 0, 0, 0, 0, 0};
+    for (int j = lo; j < hi; ++j) {
+        float4 p = map[order[j]];
+        double d0 = p.x - mu[0], d1 = p.y - mu[1], d2 = p.z - mu[2];
+        m2[0] += d0 * d0; m2[1] += d0 * d1; m2[2] += d0 * d2;
+        m2[3] += d1 * d1; m2[4] += d1 * d2; m2[5] += d2 * d2;
+    }
+    double A[3][3] = {{m2[0], m2[1], m2[2]}, {m2[1], m2[3], m2[4]}, {m2[2], m2[4], m2[5]}};
+    for (int r = 0; r < 3; ++r)
+        for (int q = 0; q < 3; ++q) A[r][q] /= (cnt - 1);
+    double V[3][3], w[3];
+    jacobi3(A, V, w);
+    double wmax = fmax(w[0], fmax(w[1], w[2]));
+    if (!(wmax > 0.0) || !isfinite(wmax)) return;
+    double floor_v = eig_ratio * wmax;
+    double inv_w[3];
+    for (int e = 0; e < 3; ++e) {
+        double we = w[e] < floor_v ? floor_v : w[e];
+        if (!(we > 0.0)) return;
+        inv_w[e] = 1.0 / we;
+    }
+    double C[9];
+    for (int r = 0; r < 3; ++r)
+        for (int q = 0; q < 3; ++q)
+            C[3 * r + q] = V[r][0] * inv_w[0] * V[q][0] + V[r][1] * inv_w[1] * V[q][1] + V[r][2] * inv_w[2] * V[q][2];
+    write_records(s, mu, C, buf);
+    buf.index[seg_cell[s]] = s;
+}
+
+__global__ void store_occupied_kernel(const int *__restrict__ nseg, GridMeta *__restrict__ meta) {
+    if (threadIdx.x == 0) meta->occupied = *nseg;
+}
+
+inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+size_t grid_scratch_bytes(int m) {
+    size_t nblk = (size_t)div_up(m, kSortTile);
+    size_t b = 0;
+    b += 4 * sizeof(uint32_t) * (size_t)m;   // keys/vals ping-pong
+    b += sizeof(int) * 256 * nblk + 64;      // radix histogram
+    b += sizeof(int) * (nblk + 1) + 64;      // segment block counts
+    b += sizeof(float) * 6 * 1024 + 64;      // bbox partials
+    b += 4 * 64;                             // small scalars
+    return b + 4096;
+}
+
+int grid_bbox(const float4 *d_map, int m, float res, GridMeta *d_meta, void *scratch, cudaStream_t st) {
+    char *p = (char *)scratch;
+    float *part = (float *)p;
+    int *nonfinite = (int *)(p + sizeof(float) * 6 * 1024);
+    int nblk = div_up(m, kThreads);
+    if (nblk > 1024) nblk = 1024;
+    cudaMemsetAsync(nonfinite, 0, sizeof(int), st);
+    bbox_partial_kernel<<<nblk, kThreads, 0, st>>>(d_map, m, part, nonfinite);
+    bbox_final_kernel<<<1, 32, 0, st>>>(part, nblk, res, nonfinite, d_meta);
+    return (int)cudaGetLastError();
+}
+
+int grid_build(const float4 *d_map, int m, const GridMeta &meta_host, GridMeta *d_meta, const NdtGridOptions &opt,
+               GridBuffers buf, void *scratch, cudaStream_t st, int *launches) {
+    const int nblk = div_up(m, kSortTile);
+    char *p = (char *)scratch;
+    auto take = [&](size_t bytes) {
+        char *r = p;
+        p += (bytes + 255) & ~(size_t)255;
+        return (void *)r;
+    };
+    uint32_t *k0 = (uint32_t *)take(sizeof(uint32_t) * (size_t)m);
+    uint32_t *v0 = (uint32_t *)take(sizeof(uint32_t) * (size_t)m);
+    uint32_t *k1 = (uint32_t *)take(sizeof(uint32_t) * (size_t)m);
+    uint32_t *v1 = (uint32_t *)take(sizeof(uint32_t) * (size_t)m);
+    int *hist = (int *)take(sizeof(int) * 256 * (size_t)nblk);
+    int *segc = (int *)take(sizeof(int) * (size_t)(nblk + 1));
+    int *nseg = (int *)take(sizeof(int));
+    int nl = 0;
+
+    cudaMemsetAsync(buf.index, 0xff, sizeof(int32_t) * (size_t)meta_host.G, st);
+    cell_key_kernel<<<div_up(m, kThreads), kThreads, 0, st>>>(d_map, m, d_meta, k0, v0);
+    ++nl;
+    // digit width: passes = ceil(bits / 8), width = ceil(bits / passes)
+    int bits = 1;
+    while (bits < 31 && (1LL << bits) < meta_host.G) ++bits;
+    int passes = (bits + 7) / 8;
+    int width = (bits + passes - 1) / passes;
+    int shift = 0;
+    for (int ps = 0; ps < passes; ++ps) {
+        int w = width;
+        if (shift + w > bits) w = bits - shift;
+        size_t smem_up = sizeof(int) << w;
+        size_t smem_dn = sizeof(int) * kWarps << w;
+        radix_upsweep_kernel<<<nblk, kThreads, smem_up, st>>>(k0, m, shift, w, hist);
+        scan_single_block_kernel<<<1, 1024, 0, st>>>(hist, nblk << w, nullptr);
+        radix_downsweep_kernel<<<nblk, kThreads, smem_dn, st>>>(k0, v0, k1, v1, m, shift, w, hist);
+        nl += 3;
+        uint32_t *t = k0; k0 = k1; k1 = t;
+        t = v0; v0 = v1; v1 = t;
+        shift += w;
+    }
+    seg_count_kernel<<<nblk, kThreads, 0, st>>>(k0, m, segc);
+    scan_single_block_kernel<<<1, 1024, 0, st>>>(segc, nblk, nseg);
+    seg_write_kernel<<<nblk, kThreads, 0, st>>>(k0, m, segc, buf.seg_start, buf.seg_cell);
+    nl += 3;
+    // at most m segments: launch for m, kernels read the true count
+    if (opt.compat) {
+        cell_finalize_compat_kernel<<<div_up(m, 128), 128, 0, st>>>(d_map, v0, buf.seg_start, buf.seg_cell, nseg,
+                                                                    m, d_meta, buf);
+    } else {
+        cell_finalize_corrected_kernel<<<div_up(m, 128), 128, 0, st>>>(d_map, v0, buf.seg_start, buf.seg_cell,
+                                                                       nseg, m, opt.min_points, opt.eigen_ratio,
+                                                                       buf);
+    }
+    store_occupied_kernel<<<1, 32, 0, st>>>(nseg, d_meta);
+    nl += 2;
+    if (launches) *launches += nl + 2;
+    return (int)cudaGetLastError();
+}
+
+}  // namespace ndt

@@ -1,0 +1,93 @@
+// Types shared by the host engine and the device kernels.
+#pragma once
+#include <stdint.h>
+
+namespace ndt {
+
+constexpr int kTile = 256;      // scan points per derivative-pass tile (= threads per block)
+constexpr int kPartial = 44;    // per-tile partial: score, g[6], H[36], pair count
+constexpr int kAngle = 69;      // angle terms: j_ang a..h (8 x 3) + h_ang a2..f3 (15 x 3)
+
+// What the derivative pass must compute for one alignment this round.
+enum EvalMode : int32_t {
+    kEvalNone = 0,
+    kEvalFull = 1,      // score, gradient, Hessian (computeDerivatives(..., true))
+    kEvalGradient = 2,  // score, gradient; Hessian reset to 0 (computeDerivatives(..., false))
+    kEvalHessian = 3,   // Hessian only (computeHessian)
+};
+
+// Phases of the per-alignment registration state machine (one Newton
+// iteration = solve + More-Thuente step length + pose update).
+enum Phase : int32_t {
+    kPhaseInitEval = 0,  // waiting for the first evaluation at the guess
+    kPhaseMTFirst = 1,   // waiting for the first line-search evaluation
+    kPhaseMTIter = 2,    // waiting for a later line-search evaluation
+    kPhaseMTHess = 3,    // waiting for the closing Hessian pass
+    kPhaseDone = 4,
+};
+
+// Grid geometry (dense addressing as the reference's initCompute).
+struct GridMeta {
+    float minv[3];
+    float maxv[3];
+    int32_t dim[3];
+    float res;
+    int64_t G;         // dense cell count
+    int32_t occupied;  // cells with >= 1 point (compat) / usable cells (corrected)
+    int32_t error;     // nonzero: G does not fit 32-bit indices
+};
+
+// Device pointers of a built grid.
+struct GridDev {
+    GridMeta meta;
+    const int32_t *index;    // G: dense cell -> voxel slot, -1 = none
+    const double4 *mean;     // K: mean xyz (FP64), w = 1 when the FP32 path must not be used
+    const float4 *icov32;    // 2K: {c00 c01 c02 c11}, {c12 c22 0 0} (symmetrised, FP32)
+    const double *icov64;    // 9K: inverse covariance as the reference stores it (row major)
+};
+
+// Per-alignment state (FP64 control, float transform), one per alignment.
+struct __align__(16) AlignState {
+    // evaluation request read by the derivative pass
+    float T[16];             // final_transformation_ used for the current evaluation
+    float angf[kAngle];      // angle terms (FP32 copy)
+    int32_t eval_mode;
+    int32_t phase;
+    double angd[kAngle];     // angle terms (FP64)
+    // Newton / More-Thuente state (kernel.cpp:1015-1272 variables)
+    double p[6];             // current pose vector
+    double x_t[6];           // trial pose
+    double dir[6];           // step direction (delta_p)
+    double g[6];
+    double H[36];
+    double score;
+    double phi_0, d_phi_0, a_l, f_l, g_l, a_u, f_u, g_u, a_t, phi_t, d_phi_t, psi_t, d_psi_t;
+    double step_max, step_min;
+    int32_t nr_iterations;
+    int32_t step_iterations;
+    int32_t open_interval;
+    int32_t interval_converged;
+    int32_t converged;
+    int32_t evals;
+    int32_t status;
+    int32_t n;               // scan points
+};
+
+// Work counters (device, 64-bit).
+struct Counters {
+    unsigned long long evaluations;
+    unsigned long long points;
+    unsigned long long probes;
+    unsigned long long occupied_probes;
+    unsigned long long pairs;
+    unsigned long long rounds;
+};
+
+struct Tile {
+    int32_t align;
+    int32_t start;   // first point (global index into the concatenated scans)
+    int32_t end;     // one past the last point
+    int32_t slot;    // partial slot of this tile
+};
+
+}  // namespace ndt

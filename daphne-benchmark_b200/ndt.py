@@ -1,0 +1,241 @@
+"""ctypes binding of libndt_b200.so (include/ndt_b200.h) with numpy buffers.
+
+The host-side mirror of the reference's align call: `Context.align(scan, guess)`
+is partial_points_callback (src/CPU/ndt_mapping/kernel.cpp:1405) against the
+map set by `Context.set_map`, returning (final_transformation[16], converged,
+fitness).  There is no CPU fallback: loading fails loudly when the CUDA library
+has not been built, and every call raises NdtError when the library reports an
+error (no device, bad argument, ...).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import pathlib
+import subprocess
+
+import numpy as np
+
+PKG = pathlib.Path(__file__).resolve().parent
+LIB_PATH = PKG / "_build" / "libndt_b200.so"
+CSRC = PKG / "csrc"
+
+NDT_OK = 0
+ERRORS = {-1: "NDT_E_ARG", -2: "NDT_E_CUDA", -3: "NDT_E_NOMAP", -4: "NDT_E_GRID", -5: "NDT_E_WATCHDOG",
+          -6: "NDT_E_CAPACITY"}
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+
+
+class NdtError(RuntimeError):
+    pass
+
+
+class Params(C.Structure):
+    """ndt_params (include/ndt_b200.h)."""
+
+    _fields_ = [
+        ("resolution", C.c_float),
+        ("_pad0", C.c_float),
+        ("outlier_ratio", C.c_double),
+        ("step_size", C.c_double),
+        ("transformation_epsilon", C.c_double),
+        ("max_iterations", C.c_int32),
+        ("compat", C.c_int32),
+        ("min_points_per_voxel", C.c_int32),
+        ("precision", C.c_int32),
+        ("eigen_ratio", C.c_double),
+        ("watchdog_evals", C.c_int32),
+        ("_pad1", C.c_int32),
+    ]
+
+
+class Counters(C.Structure):
+    _fields_ = [("evaluations", C.c_int64), ("points", C.c_int64), ("probes", C.c_int64), ("pairs", C.c_int64),
+                ("launches", C.c_int64)]
+
+
+def build(quiet=True):
+    """Compile libndt_b200.so for sm_100a (nvcc cross-compiles without a GPU)."""
+    subprocess.run(["make", "-C", str(CSRC), "-j4"], check=True, stdout=subprocess.DEVNULL if quiet else None)
+    return LIB_PATH
+
+
+_LIB = None
+
+
+def lib():
+    """The loaded CUDA library (raises if it was not built)."""
+    global _LIB
+    if _LIB is None:
+        if not LIB_PATH.exists():
+            raise NdtError(f"{LIB_PATH} is missing: build the CUDA library first (make -C {CSRC})")
+        L = C.CDLL(str(LIB_PATH))
+        P = C.POINTER(Params)
+        ctxp = C.c_void_p
+        L.ndt_params_reference.argtypes = [P]
+        L.ndt_params_corrected.argtypes = [P]
+        L.ndt_create.argtypes = [P, C.c_int, C.POINTER(ctxp)]
+        L.ndt_destroy.argtypes = [ctxp]
+        L.ndt_last_error.argtypes = [ctxp]
+        L.ndt_last_error.restype = C.c_char_p
+        L.ndt_set_map.argtypes = [ctxp, _f32p, C.c_int]
+        L.ndt_set_map_device.argtypes = [ctxp, C.c_void_p, C.c_int]
+        L.ndt_align.argtypes = [ctxp, _f32p, C.c_int, _f32p, _f32p, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+        L.ndt_align_with_map.argtypes = [ctxp, _f32p, C.c_int, _f32p, _f32p, C.c_int, _f32p, C.POINTER(C.c_int),
+                                         C.POINTER(C.c_double)]
+        L.ndt_align_batch.argtypes = [ctxp, C.c_int, C.c_void_p, _i32p, _f32p, _f32p, _i32p, _f64p, C.c_void_p]
+        L.ndt_align_batch_device.argtypes = [ctxp, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ndt_synchronize.argtypes = [ctxp]
+        L.ndt_stream.argtypes = [ctxp]
+        L.ndt_stream.restype = C.c_void_p
+        L.ndt_get_counters.argtypes = [ctxp, C.POINTER(Counters)]
+        L.ndt_grid_info.argtypes = [ctxp, _f32p, _i32p, C.POINTER(C.c_int)]
+        L.ndt_grid_cells.argtypes = [ctxp, C.c_int, _i32p, _i32p, _f64p, _f64p]
+        L.ndt_derivatives.argtypes = [ctxp, _f32p, _f32p, C.c_int, _f64p, C.POINTER(C.c_double), _f64p, _f64p]
+        for name in ("ndt_create", "ndt_set_map", "ndt_set_map_device", "ndt_align", "ndt_align_with_map",
+                     "ndt_align_batch", "ndt_align_batch_device", "ndt_synchronize", "ndt_get_counters",
+                     "ndt_grid_info", "ndt_grid_cells", "ndt_derivatives"):
+            getattr(L, name).restype = C.c_int
+        _LIB = L
+    return _LIB
+
+
+def reference_params(resolution=1.0, precision=0):
+    p = Params()
+    lib().ndt_params_reference(C.byref(p))
+    p.resolution = resolution
+    p.precision = precision
+    return p
+
+
+def corrected_params(resolution=1.0, precision=0):
+    p = Params()
+    lib().ndt_params_corrected(C.byref(p))
+    p.resolution = resolution
+    p.precision = precision
+    return p
+
+
+def _f32(a, cols=4):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    return a.reshape(-1, cols) if cols else a
+
+
+class Context:
+    """One ndt_ctx: a device, a stream, a map grid and batch buffers."""
+
+    def __init__(self, params: Params | None = None, device: int = 0):
+        self.L = lib()
+        self.params = params if params is not None else reference_params()
+        h = C.c_void_p()
+        rc = self.L.ndt_create(C.byref(self.params), device, C.byref(h))
+        if rc != NDT_OK:
+            raise NdtError(f"ndt_create failed: {ERRORS.get(rc, rc)}")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.ndt_destroy(self.h)
+            self.h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc < 0:
+            msg = self.L.ndt_last_error(self.h)
+            raise NdtError(f"{what}: {ERRORS.get(rc, rc)}: {msg.decode() if msg else ''}")
+        return rc
+
+    @property
+    def stream(self):
+        return self.L.ndt_stream(self.h)
+
+    def set_map(self, cloud):
+        cloud = _f32(cloud)
+        self._check(self.L.ndt_set_map(self.h, cloud, cloud.shape[0]), "ndt_set_map")
+
+    def set_map_device(self, ptr: int, m: int):
+        self._check(self.L.ndt_set_map_device(self.h, C.c_void_p(ptr), m), "ndt_set_map_device")
+
+    def align(self, scan, guess):
+        scan = _f32(scan)
+        out = np.zeros(16, np.float32)
+        conv, fit = C.c_int(), C.c_double()
+        self._check(self.L.ndt_align(self.h, scan, scan.shape[0], _f32(guess, 0).reshape(16), out, C.byref(conv),
+                                     C.byref(fit)), "ndt_align")
+        return out, conv.value, fit.value
+
+    def align_with_map(self, scan, guess, cloud):
+        scan, cloud = _f32(scan), _f32(cloud)
+        out = np.zeros(16, np.float32)
+        conv, fit = C.c_int(), C.c_double()
+        self._check(self.L.ndt_align_with_map(self.h, scan, scan.shape[0], _f32(guess, 0).reshape(16), cloud,
+                                              cloud.shape[0], out, C.byref(conv), C.byref(fit)),
+                    "ndt_align_with_map")
+        return out, conv.value, fit.value
+
+    def align_batch(self, scans, guesses):
+        scans = [_f32(s) for s in scans]
+        B = len(scans)
+        ptrs = (C.c_void_p * B)(*[s.ctypes.data for s in scans])
+        ns = np.array([s.shape[0] for s in scans], np.int32)
+        g = np.ascontiguousarray(np.asarray(guesses, np.float32).reshape(B, 16))
+        out = np.zeros((B, 16), np.float32)
+        conv = np.zeros(B, np.int32)
+        fit = np.zeros(B, np.float64)
+        status = np.zeros(B, np.int32)
+        self._check(self.L.ndt_align_batch(self.h, B, ptrs, ns, g, out, conv, fit, status.ctypes.data),
+                    "ndt_align_batch")
+        return out, conv, fit, status
+
+    def align_batch_device(self, B, d_points, d_offsets, total, d_guesses, d_out, d_conv, d_fit, d_status=0):
+        """Device pointers (ints, e.g. torch tensor .data_ptr()); enqueued on self.stream."""
+        self._check(self.L.ndt_align_batch_device(self.h, B, C.c_void_p(d_points), C.c_void_p(d_offsets), total,
+                                                  C.c_void_p(d_guesses), C.c_void_p(d_out), C.c_void_p(d_conv),
+                                                  C.c_void_p(d_fit), C.c_void_p(d_status)), "ndt_align_batch_device")
+
+    def synchronize(self):
+        self._check(self.L.ndt_synchronize(self.h), "ndt_synchronize")
+
+    def counters(self):
+        k = Counters()
+        self._check(self.L.ndt_get_counters(self.h, C.byref(k)), "ndt_get_counters")
+        return {f: getattr(k, f) for f, _ in Counters._fields_}
+
+    def grid_info(self):
+        bbox = np.zeros(6, np.float32)
+        dims = np.zeros(3, np.int32)
+        occ = C.c_int()
+        self._check(self.L.ndt_grid_info(self.h, bbox, dims, C.byref(occ)), "ndt_grid_info")
+        return bbox, dims, occ.value
+
+    def grid_cells(self):
+        _, _, K = self.grid_info()
+        cell = np.zeros(max(K, 1), np.int32)
+        count = np.zeros(max(K, 1), np.int32)
+        mean = np.zeros((max(K, 1), 3), np.float64)
+        icov = np.zeros((max(K, 1), 9), np.float64)
+        self._check(self.L.ndt_grid_cells(self.h, max(K, 1), cell, count, mean, icov), "ndt_grid_cells")
+        return cell[:K], count[:K], mean[:K], icov[:K]
+
+    def derivatives(self, scan, trans, p6):
+        scan, trans = _f32(scan), _f32(trans)
+        score = C.c_double()
+        g = np.zeros(6)
+        H = np.zeros(36)
+        self._check(self.L.ndt_derivatives(self.h, scan, trans, scan.shape[0], np.ascontiguousarray(p6, np.float64),
+                                           C.byref(score), g, H), "ndt_derivatives")
+        return score.value, g, H.reshape(6, 6)

@@ -1,0 +1,173 @@
+/*
+ * ndt_b200 -- C ABI of the B200 NDT scan-to-map registration library.
+ *
+ * This is the drop-in boundary for the DAPHNE ndt_mapping align call.  The
+ * reference binds it as a C++ member function,
+ *     CallbackResult ndt_mapping::partial_points_callback(
+ *         PointCloud& input_cloud, Matrix4f& init_guess, PointCloud& target_cloud)
+ * (src/CPU/ndt_mapping/kernel.cpp:1405; CUDA port src/Cuda/ndt_mapping/kernel.cu:1489),
+ * with CallbackResult{bool converged; Matrix4f final_transformation; double fitness_score}
+ * (src/CPU/ndt_mapping/datatypes.h:51-55), PointXYZI = float[4] and Matrix4f =
+ * float[4][4] row major (datatypes.h:11-17).  Every entry point here takes plain
+ * pointers and sizes with exactly those layouts: a cloud is `n` consecutive
+ * float[4] (x, y, z, intensity) records, a transform is 16 floats row major.
+ *
+ * Status codes: 0 = ok, negative = error (see NDT_E_*); ndt_last_error()
+ * returns a message for the last failing call on a context.  A context owns
+ * its device buffers and CUDA stream; use one context per host thread.
+ * There is no CPU fallback: without a usable sm_100 device every call that
+ * needs the GPU returns NDT_E_CUDA.
+ */
+#ifndef NDT_B200_H
+#define NDT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define NDT_API __attribute__((visibility("default")))
+#else
+#define NDT_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NDT_OK 0
+#define NDT_E_ARG (-1)       /* bad argument (NULL pointer, negative size, ...) */
+#define NDT_E_CUDA (-2)      /* a CUDA runtime call failed (message in ndt_last_error) */
+#define NDT_E_NOMAP (-3)     /* align called before a map was set */
+#define NDT_E_GRID (-4)      /* voxel grid too large for 32-bit cell indices */
+#define NDT_E_WATCHDOG (-5)  /* the iteration watchdog stopped an alignment */
+#define NDT_E_CAPACITY (-6)  /* a size exceeds a fixed capacity of the call */
+
+/* Per-alignment status bits written by the batch calls. */
+#define NDT_ST_OK 0
+#define NDT_ST_WATCHDOG 1
+
+/*
+ * Registration parameters.  ndt_params_reference() fills the values the
+ * reference kernel hard-codes (kernel.cpp:37-57): outlier 0.55, resolution 1.0,
+ * step 0.1, transformation_epsilon 0.1, max_iterations 0, compat 1.
+ *
+ * compat = 1 reproduces the reference kernel's behaviour bit for bit where it
+ * is deterministic (dense grid scaled by the grid size, permuted quaternion
+ * pose build without translation, fixed Newton step, its Hessian formula).
+ * compat = 0 runs the corrected NDT (per-voxel covariance with a minimum point
+ * count and eigenvalue floor, T = Trans * Rx * Ry * Rz, More-Thuente line
+ * search, ||dp|| stop test) whose FP64 restatement is the accuracy oracle.
+ */
+typedef struct ndt_params {
+    float resolution;              /* voxel edge length [m] (kernel.cpp:38) */
+    float _pad0;
+    double outlier_ratio;          /* kernel.cpp:37 */
+    double step_size;              /* More-Thuente step_max (kernel.cpp:40) */
+    double transformation_epsilon; /* step_min = eps/2 and |step| < eps stop (kernel.cpp:56) */
+    int32_t max_iterations;        /* Newton iterations beyond the first (kernel.cpp:57) */
+    int32_t compat;                /* 1 = reference behaviour, 0 = corrected NDT */
+    int32_t min_points_per_voxel;  /* compat = 0 only: voxels with fewer points are empty */
+    int32_t precision;             /* per-pair arithmetic: 0 = FP32 (default), 1 = FP64 */
+    double eigen_ratio;            /* compat = 0 only: covariance eigenvalue floor ratio */
+    int32_t watchdog_evals;        /* max derivative evaluations per alignment (0 = 1024) */
+    int32_t _pad1;
+} ndt_params;
+
+typedef struct ndt_ctx ndt_ctx;
+
+/* Parameter presets. */
+NDT_API void ndt_params_reference(ndt_params *p); /* reference kernel values, compat = 1 */
+NDT_API void ndt_params_corrected(ndt_params *p); /* corrected NDT: compat = 0, eps 0.01, 30 iterations */
+
+/* Context life cycle.  device = CUDA ordinal. */
+NDT_API int ndt_create(const ndt_params *params, int device, ndt_ctx **out);
+NDT_API void ndt_destroy(ndt_ctx *ctx);
+NDT_API const char *ndt_last_error(const ndt_ctx *ctx);
+
+/*
+ * Map (target cloud) upload + voxel grid build, once per map.  Replaces the
+ * per-call grid rebuild of ndt_mapping::initCompute (kernel.cpp:1302-1373);
+ * the resulting grid is identical to the one the reference builds for the
+ * same cloud.  `map` is a HOST pointer to m float[4] points.
+ */
+NDT_API int ndt_set_map(ndt_ctx *ctx, const float *map, int m);
+/* Same, but `map` is a device pointer (no host copy). */
+NDT_API int ndt_set_map_device(ndt_ctx *ctx, const float *d_map, int m);
+
+/*
+ * One alignment with host buffers: the partial_points_callback call
+ * (kernel.cpp:1405-1414) against the map set by ndt_set_map.
+ * out16 = final transformation, *converged, *fitness (NDT score per point;
+ * the reference never fills fitness_score).
+ */
+NDT_API int ndt_align(ndt_ctx *ctx, const float *scan, int n, const float guess16[16], float out16[16],
+              int *converged, double *fitness);
+
+/*
+ * partial_points_callback exactly as the reference shapes it: the map comes
+ * with the call and the grid is built from it (kernel.cpp:1375-1392).
+ */
+NDT_API int ndt_align_with_map(ndt_ctx *ctx, const float *scan, int n, const float guess16[16],
+                       const float *map, int m, float out16[16], int *converged,
+                       double *fitness);
+
+/*
+ * B independent alignments against the current map in one batched GPU pass
+ * (the loop of ndt_mapping::run, kernel.cpp:1425-1429, for one map).
+ * scans[b] -> ns[b] points (HOST pointers), guesses = B x 16 floats,
+ * out = B x 16 floats, converged/fitness/status = B entries (status may be NULL).
+ */
+NDT_API int ndt_align_batch(ndt_ctx *ctx, int B, const float *const *scans, const int *ns,
+                    const float *guesses, float *out, int *converged, double *fitness,
+                    int *status);
+
+/*
+ * Device-resident batch: scans concatenated in d_points (sum(ns) float[4]),
+ * d_offsets = B+1 prefix offsets (int32, device), d_guesses = B x 16 floats
+ * (device); results to device buffers d_out (B x 16), d_conv (B), d_fit (B),
+ * d_status (B).  Enqueued on the context stream; call ndt_synchronize().
+ */
+NDT_API int ndt_align_batch_device(ndt_ctx *ctx, int B, const float *d_points, const int *d_offsets,
+                           int total_points, const float *d_guesses, float *d_out, int *d_conv,
+                           double *d_fit, int *d_status);
+NDT_API int ndt_synchronize(ndt_ctx *ctx);
+
+/* The context's CUDA stream (cudaStream_t), for callers that time or order work. */
+NDT_API void *ndt_stream(ndt_ctx *ctx);
+
+/*
+ * Work counters of the last batch: derivative evaluations (kernel launches of
+ * the derivative pass), scan points visited, cell probes, accepted
+ * (point, voxel) pairs, summed over all evaluations.
+ */
+typedef struct ndt_counters {
+    int64_t evaluations;
+    int64_t points;
+    int64_t probes;
+    int64_t pairs;
+    int64_t launches;
+} ndt_counters;
+NDT_API int ndt_get_counters(ndt_ctx *ctx, ndt_counters *out);
+
+/*
+ * Grid inspection (tests): bbox (min xyz, max xyz), dims, number of occupied
+ * cells, and for each occupied cell its linear index, point count, mean[3]
+ * (FP64) and inverse covariance[9] (FP64) as the reference stores them.
+ * Pass NULL arrays to query sizes only.
+ */
+NDT_API int ndt_grid_info(ndt_ctx *ctx, float *bbox6, int *dims3, int *occupied);
+NDT_API int ndt_grid_cells(ndt_ctx *ctx, int cap, int *cell_index, int *count, double *mean3,
+                   double *icov9);
+
+/*
+ * One derivative evaluation (computeDerivatives, kernel.cpp:651-705) of a
+ * scan already transformed by the caller, at pose vector p6 (for the angle
+ * terms), against the current map.  HOST buffers.  Returns score via *score.
+ */
+NDT_API int ndt_derivatives(ndt_ctx *ctx, const float *scan, const float *trans, int n,
+                    const double p6[6], double *score, double g6[6], double H36[36]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NDT_B200_H */

@@ -1,0 +1,184 @@
+"""GPU parity: the CUDA path (through the C ABI) against the reference's
+results (golden fixtures made by the compiled reference) and the FP64 oracle.
+
+Tolerances
+  * voxel grid (compat and corrected): bit-exact (same FP64 operations in the
+    same point order as the reference / oracle);
+  * derivative pass, FP64 pair arithmetic: relative 1e-9 of the largest
+    entry (only the summation order differs);
+  * derivative pass, FP32 pair arithmetic: relative 2e-3 of the largest entry
+    of each block (score, gradient, Hessian);
+  * full alignment, compat: translation column bit-exact, converged equal,
+    NaN pattern equal, rotation entries within 1e-6 (FP64) / 2e-3 (FP32),
+    and the reference's own check_next_outputs rule passes;
+  * corrected mode: <= 2 cm translation and <= 0.1 deg rotation against the
+    FP64 oracle.
+"""
+import json
+import math
+import pathlib
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = pathlib.Path(__file__).resolve().parent / "golden" / "reference_cases.json"
+
+
+@pytest.fixture(scope="module")
+def cases():
+    return json.loads(GOLDEN.read_text())["cases"]
+
+
+def _config(pkg, c):
+    cfg = c["config"]
+    return pkg.synth.Config(cfg["name"], cfg["map_points"], cfg["area"], cfg["walls"], cfg["resolution"], 1,
+                            cfg["scan_min"], cfg["scan_min"], False, cfg["dt"], cfg["dyaw_deg"], radius=cfg["radius"],
+                            seed=cfg["seed"])
+
+
+_SCENES = {}
+
+
+def _inputs(pkg, c):
+    cfg = _config(pkg, c)
+    key = (cfg.seed, cfg.map_points, cfg.area, cfg.walls)
+    if key not in _SCENES:
+        _SCENES[key] = pkg.synth.make_scene(cfg)
+    scene = _SCENES[key]
+    a = pkg.synth.make_alignment(cfg, scene, c["index"])
+    assert pkg.synth.digest(a.scan, a.guess, scene.map) == c["input_sha256"], "generator no longer reproduces fixture"
+    return cfg, scene, a
+
+
+def _rot_err_deg(A, B):
+    R = A.reshape(4, 4)[:3, :3].astype(np.float64) @ B.reshape(4, 4)[:3, :3].astype(np.float64).T
+    c = (np.trace(R) - 1.0) / 2.0
+    return math.degrees(math.acos(max(-1.0, min(1.0, c))))
+
+
+@pytest.mark.parametrize("compat", [1, 0])
+def test_grid_bitexact_vs_oracle(pkg, oracle, binding_mod, cases, compat):
+    for c in cases[:6]:
+        cfg, scene, _ = _inputs(pkg, c)
+        gp = pkg.ndt.reference_params(cfg.resolution) if compat else pkg.ndt.corrected_params(cfg.resolution)
+        op = binding_mod.reference_params(cfg.resolution) if compat else binding_mod.corrected_params(cfg.resolution)
+        with pkg.ndt.Context(gp) as ctx:
+            ctx.set_map(scene.map)
+            bbox, dims, K = ctx.grid_info()
+            cell, count, mean, icov = ctx.grid_cells()
+        obox, odims, ocells = oracle.grid(op, scene.map)
+        assert np.array_equal(bbox.view(np.uint32), obox.view(np.uint32))
+        assert np.array_equal(dims, odims)
+        occ = np.nonzero(ocells[:, 12] != 0)[0] if compat else np.nonzero(ocells[:, 12] > 0)[0]
+        assert K == (ocells[:, 12] > 0).sum() if compat else True
+        if compat:
+            assert np.array_equal(np.sort(cell), occ)
+        # compare every usable cell bit for bit
+        order = np.argsort(cell)
+        cell, count, mean, icov = cell[order], count[order], mean[order], icov[order]
+        if not compat:
+            keep = ocells[cell, 12] > 0
+            cell, count, mean, icov = cell[keep], count[keep], mean[keep], icov[keep]
+        ref = ocells[cell]
+        assert np.array_equal(count, np.abs(ref[:, 12]).astype(np.int32))
+        same_mean = (mean.view(np.uint64) == ref[:, 0:3].copy().view(np.uint64)) | (np.isnan(mean) & np.isnan(ref[:, 0:3]))
+        same_icov = (icov.view(np.uint64) == ref[:, 3:12].copy().view(np.uint64)) | (np.isnan(icov) & np.isnan(ref[:, 3:12]))
+        assert same_mean.all(), f"{c['name']}: mean mismatch in {np.count_nonzero(~same_mean)} entries"
+        assert same_icov.all(), f"{c['name']}: icov mismatch in {np.count_nonzero(~same_icov)} entries"
+
+
+def test_grid_matches_reference_digest(pkg, cases):
+    """The GPU grid's occupied cells hash to the reference's (fixture)."""
+    import hashlib
+    for c in cases:
+        if c["grid"] is None:
+            continue
+        cfg, scene, _ = _inputs(pkg, c)
+        with pkg.ndt.Context(pkg.ndt.reference_params()) as ctx:
+            ctx.set_map(scene.map)
+            bbox, dims, K = ctx.grid_info()
+            cell, count, mean, icov = ctx.grid_cells()
+        assert bbox.view(np.uint32).tolist() == c["grid"]["bbox_bits"]
+        assert dims.tolist() == c["grid"]["dims"]
+        assert K == c["grid"]["occupied"]
+        order = np.argsort(cell)
+        rows = np.concatenate([mean[order], icov[order], count[order][:, None].astype(np.float64)], axis=1)
+        assert hashlib.sha256(np.ascontiguousarray(rows).tobytes()).hexdigest() == c["grid"]["occupied_sha256"]
+
+
+@pytest.mark.parametrize("precision", [1, 0])
+def test_derivatives_vs_reference(pkg, cases, precision):
+    for c in cases:
+        if c["derivatives"] is None:
+            continue
+        cfg, scene, a = _inputs(pkg, c)
+        d = c["derivatives"]
+        with pkg.ndt.Context(pkg.ndt.reference_params(precision=precision)) as ctx:
+            ctx.set_map(scene.map)
+            # transformPointCloud by the guess, float (same as the reference)
+            G = a.guess.reshape(4, 4)
+            trans = np.zeros_like(a.scan)
+            for r in range(3):
+                trans[:, r] = ((G[r, 0] * a.scan[:, 0] + G[r, 1] * a.scan[:, 1]) + G[r, 2] * a.scan[:, 2]) + G[r, 3]
+            s, g, H = ctx.derivatives(a.scan, trans, np.array(d["p6"]))
+        rs, rg, rH = d["score"], np.array(d["gradient"]), np.array(d["hessian"]).reshape(6, 6)
+        tol = 1e-9 if precision == 1 else 2e-3
+        assert abs(s - rs) <= tol * max(1.0, abs(rs)), (c["name"], s, rs)
+        assert np.max(np.abs(g - rg)) <= tol * max(1.0, np.max(np.abs(rg))), (c["name"], g, rg)
+        assert np.max(np.abs(H - rH)) <= tol * max(1.0, np.max(np.abs(rH))), (c["name"], H, rH)
+
+
+@pytest.mark.parametrize("precision", [1, 0])
+def test_align_compat_vs_reference(pkg, cases, precision):
+    rot_tol = 1e-6 if precision == 1 else 2e-3
+    worst = 0.0
+    for c in cases:
+        if c["source"] != "reference":
+            continue
+        cfg, scene, a = _inputs(pkg, c)
+        ref = np.array(c["out_bits"], np.uint32).view(np.float32)
+        with pkg.ndt.Context(pkg.ndt.reference_params(precision=precision)) as ctx:
+            out, conv, fit = ctx.align_with_map(a.scan, a.guess, scene.map)
+        assert conv == c["converged"]
+        assert np.array_equal(np.isnan(out), np.isnan(ref))
+        T, R = out.reshape(4, 4), ref.reshape(4, 4)
+        assert np.array_equal(T[:, 3].view(np.uint32), R[:, 3].view(np.uint32)), "translation column must be exact"
+        assert np.array_equal(T[3].view(np.uint32), R[3].view(np.uint32))
+        d = np.nanmax(np.abs(T[:3, :3] - R[:3, :3]))
+        worst = max(worst, d)
+        assert d <= rot_tol, (c["name"], d)
+        ok, _ = pkg.datfile.reference_check(out, conv, ref, c["converged"])
+        assert ok
+    print(f"worst rotation-entry delta (precision {precision}): {worst:.3e}")
+
+
+def test_batch_equals_single(pkg, cases):
+    c0 = [c for c in cases if c["config"]["name"] == "s8k"]
+    cfg, scene, _ = _inputs(pkg, c0[0])
+    aligns = [pkg.synth.make_alignment(cfg, scene, i) for i in range(6)]
+    with pkg.ndt.Context(pkg.ndt.reference_params()) as ctx:
+        ctx.set_map(scene.map)
+        out, conv, fit, status = ctx.align_batch([a.scan for a in aligns], [a.guess for a in aligns])
+        for i, a in enumerate(aligns):
+            o1, c1, f1 = ctx.align(a.scan, a.guess)
+            assert np.array_equal(o1.view(np.uint32), out[i].view(np.uint32))
+            assert c1 == conv[i]
+    assert (status == 0).all()
+
+
+def test_corrected_vs_fp64_oracle(pkg, oracle, binding_mod):
+    cfg = pkg.synth.small_config("cf", 20000, 40.0, 16, 1500, seed=21)
+    scene = pkg.synth.make_scene(cfg)
+    aligns = [pkg.synth.make_alignment(cfg, scene, i) for i in range(8)]
+    with pkg.ndt.Context(pkg.ndt.corrected_params()) as ctx:
+        ctx.set_map(scene.map)
+        out, conv, fit, status = ctx.align_batch([a.scan for a in aligns], [a.guess for a in aligns])
+    ref, rconv, rfit, _ = oracle.align_batch(binding_mod.corrected_params(), [a.scan for a in aligns],
+                                             [a.guess for a in aligns], scene.map)
+    for i in range(len(aligns)):
+        dt = np.linalg.norm(out[i].reshape(4, 4)[:3, 3] - ref[i].reshape(4, 4)[:3, 3])
+        dr = _rot_err_deg(out[i], ref[i])
+        assert dt <= 0.02 and dr <= 0.1, (i, dt, dr)
+        assert conv[i] == 1
