@@ -1,0 +1,460 @@
+#!/usr/bin/env python3
+"""Throughput benchmark of the B200 NDT align path (DAPHNE ndt_mapping).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config c2] [--mode compat|corrected] [--precision 0|1]
+
+A step is one batch of the configuration's alignments against its map: the
+voxel grid is built from the map and every alignment runs to completion.  At
+the default configuration (c2) a step is 256 alignments of 8000-point scans
+against a 400k-point map (150 x 150 m, 120 walls), resolution 1.0 m, guesses
++-0.5 m / +-3 deg off the ground truth, with the reference kernel's semantics
+(compat mode: the drop-in for partial_points_callback).  Inputs are seeded
+synthetic clouds (the reference's input file is not distributed).
+
+Our arm prints one JSON line with `value` (aligns/s with inputs resident in
+HBM, L2 flushed between steps), `e2e` (aligns/s through the C ABI with pinned
+host buffers, copies inside the timed region), the derivative kernel's
+roofline, the CPU baseline (the compiled reference kernel on the host cores,
+rank 0) and the SM clocks sampled during the timed region.  With torchrun
+(N > 1) every rank aligns its own batch (weak scaling; no collective on the
+data path) and the timing is the max over ranks.
+
+--impl reference times the reference's own CPU implementation (the compiled
+src/CPU/ndt_mapping kernel in oracle/_ref, one reference object per host
+thread on all host cores; the restated oracle when that library is absent) on
+the same workload and prints the same line with "impl": "reference".
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import math
+import os
+import pathlib
+import statistics
+import sys
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+PKG_DIR = ROOT / "daphne-benchmark_b200"
+sys.path.insert(0, str(ROOT / "oracle"))
+
+L2_FLUSH_BYTES = 256 << 20
+METRIC = "NDT aligns/sec on 1 B200, learned-init vs plain, at <=2cm/0.1deg pose error"
+
+
+def load_pkg():
+    name = "daphne_benchmark_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, PKG_DIR / "__init__.py",
+                                                  submodule_search_locations=[str(PKG_DIR)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """SM clock and throttle-reason samples of one GPU during the timed region.
+
+    NVML (nvidia_ml_py) polled every 5 ms from a thread.  Reading clocks
+    changes no GPU setting.
+    """
+
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
+
+    def __init__(self, device_index: int, uuid: str | None):
+        import threading
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self.stop_flag = threading.Event()
+        self.nvml = None
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByUUID(uuid) if uuid else nv.nvmlDeviceGetHandleByIndex(device_index)
+            self.nvml, self.h = nv, h
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        except Exception:
+            self.nvml = None
+        self.thread = threading.Thread(target=self._run, daemon=True)
+        self.thread.start()
+
+    def _run(self):
+        if self.nvml is None:
+            return
+        nv = self.nvml
+        while not self.stop_flag.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for name, mask in self.REASONS.items():
+                    if bits & mask:
+                        self.reasons.add(name)
+            except Exception:
+                return
+            time.sleep(0.005)
+
+    def stop(self):
+        self.stop_flag.set()
+        self.thread.join(timeout=2)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["no NVML samples"], "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples), "source": "NVML, 5 ms"}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def workload(pkg, cfg_name, rank, count=None):
+    cfg = pkg.synth.CONFIGS[cfg_name]
+    scene = pkg.synth.make_scene(cfg)
+    B = cfg.aligns if count is None else count
+    aligns = [pkg.synth.make_alignment(cfg, scene, rank * B + i) for i in range(B)]
+    return cfg, scene, aligns
+
+
+def config_block(cfg, mode, precision, B, npts):
+    return {
+        "workload": (f"{cfg.name}: {cfg.map_points}-point map ({cfg.area:g} x {cfg.area:g} m, {cfg.walls} walls), "
+                     f"{B} alignments x {npts // B if B else 0} scan points per step, resolution {cfg.resolution:g} m, "
+                     f"guesses +-{cfg.dt:g} m / +-{cfg.dyaw_deg:g} deg"),
+        "map_points": cfg.map_points,
+        "alignments_per_step": B,
+        "scan_points_per_step": npts,
+        "resolution_m": cfg.resolution,
+        "mode": mode,
+        "pair_arithmetic": "fp64" if precision == 1 else "fp32",
+        "grid_build": "inside every step (from the map)",
+        "l2": f"flushed between timed steps ({L2_FLUSH_BYTES >> 20} MiB write); e2e inputs from pinned host memory",
+    }
+
+
+def rot_deg(A, B):
+    """Angle between two rotation blocks, 2 asin(||Ra - Rb||_F / sqrt 8), well conditioned near 0."""
+    d = A.reshape(4, 4)[:3, :3].astype(np.float64) - B.reshape(4, 4)[:3, :3].astype(np.float64)
+    return math.degrees(2.0 * math.asin(min(1.0, float(np.linalg.norm(d)) / math.sqrt(8.0))))
+
+
+# ---------------------------------------------------------------------------
+def run_reference_arm(args, pkg, world, rank):
+    if rank != 0:
+        return 0
+    import binding
+    cfg, scene, aligns = workload(pkg, args.config, 0)
+    B = len(aligns)
+    npts = sum(a.scan.shape[0] for a in aligns)
+    cores = os.cpu_count() or 1
+    scans = [a.scan for a in aligns]
+    guesses = np.stack([a.guess for a in aligns])
+    if binding.Reference.available("serial"):
+        ref = binding.Reference("serial")
+        kind = "reference"
+
+        def step():
+            ref.align_batch(scans, guesses, [scene.map] * B, nthreads=cores)
+    else:
+        orc = binding.Oracle()
+        prm = binding.reference_params(cfg.resolution) if args.mode == "compat" else \
+            binding.corrected_params(cfg.resolution)
+        kind = "port"
+
+        def step():
+            # the restated reference; grid rebuilt per alignment like the reference's call
+            for i in range(B):
+                orc.align(prm, scans[i], guesses[i], scene.map)
+    for _ in range(args.warmup):
+        step()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        step()
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = B * args.steps / total
+    sample = (f"every step: all {B} alignments of the workload, one reference object per thread "
+              f"on {cores} host threads (grid rebuilt per alignment, as partial_points_callback does)")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "aligns/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64 (reference CPU)",
+        "data": "synthetic (seeded plane + walls generator)",
+        "config": config_block(cfg, args.mode, args.precision, B, npts),
+        "cpu_baseline": {"value": value, "unit": "aligns/s", "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": "aligns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def cpu_baseline(pkg, scene, aligns, mode):
+    """Reference kernel on the host cores (oracle/_ref), bounded sample."""
+    import binding
+    cores = os.cpu_count() or 1
+    n = min(len(aligns), max(16, 4 * cores))
+    scans = [a.scan for a in aligns[:n]]
+    guesses = np.stack([a.guess for a in aligns[:n]])
+    if mode == "compat" and binding.Reference.available("serial"):
+        ref = binding.Reference("serial")
+        kind = "reference"
+        fn = lambda: ref.align_batch(scans, guesses, [scene.map] * n, nthreads=cores)  # noqa: E731
+        what = "compiled reference src/CPU/ndt_mapping, one object per thread"
+    else:
+        orc = binding.Oracle()
+        prm = binding.reference_params() if mode == "compat" else binding.corrected_params()
+        kind = "port"
+        fn = lambda: orc.align_batch(prm, scans, guesses, scene.map, nthreads=cores)  # noqa: E731
+        what = "FP64 restatement (oracle), shared grid"
+    fn()  # warm
+    reps, t = 0, 0.0
+    while t < 3.0 and reps < 20:
+        t0 = time.perf_counter()
+        fn()
+        t += time.perf_counter() - t0
+        reps += 1
+    return {"value": n * reps / t, "unit": "aligns/s", "cores": cores, "kind": kind,
+            "sample": f"{n} alignments of the step x {reps} repetitions ({t:.1f} s wall), {what}"}
+
+
+def accuracy(pkg, scene, aligns, out, conv, mode, resolution):
+    """Pose error of every alignment of the step against the FP64 oracle."""
+    import binding
+    prm = binding.reference_params(resolution) if mode == "compat" else binding.corrected_params(resolution)
+    orc = binding.Oracle()
+    ref, rconv, _, _ = orc.align_batch(prm, [a.scan for a in aligns], [a.guess for a in aligns], scene.map)
+    dt = np.linalg.norm(out.reshape(-1, 4, 4)[:, :3, 3] - ref.reshape(-1, 4, 4)[:, :3, 3], axis=1)
+    dr = np.array([rot_deg(out[i], ref[i]) for i in range(len(aligns))])
+    ok = int(np.sum((dt <= 0.02) & (dr <= 0.1) & (conv == rconv)))
+    return {"alignments": len(aligns), "within_2cm_0.1deg": ok, "max_translation_m": float(dt.max()),
+            "max_rotation_deg": float(dr.max()), "converged_equal": int(np.sum(conv == rconv)),
+            "oracle": "FP64 restatement of the reference (bit-identical to it)" if mode == "compat"
+            else "FP64 corrected-NDT oracle"}
+
+
+def run_ours(args, pkg, world, rank, local):
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", device_id=dev, timeout=__import__("datetime").timedelta(seconds=120))
+    ndt = pkg.ndt
+    cfg, scene, aligns = workload(pkg, args.config, rank)
+    B = len(aligns)
+    offs = np.zeros(B + 1, np.int32)
+    offs[1:] = np.cumsum([a.scan.shape[0] for a in aligns])
+    npts = int(offs[-1])
+    points = np.ascontiguousarray(np.concatenate([a.scan for a in aligns]))
+    guesses = np.ascontiguousarray(np.stack([a.guess for a in aligns]).astype(np.float32))
+    M = scene.map.shape[0]
+    prm = ndt.reference_params(cfg.resolution, args.precision) if args.mode == "compat" else \
+        ndt.corrected_params(cfg.resolution, args.precision)
+    ctx = ndt.Context(prm, device=local)
+    if args.variant is not None:
+        ctx.set_kernel_variant(args.variant)
+    ctx.set_profiling(True)
+    st = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    # device-resident inputs and outputs
+    d_map = torch.from_numpy(scene.map).to(dev)
+    d_pts = torch.from_numpy(points).to(dev)
+    d_off = torch.from_numpy(offs).to(dev)
+    d_g = torch.from_numpy(guesses).to(dev)
+    d_out = torch.zeros(B, 16, device=dev)
+    d_conv = torch.zeros(B, dtype=torch.int32, device=dev)
+    d_fit = torch.zeros(B, dtype=torch.float64, device=dev)
+    d_status = torch.zeros(B, dtype=torch.int32, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+
+    def device_step():
+        ctx.set_map_device(d_map.data_ptr(), M)
+        ctx.align_batch_device(B, d_pts.data_ptr(), d_off.data_ptr(), npts, d_g.data_ptr(), d_out.data_ptr(),
+                               d_conv.data_ptr(), d_fit.data_ptr(), d_status.data_ptr())
+
+    def flush_l2():
+        with torch.cuda.stream(st):
+            flush.fill_(float(np.random.random()))
+
+    for _ in range(args.warmup):
+        flush_l2()
+        device_step()
+    ctx.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        uuid = None
+    clocks = ClockSampler(local, uuid)
+    launches0 = ctx.counters()["launches"]
+    step_ms, agg = [], {"points": 0, "probes": 0, "occupied_probes": 0, "pairs": 0, "tiles": 0,
+                        "deriv_launches": 0, "deriv_ms": 0.0, "grid_ms": 0.0, "evaluations": 0, "rounds": 0}
+    wall0 = time.perf_counter()
+    for _ in range(args.steps):
+        flush_l2()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        device_step()
+        e1.record(st)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        k = ctx.counters()
+        for key in agg:
+            agg[key] += k[key]
+    wall = time.perf_counter() - wall0
+    launches = ctx.counters()["launches"] - launches0
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    total_ms = sum(step_ms)
+    out_dev = (d_out.cpu().numpy(), d_conv.cpu().numpy(), d_status.cpu().numpy())
+
+    # ---- end to end through the C ABI with pinned host buffers
+    h_map = torch.from_numpy(scene.map).pin_memory()
+    h_pts = torch.from_numpy(points).pin_memory()
+    h_off = torch.from_numpy(offs).pin_memory()
+    h_g = torch.from_numpy(guesses).pin_memory()
+    h_out = torch.zeros(B, 16).pin_memory()
+    h_conv = torch.zeros(B, dtype=torch.int32).pin_memory()
+    h_fit = torch.zeros(B, dtype=torch.float64).pin_memory()
+    h_status = torch.zeros(B, dtype=torch.int32).pin_memory()
+
+    def host_step():
+        ctx.set_map_ptr(h_map.data_ptr(), M)
+        ctx.align_batch_packed_ptr(B, h_pts.data_ptr(), h_off.data_ptr(), h_g.data_ptr(), h_out.data_ptr(),
+                                   h_conv.data_ptr(), h_fit.data_ptr(), h_status.data_ptr())
+
+    for _ in range(args.warmup):
+        flush_l2()
+        host_step()
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush_l2()
+        ctx.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        host_step()
+        e1.record(st)
+        e1.synchronize()
+        e2e_ms.append(e0.elapsed_time(e1))
+    e2e_total = sum(e2e_ms)
+    clk = clocks.stop()
+
+    # ---- max over ranks
+    if world > 1:
+        t = torch.tensor([total_ms, e2e_total], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms, e2e_total = float(t[0]), float(t[1])
+    value = world * B * args.steps / (total_ms / 1e3)
+    e2e_value = world * B * args.steps / (e2e_total / 1e3)
+    if rank != 0:
+        ctx.close()
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return 0
+
+    # ---- roofline of the derivative kernel
+    peak, peak_kind = measured_peaks()
+    n_launch = max(1, agg["deriv_launches"])
+    bytes_total = (16 * agg["points"] + 4 * agg["probes"] + 16 * agg["occupied_probes"] + 56 * agg["pairs"]
+                   + 8 * 44 * agg["tiles"])
+    bytes_per_launch = bytes_total / n_launch
+    launch_ms = agg["deriv_ms"] / n_launch
+    achieved = bytes_per_launch / (launch_ms / 1e3) / 1e9 if launch_ms > 0 else None
+    traffic = None
+    tf = ROOT / "profiles" / "derivative_traffic.json"
+    if tf.exists():
+        try:
+            td = json.loads(tf.read_text())
+            key = f"{args.config}/{args.mode}/p{args.precision}"
+            if key in td:
+                traffic = td[key]["bytes_per_launch"]
+        except Exception:
+            traffic = None
+    roofline = {"kernel": "derivative pass (derivative_f32_kernel / derivative_f64_kernel)", "bound": "hbm",
+                "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                else "fallback 6650 GB/s",
+                "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": launch_ms,
+                "launches": agg["deriv_launches"],
+                "bytes_model": "16 B/point + 4 B/in-bounds probe + 16 B/occupied probe + 56 B/accepted pair "
+                               "+ 352 B/tile partial",
+                "share_of_step": agg["deriv_ms"] / total_ms if total_ms else None,
+                "grid_build_ms_per_step": agg["grid_ms"] / args.steps}
+
+    acc = accuracy(pkg, scene, aligns, out_dev[0], out_dev[1], args.mode, cfg.resolution)
+    cpu = cpu_baseline(pkg, scene, aligns, args.mode) if world == 1 else None
+    h2d = scene.map.nbytes + points.nbytes + offs.nbytes + guesses.nbytes
+    d2h = B * (16 * 4 + 4 + 8 + 4)
+    line = {
+        "metric": METRIC, "value": value, "unit": "aligns/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": ("fp32 pair terms, fp64 grid/solve/line search" if args.precision == 0
+                                        else "fp64"),
+        "data": "synthetic (seeded plane + walls generator; the reference's input file is not distributed)",
+        "config": config_block(cfg, args.mode, args.precision, B, npts),
+        "e2e": {"value": e2e_value, "unit": "aligns/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": d2h,
+                "ms_per_step": e2e_total / args.steps,
+                "path": "ndt_set_map + ndt_align_batch_packed (C ABI), pinned host buffers"},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "gpu_launches": int(launches),
+        "accuracy_vs_fp64_oracle": acc,
+        "work_per_step": {k: (v / args.steps) for k, v in agg.items()},
+        "wall_s_timed_loop": wall,
+        "kernel_variant": args.variant if args.variant is not None else 0,
+        "status_nonzero": int(np.count_nonzero(out_dev[2])),
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", default="c2")
+    ap.add_argument("--mode", choices=["compat", "corrected"], default="compat")
+    ap.add_argument("--precision", type=int, choices=[0, 1], default=0)
+    ap.add_argument("--variant", type=int, default=None, help="derivative-pass launch shape (autotuner index)")
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    pkg = load_pkg()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        return run_reference_arm(args, pkg, world, rank)
+    return run_ours(args, pkg, world, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -282,8 +282,8 @@ __global__ void finalize_kernel(const AlignState *__restrict__ states, int B, fl
     if (status) status[b] = st;
 }
 
-// Tile list: ceil(n_b / kTile) tiles per alignment, in alignment order.
-__global__ void tile_count_kernel(const int *__restrict__ offsets, int B, int *__restrict__ tile_begin) {
+// Tile list: ceil(n_b / tile) tiles per alignment, in alignment order.
+__global__ void tile_count_kernel(const int *__restrict__ offsets, int B, int tile, int *__restrict__ tile_begin) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b > B) return;
     if (b == B) {
@@ -291,7 +291,7 @@ __global__ void tile_count_kernel(const int *__restrict__ offsets, int B, int *_
         return;
     }
     int n = offsets[b + 1] - offsets[b];
-    tile_begin[b] = n > 0 ? (n + kTile - 1) / kTile : 0;
+    tile_begin[b] = n > 0 ? (n + tile - 1) / tile : 0;
 }
 
 __global__ void scan_small_kernel(int *__restrict__ data, int n, int *__restrict__ total) {
@@ -328,7 +328,7 @@ __global__ void scan_small_kernel(int *__restrict__ data, int n, int *__restrict
     if (total && t == nt - 1) *total = run;
 }
 
-__global__ void tile_fill_kernel(const int *__restrict__ offsets, const int *__restrict__ tile_begin, int B,
+__global__ void tile_fill_kernel(const int *__restrict__ offsets, const int *__restrict__ tile_begin, int B, int tile,
                                  Tile *__restrict__ tiles) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (warp >= B) return;
@@ -337,8 +337,8 @@ __global__ void tile_fill_kernel(const int *__restrict__ offsets, const int *__r
     for (int t = t0 + lane; t < t1; t += 32) {
         Tile x;
         x.align = warp;
-        x.start = lo + (t - t0) * kTile;
-        x.end = min(hi, x.start + kTile);
+        x.start = lo + (t - t0) * tile;
+        x.end = min(hi, x.start + tile);
         x.slot = t;
         tiles[t] = x;
     }
@@ -370,10 +370,11 @@ int launch_prepare_eval(AlignState *d_state, const double *d_p6, int n, double *
     return (int)cudaGetLastError();
 }
 
-int launch_tiles(const int *d_offsets, int B, int *d_tile_begin, Tile *d_tiles, int *d_num_tiles, cudaStream_t st) {
-    tile_count_kernel<<<(B + 1 + 255) / 256, 256, 0, st>>>(d_offsets, B, d_tile_begin);
+int launch_tiles(const int *d_offsets, int B, int tile, int *d_tile_begin, Tile *d_tiles, int *d_num_tiles,
+                 cudaStream_t st) {
+    tile_count_kernel<<<(B + 1 + 255) / 256, 256, 0, st>>>(d_offsets, B, tile, d_tile_begin);
     scan_small_kernel<<<1, 1024, 0, st>>>(d_tile_begin, B + 1, d_num_tiles);
-    tile_fill_kernel<<<(B * 32 + 255) / 256, 256, 0, st>>>(d_offsets, d_tile_begin, B, d_tiles);
+    tile_fill_kernel<<<(B * 32 + 255) / 256, 256, 0, st>>>(d_offsets, d_tile_begin, B, tile, d_tiles);
     return (int)cudaGetLastError();
 }
 

@@ -17,7 +17,8 @@ struct StepParams {
     int watchdog_evals;
 };
 
-int launch_tiles(const int *d_offsets, int B, int *d_tile_begin, Tile *d_tiles, int *d_num_tiles, cudaStream_t st);
+int launch_tiles(const int *d_offsets, int B, int tile, int *d_tile_begin, Tile *d_tiles, int *d_num_tiles,
+                 cudaStream_t st);
 int launch_init(AlignState *d_states, const float *d_guesses, const int *d_offsets, int B, const StepParams &P,
                 double *d_exc, cudaStream_t st);
 int launch_step(AlignState *d_states, const double *d_partials, const int *d_tile_begin, double *d_exc, int B,

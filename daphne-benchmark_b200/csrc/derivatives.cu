@@ -42,7 +42,6 @@ namespace ndt {
 namespace {
 
 constexpr int kWarpsE = kTile / 32;
-constexpr int kRing = 64;   // per-warp pair ring (entries)
 constexpr int kAcc = 37;    // score, g[6], S[21], R[9]
 constexpr unsigned kFull = 0xffffffffu;
 
@@ -99,72 +98,139 @@ __device__ __forceinline__ ProbeStart probe_start(float px, float py, float pz, 
     return s;
 }
 
-// Walk the probes of every lane's point in the reference's order, calling
-// on_full(head) whenever >= 32 accepted pairs are queued and on_tail(head, n)
-// once at the end.  Ring entries: {code, x'0, x'1, x'2} with
-// code = slot << 6 | flag << 5 | lane.
-template <class Full, class Tail>
-__device__ __forceinline__ void probe_walk(const GridDev &grid, float px, float py, float pz, bool valid,
-                                           float4 *ring, unsigned long long &n_probe, unsigned long long &n_occ,
-                                           Full on_full, Tail on_tail) {
+constexpr int kList = 27 * 32;  // per-warp pair list: all 27 probes of all 32 lanes
+
+// Append the accepted (point, voxel) pairs of one probe step of the warp to
+// the list (code = slot << 6 | flag << 5 | lane), in lane order.
+__device__ __forceinline__ void list_append(unsigned *list, int &n, bool acc, unsigned code, unsigned lt) {
+    const unsigned b = __ballot_sync(kFull, acc);
+    if (acc) list[n + __popc(b & lt)] = code;
+    n += __popc(b);
+}
+
+// Probe the reference's 27 cells around every lane's point (z outer, x
+// inner; voxelRadiusSearch, kernel.cpp:246-286) and collect the accepted
+// pairs in `list`.  Fast path (trip counts <= 3, i.e. every finite coordinate
+// below ~1e6 m): the 27 index loads, then the voxel-mean loads of one
+// z-layer at a time, are all in flight together, and the list (27 x 32
+// entries) cannot overflow.  Generic path (up to 4 x 4 x 4 probes): one probe
+// at a time, calling flush(n) whenever the list could overflow.
+template <class Flush>
+__device__ __forceinline__ int probe_list(const GridDev &grid, float px, float py, float pz, bool valid,
+                                          unsigned *list, unsigned &n_probe, unsigned &n_occ, Flush flush) {
     const int lane = threadIdx.x & 31;
     const unsigned lt = lanemask_lt();
     const GridMeta &g = grid.meta;
     const float res = g.res;
     const double radius = (double)res;
-    ProbeStart ps = probe_start(px, py, pz, res, valid);
+    const ProbeStart ps = probe_start(px, py, pz, res, valid);
     const int mz = __reduce_max_sync(kFull, ps.nz);
     const int my = __reduce_max_sync(kFull, ps.ny);
     const int mx = __reduce_max_sync(kFull, ps.nx);
-    int head = 0, count = 0;
+    int n = 0;
+    if (mz <= 3 && my <= 3 && mx <= 3) {
+        float zc[3], yc[3], xc[3];
+        zc[0] = ps.z0; zc[1] = zc[0] + res; zc[2] = zc[1] + res;
+        yc[0] = ps.y0; yc[1] = yc[0] + res; yc[2] = yc[1] + res;
+        xc[0] = ps.x0; xc[1] = xc[0] + res; xc[2] = xc[1] + res;
+        int v[27];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const float z = zc[a], y = yc[b], x = xc[c];
+                    const bool act = a < ps.nz && b < ps.ny && c < ps.nx;
+                    const bool inb = act && !((x < g.minv[0]) || (x > g.maxv[0]) || (y < g.minv[1]) ||
+                                              (y > g.maxv[1]) || (z < g.minv[2]) || (z > g.maxv[2]));
+                    int slot = -1;
+                    if (inb) {
+                        const int ix = (int)((x - g.minv[0]) / res);
+                        const int iy = (int)((y - g.minv[1]) / res);
+                        const int iz = (int)((z - g.minv[2]) / res);
+                        slot = __ldg(grid.index + (ix + g.dim[0] * (iy + g.dim[1] * iz)));
+                        ++n_probe;
+                    }
+                    v[9 * a + 3 * b + c] = slot;
+                }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            float4 mf[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                const int slot = v[9 * a + k];
+                if (slot >= 0) mf[k] = __ldg(grid.mean32 + (slot & kSlotMask));
+            }
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                const int slot = v[9 * a + k];
+                bool acc = false;
+                if (slot >= 0) {
+                    ++n_occ;
+                    // FP32-mean distance; it differs from the reference's
+                    // (FP64 mean, float differences) by less than tol, so
+                    // only distances within tol of r need the exact test
+                    const float fx = mf[k].x - px, fy = mf[k].y - py, fz = mf[k].z - pz;
+                    const float fd = sqrtf(fx * fx + fy * fy + fz * fz);
+                    const float tol = 1e-6f + 2.384185791e-7f * (fabsf(mf[k].x) + fabsf(mf[k].y) + fabsf(mf[k].z));
+                    if (fd < res - tol) {
+                        acc = true;
+                    } else if (fd <= res + tol) {
+                        const double4 m = ldg_d4(grid.mean + (slot & kSlotMask));
+                        const float dx = (float)(m.x - (double)px);
+                        const float dy = (float)(m.y - (double)py);
+                        const float dz = (float)(m.z - (double)pz);
+                        const float dist = sqrtf(dx * dx + dy * dy + dz * dz);
+                        acc = (double)dist < radius;
+                    }
+                }
+                const unsigned code = ((unsigned)(slot & kSlotMask) << 6) | ((slot & kSlotFlag) ? 32u : 0u) | lane;
+                list_append(list, n, acc, code, lt);
+            }
+        }
+        return n;
+    }
+    // generic path
     float zc = ps.z0;
     for (int az = 0; az < mz; ++az, zc = zc + res) {
         float yc = ps.y0;
         for (int ay = 0; ay < my; ++ay, yc = yc + res) {
             float xc = ps.x0;
             for (int ax = 0; ax < mx; ++ax, xc = xc + res) {
-                bool act = az < ps.nz && ay < ps.ny && ax < ps.nx;
-                bool inb = act && !((xc < g.minv[0]) || (xc > g.maxv[0]) || (yc < g.minv[1]) ||
-                                    (yc > g.maxv[1]) || (zc < g.minv[2]) || (zc > g.maxv[2]));
+                const bool act = az < ps.nz && ay < ps.ny && ax < ps.nx;
+                const bool inb = act && !((xc < g.minv[0]) || (xc > g.maxv[0]) || (yc < g.minv[1]) ||
+                                          (yc > g.maxv[1]) || (zc < g.minv[2]) || (zc > g.maxv[2]));
                 int slot = -1;
                 if (inb) {
-                    int ix = (int)((xc - g.minv[0]) / res);
-                    int iy = (int)((yc - g.minv[1]) / res);
-                    int iz = (int)((zc - g.minv[2]) / res);
+                    const int ix = (int)((xc - g.minv[0]) / res);
+                    const int iy = (int)((yc - g.minv[1]) / res);
+                    const int iz = (int)((zc - g.minv[2]) / res);
                     slot = __ldg(grid.index + (ix + g.dim[0] * (iy + g.dim[1] * iz)));
                     ++n_probe;
                 }
                 bool acc = false;
-                float4 entry;
                 if (slot >= 0) {
                     ++n_occ;
-                    double4 m = ldg_d4(grid.mean + slot);
-                    float dx = (float)(m.x - (double)px);
-                    float dy = (float)(m.y - (double)py);
-                    float dz = (float)(m.z - (double)pz);
-                    float dist = sqrtf(dx * dx + dy * dy + dz * dz);
+                    const double4 m = ldg_d4(grid.mean + (slot & kSlotMask));
+                    const float dx = (float)(m.x - (double)px);
+                    const float dy = (float)(m.y - (double)py);
+                    const float dz = (float)(m.z - (double)pz);
+                    const float dist = sqrtf(dx * dx + dy * dy + dz * dz);
                     acc = (double)dist < radius;
-                    // x' = x_trans - mean (kernel.cpp:692-694), rounded to float
-                    entry = make_float4(__int_as_float((slot << 6) | ((m.w != 0.0) ? 32 : 0) | lane),
-                                        (float)((double)px - m.x), (float)((double)py - m.y),
-                                        (float)((double)pz - m.z));
                 }
-                unsigned b = __ballot_sync(kFull, acc);
-                if (acc) ring[(head + count + __popc(b & lt)) & (kRing - 1)] = entry;
-                count += __popc(b);
-                if (count >= 32) {
+                if (n > kList - 32) {
                     __syncwarp();
-                    on_full(head);
+                    flush(n);
                     __syncwarp();
-                    head = (head + 32) & (kRing - 1);
-                    count -= 32;
+                    n = 0;
                 }
+                const unsigned code = ((unsigned)(slot & kSlotMask) << 6) | ((slot & kSlotFlag) ? 32u : 0u) | lane;
+                list_append(list, n, acc, code, lt);
             }
         }
     }
-    __syncwarp();
-    if (count > 0) on_tail(head, count);
-    __syncwarp();
+    return n;
 }
 
 // ---------------------------------------------------------------------------
@@ -330,32 +396,131 @@ __device__ __forceinline__ double h_entry(const double *tot, int i, int j, doubl
     return v;
 }
 
-__global__ void __launch_bounds__(kTile, 2) derivative_f32_kernel(EvalArgs args) {
+// Dynamic shared memory of the FP32 kernel (W warps).
+template <int W>
+struct F32Smem {
+    float acc[kAcc][W * 32];  // per-lane sums of the current alignment run
+    float terms[W][kTerms][32];
+    float xt[W][3][32];
+    unsigned list[W][kList];
+    float2 red[W][kAcc];
+};
+
+// Generic-path overflow (coordinates beyond ~1e6 m only): evaluate the queued
+// pairs through the FP64 side path, whose sums land in exc with atomics.
+__device__ __noinline__ void flush_fp64(const unsigned *list, int n, const float (*terms)[32], const float (*xts)[32],
+                                        const GridDev &grid, double *exc, double d1, double d2, bool hess,
+                                        bool compat) {
+    const int lane = threadIdx.x & 31;
+    for (int k = lane; k < n; k += 32) {
+        const unsigned code = list[k];
+        const int owner = code & 31;
+        const int slot = (int)(code >> 6);
+        const double4 m = ldg_d4(grid.mean + slot);
+        pair_fp64_flagged(exc, terms, owner, (float)((double)xts[0][owner] - m.x), (float)((double)xts[1][owner] - m.y),
+                          (float)((double)xts[2][owner] - m.z), grid.icov64 + 9 * (size_t)slot, d1, d2, hess, compat);
+    }
+}
+
+// Block-wide reduction of the per-lane sums of one alignment run (TwoSum
+// compensated across lanes and warps), written as the FP64 partial of the
+// run's first tile; resets the sums.
+template <int W>
+__device__ void reduce_run(F32Smem<W> &sm, double *s_tot, const unsigned (*s_cnt)[3], double *out, double kR,
+                           bool compat) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+#pragma unroll 1
+    for (int k = 0; k < kAcc; ++k) {
+        float s = sm.acc[k][threadIdx.x], e = 0.0f;
+        sm.acc[k][threadIdx.x] = 0.0f;
+        warp_two_sum_reduce(s, e);
+        if (lane == 0) sm.red[warp][k] = make_float2(s, e);
+    }
+    __syncthreads();
+    if (threadIdx.x < kAcc) {
+        float s = sm.red[0][threadIdx.x].x, e = sm.red[0][threadIdx.x].y;
+        for (int w = 1; w < W; ++w) {
+            float t, err;
+            two_sum(s, sm.red[w][threadIdx.x].x, t, err);
+            s = t;
+            e = __fadd_rn(__fadd_rn(e, sm.red[w][threadIdx.x].y), err);
+        }
+        s_tot[threadIdx.x] = (double)s + (double)e;
+    }
+    __syncthreads();
+    if (threadIdx.x < kPartial) {
+        const int k = threadIdx.x;
+        double v;
+        if (k < 7) {
+            v = s_tot[k];
+        } else if (k < 43) {
+            v = h_entry(s_tot, (k - 7) / 6, (k - 7) % 6, kR, compat);
+        } else {
+            unsigned np = 0;
+            for (int w = 0; w < W; ++w) np += s_cnt[w][2];
+            v = (double)np;
+        }
+        out[k] = v;
+    }
+}
+
+// FP32 derivative pass.  Block b owns the contiguous tile range
+// [b * per, (b + 1) * per) of the tile list (tiles of one alignment are
+// consecutive), keeps per-lane sums in shared memory across the tiles of one
+// alignment and reduces once per alignment run; the run's partial goes to the
+// slot of its first tile, the other slots of the run get zeros.
+template <int TILE, int MINB>
+__global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(EvalArgs args) {
+    constexpr int kW = TILE / 32;
     __shared__ float s_T[12];
     __shared__ float s_ang[kAngle];
     __shared__ int s_mode;
-    __shared__ float s_terms[kWarpsE][kTerms][32];
-    __shared__ float4 s_ring[kWarpsE][kRing];
-    __shared__ float2 s_red[kWarpsE][kAcc];
     __shared__ double s_tot[kAcc];
-    __shared__ unsigned long long s_cnt[kWarpsE][3];
+    __shared__ unsigned s_cnt[kW][3];
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    F32Smem<kW> &sm = *reinterpret_cast<F32Smem<kW> *>(s_dyn);
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const bool compat = args.compat != 0;
     const float d1f = (float)args.d1, d2f = (float)args.d2;
+    const double kR = compat ? -args.d2 : 1.0;
     const GridDev &grid = args.grid;
-    float4 *ring = s_ring[warp];
-    float (*terms)[32] = s_terms[warp];
+    float (*terms)[32] = sm.terms[warp];
+    float (*xts)[32] = sm.xt[warp];
+    unsigned *list = sm.list[warp];
 
-    for (int ti = blockIdx.x, nt = *args.num_tiles; ti < nt; ti += gridDim.x) {
+    const int nt = *args.num_tiles;
+    const int per = (nt + gridDim.x - 1) / gridDim.x;
+    const int t_begin = blockIdx.x * per;
+    const int t_end = min(nt, t_begin + per);
+    for (int k = 0; k < kAcc; ++k) sm.acc[k][threadIdx.x] = 0.0f;
+    if (lane == 0) s_cnt[warp][0] = s_cnt[warp][1] = s_cnt[warp][2] = 0;
+    unsigned long long blk_probe = 0, blk_occ = 0, blk_pair = 0, blk_pts = 0, blk_tiles = 0;
+    int cur = -1, run_first = -1, mode = kEvalNone;
+    double *exc = nullptr;
+
+    for (int ti = t_begin; ti < t_end; ++ti) {
         const Tile tile = args.tiles[ti];
-        const AlignState *st = args.states + tile.align;
-        __syncthreads();
-        if (threadIdx.x == 0) s_mode = st->eval_mode;
-        if (threadIdx.x < 12) s_T[threadIdx.x] = st->T[threadIdx.x];
-        if (threadIdx.x < kAngle) s_ang[threadIdx.x] = st->angf[threadIdx.x];
-        __syncthreads();
-        const int mode = s_mode;
+        if (tile.align != cur) {
+            if (cur >= 0 && mode != kEvalNone) {
+                reduce_run<kW>(sm, s_tot, s_cnt, args.partials + (size_t)run_first * kPartial, kR, compat);
+                __syncthreads();
+                if (lane == 0) s_cnt[warp][0] = s_cnt[warp][1] = s_cnt[warp][2] = 0;
+            }
+            __syncthreads();
+            const AlignState *st = args.states + tile.align;
+            if (threadIdx.x == 0) s_mode = st->eval_mode;
+            if (threadIdx.x < 12) s_T[threadIdx.x] = st->T[threadIdx.x];
+            if (threadIdx.x < kAngle) s_ang[threadIdx.x] = st->angf[threadIdx.x];
+            __syncthreads();
+            cur = tile.align;
+            run_first = ti;
+            mode = s_mode;
+            exc = args.exc + (size_t)tile.align * kPartial;
+        } else if (mode != kEvalNone && threadIdx.x < kPartial) {
+            args.partials[(size_t)ti * kPartial + threadIdx.x] = 0.0;
+        }
         if (mode == kEvalNone) continue;
         const bool hess = mode != kEvalGradient;
 
@@ -372,105 +537,80 @@ __global__ void __launch_bounds__(kTile, 2) derivative_f32_kernel(EvalArgs args)
             py = s_T[4] * x.x + s_T[5] * x.y + s_T[6] * x.z + s_T[7];
             pz = s_T[8] * x.x + s_T[9] * x.y + s_T[10] * x.z + s_T[11];
         }
+        __syncwarp();
+        xts[0][lane] = px;
+        xts[1][lane] = py;
+        xts[2][lane] = pz;
         // per-point terms of the ORIGINAL point (computePointDerivatives)
         {
             const float *ja = s_ang;
 #pragma unroll
             for (int k = 0; k < 8; ++k) terms[k][lane] = dot3f(x.x, x.y, x.z, ja + 3 * k);
             const float *h = s_ang + 24;
-            // a2 a3 b2 b3 c2 c3 (second/third components), d1..3, e1..3, f1..3
 #pragma unroll
             for (int k = 0; k < 15; ++k) terms[8 + k][lane] = dot3f(x.x, x.y, x.z, h + 3 * k);
         }
+        unsigned n_probe = 0, n_occ = 0, n_pair = 0;
+        auto flush = [&](int n) {
+            flush_fp64(list, n, terms, xts, grid, exc, args.d1, args.d2, hess, compat);
+            n_pair += (lane < n) ? (unsigned)((n - lane + 31) / 32) : 0u;
+        };
+        __syncwarp();
+        const int n = probe_list(grid, px, py, pz, valid, list, n_probe, n_occ, flush);
+        __syncwarp();
         AccF A;
 #pragma unroll
         for (int k = 0; k < kAcc; ++k) A.v[k] = 0.0f;
-        unsigned long long n_probe = 0, n_occ = 0, n_pair = 0;
-
-        auto eval_entry = [&](int idx) {
-            const float4 en = ring[idx & (kRing - 1)];
-            const int code = __float_as_int(en.x);
+        // evaluate list[0, n): one entry per lane per round
+        for (int base = 0; base < n; base += 32) {
+            const int k = base + lane;
+            if (k >= n) break;
+            const unsigned code = list[k];
             const int owner = code & 31;
-            const int slot = code >> 6;
+            const int slot = (int)(code >> 6);
+            const double2 *q = reinterpret_cast<const double2 *>(grid.mean + slot);
+            const double2 m01 = __ldg(q);
+            const double m2 = __ldg(reinterpret_cast<const double *>(q + 1));
+            // x' = x_trans - mean (kernel.cpp:692-694), rounded to float
+            const float p0 = (float)((double)xts[0][owner] - m01.x);
+            const float p1 = (float)((double)xts[1][owner] - m01.y);
+            const float p2 = (float)((double)xts[2][owner] - m2);
+            ++n_pair;
             if (code & 32) {
-                pair_fp64_flagged(args.exc + (size_t)tile.align * kPartial, terms, owner, en.y, en.z, en.w,
-                                  grid.icov64 + 9 * (size_t)slot, args.d1, args.d2, hess, compat);
+                pair_fp64_flagged(exc, terms, owner, p0, p1, p2, grid.icov64 + 9 * (size_t)slot, args.d1, args.d2,
+                                  hess, compat);
             } else {
                 const float4 ca = __ldg(grid.icov32 + 2 * slot);
                 const float4 cb = __ldg(grid.icov32 + 2 * slot + 1);
-                pair_fp32(A, terms, owner, en.y, en.z, en.w, ca, cb, d1f, d2f, hess, compat);
+                pair_fp32(A, terms, owner, p0, p1, p2, ca, cb, d1f, d2f, hess, compat);
             }
-        };
-        auto on_full = [&](int head) {
-            eval_entry(head + lane);
-            ++n_pair;
-        };
-        auto on_tail = [&](int head, int n) {
-            if (lane < n) {
-                eval_entry(head + lane);
-                ++n_pair;
-            }
-        };
-        __syncwarp();
-        probe_walk(grid, px, py, pz, valid, ring, n_probe, n_occ, on_full, on_tail);
-
-        // ---- reduction: lane sums -> warp (TwoSum) -> block (TwoSum) -> FP64
-#pragma unroll
-        for (int k = 0; k < kAcc; ++k) {
-            float s = A.v[k], e = 0.0f;
-            warp_two_sum_reduce(s, e);
-            if (lane == 0) s_red[warp][k] = make_float2(s, e);
         }
+#pragma unroll
+        for (int k = 0; k < kAcc; ++k) sm.acc[k][threadIdx.x] += A.v[k];
+        // per-warp work counters of the run (pairs feed the partial's count)
         for (int o = 16; o > 0; o >>= 1) {
             n_probe += __shfl_xor_sync(kFull, n_probe, o);
             n_occ += __shfl_xor_sync(kFull, n_occ, o);
             n_pair += __shfl_xor_sync(kFull, n_pair, o);
         }
-        if (lane == 0) {
-            s_cnt[warp][0] = n_probe;
-            s_cnt[warp][1] = n_occ;
-            s_cnt[warp][2] = n_pair;
+        if (lane == 0) s_cnt[warp][2] += n_pair;
+        blk_probe += n_probe;
+        blk_occ += n_occ;
+        blk_pair += n_pair;
+        blk_pts += (unsigned long long)(tile.end - tile.start);
+        blk_tiles += 1;
+    }
+    if (cur >= 0 && mode != kEvalNone)
+        reduce_run<kW>(sm, s_tot, s_cnt, args.partials + (size_t)run_first * kPartial, kR, compat);
+    if (args.counters && lane == 0 && blk_tiles) {
+        // every warp holds the warp-summed counts; warp 0 reports per-block totals of probes and pairs
+        if (warp == 0) {
+            atomicAdd(&args.counters->points, blk_pts);
+            atomicAdd(&args.counters->tiles, blk_tiles);
         }
-        __syncthreads();
-        if (threadIdx.x < kAcc) {
-            float s = s_red[0][threadIdx.x].x, e = s_red[0][threadIdx.x].y;
-            for (int w = 1; w < kWarpsE; ++w) {
-                float t, err;
-                two_sum(s, s_red[w][threadIdx.x].x, t, err);
-                s = t;
-                e = __fadd_rn(__fadd_rn(e, s_red[w][threadIdx.x].y), err);
-            }
-            s_tot[threadIdx.x] = (double)s + (double)e;
-        }
-        __syncthreads();
-        double *out = args.partials + (size_t)tile.slot * kPartial;
-        const double kR = compat ? -args.d2 : 1.0;
-        if (threadIdx.x < kPartial) {
-            const int k = threadIdx.x;
-            double v;
-            if (k < 7) {
-                v = s_tot[k];
-            } else if (k < 43) {
-                v = h_entry(s_tot, (k - 7) / 6, (k - 7) % 6, kR, compat);
-            } else {
-                unsigned long long np = 0;
-                for (int w = 0; w < kWarpsE; ++w) np += s_cnt[w][2];
-                v = (double)np;
-            }
-            out[k] = v;
-        }
-        if (threadIdx.x == 0 && args.counters) {
-            unsigned long long a0 = 0, a1 = 0, a2 = 0;
-            for (int w = 0; w < kWarpsE; ++w) {
-                a0 += s_cnt[w][0];
-                a1 += s_cnt[w][1];
-                a2 += s_cnt[w][2];
-            }
-            atomicAdd(&args.counters->probes, a0);
-            atomicAdd(&args.counters->occupied_probes, a1);
-            atomicAdd(&args.counters->pairs, a2);
-            atomicAdd(&args.counters->points, (unsigned long long)(tile.end - tile.start));
-        }
+        atomicAdd(&args.counters->probes, blk_probe);
+        atomicAdd(&args.counters->occupied_probes, blk_occ);
+        atomicAdd(&args.counters->pairs, blk_pair);
     }
 }
 
@@ -552,14 +692,14 @@ __global__ void __launch_bounds__(kTile, 1) derivative_f64_kernel(EvalArgs args)
     __shared__ double s_ang[kAngle];
     __shared__ int s_mode;
     __shared__ float s_pts[kWarpsE][6][32];  // original xyz, transformed xyz
-    __shared__ float4 s_ring[kWarpsE][kRing];
+    __shared__ unsigned s_list[kWarpsE][kList];
     __shared__ double s_red[kWarpsE][43];
-    __shared__ unsigned long long s_cnt[kWarpsE][3];
+    __shared__ unsigned s_cnt[kWarpsE][3];
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const bool compat = args.compat != 0;
     const GridDev &grid = args.grid;
-    float4 *ring = s_ring[warp];
+    unsigned *list = s_list[warp];
     float (*pts)[32] = s_pts[warp];
 
     for (int ti = blockIdx.x, nt = *args.num_tiles; ti < nt; ti += gridDim.x) {
@@ -589,30 +729,26 @@ __global__ void __launch_bounds__(kTile, 1) derivative_f64_kernel(EvalArgs args)
         pts[3][lane] = px; pts[4][lane] = py; pts[5][lane] = pz;
         AccD A;
         for (int k = 0; k < 43; ++k) A.v[k] = 0.0;
-        unsigned long long n_probe = 0, n_occ = 0, n_pair = 0;
-        auto eval_entry = [&](int idx) {
-            const float4 en = ring[idx & (kRing - 1)];
-            const int code = __float_as_int(en.x);
-            const int owner = code & 31;
-            const int slot = code >> 6;
-            const double4 m = ldg_d4(grid.mean + slot);
-            const double xo[3] = {pts[0][owner], pts[1][owner], pts[2][owner]};
-            const double xt[3] = {(double)pts[3][owner] - m.x, (double)pts[4][owner] - m.y,
-                                  (double)pts[5][owner] - m.z};
-            pair_fp64(A, xo, s_ang, xt, grid.icov64 + 9 * (size_t)slot, args.d1, args.d2, hess, compat);
-        };
-        auto on_full = [&](int head) {
-            eval_entry(head + lane);
-            ++n_pair;
-        };
-        auto on_tail = [&](int head, int n) {
-            if (lane < n) {
-                eval_entry(head + lane);
+        unsigned n_probe = 0, n_occ = 0, n_pair = 0;
+        auto process = [&](int n) {
+            for (int base = 0; base < n; base += 32) {
+                const int kk = base + lane;
+                if (kk >= n) break;
+                const unsigned code = list[kk];
+                const int owner = code & 31;
+                const int slot = (int)(code >> 6);
+                const double4 m = ldg_d4(grid.mean + slot);
+                const double xo[3] = {pts[0][owner], pts[1][owner], pts[2][owner]};
+                const double xt[3] = {(double)pts[3][owner] - m.x, (double)pts[4][owner] - m.y,
+                                      (double)pts[5][owner] - m.z};
+                pair_fp64(A, xo, s_ang, xt, grid.icov64 + 9 * (size_t)slot, args.d1, args.d2, hess, compat);
                 ++n_pair;
             }
         };
         __syncwarp();
-        probe_walk(grid, px, py, pz, valid, ring, n_probe, n_occ, on_full, on_tail);
+        const int n = probe_list(grid, px, py, pz, valid, list, n_probe, n_occ, process);
+        __syncwarp();
+        process(n);
         for (int k = 0; k < 43; ++k) {
             double v = A.v[k];
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
@@ -636,7 +772,7 @@ __global__ void __launch_bounds__(kTile, 1) derivative_f64_kernel(EvalArgs args)
             if (k < 43) {
                 for (int w = 0; w < kWarpsE; ++w) v += s_red[w][k];
             } else {
-                unsigned long long np = 0;
+                unsigned np = 0;
                 for (int w = 0; w < kWarpsE; ++w) np += s_cnt[w][2];
                 v = (double)np;
             }
@@ -653,19 +789,60 @@ __global__ void __launch_bounds__(kTile, 1) derivative_f64_kernel(EvalArgs args)
             atomicAdd(&args.counters->occupied_probes, a1);
             atomicAdd(&args.counters->pairs, a2);
             atomicAdd(&args.counters->points, (unsigned long long)(tile.end - tile.start));
+            atomicAdd(&args.counters->tiles, 1ull);
         }
     }
 }
 
 }  // namespace
 
-int launch_derivatives(const EvalArgs &args, int precision, int grid_blocks, cudaStream_t st) {
+namespace {
+template <int TILE, int MINB>
+cudaError_t prepare_one() {
+    return cudaFuncSetAttribute(derivative_f32_kernel<TILE, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(F32Smem<TILE / 32>));
+}
+template <int TILE, int MINB>
+void launch_one(const EvalArgs &args, int blocks, cudaStream_t st) {
+    derivative_f32_kernel<TILE, MINB><<<blocks, TILE, sizeof(F32Smem<TILE / 32>), st>>>(args);
+}
+}  // namespace
+
+const DerivVariant kDerivVariants[kNumDerivVariants] = {
+    {256, 2}, {256, 1}, {128, 4}, {128, 3}, {128, 2},
+};
+
+int prepare_derivatives() {
+    cudaError_t e = cudaSuccess;
+    cudaError_t r;
+    if ((r = prepare_one<256, 2>()) != cudaSuccess) e = r;
+    if ((r = prepare_one<256, 1>()) != cudaSuccess) e = r;
+    if ((r = prepare_one<128, 4>()) != cudaSuccess) e = r;
+    if ((r = prepare_one<128, 3>()) != cudaSuccess) e = r;
+    if ((r = prepare_one<128, 2>()) != cudaSuccess) e = r;
+    return (int)e;
+}
+
+int launch_derivatives(const EvalArgs &args, int precision, int variant, int sms, cudaStream_t st) {
     if (args.max_tiles <= 0) return 0;
-    int blocks = grid_blocks < args.max_tiles ? grid_blocks : args.max_tiles;
-    if (precision == 1)
+    if (precision == 1) {
+        if (args.tile_size != kTile) return (int)cudaErrorInvalidValue;
+        int blocks = sms < args.max_tiles ? sms : args.max_tiles;
         derivative_f64_kernel<<<blocks, kTile, 0, st>>>(args);
-    else
-        derivative_f32_kernel<<<blocks, kTile, 0, st>>>(args);
+        return (int)cudaGetLastError();
+    }
+    if (variant < 0 || variant >= kNumDerivVariants) variant = 0;
+    const DerivVariant v = kDerivVariants[variant];
+    if (args.tile_size != v.tile) return (int)cudaErrorInvalidValue;
+    long long want = (long long)sms * v.min_blocks;
+    int blocks = (int)(want < args.max_tiles ? want : args.max_tiles);
+    switch (variant) {
+        case 0: launch_one<256, 2>(args, blocks, st); break;
+        case 1: launch_one<256, 1>(args, blocks, st); break;
+        case 2: launch_one<128, 4>(args, blocks, st); break;
+        case 3: launch_one<128, 3>(args, blocks, st); break;
+        default: launch_one<128, 2>(args, blocks, st); break;
+    }
     return (int)cudaGetLastError();
 }
 

@@ -13,6 +13,7 @@ struct EvalArgs {
     const Tile *tiles;
     const int *num_tiles;  // device: number of tiles
     int max_tiles;         // host-side upper bound (grid sizing)
+    int tile_size;         // points per tile (must equal the kernel variant's block size)
     AlignState *states;
     double *partials;      // [tile slot][kPartial]
     double *exc;           // [alignment][kPartial] FP64 side sums of flagged voxels (FP32 path)
@@ -21,8 +22,21 @@ struct EvalArgs {
     Counters *counters;    // may be null
 };
 
-// precision 0 = FP32 pair arithmetic, 1 = FP64.  grid_blocks caps the
-// persistent grid (blocks loop over tiles).
-int launch_derivatives(const EvalArgs &args, int precision, int grid_blocks, cudaStream_t st);
+// Per-device set-up (dynamic shared memory opt-in); call with the device current.
+int prepare_derivatives();
+
+// FP32 derivative-pass launch shapes the autotuner chooses from:
+// (points per tile = threads per block, resident blocks per SM).
+struct DerivVariant {
+    int tile;
+    int min_blocks;
+};
+constexpr int kNumDerivVariants = 5;
+extern const DerivVariant kDerivVariants[kNumDerivVariants];
+
+// precision 0 = FP32 pair arithmetic (launch shape `variant`), 1 = FP64
+// (256-point tiles).  The persistent grid is sms x resident blocks; blocks
+// loop over the tiles.
+int launch_derivatives(const EvalArgs &args, int precision, int variant, int sms, cudaStream_t st);
 
 }  // namespace ndt

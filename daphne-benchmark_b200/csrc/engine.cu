@@ -80,7 +80,7 @@ struct ndt_ctx {
     std::string err;
     double d1 = 0, d2 = 0;
     // grid
-    DevBuf map, index, mean, icov32, icov64, count, cell, seg_start, seg_cell, scratch, meta;
+    DevBuf map, index, mean, mean32, icov32, icov64, count, cell, seg_start, seg_cell, scratch, meta;
     GridMeta meta_host{};
     bool have_map = false;
     int map_points = 0;
@@ -90,6 +90,13 @@ struct ndt_ctx {
     HostBuf h_offsets, h_active, h_counters, h_out;
     ndt_counters last{};
     long long launches = 0;
+    int variant = 0;  // FP32 derivative-pass launch shape (kDerivVariants)
+    // profiling: event pairs around derivative launches and the grid build
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev;
+    int ev_used = 0;
+    cudaEvent_t grid_ev[2] = {nullptr, nullptr};
+    bool grid_timed = false;
 };
 
 namespace {
@@ -136,6 +143,7 @@ GridBuffers grid_buffers(ndt_ctx *c) {
     GridBuffers b;
     b.index = c->index.as<int32_t>();
     b.mean = c->mean.as<double4>();
+    b.mean32 = c->mean32.as<float4>();
     b.icov32 = c->icov32.as<float4>();
     b.icov64 = c->icov64.as<double>();
     b.count = c->count.as<int32_t>();
@@ -150,9 +158,19 @@ GridDev grid_dev(ndt_ctx *c) {
     g.meta = c->meta_host;
     g.index = c->index.as<int32_t>();
     g.mean = c->mean.as<double4>();
+    g.mean32 = c->mean32.as<float4>();
     g.icov32 = c->icov32.as<float4>();
     g.icov64 = c->icov64.as<double>();
     return g;
+}
+
+cudaEvent_t next_event(ndt_ctx *c) {
+    if (c->ev_used >= (int)c->ev.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+        c->ev.push_back(e);
+    }
+    return c->ev[c->ev_used++];
 }
 
 int set_device(ndt_ctx *c) {
@@ -167,6 +185,12 @@ int build_grid(ndt_ctx *c, const float4 *d_map, int m) {
     // voxel slots travel in 26 bits of a packed pair code (slot << 6 | flag << 5 | lane)
     if (m >= (1 << 25)) return fail(c, NDT_E_CAPACITY, "map larger than 2^25 points");
     c->have_map = false;
+    c->grid_timed = false;
+    if (c->profiling) {
+        if (!c->grid_ev[0]) CK(cudaEventCreate(&c->grid_ev[0]));
+        if (!c->grid_ev[1]) CK(cudaEventCreate(&c->grid_ev[1]));
+        CK(cudaEventRecord(c->grid_ev[0], c->stream));
+    }
     CK(c->scratch.ensure(ndt::grid_scratch_bytes(m)));
     CK(c->meta.ensure(sizeof(GridMeta)));
     int rc = grid_bbox(d_map, m, c->prm.resolution, c->meta.as<GridMeta>(), c->scratch.p, c->stream);
@@ -179,6 +203,7 @@ int build_grid(ndt_ctx *c, const float4 *d_map, int m) {
     const size_t G = (size_t)c->meta_host.G;
     CK(c->index.ensure(sizeof(int32_t) * G));
     CK(c->mean.ensure(sizeof(double4) * (size_t)m));
+    CK(c->mean32.ensure(sizeof(float4) * (size_t)m));
     CK(c->icov32.ensure(2 * sizeof(float4) * (size_t)m));
     CK(c->icov64.ensure(9 * sizeof(double) * (size_t)m));
     CK(c->count.ensure(sizeof(int32_t) * (size_t)m));
@@ -193,6 +218,10 @@ int build_grid(ndt_ctx *c, const float4 *d_map, int m) {
     rc = grid_build(d_map, m, c->meta_host, c->meta.as<GridMeta>(), opt, grid_buffers(c), c->scratch.p, c->stream, &nl);
     if (rc) return cuda_fail(c, (cudaError_t)rc, "grid_build");
     c->launches += nl;
+    if (c->profiling) {
+        CK(cudaEventRecord(c->grid_ev[1], c->stream));
+        c->grid_timed = true;
+    }
     c->have_map = true;
     c->map_points = m;
     return NDT_OK;
@@ -203,7 +232,8 @@ int run_batch(ndt_ctx *c, int B, const float4 *d_points, const int *d_offsets, i
               float *d_out, int *d_conv, double *d_fit, int *d_status) {
     if (!c->have_map) return fail(c, NDT_E_NOMAP, "no map set");
     if (B <= 0 || total < 0) return fail(c, NDT_E_ARG, "empty batch");
-    const int max_tiles = total / kTile + B + 1;
+    const int tile = c->prm.precision == 1 ? kTile : kDerivVariants[c->variant].tile;
+    const int max_tiles = total / tile + B + 1;
     CK(c->states.ensure(sizeof(AlignState) * (size_t)B));
     CK(c->tile_begin.ensure(sizeof(int) * (size_t)(B + 1)));
     CK(c->tiles.ensure(sizeof(Tile) * (size_t)max_tiles));
@@ -215,8 +245,9 @@ int run_batch(ndt_ctx *c, int B, const float4 *d_points, const int *d_offsets, i
     CK(c->h_active.ensure(sizeof(int)));
     cudaStream_t st = c->stream;
     CK(cudaMemsetAsync(c->counters.p, 0, sizeof(Counters), st));
+    c->ev_used = 0;
     long long nl = 0;
-    int rc = launch_tiles(d_offsets, B, c->tile_begin.as<int>(), c->tiles.as<Tile>(), c->num_tiles.as<int>(), st);
+    int rc = launch_tiles(d_offsets, B, tile, c->tile_begin.as<int>(), c->tiles.as<Tile>(), c->num_tiles.as<int>(), st);
     if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_tiles");
     nl += 3;
     const StepParams P = step_params(c->prm);
@@ -230,6 +261,7 @@ int run_batch(ndt_ctx *c, int B, const float4 *d_points, const int *d_offsets, i
     ea.tiles = c->tiles.as<Tile>();
     ea.num_tiles = c->num_tiles.as<int>();
     ea.max_tiles = max_tiles;
+    ea.tile_size = tile;
     ea.states = c->states.as<AlignState>();
     ea.partials = c->partials.as<double>();
     ea.exc = c->exc.as<double>();
@@ -237,8 +269,6 @@ int run_batch(ndt_ctx *c, int B, const float4 *d_points, const int *d_offsets, i
     ea.d2 = c->d2;
     ea.compat = c->prm.compat;
     ea.counters = c->counters.as<Counters>();
-    const int per_sm = c->prm.precision == 1 ? 1 : 2;
-    const int grid_blocks = c->num_sms * per_sm;
     // With the reference's line-search test (compat, step_max > step_min)
     // every Newton iteration takes at most one evaluation, so the round count
     // is fixed and no host polling is needed.
@@ -247,8 +277,12 @@ int run_batch(ndt_ctx *c, int B, const float4 *d_points, const int *d_offsets, i
     const int poll_every = 4;
     int rounds = 0;
     for (int r = 0; r < max_rounds; ++r) {
-        rc = launch_derivatives(ea, c->prm.precision, grid_blocks, st);
+        cudaEvent_t e0 = c->profiling ? next_event(c) : nullptr;
+        if (e0) CK(cudaEventRecord(e0, st));
+        rc = launch_derivatives(ea, c->prm.precision, c->variant, c->num_sms, st);
         if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_derivatives");
+        cudaEvent_t e1 = c->profiling ? next_event(c) : nullptr;
+        if (e1) CK(cudaEventRecord(e1, st));
         CK(cudaMemsetAsync(c->active.p, 0, sizeof(int), st));
         rc = launch_step(c->states.as<AlignState>(), c->partials.as<double>(), c->tile_begin.as<int>(),
                          c->exc.as<double>(), B, P, c->active.as<int>(), c->counters.as<Counters>(), st);
@@ -266,7 +300,7 @@ int run_batch(ndt_ctx *c, int B, const float4 *d_points, const int *d_offsets, i
     nl += 1;
     c->launches += nl;
     c->last.launches = nl;
-    c->last.evaluations = rounds;
+    c->last.rounds = rounds;
     return NDT_OK;
 }
 
@@ -277,8 +311,26 @@ int read_counters(ndt_ctx *c) {
     const Counters *k = c->h_counters.as<Counters>();
     c->last.points = (int64_t)k->points;
     c->last.probes = (int64_t)k->probes;
+    c->last.occupied_probes = (int64_t)k->occupied_probes;
     c->last.pairs = (int64_t)k->pairs;
+    c->last.tiles = (int64_t)k->tiles;
     c->last.evaluations = (int64_t)k->evaluations;
+    double ms = 0.0;
+    int n = 0;
+    for (int i = 0; i + 1 < c->ev_used; i += 2) {
+        float t = 0.0f;
+        CK(cudaEventElapsedTime(&t, c->ev[i], c->ev[i + 1]));
+        ms += t;
+        ++n;
+    }
+    c->last.deriv_ms = ms;
+    c->last.deriv_launches = n;
+    c->last.grid_ms = 0.0;
+    if (c->grid_timed) {
+        float t = 0.0f;
+        CK(cudaEventElapsedTime(&t, c->grid_ev[0], c->grid_ev[1]));
+        c->last.grid_ms = t;
+    }
     return NDT_OK;
 }
 
@@ -311,6 +363,37 @@ int host_batch(ndt_ctx *c, int B, const float *const *scans, const int *ns, cons
     CK(cudaMemcpyAsync(c->offsets.p, off, sizeof(int) * (size_t)(B + 1), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(c->guesses.p, guesses, sizeof(float) * 16 * (size_t)B, cudaMemcpyHostToDevice, st));
     int rc = run_batch(c, B, c->points.as<float4>(), c->offsets.as<int>(), (int)total, c->guesses.as<float>(),
+                       c->out_T.as<float>(), c->out_conv.as<int>(), c->out_fit.as<double>(), c->out_status.as<int>());
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(out, c->out_T.p, sizeof(float) * 16 * (size_t)B, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(conv, c->out_conv.p, sizeof(int) * (size_t)B, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(fit, c->out_fit.p, sizeof(double) * (size_t)B, cudaMemcpyDeviceToHost, st));
+    if (status) CK(cudaMemcpyAsync(status, c->out_status.p, sizeof(int) * (size_t)B, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return NDT_OK;
+}
+
+// Host batch from one packed host buffer.
+int packed_batch(ndt_ctx *c, int B, const float *points, const int *offsets, const float *guesses, float *out,
+                 int *conv, double *fit, int *status) {
+    if (B <= 0 || !points || !offsets || !guesses || !out || !conv || !fit) return fail(c, NDT_E_ARG, "null argument");
+    if (offsets[0] != 0) return fail(c, NDT_E_ARG, "offsets[0] must be 0");
+    for (int b = 0; b < B; ++b)
+        if (offsets[b + 1] < offsets[b]) return fail(c, NDT_E_ARG, "offsets must be non-decreasing");
+    const int total = offsets[B];
+    cudaStream_t st = c->stream;
+    CK(c->points.ensure(sizeof(float4) * (size_t)(total > 0 ? total : 1)));
+    CK(c->offsets.ensure(sizeof(int) * (size_t)(B + 1)));
+    CK(c->guesses.ensure(sizeof(float) * 16 * (size_t)B));
+    CK(c->out_T.ensure(sizeof(float) * 16 * (size_t)B));
+    CK(c->out_conv.ensure(sizeof(int) * (size_t)B));
+    CK(c->out_fit.ensure(sizeof(double) * (size_t)B));
+    CK(c->out_status.ensure(sizeof(int) * (size_t)B));
+    if (total > 0)
+        CK(cudaMemcpyAsync(c->points.p, points, sizeof(float4) * (size_t)total, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->offsets.p, offsets, sizeof(int) * (size_t)(B + 1), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->guesses.p, guesses, sizeof(float) * 16 * (size_t)B, cudaMemcpyHostToDevice, st));
+    int rc = run_batch(c, B, c->points.as<float4>(), c->offsets.as<int>(), total, c->guesses.as<float>(),
                        c->out_T.as<float>(), c->out_conv.as<int>(), c->out_fit.as<double>(), c->out_status.as<int>());
     if (rc) return rc;
     CK(cudaMemcpyAsync(out, c->out_T.p, sizeof(float) * 16 * (size_t)B, cudaMemcpyDeviceToHost, st));
@@ -364,6 +447,7 @@ int ndt_create(const ndt_params *params, int device, ndt_ctx **out) {
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = (cudaError_t)prepare_derivatives();
     if (e != cudaSuccess) {
         delete c;
         return NDT_E_CUDA;
@@ -376,13 +460,16 @@ void ndt_destroy(ndt_ctx *c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    DevBuf *bufs[] = {&c->map, &c->index, &c->mean, &c->icov32, &c->icov64, &c->count, &c->cell, &c->seg_start,
+    DevBuf *bufs[] = {&c->map, &c->index, &c->mean, &c->mean32, &c->icov32, &c->icov64, &c->count, &c->cell, &c->seg_start,
                       &c->seg_cell, &c->scratch, &c->meta, &c->points, &c->offsets, &c->guesses, &c->states,
                       &c->tiles, &c->tile_begin, &c->num_tiles, &c->partials, &c->exc, &c->out_T, &c->out_conv,
                       &c->out_fit, &c->out_status, &c->active, &c->counters, &c->p6, &c->trans};
     for (DevBuf *b : bufs) b->release();
     HostBuf *hb[] = {&c->h_offsets, &c->h_active, &c->h_counters, &c->h_out};
     for (HostBuf *b : hb) b->release();
+    for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
+    for (cudaEvent_t e : c->grid_ev)
+        if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -434,6 +521,19 @@ int ndt_align_batch(ndt_ctx *c, int B, const float *const *scans, const int *ns,
     return host_batch(c, B, scans, ns, guesses, out, converged, fitness, status);
 }
 
+int ndt_align_batch_packed(ndt_ctx *c, int B, const float *points, const int *offsets, const float *guesses,
+                           float *out, int *converged, double *fitness, int *status) {
+    if (!c) return NDT_E_ARG;
+    if (int rc = set_device(c)) return rc;
+    return packed_batch(c, B, points, offsets, guesses, out, converged, fitness, status);
+}
+
+int ndt_set_profiling(ndt_ctx *c, int on) {
+    if (!c) return NDT_E_ARG;
+    c->profiling = on != 0;
+    return NDT_OK;
+}
+
 int ndt_align_batch_device(ndt_ctx *c, int B, const float *d_points, const int *d_offsets, int total_points,
                            const float *d_guesses, float *d_out, int *d_conv, double *d_fit, int *d_status) {
     if (!c || !d_points || !d_offsets || !d_guesses || !d_out || !d_conv || !d_fit)
@@ -441,6 +541,21 @@ int ndt_align_batch_device(ndt_ctx *c, int B, const float *d_points, const int *
     if (int rc = set_device(c)) return rc;
     return run_batch(c, B, (const float4 *)d_points, d_offsets, total_points, d_guesses, d_out, d_conv, d_fit,
                      d_status);
+}
+
+int ndt_kernel_variants(void) { return kNumDerivVariants; }
+
+int ndt_set_kernel_variant(ndt_ctx *c, int variant) {
+    if (!c || variant < 0 || variant >= kNumDerivVariants) return fail(c, NDT_E_ARG, "bad kernel variant");
+    c->variant = variant;
+    return NDT_OK;
+}
+
+int ndt_kernel_variant_shape(int variant, int *tile, int *blocks_per_sm) {
+    if (variant < 0 || variant >= kNumDerivVariants || !tile || !blocks_per_sm) return NDT_E_ARG;
+    *tile = kDerivVariants[variant].tile;
+    *blocks_per_sm = kDerivVariants[variant].min_blocks;
+    return NDT_OK;
 }
 
 int ndt_get_counters(ndt_ctx *c, ndt_counters *out) {
@@ -499,7 +614,8 @@ int ndt_derivatives(ndt_ctx *c, const float *scan, const float *trans, int n, co
     if (!c->have_map) return fail(c, NDT_E_NOMAP, "no map set");
     if (int rc = set_device(c)) return rc;
     cudaStream_t st = c->stream;
-    const int max_tiles = n / kTile + 2;
+    const int tile = c->prm.precision == 1 ? kTile : kDerivVariants[c->variant].tile;
+    const int max_tiles = n / tile + 2;
     CK(c->points.ensure(sizeof(float4) * (size_t)n));
     CK(c->trans.ensure(sizeof(float4) * (size_t)n));
     CK(c->offsets.ensure(sizeof(int) * 2));
@@ -520,7 +636,7 @@ int ndt_derivatives(ndt_ctx *c, const float *scan, const float *trans, int n, co
     CK(cudaMemcpyAsync(c->offsets.p, off, sizeof(int) * 2, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(c->p6.p, p6, sizeof(double) * 6, cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(c->counters.p, 0, sizeof(Counters), st));
-    int rc = launch_tiles(c->offsets.as<int>(), 1, c->tile_begin.as<int>(), c->tiles.as<Tile>(),
+    int rc = launch_tiles(c->offsets.as<int>(), 1, tile, c->tile_begin.as<int>(), c->tiles.as<Tile>(),
                           c->num_tiles.as<int>(), st);
     if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_tiles");
     rc = launch_prepare_eval(c->states.as<AlignState>(), c->p6.as<double>(), n, c->exc.as<double>(), st);
@@ -532,6 +648,7 @@ int ndt_derivatives(ndt_ctx *c, const float *scan, const float *trans, int n, co
     ea.tiles = c->tiles.as<Tile>();
     ea.num_tiles = c->num_tiles.as<int>();
     ea.max_tiles = max_tiles;
+    ea.tile_size = tile;
     ea.states = c->states.as<AlignState>();
     ea.partials = c->partials.as<double>();
     ea.exc = c->exc.as<double>();
@@ -539,7 +656,7 @@ int ndt_derivatives(ndt_ctx *c, const float *scan, const float *trans, int n, co
     ea.d2 = c->d2;
     ea.compat = c->prm.compat;
     ea.counters = c->counters.as<Counters>();
-    rc = launch_derivatives(ea, c->prm.precision, c->num_sms * 2, st);
+    rc = launch_derivatives(ea, c->prm.precision, c->variant, c->num_sms, st);
     if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_derivatives");
     int nt = 0;
     std::vector<double> part((size_t)max_tiles * kPartial), exc(kPartial);

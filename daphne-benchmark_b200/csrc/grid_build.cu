@@ -79,12 +79,24 @@ __global__ void bbox_partial_kernel(const float4 *__restrict__ map, int m, float
 // (float arithmetic, truncated to int).
 __global__ void bbox_final_kernel(const float *__restrict__ part, int nblk, float res,
                                   const int *__restrict__ nonfinite, GridMeta *__restrict__ meta) {
+    // min/max of the block partials (exact in any order), then the
+    // reference's float arithmetic on one thread
+    float v[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x)
+        for (int k = 0; k < 6; ++k) v[k] = k < 3 ? fminf(v[k], part[6 * b + k]) : fmaxf(v[k], part[6 * b + k]);
+    for (int o = 16; o > 0; o >>= 1)
+        for (int k = 0; k < 6; ++k) {
+            float u = __shfl_xor_sync(0xffffffffu, v[k], o);
+            v[k] = k < 3 ? fminf(v[k], u) : fmaxf(v[k], u);
+        }
+    __shared__ float s[kWarps][6];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+        for (int k = 0; k < 6; ++k) s[w][k] = v[k];
+    __syncthreads();
     if (threadIdx.x != 0) return;
-    float v[6];
-    for (int k = 0; k < 6; ++k) v[k] = part[k];
-    for (int b = 1; b < nblk; ++b)
-        for (int k = 0; k < 6; ++k)
-            v[k] = k < 3 ? fminf(v[k], part[6 * b + k]) : fmaxf(v[k], part[6 * b + k]);
+    for (int ww = 1; ww < (int)(blockDim.x >> 5); ++ww)
+        for (int k = 0; k < 6; ++k) v[k] = k < 3 ? fminf(v[k], s[ww][k]) : fmaxf(v[k], s[ww][k]);
     GridMeta g;
     g.res = res;
     g.occupied = 0;
@@ -288,7 +300,7 @@ __global__ void seg_write_kernel(const uint32_t *__restrict__ keys, int n, const
 
 // ---------------------------------------------------------------------------
 // Voxel records.
-__device__ void write_records(int s, const double *mu, const double *C, GridBuffers buf) {
+__device__ bool write_records(int s, const double *mu, const double *C, GridBuffers buf) {
     bool bad = false;
     for (int k = 0; k < 9; ++k) {
         double v = C[k];
@@ -297,11 +309,13 @@ __device__ void write_records(int s, const double *mu, const double *C, GridBuff
     for (int k = 0; k < 3; ++k)
         if (!isfinite(mu[k])) bad = true;
     buf.mean[s] = make_double4(mu[0], mu[1], mu[2], bad ? 1.0 : 0.0);
+    buf.mean32[s] = make_float4((float)mu[0], (float)mu[1], (float)mu[2], 0.0f);
     float c00 = (float)C[0], c11 = (float)C[4], c22 = (float)C[8];
     float c01 = (float)((C[1] + C[3]) * 0.5), c02 = (float)((C[2] + C[6]) * 0.5), c12 = (float)((C[5] + C[7]) * 0.5);
     buf.icov32[2 * s] = make_float4(c00, c01, c02, c11);
     buf.icov32[2 * s + 1] = make_float4(c12, c22, 0.0f, 0.0f);
     for (int k = 0; k < 9; ++k) buf.icov64[9 * (size_t)s + k] = C[k];
+    return bad;
 }
 
 // Reference voxel (kernel.cpp:1324-1372): sums start at mean = 0 and
@@ -359,10 +373,10 @@ __global__ void cell_finalize_compat_kernel(const float4 *__restrict__ map, cons
     t[8] = m[4] * m[0] - m[3] * m[1];
     double C[9];
     for (int k = 0; k < 9; ++k) C[k] = t[k] * inv_det;
-    write_records(s, mu, C, buf);
+    const bool flag = write_records(s, mu, C, buf);
     buf.count[s] = cnt;
     buf.cell[s] = (int)seg_cell[s];
-    buf.index[seg_cell[s]] = s;
+    buf.index[seg_cell[s]] = s | (flag ? kSlotFlag : 0);
 }
 
 // Symmetric 3x3 eigen-decomposition by cyclic Jacobi rotations (V columns =
@@ -450,8 +464,8 @@ __global__ void cell_finalize_corrected_kernel(const float4 *__restrict__ map, c
     for (int r = 0; r < 3; ++r)
         for (int q = 0; q < 3; ++q)
             C[3 * r + q] = V[r][0] * inv_w[0] * V[q][0] + V[r][1] * inv_w[1] * V[q][1] + V[r][2] * inv_w[2] * V[q][2];
-    write_records(s, mu, C, buf);
-    buf.index[seg_cell[s]] = s;
+    const bool flag = write_records(s, mu, C, buf);
+    buf.index[seg_cell[s]] = s | (flag ? kSlotFlag : 0);
 }
 
 __global__ void store_occupied_kernel(const int *__restrict__ nseg, GridMeta *__restrict__ meta) {
@@ -482,7 +496,7 @@ int grid_bbox(const float4 *d_map, int m, float res, GridMeta *d_meta, void *scr
     if (nblk > 1024) nblk = 1024;
     cudaMemsetAsync(nonfinite, 0, sizeof(int), st);
     bbox_partial_kernel<<<nblk, kThreads, 0, st>>>(d_map, m, part, nonfinite);
-    bbox_final_kernel<<<1, 32, 0, st>>>(part, nblk, res, nonfinite, d_meta);
+    bbox_final_kernel<<<1, kThreads, 0, st>>>(part, nblk, res, nonfinite, d_meta);
     return (int)cudaGetLastError();
 }
 

@@ -8,6 +8,12 @@ constexpr int kTile = 256;      // scan points per derivative-pass tile (= threa
 constexpr int kPartial = 44;    // per-tile partial: score, g[6], H[36], pair count
 constexpr int kAngle = 69;      // angle terms: j_ang a..h (8 x 3) + h_ang a2..f3 (15 x 3)
 
+// Dense index entries: voxel slot in the low bits, kSlotFlag set when the
+// voxel's inverse covariance must be evaluated in FP64 (non-finite entries or
+// entries beyond 1e30); -1 = no usable voxel.
+constexpr int32_t kSlotFlag = 1 << 30;
+constexpr int32_t kSlotMask = kSlotFlag - 1;
+
 // What the derivative pass must compute for one alignment this round.
 enum EvalMode : int32_t {
     kEvalNone = 0,
@@ -40,8 +46,9 @@ struct GridMeta {
 // Device pointers of a built grid.
 struct GridDev {
     GridMeta meta;
-    const int32_t *index;    // G: dense cell -> voxel slot, -1 = none
+    const int32_t *index;    // G: dense cell -> voxel slot | kSlotFlag, -1 = none
     const double4 *mean;     // K: mean xyz (FP64), w = 1 when the FP32 path must not be used
+    const float4 *mean32;    // K: mean xyz rounded to FP32 (the probe's first, conservative distance test)
     const float4 *icov32;    // 2K: {c00 c01 c02 c11}, {c12 c22 0 0} (symmetrised, FP32)
     const double *icov64;    // 9K: inverse covariance as the reference stores it (row major)
 };
@@ -80,7 +87,7 @@ struct Counters {
     unsigned long long probes;
     unsigned long long occupied_probes;
     unsigned long long pairs;
-    unsigned long long rounds;
+    unsigned long long tiles;
 };
 
 struct Tile {

@@ -52,8 +52,12 @@ class Params(C.Structure):
 
 
 class Counters(C.Structure):
-    _fields_ = [("evaluations", C.c_int64), ("points", C.c_int64), ("probes", C.c_int64), ("pairs", C.c_int64),
-                ("launches", C.c_int64)]
+    """ndt_counters (include/ndt_b200.h)."""
+
+    _fields_ = [("evaluations", C.c_int64), ("points", C.c_int64), ("probes", C.c_int64),
+                ("occupied_probes", C.c_int64), ("pairs", C.c_int64), ("tiles", C.c_int64), ("launches", C.c_int64),
+                ("rounds", C.c_int64), ("deriv_launches", C.c_int64), ("deriv_ms", C.c_double),
+                ("grid_ms", C.c_double)]
 
 
 def build(quiet=True):
@@ -80,7 +84,7 @@ def lib():
         L.ndt_destroy.argtypes = [ctxp]
         L.ndt_last_error.argtypes = [ctxp]
         L.ndt_last_error.restype = C.c_char_p
-        L.ndt_set_map.argtypes = [ctxp, _f32p, C.c_int]
+        L.ndt_set_map.argtypes = [ctxp, C.c_void_p, C.c_int]
         L.ndt_set_map_device.argtypes = [ctxp, C.c_void_p, C.c_int]
         L.ndt_align.argtypes = [ctxp, _f32p, C.c_int, _f32p, _f32p, C.POINTER(C.c_int), C.POINTER(C.c_double)]
         L.ndt_align_with_map.argtypes = [ctxp, _f32p, C.c_int, _f32p, _f32p, C.c_int, _f32p, C.POINTER(C.c_int),
@@ -88,6 +92,12 @@ def lib():
         L.ndt_align_batch.argtypes = [ctxp, C.c_int, C.c_void_p, _i32p, _f32p, _f32p, _i32p, _f64p, C.c_void_p]
         L.ndt_align_batch_device.argtypes = [ctxp, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
                                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ndt_align_batch_packed.argtypes = [ctxp, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ndt_set_profiling.argtypes = [ctxp, C.c_int]
+        L.ndt_kernel_variants.argtypes = []
+        L.ndt_kernel_variant_shape.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.ndt_set_kernel_variant.argtypes = [ctxp, C.c_int]
         L.ndt_synchronize.argtypes = [ctxp]
         L.ndt_stream.argtypes = [ctxp]
         L.ndt_stream.restype = C.c_void_p
@@ -97,10 +107,23 @@ def lib():
         L.ndt_derivatives.argtypes = [ctxp, _f32p, _f32p, C.c_int, _f64p, C.POINTER(C.c_double), _f64p, _f64p]
         for name in ("ndt_create", "ndt_set_map", "ndt_set_map_device", "ndt_align", "ndt_align_with_map",
                      "ndt_align_batch", "ndt_align_batch_device", "ndt_synchronize", "ndt_get_counters",
-                     "ndt_grid_info", "ndt_grid_cells", "ndt_derivatives"):
+                     "ndt_grid_info", "ndt_grid_cells", "ndt_derivatives", "ndt_align_batch_packed",
+                     "ndt_set_profiling", "ndt_kernel_variants", "ndt_kernel_variant_shape",
+                     "ndt_set_kernel_variant"):
             getattr(L, name).restype = C.c_int
         _LIB = L
     return _LIB
+
+
+def kernel_variants():
+    """[(tile, blocks_per_sm), ...] of the FP32 derivative-pass launch shapes."""
+    L = lib()
+    out = []
+    for v in range(L.ndt_kernel_variants()):
+        t, b = C.c_int(), C.c_int()
+        L.ndt_kernel_variant_shape(v, C.byref(t), C.byref(b))
+        out.append((t.value, b.value))
+    return out
 
 
 def reference_params(resolution=1.0, precision=0):
@@ -165,7 +188,7 @@ class Context:
 
     def set_map(self, cloud):
         cloud = _f32(cloud)
-        self._check(self.L.ndt_set_map(self.h, cloud, cloud.shape[0]), "ndt_set_map")
+        self._check(self.L.ndt_set_map(self.h, cloud.ctypes.data, cloud.shape[0]), "ndt_set_map")
 
     def set_map_device(self, ptr: int, m: int):
         self._check(self.L.ndt_set_map_device(self.h, C.c_void_p(ptr), m), "ndt_set_map_device")
@@ -206,6 +229,31 @@ class Context:
         self._check(self.L.ndt_align_batch_device(self.h, B, C.c_void_p(d_points), C.c_void_p(d_offsets), total,
                                                   C.c_void_p(d_guesses), C.c_void_p(d_out), C.c_void_p(d_conv),
                                                   C.c_void_p(d_fit), C.c_void_p(d_status)), "ndt_align_batch_device")
+
+    def align_batch_packed(self, points, offsets, guesses, out, conv, fit, status=None):
+        """One packed host batch; all arguments are host numpy arrays (pinned or not)."""
+        B = len(offsets) - 1
+        self._check(self.L.ndt_align_batch_packed(self.h, B, points.ctypes.data, offsets.ctypes.data,
+                                                  guesses.ctypes.data, out.ctypes.data, conv.ctypes.data,
+                                                  fit.ctypes.data, status.ctypes.data if status is not None else None),
+                    "ndt_align_batch_packed")
+
+    def align_batch_packed_ptr(self, B, points, offsets, guesses, out, conv, fit, status=0):
+        """Same, with raw host pointers (ints), e.g. pinned torch tensors."""
+        self._check(self.L.ndt_align_batch_packed(self.h, B, C.c_void_p(points), C.c_void_p(offsets),
+                                                  C.c_void_p(guesses), C.c_void_p(out), C.c_void_p(conv),
+                                                  C.c_void_p(fit), C.c_void_p(status) if status else None),
+                    "ndt_align_batch_packed")
+
+    def set_map_ptr(self, ptr: int, m: int):
+        """Host map by raw pointer (e.g. a pinned torch tensor)."""
+        self._check(self.L.ndt_set_map(self.h, C.c_void_p(ptr), m), "ndt_set_map")
+
+    def set_profiling(self, on=True):
+        self._check(self.L.ndt_set_profiling(self.h, int(on)), "ndt_set_profiling")
+
+    def set_kernel_variant(self, v):
+        self._check(self.L.ndt_set_kernel_variant(self.h, int(v)), "ndt_set_kernel_variant")
 
     def synchronize(self):
         self._check(self.L.ndt_synchronize(self.h), "ndt_synchronize")

@@ -7,7 +7,8 @@ height U(1, 4) m, the same noise across the wall), sampled uniformly by surface
 area.  A scan is a fresh sample of the same surfaces within 40 m of a sensor
 pose (xy uniform in the inner half of the area, any yaw, z = 0), expressed in
 the sensor frame; the guess is the ground truth perturbed by uniform +-dt in x,
-y and +-dyaw in yaw.  Points are float32 (x, y, z, 1).
+y and +-dyaw in yaw.  Points are float32 (x, y, z, 1); a scan's points are
+ordered like a voxel-grid filtered scan (by 2 m leaf index, x fastest).
 
 Reproducibility: only IEEE basic arithmetic (+ - * / and comparisons) is applied
 to random numbers -- headings come from the rational parametrisation
@@ -191,6 +192,7 @@ def make_alignment(cfg: Config, scene: Scene, index: int, n_points: int | None =
     scan[:, 0] = lx.astype(np.float32)
     scan[:, 1] = ly.astype(np.float32)
     scan[:, 2] = pz.astype(np.float32)
+    scan = scan[leaf_order(scan)]
     truth = np.eye(4)
     truth[0, 0], truth[0, 1], truth[1, 0], truth[1, 1] = c, -s, s, c
     truth[0, 3], truth[1, 3] = sx, sy
@@ -202,6 +204,18 @@ def make_alignment(cfg: Config, scene: Scene, index: int, n_points: int | None =
     guess[0, 0], guess[0, 1], guess[1, 0], guess[1, 1] = gc, -gs, gs, gc
     guess[0, 3], guess[1, 3] = sx + ex, sy + ey
     return Alignment(scan=scan, guess=guess.astype(np.float32).reshape(16), truth=truth)
+
+
+def leaf_order(scan, leaf=2.0):
+    """Point order of a voxel-grid filtered scan: by 2 m leaf index, x fastest.
+
+    The align call's input is a "filtered_scan" (a voxel-grid downsampled
+    LiDAR scan), whose points come out ordered by leaf index; this reproduces
+    that order (stable integer sort, machine independent).
+    """
+    q = np.floor(scan[:, :3].astype(np.float64) / leaf).astype(np.int64) + 1024
+    key = (q[:, 2] * 2048 + q[:, 1]) * 2048 + q[:, 0]
+    return np.argsort(key, kind="stable")
 
 
 def scan_size(cfg: Config, index: int) -> int:

@@ -132,22 +132,53 @@ NDT_API int ndt_align_batch_device(ndt_ctx *ctx, int B, const float *d_points, c
                            double *d_fit, int *d_status);
 NDT_API int ndt_synchronize(ndt_ctx *ctx);
 
+/*
+ * Host batch with the scans packed in one HOST buffer: points = sum(ns)
+ * float[4], offsets = B+1 prefix offsets (int32).  One host-to-device copy;
+ * the call returns when the results are in `out`, `converged`, `fitness`,
+ * `status` (status may be NULL).  The batch form of ndt_mapping::run's loop
+ * (kernel.cpp:1425-1429) for one map.
+ */
+NDT_API int ndt_align_batch_packed(ndt_ctx *ctx, int B, const float *points, const int *offsets,
+                                   const float *guesses, float *out, int *converged, double *fitness,
+                                   int *status);
+
 /* The context's CUDA stream (cudaStream_t), for callers that time or order work. */
 NDT_API void *ndt_stream(ndt_ctx *ctx);
 
 /*
- * Work counters of the last batch: derivative evaluations (kernel launches of
- * the derivative pass), scan points visited, cell probes, accepted
- * (point, voxel) pairs, summed over all evaluations.
+ * Work counters of the last batch call (reset by each batch / set_map call):
+ * alignment-evaluations, derivative-pass work (scan points visited, in-bounds
+ * cell probes, probes that found a voxel, accepted (point, voxel) pairs),
+ * kernel launches, lockstep rounds and, with profiling on (ndt_set_profiling),
+ * the summed derivative-pass time and the grid-build time measured with CUDA
+ * events on the context stream.  No reference counterpart.
  */
 typedef struct ndt_counters {
     int64_t evaluations;
     int64_t points;
     int64_t probes;
+    int64_t occupied_probes;
     int64_t pairs;
+    int64_t tiles;
     int64_t launches;
+    int64_t rounds;
+    int64_t deriv_launches;
+    double deriv_ms;
+    double grid_ms;
 } ndt_counters;
+NDT_API int ndt_set_profiling(ndt_ctx *ctx, int on);
 NDT_API int ndt_get_counters(ndt_ctx *ctx, ndt_counters *out);
+
+/*
+ * Launch shape of the FP32 derivative pass (points per tile = threads per
+ * block, resident blocks per SM).  The autotuner (daphne-benchmark_b200/
+ * autotune.py) times every variant on a sample batch and selects one.
+ * No reference counterpart (the reference has no GPU derivative pass).
+ */
+NDT_API int ndt_kernel_variants(void);
+NDT_API int ndt_kernel_variant_shape(int variant, int *tile, int *blocks_per_sm);
+NDT_API int ndt_set_kernel_variant(ndt_ctx *ctx, int variant);
 
 /*
  * Grid inspection (tests): bbox (min xyz, max xyz), dims, number of occupied

@@ -53,9 +53,8 @@ def _inputs(pkg, c):
 
 
 def _rot_err_deg(A, B):
-    R = A.reshape(4, 4)[:3, :3].astype(np.float64) @ B.reshape(4, 4)[:3, :3].astype(np.float64).T
-    c = (np.trace(R) - 1.0) / 2.0
-    return math.degrees(math.acos(max(-1.0, min(1.0, c))))
+    d = A.reshape(4, 4)[:3, :3].astype(np.float64) - B.reshape(4, 4)[:3, :3].astype(np.float64)
+    return math.degrees(2.0 * math.asin(min(1.0, float(np.linalg.norm(d)) / math.sqrt(8.0))))
 
 
 @pytest.mark.parametrize("compat", [1, 0])
