@@ -270,7 +270,8 @@ __global__ void step_kernel(AlignState *__restrict__ states, const double *__res
 }
 
 __global__ void finalize_kernel(const AlignState *__restrict__ states, int B, float *__restrict__ out,
-                                int *__restrict__ conv, double *__restrict__ fit, int *__restrict__ status) {
+                                int *__restrict__ conv, double *__restrict__ fit, int *__restrict__ status,
+                                const int *__restrict__ overflow) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= B) return;
     const AlignState &s = states[b];
@@ -279,6 +280,7 @@ __global__ void finalize_kernel(const AlignState *__restrict__ states, int B, fl
     fit[b] = s.n > 0 ? s.score / (double)s.n : 0.0;
     int st = s.status;
     if (s.phase != kPhaseDone && st == 0) st = NDT_ST_WATCHDOG_DEV;
+    if (overflow && *overflow) st |= NDT_ST_OVERFLOW_DEV;
     if (status) status[b] = st;
 }
 
@@ -391,8 +393,8 @@ int launch_step(AlignState *d_states, const double *d_partials, const int *d_til
 }
 
 int launch_finalize(const AlignState *d_states, int B, float *d_out, int *d_conv, double *d_fit, int *d_status,
-                    cudaStream_t st) {
-    finalize_kernel<<<(B + 127) / 128, 128, 0, st>>>(d_states, B, d_out, d_conv, d_fit, d_status);
+                    const int *d_overflow, cudaStream_t st) {
+    finalize_kernel<<<(B + 127) / 128, 128, 0, st>>>(d_states, B, d_out, d_conv, d_fit, d_status, d_overflow);
     return (int)cudaGetLastError();
 }
 

@@ -7,6 +7,7 @@
 namespace ndt {
 
 constexpr int NDT_ST_WATCHDOG_DEV = 1;
+constexpr int NDT_ST_OVERFLOW_DEV = 2;
 
 struct StepParams {
     int compat;
@@ -25,6 +26,6 @@ int launch_step(AlignState *d_states, const double *d_partials, const int *d_til
                 const StepParams &P, int *d_active, Counters *d_counters, cudaStream_t st);
 int launch_prepare_eval(AlignState *d_state, const double *d_p6, int n, double *d_exc, cudaStream_t st);
 int launch_finalize(const AlignState *d_states, int B, float *d_out, int *d_conv, double *d_fit, int *d_status,
-                    cudaStream_t st);
+                    const int *d_overflow, cudaStream_t st);
 
 }  // namespace ndt

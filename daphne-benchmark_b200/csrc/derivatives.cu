@@ -3,31 +3,39 @@
 // src/CPU/ndt_mapping/kernel.cpp:562-705, with voxelRadiusSearch :246-286,
 // computePointDerivatives :495-560 and updateDerivatives :438-493 fused in).
 //
-// One block (256 threads) handles one tile of up to 256 consecutive points of
-// ONE alignment; blocks loop over the tile list (persistent grid), skipping
-// tiles whose alignment has nothing to evaluate this round.
+// Work decomposition: the tile list holds ceil(n_a / TILE) tiles of TILE
+// consecutive points per alignment.  Block b of the persistent grid owns the
+// contiguous tile range [b * per, (b + 1) * per), so the tiles of one
+// alignment are met in a row; each lane keeps its FP32 sums of the current
+// alignment in shared memory and the block reduces them once per alignment
+// run (TwoSum-compensated across lanes and warps), writing the run's FP64
+// partial to the slot of its first tile (the run's other slots get zeros).
 //
 // Per point (one thread):
 //   1. transform by the alignment's float 3x4 (transformPointCloud :385-404,
 //      same float operation order);
-//   2. the reference's 27 float probe points p + {-r, 0, r}^3 with its bounds
-//      test, cell linearisation and the `dist < r` test on the FP64 voxel mean,
-//      all with the reference's float/double roundings, so the set and order
-//      of accepted (point, voxel) pairs equals the reference's;
-//   3. accepted pairs are appended to a per-warp ring in shared memory
-//      (ballot + popc); whenever 32 are queued the warp evaluates them one per
-//      lane, so the per-pair work stays load-balanced across lanes whatever
-//      the neighbour counts are.
-// Per pair (FP32 path): q = C x', xCx, e = exp(-d2 xCx / 2), the validity test
-// of :456, gradient a_i = x'^T C J_i and the Hessian split as
+//   2. the reference's 27 float probe points p + {-r, 0, r}^3: coordinates by
+//      the reference's float recurrence, its bounds test and cell
+//      linearisation (division by r replaced by the exactly equal product
+//      with 1/r when r is a power of two), one z-layer of 9 probes at a time
+//      with all their loads in flight;
+//   3. the reference's test float(sqrt(dx^2 + dy^2 + dz^2)) < r with
+//      dx = float(mean - x) on the FP64 mean, decided without the square
+//      root as s <= s_max (s_max = the largest float whose correctly rounded
+//      square root is below r), first on the FP32 copy of the mean with a
+//      proven error margin and, only inside that margin, exactly on the FP64
+//      mean -- so the accepted (point, voxel) pairs are the reference's;
+//   4. accepted pairs are compacted per warp in shared memory (ballot + popc)
+//      and evaluated one per lane, so per-pair work is balanced across lanes.
+// Per pair (FP32 path): x' from the (hi, lo) float split of the FP64 mean,
+// q = C x', xCx, e = exp(-d2 xCx / 2), the validity test of :456, gradient
+// a_i = x'^T C J_i and the Hessian split as
 //   H_ij = S_ij + k R_ij,  S_ij = w (-d2 a_i a_j + J_j^T C J_i)   (i <= j)
 //   compat:    R_ij = w a_i b_ij, k = -d2  (the reference's :486-488 form)
 //   corrected: R_ij = w b_ij,     k = 1    (Magnusson eq. 6.13)
-// with b_ij = x'^T C H_ij (nonzero for i, j >= 3 only).  37 FP32 lane sums are
-// reduced with error-free TwoSum across the warp and the block; the tile
-// partial is written as FP64 (hi + lo).  Voxels flagged by the grid build
-// (inverse-covariance entries non-finite or beyond 1e30) are evaluated in
-// FP64 so that infinities and NaNs propagate as in the reference.
+// with b_ij = x'^T C H_ij (nonzero for i, j >= 3 only).  Voxels flagged by the
+// grid build (inverse-covariance entries non-finite or beyond 1e30) are
+// evaluated in FP64 so that infinities and NaNs propagate as in the reference.
 //
 // The FP64 variant (precision = 1) evaluates every pair with the reference's
 // literal FP64 expressions and accumulates in FP64.
@@ -41,8 +49,9 @@ namespace ndt {
 
 namespace {
 
-constexpr int kWarpsE = kTile / 32;
-constexpr int kAcc = 37;    // score, g[6], S[21], R[9]
+constexpr int kAcc = 37;      // score, g[6], S[21], R[9]
+constexpr int kTerms = 23;    // per-point terms (see below)
+constexpr int kList = 27 * 32;  // per-warp pair list: all 27 probes of all 32 lanes
 constexpr unsigned kFull = 0xffffffffu;
 
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -64,173 +73,183 @@ __device__ __forceinline__ float dot3f(float a0, float a1, float a2, const float
 // Per-point terms (point Jacobian columns 3-5 and point Hessian blocks), FP32.
 // Index: 0 J13, 1 J23, 2 J04, 3 J14, 4 J24, 5 J05, 6 J15, 7 J25,
 //        8 a1, 9 a2, 10 b1, 11 b2, 12 c1, 13 c2, 14-16 d, 17-19 e, 20-22 f.
-constexpr int kTerms = 23;
 
-// The reference's probe walk for one transformed point: trip counts of the
-// three float loops (z outer, x inner), capped at 4 (the reference's loops run
-// 3 times for finite coordinates below ~1e6 m; the cap only stops the endless
-// loop it enters for infinite coordinates).
-struct ProbeStart {
-    float x0, y0, z0;
-    int nx, ny, nz;
+// ---------------------------------------------------------------------------
+// Probe geometry of one axis: the reference's float loop
+//   for (float v = p - r; v <= p + rf; v += res)           (kernel.cpp:256-258)
+// gives up to 3 coordinates for any finite |p| below ~1e6 m (trip count n;
+// n = 4 only for larger or infinite coordinates, handled by the generic
+// path).  For each coordinate: inside the bbox (kernel.cpp:261-269) and its
+// cell index (linearizeCoord, :239-241).
+struct Axis {
+    float c0, c1, c2;
+    int i0, i1, i2;
+    unsigned in;  // bit k: coordinate k is active and inside the bbox
+    int n;
 };
 
-__device__ __forceinline__ int trips(float start, float limit, float res) {
-    int n = 0;
-    float v = start;
-    while (n < 4 && v <= limit) {
-        ++n;
-        v = v + res;
-    }
-    return n;
+__device__ __forceinline__ int cell_component(float v, float minv, float res, float inv_res) {
+    return inv_res > 0.0f ? (int)((v - minv) * inv_res) : (int)((v - minv) / res);
 }
 
-__device__ __forceinline__ ProbeStart probe_start(float px, float py, float pz, float res, bool valid) {
+__device__ __forceinline__ Axis make_axis(float p, float minv, float maxv, float res, float inv_res, bool valid) {
     const double radius = (double)res;
     const float rf = (float)(radius + (double)0.001f);  // radiusFinal, kernel.cpp:254
-    ProbeStart s;
-    s.x0 = (float)((double)px - radius);
-    s.y0 = (float)((double)py - radius);
-    s.z0 = (float)((double)pz - radius);
-    s.nx = valid ? trips(s.x0, px + rf, res) : 0;
-    s.ny = valid ? trips(s.y0, py + rf, res) : 0;
-    s.nz = valid ? trips(s.z0, pz + rf, res) : 0;
-    return s;
+    Axis a;
+    a.c0 = (float)((double)p - radius);
+    a.c1 = a.c0 + res;
+    a.c2 = a.c1 + res;
+    const float lim = p + rf;
+    int n = 0;
+    if (valid) {
+        float v = a.c0;
+        while (n < 4 && v <= lim) {
+            ++n;
+            v = v + res;
+        }
+    }
+    a.n = n;
+    unsigned in = 0;
+    if (n > 0 && !(a.c0 < minv || a.c0 > maxv)) in |= 1u;
+    if (n > 1 && !(a.c1 < minv || a.c1 > maxv)) in |= 2u;
+    if (n > 2 && !(a.c2 < minv || a.c2 > maxv)) in |= 4u;
+    a.in = in;
+    a.i0 = (in & 1u) ? cell_component(a.c0, minv, res, inv_res) : 0;
+    a.i1 = (in & 2u) ? cell_component(a.c1, minv, res, inv_res) : 0;
+    a.i2 = (in & 4u) ? cell_component(a.c2, minv, res, inv_res) : 0;
+    return a;
 }
 
-constexpr int kList = 27 * 32;  // per-warp pair list: all 27 probes of all 32 lanes
+__device__ __forceinline__ float axis_c(const Axis &a, int k) { return k == 0 ? a.c0 : (k == 1 ? a.c1 : a.c2); }
+__device__ __forceinline__ int axis_i(const Axis &a, int k) { return k == 0 ? a.i0 : (k == 1 ? a.i1 : a.i2); }
 
-// Append the accepted (point, voxel) pairs of one probe step of the warp to
-// the list (code = slot << 6 | flag << 5 | lane), in lane order.
-__device__ __forceinline__ void list_append(unsigned *list, int &n, bool acc, unsigned code, unsigned lt) {
-    const unsigned b = __ballot_sync(kFull, acc);
-    if (acc) list[n + __popc(b & lt)] = code;
-    n += __popc(b);
+// Margin of the FP32 pre-test of the radius check for a point p: the FP32
+// difference hi - p and the reference's float(mean - p) (FP64 mean) differ by
+// at most E = 2^-23 (|m| + |dx|) per axis, and a candidate mean lies within
+// 3r of p, so |m| <= |p| + 3r; the squared distances then differ by at most
+// sum_axes 2 E (|dx| + E) <= 20 r E + 3 E^2 with E = 2^-23 (|p|_1 + 14 r + 1).
+__device__ __forceinline__ float radius_margin(float px, float py, float pz, float res) {
+    const float E = 1.2e-7f * (fabsf(px) + fabsf(py) + fabsf(pz) + 14.0f * res + 1.0f);
+    return 20.0f * res * E + 3.0f * E * E;
 }
 
-// Probe the reference's 27 cells around every lane's point (z outer, x
-// inner; voxelRadiusSearch, kernel.cpp:246-286) and collect the accepted
-// pairs in `list`.  Fast path (trip counts <= 3, i.e. every finite coordinate
-// below ~1e6 m): the 27 index loads, then the voxel-mean loads of one
-// z-layer at a time, are all in flight together, and the list (27 x 32
-// entries) cannot overflow.  Generic path (up to 4 x 4 x 4 probes): one probe
-// at a time, calling flush(n) whenever the list could overflow.
-template <class Flush>
-__device__ __forceinline__ int probe_list(const GridDev &grid, float px, float py, float pz, bool valid,
-                                          unsigned *list, unsigned &n_probe, unsigned &n_occ, Flush flush) {
+// The reference's distance test for one occupied probe, decided as
+// s <= s_max (see the file comment): first with the FP32 mean and the margin
+// tol, then, inside the margin, exactly on the FP64 mean.
+__device__ __forceinline__ bool accept(const GridDev &grid, int slot, float4 hi, float px, float py, float pz,
+                                       float tol) {
+    const float s_max = grid.s_max;
+    const float fx = hi.x - px, fy = hi.y - py, fz = hi.z - pz;
+    const float sf = fmaf(fx, fx, fmaf(fy, fy, fz * fz));
+    if (sf < s_max - tol) return true;
+    if (sf > s_max + tol) return false;
+    const double4 m = ldg_d4(grid.mean + slot);
+    const float dx = (float)(m.x - (double)px);
+    const float dy = (float)(m.y - (double)py);
+    const float dz = (float)(m.z - (double)pz);
+    const float s = dx * dx + dy * dy + dz * dz;
+    return s <= s_max;
+}
+
+// Probe every lane's point in the reference's order (z outer, x inner;
+// voxelRadiusSearch, kernel.cpp:256-284) and collect the accepted pairs in
+// `list` (capacity 27 x 32); `consume(n)` then evaluates list[0, n) (the
+// generic path calls it whenever the list could overflow).
+// List code = slot << 6 | flag << 5 | lane.
+template <class Consume>
+__device__ __forceinline__ void probe_point(const GridDev &grid, float px, float py, float pz, bool valid,
+                                            unsigned *list, unsigned &n_probe, unsigned &n_occ, Consume consume) {
     const int lane = threadIdx.x & 31;
     const unsigned lt = lanemask_lt();
     const GridMeta &g = grid.meta;
-    const float res = g.res;
-    const double radius = (double)res;
-    const ProbeStart ps = probe_start(px, py, pz, res, valid);
-    const int mz = __reduce_max_sync(kFull, ps.nz);
-    const int my = __reduce_max_sync(kFull, ps.ny);
-    const int mx = __reduce_max_sync(kFull, ps.nx);
+    const float res = g.res, inv_res = grid.inv_res;
+    const Axis ax = make_axis(px, g.minv[0], g.maxv[0], res, inv_res, valid);
+    const Axis ay = make_axis(py, g.minv[1], g.maxv[1], res, inv_res, valid);
+    const Axis az = make_axis(pz, g.minv[2], g.maxv[2], res, inv_res, valid);
+    const int mx = __reduce_max_sync(kFull, ax.n), my = __reduce_max_sync(kFull, ay.n),
+              mz = __reduce_max_sync(kFull, az.n);
+    const float tol = radius_margin(px, py, pz, res);
     int n = 0;
-    if (mz <= 3 && my <= 3 && mx <= 3) {
-        float zc[3], yc[3], xc[3];
-        zc[0] = ps.z0; zc[1] = zc[0] + res; zc[2] = zc[1] + res;
-        yc[0] = ps.y0; yc[1] = yc[0] + res; yc[2] = yc[1] + res;
-        xc[0] = ps.x0; xc[1] = xc[0] + res; xc[2] = xc[1] + res;
-        int v[27];
+    if (mx <= 3 && my <= 3 && mz <= 3) {
+        // no lane has an in-bounds probe: nothing to do
+        if (!__any_sync(kFull, (ax.in != 0u) && (ay.in != 0u) && (az.in != 0u))) return;
+#pragma unroll 1
+        for (int a = 0; a < mz; ++a) {
+            const bool za = (az.in >> a) & 1u;
+            if (!__any_sync(kFull, za && ax.in != 0u && ay.in != 0u)) continue;
+            const int zbase = g.dim[1] * axis_i(az, a);
+            int slot[9];
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int b = 0; b < 3; ++b)
+            for (int b = 0; b < 3; ++b) {
+                const bool yb = za && ((ay.in >> b) & 1u);
+                const int base = g.dim[0] * (axis_i(ay, b) + zbase);
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
-                    const float z = zc[a], y = yc[b], x = xc[c];
-                    const bool act = a < ps.nz && b < ps.ny && c < ps.nx;
-                    const bool inb = act && !((x < g.minv[0]) || (x > g.maxv[0]) || (y < g.minv[1]) ||
-                                              (y > g.maxv[1]) || (z < g.minv[2]) || (z > g.maxv[2]));
-                    int slot = -1;
-                    if (inb) {
-                        const int ix = (int)((x - g.minv[0]) / res);
-                        const int iy = (int)((y - g.minv[1]) / res);
-                        const int iz = (int)((z - g.minv[2]) / res);
-                        slot = __ldg(grid.index + (ix + g.dim[0] * (iy + g.dim[1] * iz)));
-                        ++n_probe;
-                    }
-                    v[9 * a + 3 * b + c] = slot;
+                    const bool on = yb && ((ax.in >> c) & 1u);
+                    slot[3 * b + c] = on ? __ldg(grid.index + (axis_i(ax, c) + base)) : -2;
                 }
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            float4 mf[9];
+            }
+            float4 hi[9];
 #pragma unroll
             for (int k = 0; k < 9; ++k) {
-                const int slot = v[9 * a + k];
-                if (slot >= 0) mf[k] = __ldg(grid.mean32 + (slot & kSlotMask));
+                n_probe += slot[k] != -2;
+                if (slot[k] >= 0) hi[k] = __ldg(grid.mean_hi + (slot[k] & kSlotMask));
             }
 #pragma unroll
             for (int k = 0; k < 9; ++k) {
-                const int slot = v[9 * a + k];
+                const int v = slot[k];
                 bool acc = false;
-                if (slot >= 0) {
+                if (v >= 0) {
                     ++n_occ;
-                    // FP32-mean distance; it differs from the reference's
-                    // (FP64 mean, float differences) by less than tol, so
-                    // only distances within tol of r need the exact test
-                    const float fx = mf[k].x - px, fy = mf[k].y - py, fz = mf[k].z - pz;
-                    const float fd = sqrtf(fx * fx + fy * fy + fz * fz);
-                    const float tol = 1e-6f + 2.384185791e-7f * (fabsf(mf[k].x) + fabsf(mf[k].y) + fabsf(mf[k].z));
-                    if (fd < res - tol) {
-                        acc = true;
-                    } else if (fd <= res + tol) {
-                        const double4 m = ldg_d4(grid.mean + (slot & kSlotMask));
-                        const float dx = (float)(m.x - (double)px);
-                        const float dy = (float)(m.y - (double)py);
-                        const float dz = (float)(m.z - (double)pz);
-                        const float dist = sqrtf(dx * dx + dy * dy + dz * dz);
-                        acc = (double)dist < radius;
-                    }
+                    acc = accept(grid, v & kSlotMask, hi[k], px, py, pz, tol);
                 }
-                const unsigned code = ((unsigned)(slot & kSlotMask) << 6) | ((slot & kSlotFlag) ? 32u : 0u) | lane;
-                list_append(list, n, acc, code, lt);
+                const unsigned b = __ballot_sync(kFull, acc);
+                if (acc) list[n + __popc(b & lt)] = ((unsigned)(v & kSlotMask) << 6) | ((v & kSlotFlag) ? 32u : 0u) | lane;
+                n += __popc(b);
             }
         }
-        return n;
+        __syncwarp();
+        consume(n);
+        __syncwarp();
+        return;
     }
-    // generic path
-    float zc = ps.z0;
-    for (int az = 0; az < mz; ++az, zc = zc + res) {
-        float yc = ps.y0;
-        for (int ay = 0; ay < my; ++ay, yc = yc + res) {
-            float xc = ps.x0;
-            for (int ax = 0; ax < mx; ++ax, xc = xc + res) {
-                const bool act = az < ps.nz && ay < ps.ny && ax < ps.nx;
+    // generic path: trip counts up to 4 (coordinates beyond ~1e6 m or inf)
+    float zc = (float)((double)pz - (double)res);
+    for (int a = 0; a < mz; ++a, zc = zc + res) {
+        float yc = (float)((double)py - (double)res);
+        for (int b = 0; b < my; ++b, yc = yc + res) {
+            float xc = (float)((double)px - (double)res);
+            for (int c = 0; c < mx; ++c, xc = xc + res) {
+                const bool act = a < az.n && b < ay.n && c < ax.n;
                 const bool inb = act && !((xc < g.minv[0]) || (xc > g.maxv[0]) || (yc < g.minv[1]) ||
                                           (yc > g.maxv[1]) || (zc < g.minv[2]) || (zc > g.maxv[2]));
-                int slot = -1;
+                int v = -1;
                 if (inb) {
-                    const int ix = (int)((xc - g.minv[0]) / res);
-                    const int iy = (int)((yc - g.minv[1]) / res);
-                    const int iz = (int)((zc - g.minv[2]) / res);
-                    slot = __ldg(grid.index + (ix + g.dim[0] * (iy + g.dim[1] * iz)));
+                    v = __ldg(grid.index + (cell_component(xc, g.minv[0], res, inv_res) +
+                                            g.dim[0] * (cell_component(yc, g.minv[1], res, inv_res) +
+                                                        g.dim[1] * cell_component(zc, g.minv[2], res, inv_res))));
                     ++n_probe;
                 }
                 bool acc = false;
-                if (slot >= 0) {
+                if (v >= 0) {
                     ++n_occ;
-                    const double4 m = ldg_d4(grid.mean + (slot & kSlotMask));
-                    const float dx = (float)(m.x - (double)px);
-                    const float dy = (float)(m.y - (double)py);
-                    const float dz = (float)(m.z - (double)pz);
-                    const float dist = sqrtf(dx * dx + dy * dy + dz * dz);
-                    acc = (double)dist < radius;
+                    acc = accept(grid, v & kSlotMask, __ldg(grid.mean_hi + (v & kSlotMask)), px, py, pz, tol);
                 }
                 if (n > kList - 32) {
                     __syncwarp();
-                    flush(n);
+                    consume(n);
                     __syncwarp();
                     n = 0;
                 }
-                const unsigned code = ((unsigned)(slot & kSlotMask) << 6) | ((slot & kSlotFlag) ? 32u : 0u) | lane;
-                list_append(list, n, acc, code, lt);
+                const unsigned bb = __ballot_sync(kFull, acc);
+                if (acc) list[n + __popc(bb & lt)] = ((unsigned)(v & kSlotMask) << 6) | ((v & kSlotFlag) ? 32u : 0u) | lane;
+                n += __popc(bb);
             }
         }
     }
-    return n;
+    __syncwarp();
+    consume(n);
+    __syncwarp();
 }
 
 // ---------------------------------------------------------------------------
@@ -328,11 +347,8 @@ __device__ __forceinline__ void pair_fp32(AccF &A, const float (*terms)[32], int
 // to the alignment's FP64 side buffer (exc[44], same layout as a tile
 // partial) with atomics; they are 0, inf or NaN in practice (a flagged
 // covariance puts xCx far from 0), so their order does not matter.
-__device__ __noinline__ void pair_fp64_flagged(double *exc, const float (*terms)[32], int owner, float p0f, float p1f,
-                                               float p2f, const double *C, double d1, double d2, bool hess,
-                                               bool compat) {
-    float t[kTerms];
-    for (int k = 0; k < kTerms; ++k) t[k] = terms[k][owner];
+__device__ void pair_fp64_flagged(double *exc, const float *t, float p0f, float p1f, float p2f, const double *C,
+                                  double d1, double d2, bool hess, bool compat) {
     const double p[3] = {p0f, p1f, p2f};
     double xCx = C[0] * p[0] * p[0] + C[4] * p[1] * p[1] + C[8] * p[2] * p[2] + (C[1] + C[3]) * p[0] * p[1] +
                  (C[2] + C[6]) * p[0] * p[2] + (C[5] + C[7]) * p[1] * p[2];
@@ -396,31 +412,49 @@ __device__ __forceinline__ double h_entry(const double *tot, int i, int j, doubl
     return v;
 }
 
+// Pairs with a flagged voxel queued by the FP32 pass: (alignment, point,
+// slot).  The point is transformed and its per-point terms recomputed exactly
+// as the FP32 pass does, then the pair is evaluated in FP64.
+__global__ void flagged_kernel(EvalArgs args) {
+    const unsigned n = *args.flag_n;
+    const unsigned m = n < args.flag_cap ? n : args.flag_cap;
+    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < m; q += gridDim.x * blockDim.x) {
+        const int4 e = args.flag_q[q];
+        const AlignState &st = args.states[e.x];
+        const int mode = st.eval_mode;
+        const bool hess = mode != kEvalGradient;
+        const float4 x = args.points[e.y];
+        float px, py, pz;
+        if (args.trans) {
+            const float4 y = args.trans[e.y];
+            px = y.x; py = y.y; pz = y.z;
+        } else {
+            const float *T = st.T;
+            px = T[0] * x.x + T[1] * x.y + T[2] * x.z + T[3];
+            py = T[4] * x.x + T[5] * x.y + T[6] * x.z + T[7];
+            pz = T[8] * x.x + T[9] * x.y + T[10] * x.z + T[11];
+        }
+        float t[kTerms];
+        for (int k = 0; k < 8; ++k) t[k] = dot3f(x.x, x.y, x.z, st.angf + 3 * k);
+        for (int k = 0; k < 15; ++k) t[8 + k] = dot3f(x.x, x.y, x.z, st.angf + 24 + 3 * k);
+        const float4 hi = args.grid.mean_hi[e.z];
+        const float4 lo = args.grid.mean_lo[e.z];
+        pair_fp64_flagged(args.exc + (size_t)e.x * kPartial, t, (px - hi.x) - lo.x, (py - hi.y) - lo.y,
+                          (pz - hi.z) - lo.z, args.grid.icov64 + 9 * (size_t)e.z, args.d1, args.d2, hess,
+                          args.compat != 0);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && n > args.flag_cap) atomicOr(args.flag_overflow, 1);
+}
+
 // Dynamic shared memory of the FP32 kernel (W warps).
 template <int W>
 struct F32Smem {
-    float acc[kAcc][W * 32];  // per-lane sums of the current alignment run
-    float terms[W][kTerms][32];
-    float xt[W][3][32];
-    unsigned list[W][kList];
+    float acc[kAcc][W * 32];      // per-lane sums of the current alignment run
+    float terms[W][kTerms][32];   // per-point terms of each warp's 32 points
+    float xt[W][3][32];           // transformed points
+    unsigned list[W][kList];      // accepted pairs of the current tile
     float2 red[W][kAcc];
 };
-
-// Generic-path overflow (coordinates beyond ~1e6 m only): evaluate the queued
-// pairs through the FP64 side path, whose sums land in exc with atomics.
-__device__ __noinline__ void flush_fp64(const unsigned *list, int n, const float (*terms)[32], const float (*xts)[32],
-                                        const GridDev &grid, double *exc, double d1, double d2, bool hess,
-                                        bool compat) {
-    const int lane = threadIdx.x & 31;
-    for (int k = lane; k < n; k += 32) {
-        const unsigned code = list[k];
-        const int owner = code & 31;
-        const int slot = (int)(code >> 6);
-        const double4 m = ldg_d4(grid.mean + slot);
-        pair_fp64_flagged(exc, terms, owner, (float)((double)xts[0][owner] - m.x), (float)((double)xts[1][owner] - m.y),
-                          (float)((double)xts[2][owner] - m.z), grid.icov64 + 9 * (size_t)slot, d1, d2, hess, compat);
-    }
-}
 
 // Block-wide reduction of the per-lane sums of one alignment run (TwoSum
 // compensated across lanes and warps), written as the FP64 partial of the
@@ -465,11 +499,6 @@ __device__ void reduce_run(F32Smem<W> &sm, double *s_tot, const unsigned (*s_cnt
     }
 }
 
-// FP32 derivative pass.  Block b owns the contiguous tile range
-// [b * per, (b + 1) * per) of the tile list (tiles of one alignment are
-// consecutive), keeps per-lane sums in shared memory across the tiles of one
-// alignment and reduces once per alignment run; the run's partial goes to the
-// slot of its first tile, the other slots of the run get zeros.
 template <int TILE, int MINB>
 __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(EvalArgs args) {
     constexpr int kW = TILE / 32;
@@ -489,12 +518,13 @@ __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(EvalArgs arg
     float (*terms)[32] = sm.terms[warp];
     float (*xts)[32] = sm.xt[warp];
     unsigned *list = sm.list[warp];
+    float *acc = &sm.acc[0][threadIdx.x];
 
     const int nt = *args.num_tiles;
     const int per = (nt + gridDim.x - 1) / gridDim.x;
     const int t_begin = blockIdx.x * per;
     const int t_end = min(nt, t_begin + per);
-    for (int k = 0; k < kAcc; ++k) sm.acc[k][threadIdx.x] = 0.0f;
+    for (int k = 0; k < kAcc; ++k) acc[k * TILE] = 0.0f;
     if (lane == 0) s_cnt[warp][0] = s_cnt[warp][1] = s_cnt[warp][2] = 0;
     unsigned long long blk_probe = 0, blk_occ = 0, blk_pair = 0, blk_pts = 0, blk_tiles = 0;
     int cur = -1, run_first = -1, mode = kEvalNone;
@@ -541,53 +571,56 @@ __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(EvalArgs arg
         xts[0][lane] = px;
         xts[1][lane] = py;
         xts[2][lane] = pz;
-        // per-point terms of the ORIGINAL point (computePointDerivatives)
-        {
-            const float *ja = s_ang;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) terms[k][lane] = dot3f(x.x, x.y, x.z, ja + 3 * k);
-            const float *h = s_ang + 24;
-#pragma unroll
-            for (int k = 0; k < 15; ++k) terms[8 + k][lane] = dot3f(x.x, x.y, x.z, h + 3 * k);
-        }
         unsigned n_probe = 0, n_occ = 0, n_pair = 0;
-        auto flush = [&](int n) {
-            flush_fp64(list, n, terms, xts, grid, exc, args.d1, args.d2, hess, compat);
-            n_pair += (lane < n) ? (unsigned)((n - lane + 31) / 32) : 0u;
+        bool have_terms = false;
+        // evaluate list[0, n): one entry per lane per round
+        auto consume = [&](int n) {
+            if (n == 0) return;
+            if (!have_terms) {
+                // per-point terms of the ORIGINAL point (computePointDerivatives),
+                // computed once a warp has pairs to evaluate
+                const float *ja = s_ang;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) terms[k][lane] = dot3f(x.x, x.y, x.z, ja + 3 * k);
+                const float *h = s_ang + 24;
+#pragma unroll
+                for (int k = 0; k < 15; ++k) terms[8 + k][lane] = dot3f(x.x, x.y, x.z, h + 3 * k);
+                have_terms = true;
+                __syncwarp();
+            }
+            AccF A;
+#pragma unroll
+            for (int k = 0; k < kAcc; ++k) A.v[k] = 0.0f;
+            for (int base = 0; base < n; base += 32) {
+                const int k = base + lane;
+                if (k >= n) break;
+                const unsigned code = list[k];
+                const int owner = code & 31;
+                const int slot = (int)(code >> 6);
+                const float4 hi = __ldg(grid.mean_hi + slot);
+                const float4 lo = __ldg(grid.mean_lo + slot);
+                // x' = x_trans - mean (kernel.cpp:692-694) from the (hi, lo) split
+                const float p0 = (xts[0][owner] - hi.x) - lo.x;
+                const float p1 = (xts[1][owner] - hi.y) - lo.y;
+                const float p2 = (xts[2][owner] - hi.z) - lo.z;
+                ++n_pair;
+                if (code & 32) {
+                    // FP64 side path, evaluated by flagged_kernel after this pass
+                    const unsigned q = atomicAdd(args.flag_n, 1u);
+                    if (q < args.flag_cap)
+                        args.flag_q[q] = make_int4(tile.align, tile.start + warp * 32 + owner, slot, 0);
+                } else {
+                    const float4 ca = __ldg(grid.icov32 + 2 * slot);
+                    const float4 cb = __ldg(grid.icov32 + 2 * slot + 1);
+                    pair_fp32(A, terms, owner, p0, p1, p2, ca, cb, d1f, d2f, hess, compat);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < kAcc; ++k) acc[k * TILE] += A.v[k];
         };
         __syncwarp();
-        const int n = probe_list(grid, px, py, pz, valid, list, n_probe, n_occ, flush);
-        __syncwarp();
-        AccF A;
-#pragma unroll
-        for (int k = 0; k < kAcc; ++k) A.v[k] = 0.0f;
-        // evaluate list[0, n): one entry per lane per round
-        for (int base = 0; base < n; base += 32) {
-            const int k = base + lane;
-            if (k >= n) break;
-            const unsigned code = list[k];
-            const int owner = code & 31;
-            const int slot = (int)(code >> 6);
-            const double2 *q = reinterpret_cast<const double2 *>(grid.mean + slot);
-            const double2 m01 = __ldg(q);
-            const double m2 = __ldg(reinterpret_cast<const double *>(q + 1));
-            // x' = x_trans - mean (kernel.cpp:692-694), rounded to float
-            const float p0 = (float)((double)xts[0][owner] - m01.x);
-            const float p1 = (float)((double)xts[1][owner] - m01.y);
-            const float p2 = (float)((double)xts[2][owner] - m2);
-            ++n_pair;
-            if (code & 32) {
-                pair_fp64_flagged(exc, terms, owner, p0, p1, p2, grid.icov64 + 9 * (size_t)slot, args.d1, args.d2,
-                                  hess, compat);
-            } else {
-                const float4 ca = __ldg(grid.icov32 + 2 * slot);
-                const float4 cb = __ldg(grid.icov32 + 2 * slot + 1);
-                pair_fp32(A, terms, owner, p0, p1, p2, ca, cb, d1f, d2f, hess, compat);
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < kAcc; ++k) sm.acc[k][threadIdx.x] += A.v[k];
-        // per-warp work counters of the run (pairs feed the partial's count)
+        probe_point(grid, px, py, pz, valid, list, n_probe, n_occ, consume);
+        // per-warp work counters (pairs feed the partial's count)
         for (int o = 16; o > 0; o >>= 1) {
             n_probe += __shfl_xor_sync(kFull, n_probe, o);
             n_occ += __shfl_xor_sync(kFull, n_occ, o);
@@ -603,7 +636,6 @@ __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(EvalArgs arg
     if (cur >= 0 && mode != kEvalNone)
         reduce_run<kW>(sm, s_tot, s_cnt, args.partials + (size_t)run_first * kPartial, kR, compat);
     if (args.counters && lane == 0 && blk_tiles) {
-        // every warp holds the warp-summed counts; warp 0 reports per-block totals of probes and pairs
         if (warp == 0) {
             atomicAdd(&args.counters->points, blk_pts);
             atomicAdd(&args.counters->tiles, blk_tiles);
@@ -687,14 +719,17 @@ __device__ void pair_fp64(AccD &A, const double *x, const double *ang, const dou
     A.v[0] += score_inc;
 }
 
-__global__ void __launch_bounds__(kTile, 1) derivative_f64_kernel(EvalArgs args) {
+constexpr int kTile64 = 256;
+
+__global__ void __launch_bounds__(kTile64, 1) derivative_f64_kernel(EvalArgs args) {
+    constexpr int kW = kTile64 / 32;
     __shared__ float s_T[12];
     __shared__ double s_ang[kAngle];
     __shared__ int s_mode;
-    __shared__ float s_pts[kWarpsE][6][32];  // original xyz, transformed xyz
-    __shared__ unsigned s_list[kWarpsE][kList];
-    __shared__ double s_red[kWarpsE][43];
-    __shared__ unsigned s_cnt[kWarpsE][3];
+    __shared__ float s_pts[kW][6][32];  // original xyz, transformed xyz
+    __shared__ unsigned s_list[kW][kList];
+    __shared__ double s_red[kW][43];
+    __shared__ unsigned s_cnt[kW][3];
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const bool compat = args.compat != 0;
@@ -725,12 +760,13 @@ __global__ void __launch_bounds__(kTile, 1) derivative_f64_kernel(EvalArgs args)
             py = s_T[4] * x.x + s_T[5] * x.y + s_T[6] * x.z + s_T[7];
             pz = s_T[8] * x.x + s_T[9] * x.y + s_T[10] * x.z + s_T[11];
         }
+        __syncwarp();
         pts[0][lane] = x.x; pts[1][lane] = x.y; pts[2][lane] = x.z;
         pts[3][lane] = px; pts[4][lane] = py; pts[5][lane] = pz;
         AccD A;
         for (int k = 0; k < 43; ++k) A.v[k] = 0.0;
         unsigned n_probe = 0, n_occ = 0, n_pair = 0;
-        auto process = [&](int n) {
+        auto consume = [&](int n) {
             for (int base = 0; base < n; base += 32) {
                 const int kk = base + lane;
                 if (kk >= n) break;
@@ -746,9 +782,7 @@ __global__ void __launch_bounds__(kTile, 1) derivative_f64_kernel(EvalArgs args)
             }
         };
         __syncwarp();
-        const int n = probe_list(grid, px, py, pz, valid, list, n_probe, n_occ, process);
-        __syncwarp();
-        process(n);
+        probe_point(grid, px, py, pz, valid, list, n_probe, n_occ, consume);
         for (int k = 0; k < 43; ++k) {
             double v = A.v[k];
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
@@ -770,17 +804,17 @@ __global__ void __launch_bounds__(kTile, 1) derivative_f64_kernel(EvalArgs args)
             const int k = threadIdx.x;
             double v = 0.0;
             if (k < 43) {
-                for (int w = 0; w < kWarpsE; ++w) v += s_red[w][k];
+                for (int w = 0; w < kW; ++w) v += s_red[w][k];
             } else {
                 unsigned np = 0;
-                for (int w = 0; w < kWarpsE; ++w) np += s_cnt[w][2];
+                for (int w = 0; w < kW; ++w) np += s_cnt[w][2];
                 v = (double)np;
             }
             out[k] = v;
         }
         if (threadIdx.x == 0 && args.counters) {
             unsigned long long a0 = 0, a1 = 0, a2 = 0;
-            for (int w = 0; w < kWarpsE; ++w) {
+            for (int w = 0; w < kW; ++w) {
                 a0 += s_cnt[w][0];
                 a1 += s_cnt[w][1];
                 a2 += s_cnt[w][2];
@@ -794,41 +828,39 @@ __global__ void __launch_bounds__(kTile, 1) derivative_f64_kernel(EvalArgs args)
     }
 }
 
-}  // namespace
-
-namespace {
 template <int TILE, int MINB>
 cudaError_t prepare_one() {
     return cudaFuncSetAttribute(derivative_f32_kernel<TILE, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(F32Smem<TILE / 32>));
 }
+
 template <int TILE, int MINB>
 void launch_one(const EvalArgs &args, int blocks, cudaStream_t st) {
     derivative_f32_kernel<TILE, MINB><<<blocks, TILE, sizeof(F32Smem<TILE / 32>), st>>>(args);
 }
+
 }  // namespace
 
 const DerivVariant kDerivVariants[kNumDerivVariants] = {
-    {256, 2}, {256, 1}, {128, 4}, {128, 3}, {128, 2},
+    {256, 2}, {256, 1}, {128, 4}, {128, 3}, {256, 3},
 };
 
 int prepare_derivatives() {
-    cudaError_t e = cudaSuccess;
-    cudaError_t r;
+    cudaError_t e = cudaSuccess, r;
     if ((r = prepare_one<256, 2>()) != cudaSuccess) e = r;
     if ((r = prepare_one<256, 1>()) != cudaSuccess) e = r;
     if ((r = prepare_one<128, 4>()) != cudaSuccess) e = r;
     if ((r = prepare_one<128, 3>()) != cudaSuccess) e = r;
-    if ((r = prepare_one<128, 2>()) != cudaSuccess) e = r;
+    if ((r = prepare_one<256, 3>()) != cudaSuccess) e = r;
     return (int)e;
 }
 
 int launch_derivatives(const EvalArgs &args, int precision, int variant, int sms, cudaStream_t st) {
     if (args.max_tiles <= 0) return 0;
     if (precision == 1) {
-        if (args.tile_size != kTile) return (int)cudaErrorInvalidValue;
+        if (args.tile_size != kTile64) return (int)cudaErrorInvalidValue;
         int blocks = sms < args.max_tiles ? sms : args.max_tiles;
-        derivative_f64_kernel<<<blocks, kTile, 0, st>>>(args);
+        derivative_f64_kernel<<<blocks, kTile64, 0, st>>>(args);
         return (int)cudaGetLastError();
     }
     if (variant < 0 || variant >= kNumDerivVariants) variant = 0;
@@ -836,13 +868,15 @@ int launch_derivatives(const EvalArgs &args, int precision, int variant, int sms
     if (args.tile_size != v.tile) return (int)cudaErrorInvalidValue;
     long long want = (long long)sms * v.min_blocks;
     int blocks = (int)(want < args.max_tiles ? want : args.max_tiles);
+    cudaMemsetAsync(args.flag_n, 0, sizeof(unsigned), st);
     switch (variant) {
         case 0: launch_one<256, 2>(args, blocks, st); break;
         case 1: launch_one<256, 1>(args, blocks, st); break;
         case 2: launch_one<128, 4>(args, blocks, st); break;
         case 3: launch_one<128, 3>(args, blocks, st); break;
-        default: launch_one<128, 2>(args, blocks, st); break;
+        default: launch_one<256, 3>(args, blocks, st); break;
     }
+    flagged_kernel<<<sms, 128, 0, st>>>(args);
     return (int)cudaGetLastError();
 }
 

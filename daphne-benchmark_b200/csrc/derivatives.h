@@ -20,6 +20,10 @@ struct EvalArgs {
     double d1, d2;         // Gauss constants (kernel.cpp:1181-1185)
     int compat;
     Counters *counters;    // may be null
+    int4 *flag_q;          // FP32 path: queue of pairs with flagged voxels (align, point, slot, -)
+    unsigned *flag_n;      // queue length (reset by launch_derivatives)
+    unsigned flag_cap;     // queue capacity
+    int *flag_overflow;    // set when the queue overflowed
 };
 
 // Per-device set-up (dynamic shared memory opt-in); call with the device current.
@@ -38,5 +42,7 @@ extern const DerivVariant kDerivVariants[kNumDerivVariants];
 // (256-point tiles).  The persistent grid is sms x resident blocks; blocks
 // loop over the tiles.
 int launch_derivatives(const EvalArgs &args, int precision, int variant, int sms, cudaStream_t st);
+// Kernel launches per launch_derivatives call (FP32: pass + flagged pairs; FP64: pass).
+constexpr int kDerivLaunchesFP32 = 2;
 
 }  // namespace ndt

@@ -80,17 +80,19 @@ struct ndt_ctx {
     std::string err;
     double d1 = 0, d2 = 0;
     // grid
-    DevBuf map, index, mean, mean32, icov32, icov64, count, cell, seg_start, seg_cell, scratch, meta;
+    DevBuf map, index, mean, mean_hi, mean_lo, icov32, icov64, count, cell, seg_start, seg_cell, scratch, meta;
     GridMeta meta_host{};
     bool have_map = false;
     int map_points = 0;
     // batch
     DevBuf points, offsets, guesses, states, tiles, tile_begin, num_tiles, partials, exc, out_T, out_conv, out_fit,
-        out_status, active, counters, p6, trans;
+        out_status, active, counters, p6, trans, flag_q, flag_n, flag_overflow;
     HostBuf h_offsets, h_active, h_counters, h_out;
     ndt_counters last{};
     long long launches = 0;
     int variant = 0;  // FP32 derivative-pass launch shape (kDerivVariants)
+    float s_max = 1.0f;    // radius test threshold (see radius_threshold)
+    float inv_res = 0.0f;  // 1 / res when res is a power of two
     // profiling: event pairs around derivative launches and the grid build
     bool profiling = false;
     std::vector<cudaEvent_t> ev;
@@ -128,6 +130,25 @@ void gauss_constants(const ndt_params &p, double &d1, double &d2) {
     d2 = -2 * std::log((-std::log(c1 * std::exp(-0.5) + c2) - d3) / d1);
 }
 
+// The reference accepts a voxel when float(sqrt(s)) < r (s = dx^2 + dy^2 +
+// dz^2 in float, kernel.cpp:276-278).  The correctly rounded float square root
+// is monotonic, so that is s <= s_max for the largest float s_max whose root
+// rounds below r.
+float radius_threshold(float r) {
+    float s = r * r;
+    while (std::sqrt(s) >= r) s = std::nextafter(s, 0.0f);
+    while (std::sqrt(std::nextafter(s, INFINITY)) < r) s = std::nextafter(s, INFINITY);
+    return s;
+}
+
+// 1 / r when r is a power of two (then (v - min) / r == (v - min) * (1 / r)
+// exactly), otherwise 0 (the kernels divide).
+float exact_reciprocal(float r) {
+    int e;
+    float m = std::frexp(r, &e);
+    return m == 0.5f ? 1.0f / r : 0.0f;
+}
+
 StepParams step_params(const ndt_params &p) {
     StepParams s;
     s.compat = p.compat;
@@ -143,7 +164,8 @@ GridBuffers grid_buffers(ndt_ctx *c) {
     GridBuffers b;
     b.index = c->index.as<int32_t>();
     b.mean = c->mean.as<double4>();
-    b.mean32 = c->mean32.as<float4>();
+    b.mean_hi = c->mean_hi.as<float4>();
+    b.mean_lo = c->mean_lo.as<float4>();
     b.icov32 = c->icov32.as<float4>();
     b.icov64 = c->icov64.as<double>();
     b.count = c->count.as<int32_t>();
@@ -158,7 +180,10 @@ GridDev grid_dev(ndt_ctx *c) {
     g.meta = c->meta_host;
     g.index = c->index.as<int32_t>();
     g.mean = c->mean.as<double4>();
-    g.mean32 = c->mean32.as<float4>();
+    g.mean_hi = c->mean_hi.as<float4>();
+    g.mean_lo = c->mean_lo.as<float4>();
+    g.s_max = c->s_max;
+    g.inv_res = c->inv_res;
     g.icov32 = c->icov32.as<float4>();
     g.icov64 = c->icov64.as<double>();
     return g;
@@ -203,7 +228,8 @@ int build_grid(ndt_ctx *c, const float4 *d_map, int m) {
     const size_t G = (size_t)c->meta_host.G;
     CK(c->index.ensure(sizeof(int32_t) * G));
     CK(c->mean.ensure(sizeof(double4) * (size_t)m));
-    CK(c->mean32.ensure(sizeof(float4) * (size_t)m));
+    CK(c->mean_hi.ensure(sizeof(float4) * (size_t)m));
+    CK(c->mean_lo.ensure(sizeof(float4) * (size_t)m));
     CK(c->icov32.ensure(2 * sizeof(float4) * (size_t)m));
     CK(c->icov64.ensure(9 * sizeof(double) * (size_t)m));
     CK(c->count.ensure(sizeof(int32_t) * (size_t)m));
@@ -224,6 +250,20 @@ int build_grid(ndt_ctx *c, const float4 *d_map, int m) {
     }
     c->have_map = true;
     c->map_points = m;
+    return NDT_OK;
+}
+
+constexpr unsigned kFlagCap = 1u << 20;  // queued pairs with flagged voxels per derivative pass
+
+int prepare_flag_queue(ndt_ctx *c, EvalArgs &ea) {
+    CK(c->flag_q.ensure(sizeof(int4) * kFlagCap));
+    CK(c->flag_n.ensure(sizeof(unsigned)));
+    CK(c->flag_overflow.ensure(sizeof(int)));
+    CK(cudaMemsetAsync(c->flag_overflow.p, 0, sizeof(int), c->stream));
+    ea.flag_q = c->flag_q.as<int4>();
+    ea.flag_n = c->flag_n.as<unsigned>();
+    ea.flag_cap = kFlagCap;
+    ea.flag_overflow = c->flag_overflow.as<int>();
     return NDT_OK;
 }
 
@@ -269,6 +309,7 @@ int run_batch(ndt_ctx *c, int B, const float4 *d_points, const int *d_offsets, i
     ea.d2 = c->d2;
     ea.compat = c->prm.compat;
     ea.counters = c->counters.as<Counters>();
+    if (int rc2 = prepare_flag_queue(c, ea)) return rc2;
     // With the reference's line-search test (compat, step_max > step_min)
     // every Newton iteration takes at most one evaluation, so the round count
     // is fixed and no host polling is needed.
@@ -287,7 +328,7 @@ int run_batch(ndt_ctx *c, int B, const float4 *d_points, const int *d_offsets, i
         rc = launch_step(c->states.as<AlignState>(), c->partials.as<double>(), c->tile_begin.as<int>(),
                          c->exc.as<double>(), B, P, c->active.as<int>(), c->counters.as<Counters>(), st);
         if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_step");
-        nl += 2;
+        nl += 1 + (c->prm.precision == 1 ? 1 : kDerivLaunchesFP32);
         ++rounds;
         if (!fixed && (r + 1) % poll_every == 0) {
             CK(cudaMemcpyAsync(c->h_active.p, c->active.p, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -295,11 +336,12 @@ int run_batch(ndt_ctx *c, int B, const float4 *d_points, const int *d_offsets, i
             if (*c->h_active.as<int>() == 0) break;
         }
     }
-    rc = launch_finalize(c->states.as<AlignState>(), B, d_out, d_conv, d_fit, d_status, st);
+    rc = launch_finalize(c->states.as<AlignState>(), B, d_out, d_conv, d_fit, d_status, c->flag_overflow.as<int>(),
+                         st);
     if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_finalize");
     nl += 1;
     c->launches += nl;
-    c->last.launches = nl;
+    c->last.launches = c->launches;
     c->last.rounds = rounds;
     return NDT_OK;
 }
@@ -444,6 +486,8 @@ int ndt_create(const ndt_params *params, int device, ndt_ctx **out) {
     c->prm = *params;
     c->device = device;
     gauss_constants(c->prm, c->d1, c->d2);
+    c->s_max = radius_threshold(c->prm.resolution);
+    c->inv_res = exact_reciprocal(c->prm.resolution);
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
@@ -460,10 +504,11 @@ void ndt_destroy(ndt_ctx *c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    DevBuf *bufs[] = {&c->map, &c->index, &c->mean, &c->mean32, &c->icov32, &c->icov64, &c->count, &c->cell, &c->seg_start,
+    DevBuf *bufs[] = {&c->map, &c->index, &c->mean, &c->mean_hi, &c->mean_lo, &c->icov32, &c->icov64, &c->count, &c->cell, &c->seg_start,
                       &c->seg_cell, &c->scratch, &c->meta, &c->points, &c->offsets, &c->guesses, &c->states,
                       &c->tiles, &c->tile_begin, &c->num_tiles, &c->partials, &c->exc, &c->out_T, &c->out_conv,
-                      &c->out_fit, &c->out_status, &c->active, &c->counters, &c->p6, &c->trans};
+                      &c->out_fit, &c->out_status, &c->active, &c->counters, &c->p6, &c->trans,
+                      &c->flag_q, &c->flag_n, &c->flag_overflow};
     for (DevBuf *b : bufs) b->release();
     HostBuf *hb[] = {&c->h_offsets, &c->h_active, &c->h_counters, &c->h_out};
     for (HostBuf *b : hb) b->release();
@@ -656,6 +701,7 @@ int ndt_derivatives(ndt_ctx *c, const float *scan, const float *trans, int n, co
     ea.d2 = c->d2;
     ea.compat = c->prm.compat;
     ea.counters = c->counters.as<Counters>();
+    if (int rc2 = prepare_flag_queue(c, ea)) return rc2;
     rc = launch_derivatives(ea, c->prm.precision, c->variant, c->num_sms, st);
     if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_derivatives");
     int nt = 0;

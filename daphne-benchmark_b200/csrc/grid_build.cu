@@ -309,7 +309,10 @@ __device__ bool write_records(int s, const double *mu, const double *C, GridBuff
     for (int k = 0; k < 3; ++k)
         if (!isfinite(mu[k])) bad = true;
     buf.mean[s] = make_double4(mu[0], mu[1], mu[2], bad ? 1.0 : 0.0);
-    buf.mean32[s] = make_float4((float)mu[0], (float)mu[1], (float)mu[2], 0.0f);
+    const float h0 = (float)mu[0], h1 = (float)mu[1], h2 = (float)mu[2];
+    buf.mean_hi[s] = make_float4(h0, h1, h2, 0.0f);
+    buf.mean_lo[s] = make_float4((float)(mu[0] - (double)h0), (float)(mu[1] - (double)h1), (float)(mu[2] - (double)h2),
+                                 0.0f);
     float c00 = (float)C[0], c11 = (float)C[4], c22 = (float)C[8];
     float c01 = (float)((C[1] + C[3]) * 0.5), c02 = (float)((C[2] + C[6]) * 0.5), c12 = (float)((C[5] + C[7]) * 0.5);
     buf.icov32[2 * s] = make_float4(c00, c01, c02, c11);

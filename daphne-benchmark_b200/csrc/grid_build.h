@@ -12,7 +12,8 @@ namespace ndt {
 struct GridBuffers {
     int32_t *index;      // G dense cell -> voxel slot (-1 = no usable voxel)
     double4 *mean;       // slot -> mean xyz, w = 1 if the FP32 pair path must not be used
-    float4 *mean32;      // slot -> mean xyz rounded to float
+    float4 *mean_hi;     // slot -> float(mean) xyz
+    float4 *mean_lo;     // slot -> float(mean - float(mean)) xyz
     float4 *icov32;      // slot -> 2 float4 (symmetrised FP32 inverse covariance)
     double *icov64;      // slot -> 9 doubles
     int32_t *count;      // slot -> points in the cell

@@ -48,7 +48,10 @@ struct GridDev {
     GridMeta meta;
     const int32_t *index;    // G: dense cell -> voxel slot | kSlotFlag, -1 = none
     const double4 *mean;     // K: mean xyz (FP64), w = 1 when the FP32 path must not be used
-    const float4 *mean32;    // K: mean xyz rounded to FP32 (the probe's first, conservative distance test)
+    const float4 *mean_hi;   // K: float(mean) xyz (the probe's first, conservative distance test)
+    const float4 *mean_lo;   // K: float(mean - float(mean)) xyz (x' = (x - hi) - lo)
+    float s_max;             // largest float s with sqrtf(s) < res (the radius test without sqrt)
+    float inv_res;           // 1 / res when res is a power of two (exact), else 0 (divide)
     const float4 *icov32;    // 2K: {c00 c01 c02 c11}, {c12 c22 0 0} (symmetrised, FP32)
     const double *icov64;    // 9K: inverse covariance as the reference stores it (row major)
 };

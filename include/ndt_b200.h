@@ -44,7 +44,8 @@ extern "C" {
 
 /* Per-alignment status bits written by the batch calls. */
 #define NDT_ST_OK 0
-#define NDT_ST_WATCHDOG 1
+#define NDT_ST_WATCHDOG 1  /* the evaluation budget ran out before convergence */
+#define NDT_ST_OVERFLOW 2  /* more pairs with degenerate voxels than the FP64 side queue holds */
 
 /*
  * Registration parameters.  ndt_params_reference() fills the values the
