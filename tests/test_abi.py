@@ -1,0 +1,62 @@
+"""The C ABI library loads here (no GPU) and exports every entry point that
+include/ndt_b200.h declares; calls that need a device fail loudly."""
+import ctypes
+import pathlib
+import re
+
+import pytest
+
+ROOT = pathlib.Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "ndt_b200.h"
+
+
+def declared_symbols():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"NDT_API\s+[\w\s\*]*?\b(ndt_\w+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    for name in ("ndt_create", "ndt_set_map", "ndt_align", "ndt_align_with_map", "ndt_align_batch",
+                 "ndt_align_batch_device", "ndt_align_batch_packed", "ndt_destroy"):
+        assert name in syms
+
+
+def test_library_exports_every_declared_symbol(pkg):
+    L = pkg.ndt.lib()
+    missing = [s for s in declared_symbols() if not hasattr(L, s)]
+    assert not missing, missing
+
+
+def test_param_presets(pkg):
+    r = pkg.ndt.reference_params()
+    assert (r.resolution, r.outlier_ratio, r.step_size, r.transformation_epsilon, r.max_iterations, r.compat) == \
+        (1.0, 0.55, 0.1, 0.1, 0, 1)
+    c = pkg.ndt.corrected_params()
+    assert (c.compat, c.transformation_epsilon, c.max_iterations, c.min_points_per_voxel, c.eigen_ratio) == \
+        (0, 0.01, 30, 6, 0.01)
+    assert ctypes.sizeof(pkg.ndt.Params) == 64
+
+
+def test_kernel_variants_listed(pkg):
+    v = pkg.ndt.kernel_variants()
+    assert len(v) >= 2 and all(t in (128, 256) and b >= 1 for t, b in v)
+
+
+def test_bad_arguments_rejected(pkg):
+    L = pkg.ndt.lib()
+    h = ctypes.c_void_p()
+    p = pkg.ndt.reference_params()
+    p.resolution = -1.0
+    assert L.ndt_create(ctypes.byref(p), 0, ctypes.byref(h)) == -1  # NDT_E_ARG
+    p = pkg.ndt.reference_params()
+    p.precision = 7
+    assert L.ndt_create(ctypes.byref(p), 0, ctypes.byref(h)) == -1
+
+
+def test_no_cpu_fallback_without_device(pkg):
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(pkg.ndt.NdtError):
+        pkg.ndt.Context(pkg.ndt.reference_params())
