@@ -14,6 +14,7 @@
 
 #include "../../include/ndt_b200.h"
 #include "align.h"
+#include "ctx_view.h"
 #include "derivatives.h"
 #include "grid_build.h"
 #include "ndt_types.h"
@@ -447,6 +448,29 @@ int packed_batch(ndt_ctx *c, int B, const float *points, const int *offsets, con
 }
 
 }  // namespace
+
+namespace ndt {
+
+int ctx_eval_view(ndt_ctx *c, CtxEvalView *v) {
+    if (!c || !v) return NDT_E_ARG;
+    v->grid = grid_dev(c);
+    v->d1 = c->d1;
+    v->d2 = c->d2;
+    v->compat = c->prm.compat;
+    v->precision = c->prm.precision;
+    v->variant = c->variant;
+    v->sms = c->num_sms;
+    v->device = c->device;
+    v->stream = c->stream;
+    v->have_map = c->have_map;
+    return NDT_OK;
+}
+
+void ctx_set_error(ndt_ctx *c, const char *msg) {
+    if (c) c->err = msg;
+}
+
+}  // namespace ndt
 
 extern "C" {
 

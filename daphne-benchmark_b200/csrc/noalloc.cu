@@ -1,0 +1,196 @@
+// ndt_derivatives_noalloc: one derivative evaluation (score, gradient,
+// Hessian of one scan against the context's voxel grid) that allocates no
+// memory at call time.
+//
+// Who needs it: callers that must not allocate device memory while they
+// run -- a real-time control loop with a fixed memory budget (cudaMalloc can
+// block, synchronise the device and take unbounded time), code that runs
+// while another component holds the device's memory pool, or a pipeline that
+// records its work into a CUDA graph (cudaMalloc is not allowed during stream
+// capture).  They set up a context and its map beforehand, then call this as
+// often as they like.
+//
+// Its scratch memory (tile list, one alignment state, per-tile partial sums,
+// the FP64 side queue, counters) is the file-scope array ndt_noalloc_scratch
+// below, sized for at most kNoAllocMaxPoints scan points.  Every GPU that
+// loads this library holds that array (256 KB) until the process
+// exits.  Host code cannot take the array's address directly (in host code
+// the symbol is a host-side stand-in); the first call on each device, with
+// that device current, looks the device address up with cudaGetSymbolAddress
+// and caches it -- make that first call before any stream capture.
+//
+// Every call shares the one array and keeps the previous call's contents:
+// each call clears what must start at zero before it runs, and two calls whose
+// work overlaps on the GPU (different streams, or contexts on different host
+// threads using the same device) race on it.  Calls on one context's stream
+// are ordered and do not overlap.
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "../../include/ndt_b200.h"
+#include "align.h"
+#include "ctx_view.h"
+#include "derivatives.h"
+#include "ndt_math.cuh"
+
+namespace ndt {
+namespace {
+
+constexpr int kNoAllocMaxPoints = 65536;
+constexpr int kNoAllocMaxTiles = kNoAllocMaxPoints / 128 + 2;  // smallest tile: 128 points
+constexpr unsigned kNoAllocFlagCap = 4096;
+
+// Layout of the scratch array.
+struct NoAllocScratch {
+    AlignState state;
+    Counters counters;
+    int offsets[2];
+    int tile_begin[2];
+    int num_tiles;
+    unsigned flag_n;
+    int flag_overflow;
+    int pad;
+    double exc[kPartial];
+    Tile tiles[kNoAllocMaxTiles];
+    int4 flag_q[kNoAllocFlagCap];
+    double partials[kNoAllocMaxTiles * kPartial];
+};
+
+constexpr size_t kNoAllocScratchBytes = (sizeof(NoAllocScratch) + 255) & ~(size_t)255;
+
+static __device__ __align__(256) unsigned char ndt_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mu;
+void *g_scratch_addr[kMaxDevices];  // device address of ndt_noalloc_scratch, per device
+
+// Clears the zero-initialised parts and sets the one evaluation request:
+// transformed points given by the caller (T unused), angle terms of p.
+struct Pose6 {
+    double p[6];
+};
+
+__global__ void noalloc_setup_kernel(NoAllocScratch *s, Pose6 pose, int n) {
+    const int t = threadIdx.x;
+    if (t < kPartial) s->exc[t] = 0.0;
+    if (t == 0) {
+        s->counters.evaluations = s->counters.points = s->counters.probes = 0;
+        s->counters.occupied_probes = s->counters.pairs = s->counters.tiles = 0;
+        s->offsets[0] = 0;
+        s->offsets[1] = n;
+        s->flag_n = 0;
+        s->flag_overflow = 0;
+        AlignState &st = s->state;
+        for (int k = 0; k < 16; ++k) st.T[k] = (k % 5 == 0) ? 1.0f : 0.0f;
+        for (int i = 0; i < 6; ++i) st.x_t[i] = st.p[i] = pose.p[i];
+        double a[kAngle];
+        angle_terms(pose.p, a);
+        for (int k = 0; k < kAngle; ++k) {
+            st.angd[k] = a[k];
+            st.angf[k] = (float)a[k];
+        }
+        st.n = n;
+        st.eval_mode = kEvalFull;
+        st.phase = kPhaseInitEval;
+    }
+}
+
+// out[k] = sum over tiles (in tile order) + side sums; out[43] = pairs, or -1
+// when the FP64 side queue overflowed.
+__global__ void noalloc_reduce_kernel(const NoAllocScratch *s, double *out) {
+    const int k = threadIdx.x;
+    if (k >= kPartial) return;
+    double v = 0.0;
+    for (int t = 0; t < s->num_tiles; ++t) v += s->partials[(size_t)t * kPartial + k];
+    v += s->exc[k];
+    if (k == kPartial - 1 && (s->flag_overflow || s->flag_n > kNoAllocFlagCap)) v = -1.0;
+    out[k] = v;
+}
+
+}  // namespace
+}  // namespace ndt
+
+using namespace ndt;
+
+extern "C" int ndt_derivatives_noalloc(ndt_ctx *ctx, const float *d_scan, const float *d_trans, int n,
+                                       const double p6[6], double *d_out) {
+    CtxEvalView v;
+    if (!ctx || !d_scan || !d_trans || !p6 || !d_out || n <= 0) {
+        ctx_set_error(ctx, "ndt_derivatives_noalloc: null pointer or empty scan");
+        return NDT_E_ARG;
+    }
+    ctx_eval_view(ctx, &v);
+    if (!v.have_map) {
+        ctx_set_error(ctx, "ndt_derivatives_noalloc: no map set");
+        return NDT_E_NOMAP;
+    }
+    if (n > kNoAllocMaxPoints) {
+        ctx_set_error(ctx, "ndt_derivatives_noalloc: more than 65536 scan points (the static scratch limit)");
+        return NDT_E_CAPACITY;
+    }
+    if (v.device < 0 || v.device >= kMaxDevices) {
+        ctx_set_error(ctx, "ndt_derivatives_noalloc: device ordinal out of range");
+        return NDT_E_ARG;
+    }
+    cudaError_t e = cudaSetDevice(v.device);
+    if (e != cudaSuccess) {
+        ctx_set_error(ctx, cudaGetErrorString(e));
+        return NDT_E_CUDA;
+    }
+    void *addr = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_mu);
+        if (!g_scratch_addr[v.device]) {
+            e = cudaGetSymbolAddress(&g_scratch_addr[v.device], ndt_noalloc_scratch);
+            if (e != cudaSuccess) {
+                g_scratch_addr[v.device] = nullptr;
+                ctx_set_error(ctx, cudaGetErrorString(e));
+                return NDT_E_CUDA;
+            }
+        }
+        addr = g_scratch_addr[v.device];
+    }
+    NoAllocScratch *s = reinterpret_cast<NoAllocScratch *>(addr);
+    const cudaStream_t st = v.stream;
+    const int tile = v.precision == 1 ? kTile : kDerivVariants[v.variant].tile;
+    Pose6 pose;
+    for (int i = 0; i < 6; ++i) pose.p[i] = p6[i];
+    noalloc_setup_kernel<<<1, 64, 0, st>>>(s, pose, n);
+    int rc = launch_tiles(s->offsets, 1, tile, s->tile_begin, s->tiles, &s->num_tiles, st);
+    if (rc) {
+        ctx_set_error(ctx, cudaGetErrorString((cudaError_t)rc));
+        return NDT_E_CUDA;
+    }
+    EvalArgs ea;
+    ea.grid = v.grid;
+    ea.points = reinterpret_cast<const float4 *>(d_scan);
+    ea.trans = reinterpret_cast<const float4 *>(d_trans);
+    ea.tiles = s->tiles;
+    ea.num_tiles = &s->num_tiles;
+    ea.max_tiles = n / tile + 2;
+    ea.tile_size = tile;
+    ea.states = &s->state;
+    ea.partials = s->partials;
+    ea.exc = s->exc;
+    ea.d1 = v.d1;
+    ea.d2 = v.d2;
+    ea.compat = v.compat;
+    ea.counters = &s->counters;
+    ea.flag_q = s->flag_q;
+    ea.flag_n = &s->flag_n;
+    ea.flag_cap = kNoAllocFlagCap;
+    ea.flag_overflow = &s->flag_overflow;
+    rc = launch_derivatives(ea, v.precision, v.variant, v.sms, st);
+    if (rc) {
+        ctx_set_error(ctx, cudaGetErrorString((cudaError_t)rc));
+        return NDT_E_CUDA;
+    }
+    noalloc_reduce_kernel<<<1, 64, 0, st>>>(s, d_out);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        ctx_set_error(ctx, cudaGetErrorString(e));
+        return NDT_E_CUDA;
+    }
+    return NDT_OK;
+}

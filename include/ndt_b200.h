@@ -199,6 +199,25 @@ NDT_API int ndt_grid_cells(ndt_ctx *ctx, int cap, int *cell_index, int *count, d
 NDT_API int ndt_derivatives(ndt_ctx *ctx, const float *scan, const float *trans, int n,
                     const double p6[6], double *score, double g6[6], double H36[36]);
 
+/*
+ * ndt_derivatives_noalloc -- no counterpart in the reference.  The same
+ * evaluation as ndt_derivatives, for callers that cannot allocate device
+ * memory while they run (a real-time loop with a fixed memory budget, work
+ * recorded into a CUDA graph, where cudaMalloc is not allowed): it allocates
+ * nothing.  Inputs are DEVICE pointers: d_scan and d_trans (n float[4] each,
+ * the original and the already transformed scan), p6 is a host array (the
+ * pose vector for the angle terms); d_out receives 44 doubles: score,
+ * gradient[6], Hessian[36] row major, pair count (-1 if more pairs hit
+ * degenerate voxels than the side queue holds).  Scratch is one static device
+ * array per GPU (256 KB, held until exit), so n is limited to 65536
+ * (NDT_E_CAPACITY beyond).  The first call on a device looks the array up
+ * (cudaGetSymbolAddress); make it before any stream capture.  Work is
+ * enqueued on the context stream (call ndt_synchronize before reading
+ * d_out); calls whose work overlaps on one GPU race on the shared scratch.
+ */
+NDT_API int ndt_derivatives_noalloc(ndt_ctx *ctx, const float *d_scan, const float *d_trans, int n,
+                                    const double p6[6], double *d_out);
+
 #ifdef __cplusplus
 }
 #endif
