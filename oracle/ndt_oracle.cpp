@@ -173,6 +173,7 @@ bool build_grid_f(Grid &g, const float *map, int m, float res, int min_points, d
     g.count.assign(G, 0);
     g.valid.assign(G, 0);
     std::vector<int> cell(m);
+    const double nan = std::nan("");
     for (int i = 0; i < m; ++i) {
         const float *p = map + 4 * (size_t)i;
         int c = cell_of(g, p[0], p[1], p[2]);
@@ -214,12 +215,17 @@ bool build_grid_f(Grid &g, const float *map, int m, float res, int min_points, d
         }
         if (!ok) continue;
         double *C = &g.icov[9 * c];
+        for (int e = 0; e < 9; ++e) C[e] = 0.0;
         for (int r = 0; r < 3; ++r)
             for (int q = 0; q < 3; ++q)
                 C[3 * r + q] = V[r][0] * inv_w[0] * V[q][0] + V[r][1] * inv_w[1] * V[q][1] +
                                V[r][2] * inv_w[2] * V[q][2];
         g.valid[c] = 1;
     }
+    // unusable cells: NaN mean, so the radius test never accepts them
+    for (long long c = 0; c < G; ++c)
+        if (!g.valid[c])
+            for (int e = 0; e < 3; ++e) g.mean[3 * c + e] = nan;
     return true;
 }
 
@@ -254,32 +260,6 @@ int radius_search_r(const Grid &g, const float *pt, double radius, int *out) {
             }
         }
     }
-    return k;
-}
-
-// Mode F: the 27 cells around the point's own cell (integer offsets, z outer,
-// x inner), usable cells only, kept when the FP64 distance to the mean < r.
-int radius_search_f(const Grid &g, const double *pt, double radius, int *out) {
-    int k = 0;
-    double f[3];
-    int ic[3];
-    for (int e = 0; e < 3; ++e) {
-        f[e] = (pt[e] - (double)g.minv[e]) / (double)g.res;
-        if (!(f[e] > -2.0 && f[e] < (double)g.dim[e] + 1.0)) return 0;
-        ic[e] = (int)std::floor(f[e]);
-    }
-    for (int dz = -1; dz <= 1; ++dz)
-        for (int dy = -1; dy <= 1; ++dy)
-            for (int dx = -1; dx <= 1; ++dx) {
-                int cx = ic[0] + dx, cy = ic[1] + dy, cz = ic[2] + dz;
-                if (cx < 0 || cy < 0 || cz < 0 || cx >= g.dim[0] || cy >= g.dim[1] || cz >= g.dim[2])
-                    continue;
-                int idx = cx + g.dim[0] * (cy + g.dim[1] * cz);
-                if (!g.valid[idx]) continue;
-                const double *c = &g.mean[3 * (size_t)idx];
-                double d0 = c[0] - pt[0], d1 = c[1] - pt[1], d2 = c[2] - pt[2];
-                if (std::sqrt(d0 * d0 + d1 * d1 + d2 * d2) < radius) out[k++] = idx;
-            }
     return k;
 }
 
@@ -596,8 +576,7 @@ struct Aligner {
     Gauss gs;
     const float *scan = nullptr;
     int n = 0;
-    std::vector<float> trans_f;   // Mode R: float transformed cloud
-    std::vector<double> trans_d;  // Mode F: FP64 transformed cloud
+    std::vector<float> trans_f;   // float transformed cloud
     float final_T[16];
     int evals = 0;
     long long pairs = 0;
@@ -605,37 +584,12 @@ struct Aligner {
     Aligner(const ndt_params &p, const Grid &g, Gauss gauss)
         : prm(p), grid(g), compat(p.compat != 0), gs(gauss) {}
 
+    // transformPointCloud (kernel.cpp:385-404): float matrix, float arithmetic,
+    // in both modes (the corrected mode builds the float matrix from the FP64
+    // pose vector).
     void apply(const float *M) {
-        if (compat) {
-            trans_f.resize(4 * (size_t)n);
-            transform_cloud(scan, n, M, trans_f.data());
-        } else {
-            double T[12];
-            for (int r = 0; r < 3; ++r)
-                for (int c = 0; c < 4; ++c) T[4 * r + c] = M[4 * r + c];
-            trans_d.resize(3 * (size_t)n);
-            for (int i = 0; i < n; ++i) {
-                const float *p = scan + 4 * (size_t)i;
-                for (int r = 0; r < 3; ++r)
-                    trans_d[3 * (size_t)i + r] = T[4 * r] * p[0] + T[4 * r + 1] * p[1] + T[4 * r + 2] * p[2] + T[4 * r + 3];
-            }
-        }
-    }
-
-    // Mode F transforms with the FP64 pose directly (no float matrix round trip).
-    void apply_pose_f(const double *p) {
-        double ca = std::cos(p[3]), sa = std::sin(p[3]);
-        double cb = std::cos(p[4]), sb = std::sin(p[4]);
-        double cc = std::cos(p[5]), sc = std::sin(p[5]);
-        double R[9] = {cb * cc, -cb * sc, sb,
-                       ca * sc + sa * sb * cc, ca * cc - sa * sb * sc, -sa * cb,
-                       sa * sc - ca * sb * cc, sa * cc + ca * sb * sc, ca * cb};
-        trans_d.resize(3 * (size_t)n);
-        for (int i = 0; i < n; ++i) {
-            const float *q = scan + 4 * (size_t)i;
-            for (int r = 0; r < 3; ++r)
-                trans_d[3 * (size_t)i + r] = R[3 * r] * q[0] + R[3 * r + 1] * q[1] + R[3 * r + 2] * q[2] + p[r];
-        }
+        trans_f.resize(4 * (size_t)n);
+        transform_cloud(scan, n, M, trans_f.data());
     }
 
     // computeDerivatives (kernel.cpp:651-705) / computeHessian (:562-602).
@@ -651,17 +605,12 @@ struct Aligner {
         int nb[64];
         PointTerms P;
         for (int idx = 0; idx < n; ++idx) {
-            double xt0[3];
-            int k;
-            if (compat) {
-                const float *tp = &trans_f[4 * (size_t)idx];
-                k = radius_search_r(grid, tp, grid.res, nb);
-                xt0[0] = tp[0]; xt0[1] = tp[1]; xt0[2] = tp[2];
-            } else {
-                const double *tp = &trans_d[3 * (size_t)idx];
-                k = radius_search_f(grid, tp, grid.res, nb);
-                xt0[0] = tp[0]; xt0[1] = tp[1]; xt0[2] = tp[2];
-            }
+            // the reference's neighbour search in both modes; the corrected
+            // grid marks cells below min_points unusable (radius_search_r
+            // skips them through their NaN means)
+            const float *tp = &trans_f[4 * (size_t)idx];
+            const int k = radius_search_r(grid, tp, grid.res, nb);
+            const double xt0[3] = {tp[0], tp[1], tp[2]};
             if (!k) continue;
             const float *sp = scan + 4 * (size_t)idx;
             double x[3] = {sp[0], sp[1], sp[2]};
@@ -679,13 +628,11 @@ struct Aligner {
     }
 
     void set_pose(const double *x_t) {
-        if (compat) {
+        if (compat)
             build_tm_r(final_T, x_t);
-            apply(final_T);
-        } else {
+        else
             build_tm_f(final_T, x_t);
-            apply_pose_f(x_t);
-        }
+        apply(final_T);
     }
 
     // computeStepLengthMT (kernel.cpp:1015-1144).
@@ -760,8 +707,8 @@ struct Aligner {
         std::memcpy(final_T, guess, sizeof(float) * 16);
         double p[6], dp[6], g6[6], H36[36];
         pose_vector(compat, final_T, p);
-        if (compat) apply(final_T);
-        else apply_pose_f(p);
+        if (!compat) build_tm_f(final_T, p);
+        apply(final_T);
         double score = derivatives(g6, H36, p, true, false);
         bool conv = false;
         int nr_iterations = 0;
@@ -887,13 +834,7 @@ ORACLE_API double oracle_derivatives(const ndt_params *prm, const float *map, in
     Aligner a(*prm, g, gs);
     a.scan = scan;
     a.n = n;
-    if (prm->compat) {
-        a.trans_f.assign(trans, trans + 4 * (size_t)n);
-    } else {
-        a.trans_d.resize(3 * (size_t)n);
-        for (int i = 0; i < n; ++i)
-            for (int r = 0; r < 3; ++r) a.trans_d[3 * (size_t)i + r] = trans[4 * (size_t)i + r];
-    }
+    a.trans_f.assign(trans, trans + 4 * (size_t)n);
     double Hd[36];
     double s = a.derivatives(g6, H36 ? H36 : Hd, p6, hessian != 0, false);
     if (pairs) *pairs = a.pairs;
