@@ -6,7 +6,7 @@
 
 namespace ndt {
 
-struct EvalArgs {
+struct EvalArgs {  // (GridDev is in ndt_types.h)
     GridDev grid;
     const float4 *points;  // all scans, concatenated (original coordinates)
     const float4 *trans;   // optional: already transformed points (then T is not applied)
@@ -24,6 +24,8 @@ struct EvalArgs {
     unsigned *flag_n;      // queue length (reset by launch_derivatives)
     unsigned flag_cap;     // queue capacity
     int *flag_overflow;    // set when the queue overflowed
+    int *work_counter;     // FP32 pass: next chunk of tiles (reset by launch_derivatives)
+    int chunk_tiles;       // FP32 pass: tiles per chunk
 };
 
 // Per-device set-up (dynamic shared memory opt-in); call with the device current.
@@ -42,6 +44,8 @@ extern const DerivVariant kDerivVariants[kNumDerivVariants];
 // (256-point tiles).  The persistent grid is sms x resident blocks; blocks
 // loop over the tiles.
 int launch_derivatives(const EvalArgs &args, int precision, int variant, int sms, cudaStream_t st);
+// The FP64 pass alone (256-point tiles).
+int launch_derivatives_f64(const EvalArgs &args, int sms, cudaStream_t st);
 // Kernel launches per launch_derivatives call (FP32: pass + flagged pairs; FP64: pass).
 constexpr int kDerivLaunchesFP32 = 2;
 

@@ -87,7 +87,7 @@ struct ndt_ctx {
     int map_points = 0;
     // batch
     DevBuf points, offsets, guesses, states, tiles, tile_begin, num_tiles, partials, exc, out_T, out_conv, out_fit,
-        out_status, active, counters, p6, trans, flag_q, flag_n, flag_overflow;
+        out_status, active, counters, p6, trans, flag_q, flag_n, flag_overflow, work_counter;
     HostBuf h_offsets, h_active, h_counters, h_out;
     ndt_counters last{};
     long long launches = 0;
@@ -185,6 +185,7 @@ GridDev grid_dev(ndt_ctx *c) {
     g.mean_lo = c->mean_lo.as<float4>();
     g.s_max = c->s_max;
     g.inv_res = c->inv_res;
+    g.radius_final = (float)((double)c->prm.resolution + (double)0.001f);
     g.icov32 = c->icov32.as<float4>();
     g.icov64 = c->icov64.as<double>();
     return g;
@@ -255,6 +256,7 @@ int build_grid(ndt_ctx *c, const float4 *d_map, int m) {
 }
 
 constexpr unsigned kFlagCap = 1u << 20;  // queued pairs with flagged voxels per derivative pass
+constexpr int kChunkTiles = 4;           // tiles per dynamically scheduled chunk of the FP32 pass
 
 int prepare_flag_queue(ndt_ctx *c, EvalArgs &ea) {
     CK(c->flag_q.ensure(sizeof(int4) * kFlagCap));
@@ -265,6 +267,9 @@ int prepare_flag_queue(ndt_ctx *c, EvalArgs &ea) {
     ea.flag_n = c->flag_n.as<unsigned>();
     ea.flag_cap = kFlagCap;
     ea.flag_overflow = c->flag_overflow.as<int>();
+    CK(c->work_counter.ensure(sizeof(int)));
+    ea.work_counter = c->work_counter.as<int>();
+    ea.chunk_tiles = kChunkTiles;
     return NDT_OK;
 }
 
@@ -532,7 +537,7 @@ void ndt_destroy(ndt_ctx *c) {
                       &c->seg_cell, &c->scratch, &c->meta, &c->points, &c->offsets, &c->guesses, &c->states,
                       &c->tiles, &c->tile_begin, &c->num_tiles, &c->partials, &c->exc, &c->out_T, &c->out_conv,
                       &c->out_fit, &c->out_status, &c->active, &c->counters, &c->p6, &c->trans,
-                      &c->flag_q, &c->flag_n, &c->flag_overflow};
+                      &c->flag_q, &c->flag_n, &c->flag_overflow, &c->work_counter};
     for (DevBuf *b : bufs) b->release();
     HostBuf *hb[] = {&c->h_offsets, &c->h_active, &c->h_counters, &c->h_out};
     for (HostBuf *b : hb) b->release();

@@ -52,6 +52,7 @@ struct GridDev {
     const float4 *mean_lo;   // K: float(mean - float(mean)) xyz (x' = (x - hi) - lo)
     float s_max;             // largest float s with sqrtf(s) < res (the radius test without sqrt)
     float inv_res;           // 1 / res when res is a power of two (exact), else 0 (divide)
+    float radius_final;      // (float)(res + 0.001f): the probe loop bound of kernel.cpp:254
     const float4 *icov32;    // 2K: {c00 c01 c02 c11}, {c12 c22 0 0} (symmetrised, FP32)
     const double *icov64;    // 9K: inverse covariance as the reference stores it (row major)
 };

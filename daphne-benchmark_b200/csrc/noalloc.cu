@@ -50,7 +50,7 @@ struct NoAllocScratch {
     int num_tiles;
     unsigned flag_n;
     int flag_overflow;
-    int pad;
+    int work_counter;
     double exc[kPartial];
     Tile tiles[kNoAllocMaxTiles];
     int4 flag_q[kNoAllocFlagCap];
@@ -181,6 +181,8 @@ extern "C" int ndt_derivatives_noalloc(ndt_ctx *ctx, const float *d_scan, const 
     ea.flag_n = &s->flag_n;
     ea.flag_cap = kNoAllocFlagCap;
     ea.flag_overflow = &s->flag_overflow;
+    ea.work_counter = &s->work_counter;
+    ea.chunk_tiles = 4;
     rc = launch_derivatives(ea, v.precision, v.variant, v.sms, st);
     if (rc) {
         ctx_set_error(ctx, cudaGetErrorString((cudaError_t)rc));

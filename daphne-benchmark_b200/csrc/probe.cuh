@@ -1,0 +1,274 @@
+// Shared device code of the derivative pass: the reference's neighbour
+// search (voxelRadiusSearch, src/CPU/ndt_mapping/kernel.cpp:246-286) per
+// point, with the pair list it feeds, and the block-reduction helpers.
+//
+// Every operation whose rounding decides which (point, voxel) pairs the
+// reference accepts is written with explicit round-to-nearest intrinsics
+// (__fadd_rn, __fsub_rn, __fmul_rn, __fdiv_rn), so this code gives the
+// reference's pairs whether or not the including file is compiled with
+// floating-point contraction.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "derivatives.h"
+#include "ndt_math.cuh"
+
+namespace ndt {
+
+constexpr int kAcc = 37;        // FP32 sums: score, g[6], S[21], R[9]
+constexpr int kTerms = 23;      // per-point terms (see below)
+constexpr int kList = 27 * 32;  // per-warp pair list: all 27 probes of all 32 lanes
+constexpr unsigned kFull = 0xffffffffu;
+
+// Per-point terms (point Jacobian columns 3-5 and point Hessian blocks), FP32.
+// Index: 0 J13, 1 J23, 2 J04, 3 J14, 4 J24, 5 J05, 6 J15, 7 J25,
+//        8 a1, 9 a2, 10 b1, 11 b2, 12 c1, 13 c2, 14-16 d, 17-19 e, 20-22 f.
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__device__ __forceinline__ double4 ldg_d4(const double4 *p) {
+    const double2 *q = reinterpret_cast<const double2 *>(p);
+    double2 a = __ldg(q), b = __ldg(q + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
+__device__ __forceinline__ float dot3f(float a0, float a1, float a2, const float *b) {
+    return fmaf(a0, b[0], fmaf(a1, b[1], a2 * b[2]));
+}
+
+// transformPointCloud (kernel.cpp:397-400): T[r][0] x + T[r][1] y + T[r][2] z
+// + T[r][3], float, left to right, every operation rounded.
+__device__ __forceinline__ float transform_row(const float *T, float x, float y, float z) {
+    return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(T[0], x), __fmul_rn(T[1], y)), __fmul_rn(T[2], z)), T[3]);
+}
+
+// ---------------------------------------------------------------------------
+// Probe geometry of one axis: the reference's float loop
+//   for (float v = p - r; v <= p + rf; v += res)           (kernel.cpp:256-258)
+// The start (float)((double)p - r) equals the float subtraction p - r: the
+// double difference of two floats is exact (for |p| < 2^28 r), so both round
+// the exact difference once.  The loop gives 3 coordinates for any finite |p|
+// below ~1e6 m (trip count n; n = 4 only for larger or infinite
+// coordinates, handled by the generic path).  For each coordinate: inside
+// the bbox (kernel.cpp:261-269) and its cell index (linearizeCoord, :239-241).
+struct Axis {
+    float c0, c1, c2;
+    int i0, i1, i2;
+    unsigned in;  // bit k: coordinate k is active and inside the bbox
+    int n;
+};
+
+__device__ __forceinline__ int cell_component(float v, float minv, float res, float inv_res) {
+    const float d = __fsub_rn(v, minv);
+    return inv_res > 0.0f ? (int)__fmul_rn(d, inv_res) : (int)__fdiv_rn(d, res);
+}
+
+__device__ __forceinline__ Axis make_axis(float p, float minv, float maxv, float res, float inv_res, float rf,
+                                          bool valid) {
+    Axis a;
+    a.c0 = __fsub_rn(p, res);
+    a.c1 = __fadd_rn(a.c0, res);
+    a.c2 = __fadd_rn(a.c1, res);
+    const float c3 = __fadd_rn(a.c2, res);
+    const float lim = __fadd_rn(p, rf);
+    // the coordinates increase, so the trip count is the number that pass
+    int n = 0;
+    if (valid) n = (a.c0 <= lim) + (a.c1 <= lim) + (a.c2 <= lim) + (c3 <= lim);
+    a.n = n;
+    unsigned in = 0;
+    if (n > 0 && !(a.c0 < minv || a.c0 > maxv)) in |= 1u;
+    if (n > 1 && !(a.c1 < minv || a.c1 > maxv)) in |= 2u;
+    if (n > 2 && !(a.c2 < minv || a.c2 > maxv)) in |= 4u;
+    a.in = in;
+    a.i0 = (in & 1u) ? cell_component(a.c0, minv, res, inv_res) : 0;
+    a.i1 = (in & 2u) ? cell_component(a.c1, minv, res, inv_res) : 0;
+    a.i2 = (in & 4u) ? cell_component(a.c2, minv, res, inv_res) : 0;
+    return a;
+}
+
+__device__ __forceinline__ int axis_i(const Axis &a, int k) { return k == 0 ? a.i0 : (k == 1 ? a.i1 : a.i2); }
+
+// Margin of the FP32 pre-test of the radius check for a point p: the FP32
+// difference hi - p and the reference's float(mean - p) (FP64 mean) differ by
+// at most E = 2^-23 (|m| + |dx|) per axis, and a candidate mean lies within
+// 3r of p, so |m| <= |p| + 3r; the squared distances then differ by at most
+// sum_axes 2 E (|dx| + E) <= 20 r E + 3 E^2 with E = 2^-23 (|p|_1 + 14 r + 1).
+__device__ __forceinline__ float radius_margin(float px, float py, float pz, float res) {
+    const float E = 1.2e-7f * (fabsf(px) + fabsf(py) + fabsf(pz) + 14.0f * res + 1.0f);
+    return 20.0f * res * E + 3.0f * E * E;
+}
+
+// The reference's distance test float(sqrt(dx^2 + dy^2 + dz^2)) < r,
+// dx = float(mean - p) on the FP64 mean (kernel.cpp:273-278), decided as
+// s <= s_max (the largest float whose correctly rounded root is below r):
+// first with the FP32 mean and the margin tol, then, inside the margin,
+// exactly on the FP64 mean.
+__device__ __forceinline__ bool accept(const GridDev &grid, int slot, float4 hi, float px, float py, float pz,
+                                       float tol) {
+    const float s_max = grid.s_max;
+    const float fx = hi.x - px, fy = hi.y - py, fz = hi.z - pz;
+    const float sf = fmaf(fx, fx, fmaf(fy, fy, fz * fz));
+    if (sf < s_max - tol) return true;
+    if (sf > s_max + tol) return false;
+    const double4 m = ldg_d4(grid.mean + slot);
+    const float dx = (float)(m.x - (double)px);
+    const float dy = (float)(m.y - (double)py);
+    const float dz = (float)(m.z - (double)pz);
+    const float s = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+    return s <= s_max;
+}
+
+__device__ __forceinline__ unsigned pair_code(int v, int lane) {
+    return ((unsigned)(v & kSlotMask) << 6) | ((v & kSlotFlag) ? 32u : 0u) | (unsigned)lane;
+}
+
+// Probe every lane's point in the reference's order (z outer, x inner) and
+// collect the accepted pairs in `list` (capacity 27 x 32), then call
+// consume(n) for list[0, n) (the generic path also calls it whenever the list
+// could overflow).  List code = slot << 6 | flag << 5 | lane.  Work that no
+// lane of the warp needs is skipped with warp-uniform branches: layers with no
+// in-bounds probe, layers with no occupied cell, distance tests of a probe no
+// lane occupies, list appends of a probe no lane accepted.
+template <class Consume>
+__device__ __forceinline__ void probe_point(const GridDev &grid, float px, float py, float pz, bool valid,
+                                            unsigned *list, unsigned &n_probe, unsigned &n_occ, Consume consume) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = lanemask_lt();
+    const GridMeta &g = grid.meta;
+    const float res = g.res, inv_res = grid.inv_res, rf = grid.radius_final;
+    const Axis ax = make_axis(px, g.minv[0], g.maxv[0], res, inv_res, rf, valid);
+    const Axis ay = make_axis(py, g.minv[1], g.maxv[1], res, inv_res, rf, valid);
+    const Axis az = make_axis(pz, g.minv[2], g.maxv[2], res, inv_res, rf, valid);
+    const bool any_in = (ax.in != 0u) && (ay.in != 0u) && (az.in != 0u);
+    if (!__any_sync(kFull, any_in)) return;
+    const int mx = __reduce_max_sync(kFull, ax.n), my = __reduce_max_sync(kFull, ay.n),
+              mz = __reduce_max_sync(kFull, az.n);
+    const float tol = radius_margin(px, py, pz, res);
+    int n = 0;
+    if (mx <= 3 && my <= 3 && mz <= 3) {
+#pragma unroll 1
+        for (int a = 0; a < 3; ++a) {
+            const bool za = any_in && ((az.in >> a) & 1u);
+            if (!__any_sync(kFull, za)) continue;
+            const int zbase = g.dim[1] * axis_i(az, a);
+            int v[9];
+            unsigned on_mask = 0, occ = 0;
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                const bool yb = za && ((ay.in >> b) & 1u);
+                const int base = g.dim[0] * (axis_i(ay, b) + zbase);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const bool on = yb && ((ax.in >> c) & 1u);
+                    v[3 * b + c] = on ? __ldg(grid.index + (axis_i(ax, c) + base)) : -1;
+                    on_mask |= (unsigned)on << (3 * b + c);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 9; ++k) occ |= (unsigned)(v[k] >= 0) << k;
+            n_probe += __popc(on_mask);
+            n_occ += __popc(occ);
+            if (!__any_sync(kFull, occ != 0u)) continue;
+            float4 hi[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k)
+                if ((occ >> k) & 1u) hi[k] = __ldg(grid.mean_hi + (v[k] & kSlotMask));
+            unsigned acc = 0;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                if (__any_sync(kFull, (occ >> k) & 1u)) {
+                    const bool ok = ((occ >> k) & 1u) && accept(grid, v[k] & kSlotMask, hi[k], px, py, pz, tol);
+                    acc |= (unsigned)ok << k;
+                }
+            }
+            if (!__any_sync(kFull, acc != 0u)) continue;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                const bool ok = (acc >> k) & 1u;
+                const unsigned bal = __ballot_sync(kFull, ok);
+                if (bal) {
+                    if (ok) list[n + __popc(bal & lt)] = pair_code(v[k], lane);
+                    n += __popc(bal);
+                }
+            }
+        }
+        __syncwarp();
+        consume(n);
+        __syncwarp();
+        return;
+    }
+    // generic path: trip counts up to 4 (coordinates beyond ~1e6 m or inf)
+    float zc = az.c0;
+    for (int a = 0; a < mz; ++a, zc = __fadd_rn(zc, res)) {
+        float yc = ay.c0;
+        for (int b = 0; b < my; ++b, yc = __fadd_rn(yc, res)) {
+            float xc = ax.c0;
+            for (int c = 0; c < mx; ++c, xc = __fadd_rn(xc, res)) {
+                const bool act = a < az.n && b < ay.n && c < ax.n;
+                const bool inb = act && !((xc < g.minv[0]) || (xc > g.maxv[0]) || (yc < g.minv[1]) ||
+                                          (yc > g.maxv[1]) || (zc < g.minv[2]) || (zc > g.maxv[2]));
+                int v = -1;
+                if (inb) {
+                    v = __ldg(grid.index + (cell_component(xc, g.minv[0], res, inv_res) +
+                                            g.dim[0] * (cell_component(yc, g.minv[1], res, inv_res) +
+                                                        g.dim[1] * cell_component(zc, g.minv[2], res, inv_res))));
+                    ++n_probe;
+                }
+                bool ok = false;
+                if (v >= 0) {
+                    ++n_occ;
+                    ok = accept(grid, v & kSlotMask, __ldg(grid.mean_hi + (v & kSlotMask)), px, py, pz, tol);
+                }
+                if (n > kList - 32) {
+                    __syncwarp();
+                    consume(n);
+                    __syncwarp();
+                    n = 0;
+                }
+                const unsigned bal = __ballot_sync(kFull, ok);
+                if (ok) list[n + __popc(bal & lt)] = pair_code(v, lane);
+                n += __popc(bal);
+            }
+        }
+    }
+    __syncwarp();
+    consume(n);
+    __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// Reduction helpers.
+__device__ __forceinline__ void warp_two_sum_reduce(float &s, float &e) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        float so = __shfl_xor_sync(kFull, s, o);
+        float eo = __shfl_xor_sync(kFull, e, o);
+        float t, err;
+        two_sum(s, so, t, err);
+        s = t;
+        e = __fadd_rn(__fadd_rn(e, eo), err);
+    }
+}
+
+__device__ __forceinline__ int sidx(int i, int j) {  // upper-triangle index, i <= j
+    return i * 6 - (i * (i - 1)) / 2 + (j - i);
+}
+
+// Tile partial layout: [0] score, [1..6] g, [7..42] H row major, [43] pairs.
+// H_ij = S_ij + kR R_ij from the FP32 sums (see derivatives_f32.cu).
+__device__ __forceinline__ double h_entry(const double *tot, int i, int j, double kR, bool compat) {
+    double v = tot[7 + (i <= j ? sidx(i, j) : sidx(j, i))];
+    if (i >= 3 && j >= 3) {
+        int a = i - 3, b = j - 3;
+        double r = compat ? tot[28 + 3 * a + b] : tot[28 + 3 * (a < b ? a : b) + (a < b ? b : a)];
+        v += kR * r;
+    }
+    return v;
+}
+
+}  // namespace ndt

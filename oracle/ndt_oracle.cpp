@@ -580,6 +580,8 @@ struct Aligner {
     float final_T[16];
     int evals = 0;
     long long pairs = 0;
+    long long *eval_pairs = nullptr;  // optional per-evaluation pair counts
+    int eval_pairs_cap = 0;
 
     Aligner(const ndt_params &p, const Grid &g, Gauss gauss)
         : prm(p), grid(g), compat(p.compat != 0), gs(gauss) {}
@@ -594,6 +596,14 @@ struct Aligner {
 
     // computeDerivatives (kernel.cpp:651-705) / computeHessian (:562-602).
     double derivatives(double *g6, double *H36, const double *p, bool hess, bool hessian_only) {
+        const long long pairs_before = pairs;
+        struct Log {
+            Aligner *a;
+            long long before;
+            ~Log() {
+                if (a->eval_pairs && a->evals - 1 < a->eval_pairs_cap) a->eval_pairs[a->evals - 1] = a->pairs - before;
+            }
+        } log_guard{this, pairs_before};
         ++evals;
         if (!hessian_only) std::memset(g6, 0, sizeof(double) * 6);
         std::memset(H36, 0, sizeof(double) * 36);
@@ -780,6 +790,23 @@ ORACLE_API int oracle_align(const ndt_params *prm, const float *scan, int n, con
     a.run(scan, n, guess16, out16, converged, fitness);
     if (evals) *evals = a.evals;
     return NDT_OK;
+}
+
+// Per-evaluation (point, voxel) pair counts of one alignment (diagnostics).
+ORACLE_API int oracle_align_trace(const ndt_params *prm, const float *scan, int n, const float *guess16,
+                                  const float *map, int m, long long *pairs, int cap) {
+    Grid g;
+    if (!build_grid(*prm, g, map, m)) return NDT_E_GRID;
+    Gauss gs;
+    gauss_consts(*prm, gs);
+    Aligner a(*prm, g, gs);
+    a.eval_pairs = pairs;
+    a.eval_pairs_cap = cap;
+    float out[16];
+    int conv;
+    double fit;
+    a.run(scan, n, guess16, out, &conv, &fit);
+    return a.evals;
 }
 
 ORACLE_API int oracle_align_batch(const ndt_params *prm, int B, const float *const *scans,
