@@ -265,8 +265,8 @@ def run_ours(args, pkg, world, rank, local):
     points = np.ascontiguousarray(np.concatenate([a.scan for a in aligns]))
     guesses = np.ascontiguousarray(np.stack([a.guess for a in aligns]).astype(np.float32))
     M = scene.map.shape[0]
-    prm = ndt.reference_params(cfg.resolution, args.precision) if args.mode == "compat" else \
-        ndt.corrected_params(cfg.resolution, args.precision)
+    prm = ndt.reference_params(cfg.resolution, args.precision, args.dense_probe) if args.mode == "compat" else \
+        ndt.corrected_params(cfg.resolution, args.precision, args.dense_probe)
     ctx = ndt.Context(prm, device=local)
     ctx.set_profiling(True)
     st = torch.cuda.ExternalStream(ctx.stream, device=dev)
@@ -453,6 +453,8 @@ def main(argv=None):
     ap.add_argument("--precision", type=int, choices=[0, 1], default=0)
     ap.add_argument("--variant", default="auto",
                     help="derivative-pass launch shape: an index, or 'auto' (autotuned on the workload)")
+    ap.add_argument("--dense-probe", type=int, choices=[0, 1], default=0,
+                    help="1: probe the dense cell index (27 cells per point) instead of the probe-window table")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -4,27 +4,24 @@
 // computePointDerivatives :495-560 and updateDerivatives :438-493 fused in).
 //
 // Work decomposition: the tile list holds ceil(n_a / TILE) tiles of TILE
-// consecutive points per alignment.  Block b of the persistent grid owns the
-// contiguous tile range [b * per, (b + 1) * per), so the tiles of one
-// alignment are met in a row; each lane keeps its FP32 sums of the current
+// consecutive points per alignment, handed out to the persistent blocks in
+// chunks of consecutive tiles.  Each lane keeps its FP32 sums of the current
 // alignment in shared memory and the block reduces them once per alignment
 // run (TwoSum-compensated across lanes and warps), writing the run's FP64
 // partial to the slot of its first tile (the run's other slots get zeros).
 //
 // Per point (one thread): the float transform and the reference's neighbour
-// search of probe.cuh (exact: the accepted pairs are the reference's); the
-// accepted pairs are compacted per warp in shared memory and evaluated one per
-// lane, so the per-pair work is balanced across lanes.
-// Per pair: x' from the (hi, lo) float split of the FP64 mean, q = C x', xCx,
-// e = exp(-d2 xCx / 2), the validity test of :456, gradient a_i = x'^T C J_i
-// and the Hessian split as
-//   H_ij = S_ij + k R_ij,  S_ij = w (-d2 a_i a_j + J_j^T C J_i)   (i <= j)
-//   compat:    R_ij = w a_i b_ij, k = -d2  (the reference's :486-488 form)
-//   corrected: R_ij = w b_ij,     k = 1    (Magnusson eq. 6.13)
-// with b_ij = x'^T C H_ij (nonzero for i, j >= 3 only).  Voxels flagged by the
-// grid build (inverse-covariance entries non-finite or beyond 1e30) are queued
-// and evaluated in FP64 by flagged_kernel, so that infinities and NaNs
-// propagate as in the reference.
+// search of probe.cuh (exact: the accepted pairs are the reference's), each
+// lane's pairs in its own column of shared memory.  Then, per warp:
+//   dense  (more than 40 pairs in the warp): each lane sums its own pairs
+//          into 16 FP32 point sums and contracts them with its point's
+//          Jacobian and Hessian terms once (factored form below);
+//   sparse: the pairs are appended to a per-warp ring and evaluated 32 at a
+//          time, one pair per lane, each contracted on its own; the ring is
+//          emptied at the end of the alignment run.
+// Voxels flagged by the grid build (inverse-covariance entries non-finite or
+// beyond 1e30) are queued and evaluated in FP64 by flagged_kernel, so that
+// infinities and NaNs propagate as in the reference.
 //
 // This file is compiled with floating-point contraction (the pair arithmetic
 // is FP32 with FMA); the exact parts live in probe.cuh with explicit
@@ -41,17 +38,36 @@ namespace ndt {
 namespace {
 
 // ---------------------------------------------------------------------------
-// FP32 pair evaluation.
-struct AccF {
-    float v[kAcc];
+// FP32 pair evaluation, factored through the point.
+//
+// For a point x with Jacobian J (3 x 6; columns e0, e1, e2, J_3, J_4, J_5) and
+// point-Hessian vectors h_ij (i, j >= 3), the pairs (x, voxel v) contribute,
+// with x' = x_trans - mean_v, C = C_v, q = C x', e = exp(-d2 x'^T q / 2),
+// w = d1 d2 e (kept when 0 <= d2 e <= 1, kernel.cpp:456) and a_i = q . J_i:
+//   score   sum -d1 e
+//   g_i     sum w a_i                              = J_i . U
+//   S_ij    sum w (-d2 a_i a_j + J_j^T C J_i)      = J_i^T (W - d2 Q) J_j
+//   R_ij    compat:    sum w a_i (q . h_ij)        = J_i^T Q h_ij
+//           corrected: sum w (q . h_ij)            = U . h_ij
+// with the point's sums U = sum w q, Q = sum w q q^T, W = sum w C.  A pair
+// therefore costs 16 FMA-type sums (PairSums) and a point one contraction
+// with its J and h (contract_add), however many pairs it has.  H = S + k R,
+// k = -d2 (compat, the reference's :486-488 form) or 1 (corrected, Magnusson
+// eq. 6.13), is assembled from the block totals.
+struct PairSums {
+    float s, u0, u1, u2;
+    float q00, q01, q02, q11, q12, q22;
+    float w00, w01, w02, w11, w12, w22;
 };
 
-__device__ __forceinline__ int sidx(int i, int j) {  // upper-triangle index, i <= j
-    return i * 6 - (i * (i - 1)) / 2 + (j - i);
+__device__ __forceinline__ void zero(PairSums &F) {
+    F.s = F.u0 = F.u1 = F.u2 = 0.0f;
+    F.q00 = F.q01 = F.q02 = F.q11 = F.q12 = F.q22 = 0.0f;
+    F.w00 = F.w01 = F.w02 = F.w11 = F.w12 = F.w22 = 0.0f;
 }
 
-__device__ __forceinline__ void pair_fp32(AccF &A, const float (*terms)[32], int owner, float p0, float p1, float p2,
-                                          float4 ca, float4 cb, float d1, float d2, bool hess, bool compat) {
+__device__ __forceinline__ void pair_sums(PairSums &F, float p0, float p1, float p2, float4 ca, float4 cb, float d1,
+                                          float d2, bool hess) {
     const float c00 = ca.x, c01 = ca.y, c02 = ca.z, c11 = ca.w, c12 = cb.x, c22 = cb.y;
     const float q0 = fmaf(c00, p0, fmaf(c01, p1, c02 * p2));
     const float q1 = fmaf(c01, p0, fmaf(c11, p1, c12 * p2));
@@ -61,72 +77,121 @@ __device__ __forceinline__ void pair_fp32(AccF &A, const float (*terms)[32], int
     const float e2 = d2 * e;
     if (!(e2 <= 1.0f && e2 >= 0.0f)) return;  // kernel.cpp:456 (also rejects NaN)
     const float w = d1 * e2;
-    A.v[0] += -d1 * e;
-    // M_i = C J_i for i = 3, 4, 5
-    const float J13 = terms[0][owner], J23 = terms[1][owner], J04 = terms[2][owner], J14 = terms[3][owner];
-    const float J24 = terms[4][owner], J05 = terms[5][owner], J15 = terms[6][owner], J25 = terms[7][owner];
-    const float M30 = fmaf(c01, J13, c02 * J23), M31 = fmaf(c11, J13, c12 * J23), M32 = fmaf(c12, J13, c22 * J23);
-    const float M40 = fmaf(c00, J04, fmaf(c01, J14, c02 * J24));
-    const float M41 = fmaf(c01, J04, fmaf(c11, J14, c12 * J24));
-    const float M42 = fmaf(c02, J04, fmaf(c12, J14, c22 * J24));
-    const float M50 = fmaf(c00, J05, fmaf(c01, J15, c02 * J25));
-    const float M51 = fmaf(c01, J05, fmaf(c11, J15, c12 * J25));
-    const float M52 = fmaf(c02, J05, fmaf(c12, J15, c22 * J25));
-    float a[6];
-    a[0] = q0;
-    a[1] = q1;
-    a[2] = q2;
-    a[3] = fmaf(p0, M30, fmaf(p1, M31, p2 * M32));
-    a[4] = fmaf(p0, M40, fmaf(p1, M41, p2 * M42));
-    a[5] = fmaf(p0, M50, fmaf(p1, M51, p2 * M52));
-    float u[6];
-#pragma unroll
-    for (int i = 0; i < 6; ++i) {
-        u[i] = w * a[i];
-        A.v[1 + i] += u[i];
-    }
+    F.s = fmaf(-d1, e, F.s);
+    const float wq0 = w * q0, wq1 = w * q1, wq2 = w * q2;
+    F.u0 += wq0;
+    F.u1 += wq1;
+    F.u2 += wq2;
     if (!hess) return;
-    // column vectors M_i (i < 3: columns of C)
-    const float M[6][3] = {{c00, c01, c02}, {c01, c11, c12}, {c02, c12, c22},
-                           {M30, M31, M32}, {M40, M41, M42}, {M50, M51, M52}};
-    // J_j . M_i
-    auto jm = [&](int j, int i) -> float {
-        switch (j) {
-            case 0: return M[i][0];
-            case 1: return M[i][1];
-            case 2: return M[i][2];
-            case 3: return fmaf(J13, M[i][1], J23 * M[i][2]);
-            case 4: return fmaf(J04, M[i][0], fmaf(J14, M[i][1], J24 * M[i][2]));
-            default: return fmaf(J05, M[i][0], fmaf(J15, M[i][1], J25 * M[i][2]));
-        }
-    };
+    F.q00 = fmaf(wq0, q0, F.q00);
+    F.q01 = fmaf(wq0, q1, F.q01);
+    F.q02 = fmaf(wq0, q2, F.q02);
+    F.q11 = fmaf(wq1, q1, F.q11);
+    F.q12 = fmaf(wq1, q2, F.q12);
+    F.q22 = fmaf(wq2, q2, F.q22);
+    F.w00 = fmaf(w, c00, F.w00);
+    F.w01 = fmaf(w, c01, F.w01);
+    F.w02 = fmaf(w, c02, F.w02);
+    F.w11 = fmaf(w, c11, F.w11);
+    F.w12 = fmaf(w, c12, F.w12);
+    F.w22 = fmaf(w, c22, F.w22);
+}
+
+// Symmetric 3 x 3 (m00 m01 m02 m11 m12 m22) times v.
+__device__ __forceinline__ void sym_mul(float m00, float m01, float m02, float m11, float m12, float m22, float v0,
+                                        float v1, float v2, float &r0, float &r1, float &r2) {
+    r0 = fmaf(m00, v0, fmaf(m01, v1, m02 * v2));
+    r1 = fmaf(m01, v0, fmaf(m11, v1, m12 * v2));
+    r2 = fmaf(m02, v0, fmaf(m12, v1, m22 * v2));
+}
+
+// Adds a point's contribution (its PairSums F contracted with its J and h) to
+// the lane's accumulators acc[k * stride]: [0] score, [1..6] g, [7..27] S
+// (upper triangle), [28..36] R (compat: 3 x 3; corrected: upper triangle).
+// ang = the alignment's FP32 angle terms (j_ang a..h, h_ang a2..f3, 3 each).
+__device__ __forceinline__ void contract_add(const PairSums &F, float x0, float x1, float x2, const float *ang,
+                                             float *acc, int stride, float d2, bool hess, bool compat) {
+    // J_3 = (0, J13, J23), J_4 = (J04, J14, J24), J_5 = (J05, J15, J25)
+    // (computePointDerivatives, kernel.cpp:512-521)
+    const float J13 = dot3f(x0, x1, x2, ang + 0), J23 = dot3f(x0, x1, x2, ang + 3);
+    const float J04 = dot3f(x0, x1, x2, ang + 6), J14 = dot3f(x0, x1, x2, ang + 9);
+    const float J24 = dot3f(x0, x1, x2, ang + 12), J05 = dot3f(x0, x1, x2, ang + 15);
+    const float J15 = dot3f(x0, x1, x2, ang + 18), J25 = dot3f(x0, x1, x2, ang + 21);
+    acc[0] += F.s;
+    acc[1 * stride] += F.u0;
+    acc[2 * stride] += F.u1;
+    acc[3 * stride] += F.u2;
+    acc[4 * stride] += fmaf(J13, F.u1, J23 * F.u2);
+    acc[5 * stride] += fmaf(J04, F.u0, fmaf(J14, F.u1, J24 * F.u2));
+    acc[6 * stride] += fmaf(J05, F.u0, fmaf(J15, F.u1, J25 * F.u2));
+    if (!hess) return;
+    // P = W - d2 Q
     const float nd2 = -d2;
-#pragma unroll
-    for (int i = 0; i < 6; ++i) {
-        const float ui = nd2 * u[i];
-#pragma unroll
-        for (int j = i; j < 6; ++j) A.v[7 + sidx(i, j)] += fmaf(ui, a[j], w * jm(j, i));
-    }
-    // b_ij = q . H_ij, i, j in 3..5
-#define T_(k) terms[k][owner]
-    const float b33 = fmaf(q1, T_(8), q2 * T_(9));
-    const float b34 = fmaf(q1, T_(10), q2 * T_(11));
-    const float b35 = fmaf(q1, T_(12), q2 * T_(13));
-    const float b44 = fmaf(q0, T_(14), fmaf(q1, T_(15), q2 * T_(16)));
-    const float b45 = fmaf(q0, T_(17), fmaf(q1, T_(18), q2 * T_(19)));
-    const float b55 = fmaf(q0, T_(20), fmaf(q1, T_(21), q2 * T_(22)));
-#undef T_
-    const float B[3][3] = {{b33, b34, b35}, {b34, b44, b45}, {b35, b45, b55}};
+    const float P00 = fmaf(nd2, F.q00, F.w00), P01 = fmaf(nd2, F.q01, F.w01), P02 = fmaf(nd2, F.q02, F.w02);
+    const float P11 = fmaf(nd2, F.q11, F.w11), P12 = fmaf(nd2, F.q12, F.w12), P22 = fmaf(nd2, F.q22, F.w22);
+    float a0, a1, a2, b0, b1, b2, c0, c1, c2;  // P J_3, P J_4, P J_5
+    sym_mul(P00, P01, P02, P11, P12, P22, 0.0f, J13, J23, a0, a1, a2);
+    sym_mul(P00, P01, P02, P11, P12, P22, J04, J14, J24, b0, b1, b2);
+    sym_mul(P00, P01, P02, P11, P12, P22, J05, J15, J25, c0, c1, c2);
+    float *S = acc + 7 * stride;  // sidx order: (0,0..5), (1,1..5), (2,2..5), (3,3..5), (4,4..5), (5,5)
+    S[0 * stride] += P00;
+    S[1 * stride] += P01;
+    S[2 * stride] += P02;
+    S[3 * stride] += a0;
+    S[4 * stride] += b0;
+    S[5 * stride] += c0;
+    S[6 * stride] += P11;
+    S[7 * stride] += P12;
+    S[8 * stride] += a1;
+    S[9 * stride] += b1;
+    S[10 * stride] += c1;
+    S[11 * stride] += P22;
+    S[12 * stride] += a2;
+    S[13 * stride] += b2;
+    S[14 * stride] += c2;
+    S[15 * stride] += fmaf(J13, a1, J23 * a2);
+    S[16 * stride] += fmaf(J13, b1, J23 * b2);
+    S[17 * stride] += fmaf(J13, c1, J23 * c2);
+    S[18 * stride] += fmaf(J04, b0, fmaf(J14, b1, J24 * b2));
+    S[19 * stride] += fmaf(J04, c0, fmaf(J14, c1, J24 * c2));
+    S[20 * stride] += fmaf(J05, c0, fmaf(J15, c1, J25 * c2));
+    // point-Hessian vectors (computePointDerivatives, kernel.cpp:523-558):
+    // h33 = (0, a2, a3), h34 = (0, b2, b3), h35 = (0, c2, c3), h44 = d,
+    // h45 = e, h55 = f
+    const float *h = ang + 24;
+    const float h33y = dot3f(x0, x1, x2, h + 0), h33z = dot3f(x0, x1, x2, h + 3);
+    const float h34y = dot3f(x0, x1, x2, h + 6), h34z = dot3f(x0, x1, x2, h + 9);
+    const float h35y = dot3f(x0, x1, x2, h + 12), h35z = dot3f(x0, x1, x2, h + 15);
+    const float h44x = dot3f(x0, x1, x2, h + 18), h44y = dot3f(x0, x1, x2, h + 21), h44z = dot3f(x0, x1, x2, h + 24);
+    const float h45x = dot3f(x0, x1, x2, h + 27), h45y = dot3f(x0, x1, x2, h + 30), h45z = dot3f(x0, x1, x2, h + 33);
+    const float h55x = dot3f(x0, x1, x2, h + 36), h55y = dot3f(x0, x1, x2, h + 39), h55z = dot3f(x0, x1, x2, h + 42);
+    float *R = acc + 28 * stride;
     if (compat) {
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) A.v[28 + 3 * i + j] += u[3 + i] * B[i][j];
+        // R[a][b] = J_{3+a} . (Q h_{3+a,3+b})
+        float t0, t1, t2;
+        sym_mul(F.q00, F.q01, F.q02, F.q11, F.q12, F.q22, 0.0f, h33y, h33z, t0, t1, t2);
+        R[0] += fmaf(J13, t1, J23 * t2);
+        sym_mul(F.q00, F.q01, F.q02, F.q11, F.q12, F.q22, 0.0f, h34y, h34z, t0, t1, t2);
+        R[1 * stride] += fmaf(J13, t1, J23 * t2);
+        R[3 * stride] += fmaf(J04, t0, fmaf(J14, t1, J24 * t2));
+        sym_mul(F.q00, F.q01, F.q02, F.q11, F.q12, F.q22, 0.0f, h35y, h35z, t0, t1, t2);
+        R[2 * stride] += fmaf(J13, t1, J23 * t2);
+        R[6 * stride] += fmaf(J05, t0, fmaf(J15, t1, J25 * t2));
+        sym_mul(F.q00, F.q01, F.q02, F.q11, F.q12, F.q22, h44x, h44y, h44z, t0, t1, t2);
+        R[4 * stride] += fmaf(J04, t0, fmaf(J14, t1, J24 * t2));
+        sym_mul(F.q00, F.q01, F.q02, F.q11, F.q12, F.q22, h45x, h45y, h45z, t0, t1, t2);
+        R[5 * stride] += fmaf(J04, t0, fmaf(J14, t1, J24 * t2));
+        R[7 * stride] += fmaf(J05, t0, fmaf(J15, t1, J25 * t2));
+        sym_mul(F.q00, F.q01, F.q02, F.q11, F.q12, F.q22, h55x, h55y, h55z, t0, t1, t2);
+        R[8 * stride] += fmaf(J05, t0, fmaf(J15, t1, J25 * t2));
     } else {
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = i; j < 3; ++j) A.v[28 + 3 * i + j] += w * B[i][j];
+        // R[a][b] = U . h_{3+a,3+b}, a <= b
+        R[0] += fmaf(F.u1, h33y, F.u2 * h33z);
+        R[1 * stride] += fmaf(F.u1, h34y, F.u2 * h34z);
+        R[2 * stride] += fmaf(F.u1, h35y, F.u2 * h35z);
+        R[4 * stride] += fmaf(F.u0, h44x, fmaf(F.u1, h44y, F.u2 * h44z));
+        R[5 * stride] += fmaf(F.u0, h45x, fmaf(F.u1, h45y, F.u2 * h45z));
+        R[8 * stride] += fmaf(F.u0, h55x, fmaf(F.u1, h55y, F.u2 * h55z));
     }
 }
 
@@ -211,12 +276,14 @@ __global__ void flagged_kernel(EvalArgs args) {
 }
 
 // Dynamic shared memory of the FP32 kernel (W warps).
+constexpr int kDefer = 128;           // per-warp ring of deferred pairs (power of two)
+constexpr int kDenseThreshold = 40;   // a warp with more pairs than this evaluates them per point
+
 template <int W>
 struct F32Smem {
-    float acc[kAcc][W * 32];      // per-lane sums of the current alignment run
-    float terms[W][kTerms][32];   // per-point terms of each warp's 32 points
-    float xt[W][3][32];           // transformed points
-    unsigned list[W][kList];      // accepted pairs of the current tile
+    float acc[kAcc][W * 32];         // per-lane sums of the current alignment run
+    unsigned own[W][kOwn][32];       // each lane's accepted pairs of the current tile
+    uint2 defer[W][kDefer];          // deferred pairs: (slot << 6 | flag << 5, point index)
 };
 
 // Block-wide reduction of the per-lane sums of one alignment run, written as
@@ -261,6 +328,68 @@ __device__ void reduce_run(F32Smem<W> &sm, double *s_tot, const unsigned (*s_cnt
     }
 }
 
+// Per-warp context of the pair evaluation.
+struct WarpPairs {
+    const EvalArgs *args;
+    const GridDev *grid;
+    const float *T;      // the alignment's transform (shared memory)
+    const float *ang;    // its FP32 angle terms (shared memory)
+    float *acc;          // this lane's accumulators, stride = block size
+    int stride;
+    int align;
+    float d1, d2;
+    bool hess, compat;
+};
+
+// Queues a pair with a flagged voxel for flagged_kernel (FP64).
+__device__ __forceinline__ void queue_flagged(const EvalArgs &args, int align, int point, int slot) {
+    const unsigned q = atomicAdd(args.flag_n, 1u);
+    if (q < args.flag_cap) args.flag_q[q] = make_int4(align, point, slot, 0);
+}
+
+// x' = x_trans - mean (kernel.cpp:692-694) from the (hi, lo) float split of
+// the FP64 mean, and the pair's sums.
+__device__ __forceinline__ void add_pair(const WarpPairs &P, PairSums &F, int slot, float px, float py, float pz) {
+    const GridDev &g = *P.grid;
+    const float4 hi = __ldg(g.mean_hi + slot);
+    const float4 lo = __ldg(g.mean_lo + slot);
+    const float4 ca = __ldg(g.icov32 + 2 * slot);
+    const float4 cb = __ldg(g.icov32 + 2 * slot + 1);
+    const float p0 = __fsub_rn(__fsub_rn(px, hi.x), lo.x);
+    const float p1 = __fsub_rn(__fsub_rn(py, hi.y), lo.y);
+    const float p2 = __fsub_rn(__fsub_rn(pz, hi.z), lo.z);
+    pair_sums(F, p0, p1, p2, ca, cb, P.d1, P.d2, P.hess);
+}
+
+// Evaluates deferred pairs [head, head + cnt) of the warp's ring (cnt <= 32),
+// one per lane: the lane reloads the pair's point, transforms it again (the
+// same float operations) and contracts the single pair.
+__device__ __forceinline__ void eval_deferred(const WarpPairs &P, const uint2 *ring, unsigned head, int cnt) {
+    const int lane = threadIdx.x & 31;
+    if (lane >= cnt) return;
+    const uint2 d = ring[(head + lane) & (kDefer - 1)];
+    const int slot = (int)(d.x >> 6);
+    const int pi = (int)d.y;
+    if (d.x & 32u) {
+        queue_flagged(*P.args, P.align, pi, slot);
+        return;
+    }
+    const float4 x = __ldg(P.args->points + pi);
+    float px, py, pz;
+    if (P.args->trans) {
+        const float4 y = __ldg(P.args->trans + pi);
+        px = y.x; py = y.y; pz = y.z;
+    } else {
+        px = transform_row(P.T, x.x, x.y, x.z);
+        py = transform_row(P.T + 4, x.x, x.y, x.z);
+        pz = transform_row(P.T + 8, x.x, x.y, x.z);
+    }
+    PairSums F;
+    zero(F);
+    add_pair(P, F, slot, px, py, pz);
+    contract_add(F, x.x, x.y, x.z, P.ang, P.acc, P.stride, P.d2, P.hess, P.compat);
+}
+
 template <int TILE, int MINB>
 __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(EvalArgs args) {
     constexpr int kW = TILE / 32;
@@ -269,28 +398,51 @@ __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(EvalArgs arg
     __shared__ int s_mode;
     __shared__ double s_tot[kAcc];
     __shared__ unsigned s_cnt[kW][3];
+    __shared__ int s_chunk[2];
     extern __shared__ __align__(16) unsigned char s_dyn[];
     F32Smem<kW> &sm = *reinterpret_cast<F32Smem<kW> *>(s_dyn);
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const bool compat = args.compat != 0;
-    const float d1f = (float)args.d1, d2f = (float)args.d2;
     const double kR = compat ? -args.d2 : 1.0;
     const GridDev &grid = args.grid;
-    float (*terms)[32] = sm.terms[warp];
-    float (*xts)[32] = sm.xt[warp];
-    unsigned *list = sm.list[warp];
-    float *acc = &sm.acc[0][threadIdx.x];
+    unsigned (*own)[32] = sm.own[warp];
+    uint2 *ring = sm.defer[warp];
+
+    WarpPairs P;
+    P.args = &args;
+    P.grid = &grid;
+    P.T = s_T;
+    P.ang = s_ang;
+    P.acc = &sm.acc[0][threadIdx.x];
+    P.stride = TILE;
+    P.d1 = (float)args.d1;
+    P.d2 = (float)args.d2;
+    P.compat = compat;
 
     const int nt = *args.num_tiles;
     const int K = args.chunk_tiles;
-    for (int k = 0; k < kAcc; ++k) acc[k * TILE] = 0.0f;
+    for (int k = 0; k < kAcc; ++k) P.acc[k * TILE] = 0.0f;
     if (lane == 0) s_cnt[warp][0] = s_cnt[warp][1] = s_cnt[warp][2] = 0;
     unsigned long long blk_probe = 0, blk_occ = 0, blk_pair = 0, blk_pts = 0, blk_tiles = 0;
     int cur = -1, run_first = -1, mode = kEvalNone;
-    double *exc = nullptr;
-    __shared__ int s_chunk[2];
+    unsigned head = 0, tail = 0;  // deferred ring of this warp (warp-uniform)
     int parity = 0;
+
+    // Ends the current alignment run: evaluates the deferred pairs, then
+    // reduces the block's sums into the run's partial.
+    auto end_run = [&]() {
+        while (tail != head) {
+            const int c = (int)min(32u, tail - head);
+            __syncwarp();
+            eval_deferred(P, ring, head, c);
+            head += c;
+        }
+        head = tail = 0;
+        reduce_run<kW>(sm, s_tot, s_cnt, args.partials + (size_t)run_first * kPartial, kR, compat);
+        __syncthreads();
+        if (lane == 0) s_cnt[warp][0] = s_cnt[warp][1] = s_cnt[warp][2] = 0;
+    };
 
     // Chunks of K consecutive tiles are handed out dynamically (one atomic per
     // chunk), so blocks finish together however uneven the alignments are.  A
@@ -304,115 +456,97 @@ __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(EvalArgs arg
         const int t_begin = chunk * K;
         if (t_begin >= nt) break;
         const int t_end = min(nt, t_begin + K);
-    for (int ti = t_begin; ti < t_end; ++ti) {
-        const Tile tile = args.tiles[ti];
-        if (tile.align != cur || ti == t_begin) {
-            if (cur >= 0 && mode != kEvalNone) {
-                reduce_run<kW>(sm, s_tot, s_cnt, args.partials + (size_t)run_first * kPartial, kR, compat);
+        for (int ti = t_begin; ti < t_end; ++ti) {
+            const Tile tile = args.tiles[ti];
+            if (tile.align != cur || ti == t_begin) {
+                if (cur >= 0 && mode != kEvalNone) end_run();
                 __syncthreads();
-                if (lane == 0) s_cnt[warp][0] = s_cnt[warp][1] = s_cnt[warp][2] = 0;
+                const AlignState *st = args.states + tile.align;
+                if (threadIdx.x == 0) s_mode = st->eval_mode;
+                if (threadIdx.x < 12) s_T[threadIdx.x] = st->T[threadIdx.x];
+                if (threadIdx.x < kAngle) s_ang[threadIdx.x] = st->angf[threadIdx.x];
+                __syncthreads();
+                cur = tile.align;
+                run_first = ti;
+                mode = s_mode;
+                P.align = cur;
+                P.hess = mode != kEvalGradient;
+            } else if (mode != kEvalNone && threadIdx.x < kPartial) {
+                args.partials[(size_t)ti * kPartial + threadIdx.x] = 0.0;
             }
-            __syncthreads();
-            const AlignState *st = args.states + tile.align;
-            if (threadIdx.x == 0) s_mode = st->eval_mode;
-            if (threadIdx.x < 12) s_T[threadIdx.x] = st->T[threadIdx.x];
-            if (threadIdx.x < kAngle) s_ang[threadIdx.x] = st->angf[threadIdx.x];
-            __syncthreads();
-            cur = tile.align;
-            run_first = ti;
-            mode = s_mode;
-            exc = args.exc + (size_t)tile.align * kPartial;
-        } else if (mode != kEvalNone && threadIdx.x < kPartial) {
-            args.partials[(size_t)ti * kPartial + threadIdx.x] = 0.0;
-        }
-        if (mode == kEvalNone) continue;
-        const bool hess = mode != kEvalGradient;
+            if (mode == kEvalNone) continue;
 
-        const int i = tile.start + threadIdx.x;
-        const bool valid = i < tile.end;
-        const float4 x = valid ? args.points[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-        // transformPointCloud (kernel.cpp:397-400), float, left to right
-        float px, py, pz;
-        if (args.trans) {
-            const float4 y = valid ? args.trans[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-            px = y.x; py = y.y; pz = y.z;
-        } else {
-            px = transform_row(s_T, x.x, x.y, x.z);
-            py = transform_row(s_T + 4, x.x, x.y, x.z);
-            pz = transform_row(s_T + 8, x.x, x.y, x.z);
-        }
-        __syncwarp();
-        xts[0][lane] = px;
-        xts[1][lane] = py;
-        xts[2][lane] = pz;
-        unsigned n_probe = 0, n_occ = 0, n_pair = 0;
-        bool have_terms = false;
-        // evaluate list[0, n): one entry per lane per round
-        auto consume = [&](int n) {
-            if (n == 0) return;
-            if (!have_terms) {
-                // per-point terms of the ORIGINAL point (computePointDerivatives),
-                // computed once a warp has pairs to evaluate
-                const float *ja = s_ang;
-#pragma unroll
-                for (int k = 0; k < 8; ++k) terms[k][lane] = dot3f(x.x, x.y, x.z, ja + 3 * k);
-                const float *h = s_ang + 24;
-#pragma unroll
-                for (int k = 0; k < 15; ++k) terms[8 + k][lane] = dot3f(x.x, x.y, x.z, h + 3 * k);
-                have_terms = true;
+            const int i = tile.start + threadIdx.x;
+            const bool valid = i < tile.end;
+            const float4 x = valid ? args.points[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+            // transformPointCloud (kernel.cpp:397-400), float, left to right
+            float px, py, pz;
+            if (args.trans) {
+                const float4 y = valid ? args.trans[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+                px = y.x; py = y.y; pz = y.z;
+            } else {
+                px = transform_row(s_T, x.x, x.y, x.z);
+                py = transform_row(s_T + 4, x.x, x.y, x.z);
+                pz = transform_row(s_T + 8, x.x, x.y, x.z);
+            }
+            unsigned n_probe = 0, n_occ = 0, n_pair = 0;
+            int resume = 0;
+            do {
                 __syncwarp();
-            }
-            AccF A;
+                OwnSink sink{own, 0};
+                collect_pairs(grid, px, py, pz, valid, sink, n_probe, n_occ, resume);
+                __syncwarp();
+                const int c = sink.c;
+                n_pair += c;
+                const int n = __reduce_add_sync(kFull, c);
+                if (n > kDenseThreshold) {
+                    // dense: each lane sums its own pairs, then one contraction
+                    PairSums F;
+                    zero(F);
+                    const int maxc = __reduce_max_sync(kFull, c);
+                    for (int k = 0; k < maxc; ++k) {
+                        if (k < c) {
+                            const unsigned code = own[k][lane];
+                            const int slot = (int)(code >> 6);
+                            if (code & 32u)
+                                queue_flagged(args, cur, i, slot);
+                            else
+                                add_pair(P, F, slot, px, py, pz);
+                        }
+                    }
+                    if (c > 0) contract_add(F, x.x, x.y, x.z, s_ang, P.acc, TILE, P.d2, P.hess, compat);
+                } else if (n > 0) {
+                    // sparse: defer into the ring, evaluate full rounds of 32
+                    int pre = c;
 #pragma unroll
-            for (int k = 0; k < kAcc; ++k) A.v[k] = 0.0f;
-            for (int base = 0; base < n; base += 32) {
-                const int k = base + lane;
-                if (k >= n) break;
-                const unsigned code = list[k];
-                const int owner = code & 31;
-                const int slot = (int)(code >> 6);
-                const float4 hi = __ldg(grid.mean_hi + slot);
-                const float4 lo = __ldg(grid.mean_lo + slot);
-                // x' = x_trans - mean (kernel.cpp:692-694) from the (hi, lo) split
-                const float p0 = __fsub_rn(__fsub_rn(xts[0][owner], hi.x), lo.x);
-                const float p1 = __fsub_rn(__fsub_rn(xts[1][owner], hi.y), lo.y);
-                const float p2 = __fsub_rn(__fsub_rn(xts[2][owner], hi.z), lo.z);
-                ++n_pair;
-                if (code & 32) {
-                    // FP64 side path, evaluated by flagged_kernel after this pass
-                    const unsigned q = atomicAdd(args.flag_n, 1u);
-                    if (q < args.flag_cap)
-                        args.flag_q[q] = make_int4(tile.align, tile.start + warp * 32 + owner, slot, 0);
-                } else {
-                    const float4 ca = __ldg(grid.icov32 + 2 * slot);
-                    const float4 cb = __ldg(grid.icov32 + 2 * slot + 1);
-                    pair_fp32(A, terms, owner, p0, p1, p2, ca, cb, d1f, d2f, hess, compat);
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int v = __shfl_up_sync(kFull, pre, o);
+                        if (lane >= o) pre += v;
+                    }
+                    pre -= c;
+                    for (int k = 0; k < c; ++k)
+                        ring[(tail + pre + k) & (kDefer - 1)] = make_uint2(own[k][lane] & ~31u, (unsigned)i);
+                    tail += n;
+                    while (tail - head >= 32) {
+                        __syncwarp();
+                        eval_deferred(P, ring, head, 32);
+                        head += 32;
+                    }
                 }
-            }
-#pragma unroll
-            for (int k = 0; k < kAcc; ++k) acc[k * TILE] += A.v[k];
-        };
-        __syncwarp();
-        probe_point(grid, px, py, pz, valid, list, n_probe, n_occ, consume);
-        // per-warp work counters (pairs feed the partial's count)
-        for (int o = 16; o > 0; o >>= 1) {
-            n_probe += __shfl_xor_sync(kFull, n_probe, o);
-            n_occ += __shfl_xor_sync(kFull, n_occ, o);
-            n_pair += __shfl_xor_sync(kFull, n_pair, o);
+            } while (resume >= 0);
+            // per-warp work counters (pairs feed the partial's count)
+            n_probe = __reduce_add_sync(kFull, n_probe);
+            n_occ = __reduce_add_sync(kFull, n_occ);
+            n_pair = __reduce_add_sync(kFull, n_pair);
+            if (lane == 0) s_cnt[warp][2] += n_pair;
+            blk_probe += n_probe;
+            blk_occ += n_occ;
+            blk_pair += n_pair;
+            blk_pts += (unsigned long long)(tile.end - tile.start);
+            blk_tiles += 1;
         }
-        if (lane == 0) s_cnt[warp][2] += n_pair;
-        blk_probe += n_probe;
-        blk_occ += n_occ;
-        blk_pair += n_pair;
-        blk_pts += (unsigned long long)(tile.end - tile.start);
-        blk_tiles += 1;
-    }
         // the run of this chunk ends with the chunk
-        if (cur >= 0 && mode != kEvalNone) {
-            reduce_run<kW>(sm, s_tot, s_cnt, args.partials + (size_t)run_first * kPartial, kR, compat);
-            __syncthreads();
-            if (lane == 0) s_cnt[warp][0] = s_cnt[warp][1] = s_cnt[warp][2] = 0;
-        }
+        if (cur >= 0 && mode != kEvalNone) end_run();
         cur = -1;
     }
     if (args.counters && lane == 0 && blk_tiles) {

@@ -147,8 +147,14 @@ __global__ void __launch_bounds__(kTile64, 1) derivative_f64_kernel(EvalArgs arg
                 ++n_pair;
             }
         };
-        __syncwarp();
-        probe_point(grid, px, py, pz, valid, list, n_probe, n_occ, consume);
+        int resume = 0;
+        do {
+            __syncwarp();
+            ListSink sink{list, 0};
+            collect_pairs(grid, px, py, pz, valid, sink, n_probe, n_occ, resume);
+            __syncwarp();
+            consume(sink.n);
+        } while (resume >= 0);
         for (int k = 0; k < 43; ++k) {
             double v = A.v[k];
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);

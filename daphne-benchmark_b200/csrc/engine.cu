@@ -8,6 +8,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -82,8 +83,10 @@ struct ndt_ctx {
     double d1 = 0, d2 = 0;
     // grid
     DevBuf map, index, mean, mean_hi, mean_lo, icov32, icov64, count, cell, seg_start, seg_cell, scratch, meta;
+    DevBuf win_off, win_ent, win_ctot;
     GridMeta meta_host{};
     bool have_map = false;
+    bool have_windows = false;
     int map_points = 0;
     // batch
     DevBuf points, offsets, guesses, states, tiles, tile_begin, num_tiles, partials, exc, out_T, out_conv, out_fit,
@@ -188,6 +191,10 @@ GridDev grid_dev(ndt_ctx *c) {
     g.radius_final = (float)((double)c->prm.resolution + (double)0.001f);
     g.icov32 = c->icov32.as<float4>();
     g.icov64 = c->icov64.as<double>();
+    g.win_off = c->have_windows ? c->win_off.as<int32_t>() : nullptr;
+    g.win_ent = c->have_windows ? c->win_ent.as<float4>() : nullptr;
+    g.win_dim[0] = c->meta_host.dim[0] + 2;
+    g.win_dim[1] = c->meta_host.dim[1] + 2;
     return g;
 }
 
@@ -205,6 +212,9 @@ int set_device(ndt_ctx *c) {
     return NDT_OK;
 }
 
+constexpr long long kMaxWindows = 1LL << 28;        // probe windows (4 B offset each)
+constexpr long long kMaxWindowEntries = 1LL << 28;  // window entries (16 B each)
+
 // Grid build from a device-resident map (any device pointer valid on the
 // context's stream for the duration of the call).
 int build_grid(ndt_ctx *c, const float4 *d_map, int m) {
@@ -212,6 +222,7 @@ int build_grid(ndt_ctx *c, const float4 *d_map, int m) {
     // voxel slots travel in 26 bits of a packed pair code (slot << 6 | flag << 5 | lane)
     if (m >= (1 << 25)) return fail(c, NDT_E_CAPACITY, "map larger than 2^25 points");
     c->have_map = false;
+    c->have_windows = false;
     c->grid_timed = false;
     if (c->profiling) {
         if (!c->grid_ev[0]) CK(cudaEventCreate(&c->grid_ev[0]));
@@ -246,6 +257,23 @@ int build_grid(ndt_ctx *c, const float4 *d_map, int m) {
     rc = grid_build(d_map, m, c->meta_host, c->meta.as<GridMeta>(), opt, grid_buffers(c), c->scratch.p, c->stream, &nl);
     if (rc) return cuda_fail(c, (cudaError_t)rc, "grid_build");
     c->launches += nl;
+    // probe-window table: W + 1 offsets and at most 27 entries per usable voxel
+    const long long W = (long long)window_count(c->meta_host);
+    const long long ent_cap = 27LL * (long long)std::min<size_t>((size_t)m, G);
+    if (!c->prm.dense_probe && W < kMaxWindows && ent_cap < kMaxWindowEntries) {
+        CK(c->win_off.ensure(sizeof(int32_t) * (size_t)(W + 1)));
+        CK(c->win_ent.ensure(sizeof(float4) * (size_t)ent_cap));
+        CK(c->win_ctot.ensure(sizeof(int32_t) * (size_t)(W / 256 + 2)));
+        WindowBuffers wb;
+        wb.off = c->win_off.as<int32_t>();
+        wb.ent = c->win_ent.as<float4>();
+        wb.ctot = c->win_ctot.as<int32_t>();
+        nl = 0;
+        rc = grid_windows(c->meta_host, c->index.as<int32_t>(), c->mean_hi.as<float4>(), wb, c->stream, &nl);
+        if (rc) return cuda_fail(c, (cudaError_t)rc, "grid_windows");
+        c->launches += nl;
+        c->have_windows = true;
+    }
     if (c->profiling) {
         CK(cudaEventRecord(c->grid_ev[1], c->stream));
         c->grid_timed = true;
@@ -533,8 +561,8 @@ void ndt_destroy(ndt_ctx *c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    DevBuf *bufs[] = {&c->map, &c->index, &c->mean, &c->mean_hi, &c->mean_lo, &c->icov32, &c->icov64, &c->count, &c->cell, &c->seg_start,
-                      &c->seg_cell, &c->scratch, &c->meta, &c->points, &c->offsets, &c->guesses, &c->states,
+    DevBuf *bufs[] = {&c->win_off, &c->win_ent, &c->win_ctot, &c->map, &c->index, &c->mean, &c->mean_hi,
+                      &c->mean_lo, &c->icov32, &c->icov64, &c->count, &c->cell, &c->seg_start, &c->seg_cell, &c->scratch, &c->meta, &c->points, &c->offsets, &c->guesses, &c->states,
                       &c->tiles, &c->tile_begin, &c->num_tiles, &c->partials, &c->exc, &c->out_T, &c->out_conv,
                       &c->out_fit, &c->out_status, &c->active, &c->counters, &c->p6, &c->trans,
                       &c->flag_q, &c->flag_n, &c->flag_overflow, &c->work_counter};
@@ -680,6 +708,22 @@ int ndt_grid_cells(ndt_ctx *c, int cap, int *cell_index, int *count, double *mea
             mean3[3 * k + 2] = mean[k].z;
         }
     return K;
+}
+
+int ndt_window_info(ndt_ctx *c, long long *windows, long long *entries) {
+    if (!c) return NDT_E_ARG;
+    if (!c->have_map) return fail(c, NDT_E_NOMAP, "no map set");
+    long long W = 0, E = 0;
+    if (c->have_windows) {
+        W = (long long)window_count(c->meta_host);
+        int32_t e = 0;
+        CK(cudaMemcpyAsync(&e, c->win_off.as<int32_t>() + W, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        E = e;
+    }
+    if (windows) *windows = W;
+    if (entries) *entries = E;
+    return NDT_OK;
 }
 
 int ndt_derivatives(ndt_ctx *c, const float *scan, const float *trans, int n, const double p6[6], double *score,

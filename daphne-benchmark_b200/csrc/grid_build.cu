@@ -471,6 +471,85 @@ __global__ void cell_finalize_corrected_kernel(const float4 *__restrict__ map, c
     buf.index[seg_cell[s]] = s | (flag ? kSlotFlag : 0);
 }
 
+// ---------------------------------------------------------------------------
+// Probe-window table (see grid_build.h).
+struct WinGeom {
+    int dim[3];
+    int wd[3];  // dim + 2
+    int W;
+};
+
+// Calls f(index entry, 9 dz + 3 dy + dx) for the usable voxels of window w in
+// the reference's probe order.
+template <class F>
+__device__ __forceinline__ void visit_window(const int32_t *__restrict__ index, const WinGeom &g, int w, F f) {
+    const int bx = w % g.wd[0] - 2;
+    const int t = w / g.wd[0];
+    const int by = t % g.wd[1] - 2;
+    const int bz = t / g.wd[1] - 2;
+#pragma unroll
+    for (int dz = 0; dz < 3; ++dz) {
+        const int z = bz + dz;
+        if (z < 0 || z >= g.dim[2]) continue;
+#pragma unroll
+        for (int dy = 0; dy < 3; ++dy) {
+            const int y = by + dy;
+            if (y < 0 || y >= g.dim[1]) continue;
+            const int row = g.dim[0] * (y + g.dim[1] * z);
+#pragma unroll
+            for (int dx = 0; dx < 3; ++dx) {
+                const int x = bx + dx;
+                if (x < 0 || x >= g.dim[0]) continue;
+                const int v = __ldg(index + row + x);
+                if (v >= 0) f(v, 9 * dz + 3 * dy + dx);
+            }
+        }
+    }
+}
+
+__global__ void window_count_kernel(const int32_t *__restrict__ index, WinGeom g, int *__restrict__ ctot) {
+    const int w = blockIdx.x * kThreads + threadIdx.x;
+    int c = 0;
+    if (w < g.W) visit_window(index, g, w, [&](int, int) { ++c; });
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    __shared__ int s[kWarps];
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int k = 0; k < kWarps; ++k) t += s[k];
+        ctot[blockIdx.x] = t;
+    }
+}
+
+// ctot holds the exclusive block offsets here.
+__global__ void window_fill_kernel(const int32_t *__restrict__ index, const float4 *__restrict__ mean_hi, WinGeom g,
+                                   const int *__restrict__ ctot, int32_t *__restrict__ off, float4 *__restrict__ ent) {
+    const int w = blockIdx.x * kThreads + threadIdx.x;
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    int c = 0;
+    if (w < g.W) visit_window(index, g, w, [&](int, int) { ++c; });
+    int incl = c;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    __shared__ int s[kWarps];
+    if (lane == 31) s[wp] = incl;
+    __syncthreads();
+    int pos = ctot[blockIdx.x] + incl - c;
+    for (int k = 0; k < wp; ++k) pos += s[k];
+    if (w >= g.W) return;
+    off[w] = pos;
+    if (w == g.W - 1) off[g.W] = pos + c;
+    visit_window(index, g, w, [&](int v, int o) {
+        const int slot = v & kSlotMask;
+        const float4 h = __ldg(mean_hi + slot);
+        const unsigned code = ((unsigned)slot << 6) | ((v & kSlotFlag) ? 32u : 0u) | (unsigned)o;
+        ent[pos++] = make_float4(h.x, h.y, h.z, __uint_as_float(code));
+    });
+}
+
 __global__ void store_occupied_kernel(const int *__restrict__ nseg, GridMeta *__restrict__ meta) {
     if (threadIdx.x == 0) meta->occupied = *nseg;
 }
@@ -500,6 +579,26 @@ int grid_bbox(const float4 *d_map, int m, float res, GridMeta *d_meta, void *scr
     cudaMemsetAsync(nonfinite, 0, sizeof(int), st);
     bbox_partial_kernel<<<nblk, kThreads, 0, st>>>(d_map, m, part, nonfinite);
     bbox_final_kernel<<<1, kThreads, 0, st>>>(part, nblk, res, nonfinite, d_meta);
+    return (int)cudaGetLastError();
+}
+
+int64_t window_count(const GridMeta &g) {
+    return (int64_t)(g.dim[0] + 2) * (int64_t)(g.dim[1] + 2) * (int64_t)(g.dim[2] + 2);
+}
+
+int grid_windows(const GridMeta &meta_host, const int32_t *index, const float4 *mean_hi, WindowBuffers wb,
+                 cudaStream_t st, int *launches) {
+    WinGeom g;
+    for (int e = 0; e < 3; ++e) {
+        g.dim[e] = meta_host.dim[e];
+        g.wd[e] = meta_host.dim[e] + 2;
+    }
+    g.W = (int)window_count(meta_host);
+    const int nb = div_up(g.W, kThreads);
+    window_count_kernel<<<nb, kThreads, 0, st>>>(index, g, wb.ctot);
+    scan_single_block_kernel<<<1, 1024, 0, st>>>(wb.ctot, nb, nullptr);
+    window_fill_kernel<<<nb, kThreads, 0, st>>>(index, mean_hi, g, wb.ctot, wb.off, wb.ent);
+    if (launches) *launches += 3;
     return (int)cudaGetLastError();
 }
 

@@ -28,6 +28,26 @@ struct NdtGridOptions {
     double eigen_ratio;
 };
 
+// Probe-window table.  The FP32 derivative pass probes, for a point p, the
+// cells [b, b + 2] on each axis, b = cell(p - res) (the reference's 3 x 3 x 3
+// probe loop, kernel.cpp:256-260, whenever its three coordinates fall in
+// consecutive cells).  Window w of base cell b, each component in
+// [-2, dim - 1], lists the usable voxels of those 27 cells in the reference's
+// probe order (z outer, x inner) as float4 {float(mean) xyz, code}, code =
+// slot << 6 | flag << 5 | 9 dz + 3 dy + dx, so a point reads 2 offsets and one
+// record per occupied cell instead of 27 dense-index entries.
+struct WindowBuffers {
+    int32_t *off;   // W + 1 entry offsets
+    float4 *ent;    // entries (capacity 27 * min(m, G))
+    int32_t *ctot;  // per-block totals (ceil(W / 256) + 1)
+};
+
+int64_t window_count(const GridMeta &g);  // W = (dim_x + 2)(dim_y + 2)(dim_z + 2)
+
+// Builds the table from the finished dense index (after grid_build).
+int grid_windows(const GridMeta &meta_host, const int32_t *index, const float4 *mean_hi, WindowBuffers wb,
+                 cudaStream_t st, int *launches);
+
 size_t grid_scratch_bytes(int m);
 
 // Phase 1: bounding box and dims into *d_meta (the caller reads it back to

@@ -55,6 +55,10 @@ struct GridDev {
     float radius_final;      // (float)(res + 0.001f): the probe loop bound of kernel.cpp:254
     const float4 *icov32;    // 2K: {c00 c01 c02 c11}, {c12 c22 0 0} (symmetrised, FP32)
     const double *icov64;    // 9K: inverse covariance as the reference stores it (row major)
+    // probe-window table (grid_build.h), nullptr when not built
+    const int32_t *win_off;  // W + 1
+    const float4 *win_ent;   // {float(mean) xyz, slot << 6 | flag << 5 | cell offset}
+    int32_t win_dim[2];      // dim_x + 2, dim_y + 2
 };
 
 // Per-alignment state (FP64 control, float transform), one per alignment.

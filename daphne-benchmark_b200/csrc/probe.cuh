@@ -1,6 +1,7 @@
 // Shared device code of the derivative pass: the reference's neighbour
 // search (voxelRadiusSearch, src/CPU/ndt_mapping/kernel.cpp:246-286) per
-// point, with the pair list it feeds, and the block-reduction helpers.
+// point, collecting the pair list that the pair evaluation consumes, and the
+// block-reduction helpers.
 //
 // Every operation whose rounding decides which (point, voxel) pairs the
 // reference accepts is written with explicit round-to-nearest intrinsics
@@ -127,30 +128,118 @@ __device__ __forceinline__ unsigned pair_code(int v, int lane) {
     return ((unsigned)(v & kSlotMask) << 6) | ((v & kSlotFlag) ? 32u : 0u) | (unsigned)lane;
 }
 
-// Probe every lane's point in the reference's order (z outer, x inner) and
-// collect the accepted pairs in `list` (capacity 27 x 32), then call
-// consume(n) for list[0, n) (the generic path also calls it whenever the list
-// could overflow).  List code = slot << 6 | flag << 5 | lane.  Work that no
-// lane of the warp needs is skipped with warp-uniform branches: layers with no
-// in-bounds probe, layers with no occupied cell, distance tests of a probe no
-// lane occupies, list appends of a probe no lane accepted.
-template <class Consume>
-__device__ __forceinline__ void probe_point(const GridDev &grid, float px, float py, float pz, bool valid,
-                                            unsigned *list, unsigned &n_probe, unsigned &n_occ, Consume consume) {
+// The probe-window table (grid_build.h) holds, for a window base cell b, the
+// usable voxels of cells [b, b + 2]^3 in probe order.  A lane's window is the
+// one whose base is the cell of its first probe coordinate on each axis; that
+// covers the reference's probe cells when each axis's in-bbox coordinates fall
+// in consecutive cells inside [0, dim).  An entry is one of the reference's
+// probes when its cell offset has an in-bbox coordinate on all three axes.
+__device__ __forceinline__ int window_base(const Axis &a, int dim, bool &ok) {
+    if (a.in == 0u) return 0;
+    const int first = (a.in & 1u) ? 0 : ((a.in & 2u) ? 1 : 2);
+    const int base = axis_i(a, first) - first;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        if (((a.in >> k) & 1u) && (axis_i(a, k) != base + k || axis_i(a, k) >= dim)) ok = false;
+    return base;
+}
+
+// Where collect_pairs puts the accepted pairs (code = slot << 6 | flag << 5 |
+// lane).  ListSink compacts the warp's pairs into one list (capacity 27 x 32,
+// `n` entries); OwnSink keeps each lane's pairs in its own column,
+// own[k][lane] for k < c (at most kOwn per lane).
+struct ListSink {
+    unsigned *list;
+    int n;
+    __device__ __forceinline__ void add(bool ok, unsigned code) {
+        const unsigned bal = __ballot_sync(kFull, ok);
+        if (ok) list[n + __popc(bal & lanemask_lt())] = code;
+        n += __popc(bal);
+    }
+    __device__ __forceinline__ bool full() const { return n > kList - 32; }
+};
+
+constexpr int kOwn = 27;  // accepted pairs per lane and collect call, at most
+
+struct OwnSink {
+    unsigned (*own)[32];
+    int c;
+    __device__ __forceinline__ void add(bool ok, unsigned code) {
+        if (ok) own[c++][threadIdx.x & 31] = code;
+    }
+    __device__ __forceinline__ bool full() const { return __any_sync(kFull, c >= kOwn); }
+};
+
+// Collects the accepted (point, voxel) pairs of every lane's point into
+// `sink`.  `resume` is 0 on the first call; it comes back -1 when the point's
+// probes are done, or, on the generic path (trip counts up to 4: coordinates
+// beyond ~1e6 m or inf), the probe position to continue from once the caller
+// has emptied the sink.  Three paths, chosen per warp:
+//   windows  the probe-window table (2 offsets + 1 record per occupied cell),
+//            when the table exists and every lane's cells are consecutive;
+//   dense    the 27 dense-index entries in 3 layers of 9 loads, skipping with
+//            warp-uniform branches the layers no lane has in bounds or
+//            occupied, the distance tests of probes no lane occupies and the
+//            appends of probes no lane accepted;
+//   generic  one probe at a time, the reference's loop as written.
+// The pairs are the reference's on every path; only their order differs.
+template <class Sink>
+__device__ __forceinline__ void collect_pairs(const GridDev &grid, float px, float py, float pz, bool valid, Sink &sink,
+                                              unsigned &n_probe, unsigned &n_occ, int &resume) {
     const int lane = threadIdx.x & 31;
-    const unsigned lt = lanemask_lt();
     const GridMeta &g = grid.meta;
     const float res = g.res, inv_res = grid.inv_res, rf = grid.radius_final;
     const Axis ax = make_axis(px, g.minv[0], g.maxv[0], res, inv_res, rf, valid);
     const Axis ay = make_axis(py, g.minv[1], g.maxv[1], res, inv_res, rf, valid);
     const Axis az = make_axis(pz, g.minv[2], g.maxv[2], res, inv_res, rf, valid);
     const bool any_in = (ax.in != 0u) && (ay.in != 0u) && (az.in != 0u);
-    if (!__any_sync(kFull, any_in)) return;
+    if (!__any_sync(kFull, any_in)) {
+        resume = -1;
+        return;
+    }
     const int mx = __reduce_max_sync(kFull, ax.n), my = __reduce_max_sync(kFull, ay.n),
               mz = __reduce_max_sync(kFull, az.n);
     const float tol = radius_margin(px, py, pz, res);
-    int n = 0;
-    if (mx <= 3 && my <= 3 && mz <= 3) {
+    const bool small = mx <= 3 && my <= 3 && mz <= 3;
+    if (small && grid.win_off) {
+        bool ok = true;
+        const int bx = window_base(ax, g.dim[0], ok);
+        const int by = window_base(ay, g.dim[1], ok);
+        const int bz = window_base(az, g.dim[2], ok);
+        if (__all_sync(kFull, ok || !any_in)) {
+            unsigned allowed = 0;
+            int beg = 0, cnt = 0;
+            if (any_in) {
+#pragma unroll
+                for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+                    for (int dy = 0; dy < 3; ++dy)
+                        if ((az.in >> dz) & (ay.in >> dy) & 1u) allowed |= ax.in << (9 * dz + 3 * dy);
+                const int w = (bx + 2) + grid.win_dim[0] * ((by + 2) + grid.win_dim[1] * (bz + 2));
+                beg = __ldg(grid.win_off + w);
+                cnt = __ldg(grid.win_off + w + 1) - beg;
+                n_probe += __popc(allowed);
+            }
+            const int maxc = __reduce_max_sync(kFull, cnt);
+            for (int j = 0; j < maxc; j += 4) {
+                float4 e[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    e[u] = j + u < cnt ? __ldg(grid.win_ent + beg + j + u) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const unsigned code = __float_as_uint(e[u].w);
+                    const bool occ = j + u < cnt && ((allowed >> (code & 31u)) & 1u);
+                    n_occ += occ;
+                    const bool ok2 = occ && accept(grid, (int)(code >> 6), e[u], px, py, pz, tol);
+                    sink.add(ok2, (code & ~31u) | (unsigned)lane);
+                }
+            }
+            resume = -1;
+            return;
+        }
+    }
+    if (small) {
 #pragma unroll 1
         for (int a = 0; a < 3; ++a) {
             const bool za = any_in && ((az.in >> a) & 1u);
@@ -190,55 +279,42 @@ __device__ __forceinline__ void probe_point(const GridDev &grid, float px, float
 #pragma unroll
             for (int k = 0; k < 9; ++k) {
                 const bool ok = (acc >> k) & 1u;
-                const unsigned bal = __ballot_sync(kFull, ok);
-                if (bal) {
-                    if (ok) list[n + __popc(bal & lt)] = pair_code(v[k], lane);
-                    n += __popc(bal);
-                }
+                if (__any_sync(kFull, ok)) sink.add(ok, pair_code(v[k], lane));
             }
         }
-        __syncwarp();
-        consume(n);
-        __syncwarp();
+        resume = -1;
         return;
     }
-    // generic path: trip counts up to 4 (coordinates beyond ~1e6 m or inf)
-    float zc = az.c0;
-    for (int a = 0; a < mz; ++a, zc = __fadd_rn(zc, res)) {
-        float yc = ay.c0;
-        for (int b = 0; b < my; ++b, yc = __fadd_rn(yc, res)) {
-            float xc = ax.c0;
-            for (int c = 0; c < mx; ++c, xc = __fadd_rn(xc, res)) {
-                const bool act = a < az.n && b < ay.n && c < ax.n;
-                const bool inb = act && !((xc < g.minv[0]) || (xc > g.maxv[0]) || (yc < g.minv[1]) ||
-                                          (yc > g.maxv[1]) || (zc < g.minv[2]) || (zc > g.maxv[2]));
-                int v = -1;
-                if (inb) {
-                    v = __ldg(grid.index + (cell_component(xc, g.minv[0], res, inv_res) +
-                                            g.dim[0] * (cell_component(yc, g.minv[1], res, inv_res) +
-                                                        g.dim[1] * cell_component(zc, g.minv[2], res, inv_res))));
-                    ++n_probe;
-                }
-                bool ok = false;
-                if (v >= 0) {
-                    ++n_occ;
-                    ok = accept(grid, v & kSlotMask, __ldg(grid.mean_hi + (v & kSlotMask)), px, py, pz, tol);
-                }
-                if (n > kList - 32) {
-                    __syncwarp();
-                    consume(n);
-                    __syncwarp();
-                    n = 0;
-                }
-                const unsigned bal = __ballot_sync(kFull, ok);
-                if (ok) list[n + __popc(bal & lt)] = pair_code(v, lane);
-                n += __popc(bal);
-            }
+    // generic: position pos = (a * my + b) * mx + c, z outer, x inner
+    const int total = mz * my * mx;
+    for (int pos = resume; pos < total; ++pos) {
+        if (sink.full()) {
+            resume = pos;
+            return;
         }
+        const int c = pos % mx, b = (pos / mx) % my, a = pos / (mx * my);
+        float xc = ax.c0, yc = ay.c0, zc = az.c0;
+        for (int k = 0; k < c; ++k) xc = __fadd_rn(xc, res);
+        for (int k = 0; k < b; ++k) yc = __fadd_rn(yc, res);
+        for (int k = 0; k < a; ++k) zc = __fadd_rn(zc, res);
+        const bool act = a < az.n && b < ay.n && c < ax.n;
+        const bool inb = act && !((xc < g.minv[0]) || (xc > g.maxv[0]) || (yc < g.minv[1]) || (yc > g.maxv[1]) ||
+                                  (zc < g.minv[2]) || (zc > g.maxv[2]));
+        int v = -1;
+        if (inb) {
+            v = __ldg(grid.index + (cell_component(xc, g.minv[0], res, inv_res) +
+                                    g.dim[0] * (cell_component(yc, g.minv[1], res, inv_res) +
+                                                g.dim[1] * cell_component(zc, g.minv[2], res, inv_res))));
+            ++n_probe;
+        }
+        bool ok = false;
+        if (v >= 0) {
+            ++n_occ;
+            ok = accept(grid, v & kSlotMask, __ldg(grid.mean_hi + (v & kSlotMask)), px, py, pz, tol);
+        }
+        sink.add(ok, pair_code(v, lane));
     }
-    __syncwarp();
-    consume(n);
-    __syncwarp();
+    resume = -1;
 }
 
 // ---------------------------------------------------------------------------

@@ -47,7 +47,7 @@ class Params(C.Structure):
         ("precision", C.c_int32),
         ("eigen_ratio", C.c_double),
         ("watchdog_evals", C.c_int32),
-        ("_pad1", C.c_int32),
+        ("dense_probe", C.c_int32),
     ]
 
 
@@ -104,12 +104,13 @@ def lib():
         L.ndt_get_counters.argtypes = [ctxp, C.POINTER(Counters)]
         L.ndt_grid_info.argtypes = [ctxp, _f32p, _i32p, C.POINTER(C.c_int)]
         L.ndt_grid_cells.argtypes = [ctxp, C.c_int, _i32p, _i32p, _f64p, _f64p]
+        L.ndt_window_info.argtypes = [ctxp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
         L.ndt_derivatives.argtypes = [ctxp, _f32p, _f32p, C.c_int, _f64p, C.POINTER(C.c_double), _f64p, _f64p]
         for name in ("ndt_create", "ndt_set_map", "ndt_set_map_device", "ndt_align", "ndt_align_with_map",
                      "ndt_align_batch", "ndt_align_batch_device", "ndt_synchronize", "ndt_get_counters",
                      "ndt_grid_info", "ndt_grid_cells", "ndt_derivatives", "ndt_align_batch_packed",
                      "ndt_set_profiling", "ndt_kernel_variants", "ndt_kernel_variant_shape",
-                     "ndt_set_kernel_variant"):
+                     "ndt_set_kernel_variant", "ndt_window_info"):
             getattr(L, name).restype = C.c_int
         _LIB = L
     return _LIB
@@ -126,19 +127,21 @@ def kernel_variants():
     return out
 
 
-def reference_params(resolution=1.0, precision=0):
+def reference_params(resolution=1.0, precision=0, dense_probe=0):
     p = Params()
     lib().ndt_params_reference(C.byref(p))
     p.resolution = resolution
     p.precision = precision
+    p.dense_probe = dense_probe
     return p
 
 
-def corrected_params(resolution=1.0, precision=0):
+def corrected_params(resolution=1.0, precision=0, dense_probe=0):
     p = Params()
     lib().ndt_params_corrected(C.byref(p))
     p.resolution = resolution
     p.precision = precision
+    p.dense_probe = dense_probe
     return p
 
 
@@ -269,6 +272,12 @@ class Context:
         occ = C.c_int()
         self._check(self.L.ndt_grid_info(self.h, bbox, dims, C.byref(occ)), "ndt_grid_info")
         return bbox, dims, occ.value
+
+    def window_info(self):
+        """(windows, entries) of the probe-window table; (0, 0) when the dense index is probed."""
+        w, e = C.c_longlong(), C.c_longlong()
+        self._check(self.L.ndt_window_info(self.h, C.byref(w), C.byref(e)), "ndt_window_info")
+        return w.value, e.value
 
     def grid_cells(self):
         _, _, K = self.grid_info()

@@ -71,7 +71,9 @@ typedef struct ndt_params {
     int32_t precision;             /* per-pair arithmetic: 0 = FP32 (default), 1 = FP64 */
     double eigen_ratio;            /* compat = 0 only: covariance eigenvalue floor ratio */
     int32_t watchdog_evals;        /* max derivative evaluations per alignment (0 = 1024) */
-    int32_t _pad1;
+    int32_t dense_probe;           /* 1 = FP32 pass probes the dense cell index for all 27 cells of a
+                                      point; 0 = it reads the probe-window table (built with the grid when
+                                      it fits, same pairs) */
 } ndt_params;
 
 typedef struct ndt_ctx ndt_ctx;
@@ -190,6 +192,14 @@ NDT_API int ndt_set_kernel_variant(ndt_ctx *ctx, int variant);
 NDT_API int ndt_grid_info(ndt_ctx *ctx, float *bbox6, int *dims3, int *occupied);
 NDT_API int ndt_grid_cells(ndt_ctx *ctx, int cap, int *cell_index, int *count, double *mean3,
                    double *icov9);
+
+/*
+ * Probe-window table of the current map (built with the grid unless
+ * params.dense_probe = 1 or it would exceed 2^28 windows or entries): number
+ * of windows and of entries; both 0 when the FP32 pass probes the dense index.
+ * No reference counterpart (a lookup structure of this library).
+ */
+NDT_API int ndt_window_info(ndt_ctx *ctx, long long *windows, long long *entries);
 
 /*
  * One derivative evaluation (computeDerivatives, kernel.cpp:651-705) of a

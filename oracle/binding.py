@@ -41,7 +41,7 @@ class NdtParams(C.Structure):
         ("precision", C.c_int32),
         ("eigen_ratio", C.c_double),
         ("watchdog_evals", C.c_int32),
-        ("_pad1", C.c_int32),
+        ("dense_probe", C.c_int32),
     ]
 
 
