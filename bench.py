@@ -44,6 +44,7 @@ PKG_DIR = ROOT / "daphne-benchmark_b200"
 sys.path.insert(0, str(ROOT / "oracle"))
 
 L2_FLUSH_BYTES = 256 << 20
+E2E_WARM_S = 1.5
 METRIC = "NDT aligns/sec on 1 B200, learned-init vs plain, at <=2cm/0.1deg pose error"
 
 
@@ -67,53 +68,62 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def _clock_worker(device_index, uuid, conn, period_s):
+    """Child process of ClockSampler: polls NVML until told to stop."""
+    samples, reasons, max_mhz = [], set(), None
+    try:
+        import pynvml as nv
+        nv.nvmlInit()
+        h = nv.nvmlDeviceGetHandleByUUID(uuid) if uuid else nv.nvmlDeviceGetHandleByIndex(device_index)
+        max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+    except Exception:
+        conn.send("ready")
+        conn.recv()
+        conn.send(([], [], None))
+        return
+    conn.send("ready")
+    while not conn.poll(period_s):
+        try:
+            samples.append(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+            bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            for name, mask in ClockSampler.REASONS.items():
+                if bits & mask:
+                    reasons.add(name)
+        except Exception:
+            break
+    conn.recv()
+    conn.send((samples, sorted(reasons), max_mhz))
+
+
 class ClockSampler:
     """SM clock and throttle-reason samples of one GPU during the timed region.
 
-    NVML (nvidia_ml_py) polled every 5 ms from a thread.  Reading clocks
-    changes no GPU setting.
+    NVML (nvidia_ml_py) polled every 5 ms from a separate process (spawned, no
+    CUDA), so that the sampling never holds this process's interpreter lock
+    while the timed steps run.  Reading clocks changes no GPU setting.
     """
 
     REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
 
     def __init__(self, device_index: int, uuid: str | None):
-        import threading
-        self.samples, self.reasons, self.max_mhz = [], set(), None
-        self.stop_flag = threading.Event()
-        self.nvml = None
-        try:
-            import pynvml as nv
-            nv.nvmlInit()
-            h = nv.nvmlDeviceGetHandleByUUID(uuid) if uuid else nv.nvmlDeviceGetHandleByIndex(device_index)
-            self.nvml, self.h = nv, h
-            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
-        except Exception:
-            self.nvml = None
-        self.thread = threading.Thread(target=self._run, daemon=True)
-        self.thread.start()
-
-    def _run(self):
-        if self.nvml is None:
-            return
-        nv = self.nvml
-        while not self.stop_flag.is_set():
-            try:
-                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
-                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
-                for name, mask in self.REASONS.items():
-                    if bits & mask:
-                        self.reasons.add(name)
-            except Exception:
-                return
-            time.sleep(0.005)
+        import multiprocessing as mp
+        ctx = mp.get_context("spawn")
+        self.conn, child = ctx.Pipe()
+        self.proc = ctx.Process(target=_clock_worker, args=(device_index, uuid, child, 0.005), daemon=True)
+        self.proc.start()
+        self.ok = self.conn.poll(120) and self.conn.recv() == "ready"
 
     def stop(self):
-        self.stop_flag.set()
-        self.thread.join(timeout=2)
-        if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["no NVML samples"], "samples": 0}
-        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
-                "reasons": sorted(self.reasons), "samples": len(self.samples), "source": "NVML, 5 ms"}
+        samples, reasons, max_mhz = [], [], None
+        if self.ok:
+            self.conn.send("stop")
+            if self.conn.poll(30):
+                samples, reasons, max_mhz = self.conn.recv()
+        self.proc.join(timeout=10)
+        if not samples:
+            return {"sm_mhz": None, "sm_max_mhz": max_mhz, "reasons": ["no NVML samples"], "samples": 0}
+        return {"sm_mhz": statistics.median(samples), "sm_max_mhz": max_mhz, "reasons": reasons,
+                "samples": len(samples), "source": "NVML, 5 ms, separate process"}
 
 
 def dist_setup():
@@ -267,6 +277,7 @@ def run_ours(args, pkg, world, rank, local):
     M = scene.map.shape[0]
     prm = ndt.reference_params(cfg.resolution, args.precision, args.dense_probe) if args.mode == "compat" else \
         ndt.corrected_params(cfg.resolution, args.precision, args.dense_probe)
+    prm.copy_groups = args.copy_groups
     ctx = ndt.Context(prm, device=local)
     ctx.set_profiling(True)
     st = torch.cuda.ExternalStream(ctx.stream, device=dev)
@@ -351,9 +362,15 @@ def run_ours(args, pkg, world, rank, local):
         ctx.align_batch_packed_ptr(B, h_pts.data_ptr(), h_off.data_ptr(), h_g.data_ptr(), h_out.data_ptr(),
                                    h_conv.data_ptr(), h_fit.data_ptr(), h_status.data_ptr())
 
-    for _ in range(args.warmup):
+    # warm-up: at least W steps and at least E2E_WARM_S seconds -- the
+    # host-to-device path of a freshly started process takes about a second of
+    # traffic to reach its steady rate (a serving loop runs warm)
+    t_warm = time.perf_counter()
+    n_warm = 0
+    while n_warm < args.warmup or time.perf_counter() - t_warm < E2E_WARM_S:
         flush_l2()
         host_step()
+        n_warm += 1
     e2e_ms = []
     for _ in range(args.steps):
         flush_l2()
@@ -366,6 +383,24 @@ def run_ours(args, pkg, world, rank, local):
         e1.synchronize()
         e2e_ms.append(e0.elapsed_time(e1))
     e2e_total = sum(e2e_ms)
+    # pinned host-to-device bandwidth on this box, for reading the e2e number
+    # (a separate pinned buffer and a torch-owned stream, so nothing here
+    # outlives the library's stream)
+    h_probe = torch.from_numpy(points).pin_memory()
+    d_tmp = torch.empty(h_probe.shape, dtype=h_probe.dtype, device=dev)
+    torch.cuda.synchronize()
+    h2d_ms = []
+    for _ in range(4):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        d_tmp.copy_(h_probe, non_blocking=True)
+        e1.record()
+        e1.synchronize()
+        h2d_ms.append(e0.elapsed_time(e1))
+    h2d_gbs = h_probe.numel() * 4 / (min(h2d_ms[1:]) / 1e3) / 1e9
+    torch.cuda.synchronize()
+    del d_tmp, h_probe
     clk = clocks.stop()
 
     # ---- max over ranks
@@ -424,6 +459,9 @@ def run_ours(args, pkg, world, rank, local):
         "config": config_block(cfg, args.mode, args.precision, B, npts),
         "e2e": {"value": e2e_value, "unit": "aligns/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_total / args.steps,
+                "pinned_h2d_gbs": round(h2d_gbs, 1),
+                "copy_groups": prm.copy_groups or "by size",
+                "warmup_steps": n_warm,
                 "path": "ndt_set_map + ndt_align_batch_packed (C ABI), pinned host buffers"},
         "roofline": roofline,
         "cpu_baseline": cpu,
@@ -455,6 +493,8 @@ def main(argv=None):
                     help="derivative-pass launch shape: an index, or 'auto' (autotuned on the workload)")
     ap.add_argument("--dense-probe", type=int, choices=[0, 1], default=0,
                     help="1: probe the dense cell index (27 cells per point) instead of the probe-window table")
+    ap.add_argument("--copy-groups", type=int, default=0,
+                    help="e2e: alignment groups whose host-to-device copy overlaps compute (0 = by size)")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

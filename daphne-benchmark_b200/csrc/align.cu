@@ -193,80 +193,112 @@ __device__ void advance(AlignState &s, const StepParams &P) {
     s.eval_mode = kEvalNone;
 }
 
-__global__ void init_kernel(AlignState *__restrict__ states, const float *__restrict__ guesses,
-                            const int *__restrict__ offsets, int B, StepParams P, double *__restrict__ exc) {
-    int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= B) return;
-    AlignState s;
-    for (int k = 0; k < 16; ++k) s.T[k] = guesses[16 * (size_t)b + k];
-    pose_vector(P.compat != 0, s.T, s.p);
-    if (!P.compat) build_tm_corrected(s.T, s.p);
-    for (int i = 0; i < 6; ++i) {
-        s.x_t[i] = s.p[i];
-        s.dir[i] = 0.0;
-        s.g[i] = 0.0;
-    }
-    for (int k = 0; k < 36; ++k) s.H[k] = 0.0;
-    s.score = 0.0;
-    s.phi_0 = s.d_phi_0 = s.a_l = s.f_l = s.g_l = s.a_u = s.f_u = s.g_u = s.a_t = 0.0;
-    s.phi_t = s.d_phi_t = s.psi_t = s.d_psi_t = 0.0;
-    s.step_max = P.step_max;
-    s.step_min = P.step_min;
-    s.nr_iterations = 0;
-    s.step_iterations = 0;
-    s.open_interval = 1;
-    s.interval_converged = 0;
-    s.converged = 0;
-    s.evals = 0;
-    s.status = 0;
-    s.n = offsets[b + 1] - offsets[b];
-    set_angles(s, s.p);
-    s.eval_mode = kEvalFull;
-    s.phase = kPhaseInitEval;
-    states[b] = s;
-    for (int k = 0; k < kPartial; ++k) exc[(size_t)b * kPartial + k] = 0.0;
+// One warp per alignment; lane 0 works on a shared-memory copy of the
+// alignment's state (the state machine is serial FP64 code that touches
+// hundreds of fields), and the warp moves the state between global and
+// shared memory in 16-byte pieces.
+constexpr int kStateWarps = 4;
+constexpr int kStateVecs = (int)(sizeof(AlignState) / sizeof(uint4));
+static_assert(sizeof(AlignState) % sizeof(uint4) == 0, "AlignState is copied in 16-byte pieces");
+
+__device__ __forceinline__ void copy_state(AlignState *dst, const AlignState *src, int lane) {
+    const uint4 *s = reinterpret_cast<const uint4 *>(src);
+    uint4 *d = reinterpret_cast<uint4 *>(dst);
+    for (int i = lane; i < kStateVecs; i += 32) d[i] = s[i];
 }
 
-// One warp per alignment: FP64 sum of the alignment's tile partials in tile
-// order (deterministic), then lane 0 advances the state machine.
-__global__ void step_kernel(AlignState *__restrict__ states, const double *__restrict__ partials,
-                            const int *__restrict__ tile_begin, double *__restrict__ exc, int B, StepParams P,
-                            int *__restrict__ active, Counters *__restrict__ counters) {
-    __shared__ double s_v[4][kPartial];
+__global__ void init_kernel(AlignState *__restrict__ states, const float *__restrict__ guesses,
+                            const int *__restrict__ offsets, int B, StepParams P, double *__restrict__ exc) {
+    __shared__ AlignState s_st[kStateWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int b = blockIdx.x * 4 + warp;
+    const int b = blockIdx.x * kStateWarps + warp;
+    if (b >= B) return;
+    for (int k = lane; k < kPartial; k += 32) exc[(size_t)b * kPartial + k] = 0.0;
+    AlignState &s = s_st[warp];
+    if (lane == 0) {
+        for (int k = 0; k < 16; ++k) s.T[k] = guesses[16 * (size_t)b + k];
+        pose_vector(P.compat != 0, s.T, s.p);
+        if (!P.compat) build_tm_corrected(s.T, s.p);
+        for (int i = 0; i < 6; ++i) {
+            s.x_t[i] = s.p[i];
+            s.dir[i] = 0.0;
+            s.g[i] = 0.0;
+        }
+        for (int k = 0; k < 36; ++k) s.H[k] = 0.0;
+        s.score = 0.0;
+        s.phi_0 = s.d_phi_0 = s.a_l = s.f_l = s.g_l = s.a_u = s.f_u = s.g_u = s.a_t = 0.0;
+        s.phi_t = s.d_phi_t = s.psi_t = s.d_psi_t = 0.0;
+        s.step_max = P.step_max;
+        s.step_min = P.step_min;
+        s.nr_iterations = 0;
+        s.step_iterations = 0;
+        s.open_interval = 1;
+        s.interval_converged = 0;
+        s.converged = 0;
+        s.evals = 0;
+        s.status = 0;
+        s.n = offsets[b + 1] - offsets[b];
+        set_angles(s, s.p);
+        s.eval_mode = kEvalFull;
+        s.phase = kPhaseInitEval;
+    }
+    __syncwarp();
+    copy_state(states + b, &s, lane);
+}
+
+// FP64 sum of the alignment's chunk partials in chunk order (deterministic;
+// each lane sums the values k = lane, lane + 32 with its loads issued 8 at a
+// time), then lane 0 advances the state machine.
+__global__ void step_kernel(AlignState *__restrict__ states, const double *__restrict__ partials,
+                            const int *__restrict__ chunk_begin, double *__restrict__ exc, int B, StepParams P,
+                            int *__restrict__ active, Counters *__restrict__ counters) {
+    __shared__ double s_v[kStateWarps][kPartial];
+    __shared__ AlignState s_st[kStateWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int b = blockIdx.x * kStateWarps + warp;
     if (b >= B) return;
     AlignState *st = states + b;
     const int mode = st->eval_mode;
     if (mode == kEvalNone) return;
-    const int t0 = tile_begin[b], t1 = tile_begin[b + 1];
+    const int c0 = chunk_begin[b], c1 = chunk_begin[b + 1];
     for (int k = lane; k < kPartial; k += 32) {
         double v = 0.0;
-        for (int t = t0; t < t1; ++t) v += partials[(size_t)t * kPartial + k];
+        int c = c0;
+        for (; c + 8 <= c1; c += 8) {
+            double t[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) t[u] = partials[(size_t)(c + u) * kPartial + k];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) v += t[u];
+        }
+        for (; c < c1; ++c) v += partials[(size_t)c * kPartial + k];
         double *e = exc + (size_t)b * kPartial + k;
         v += *e;
         *e = 0.0;
         s_v[warp][k] = v;
     }
+    AlignState &s = s_st[warp];
+    copy_state(&s, st, lane);
     __syncwarp();
-    if (lane != 0) return;
-    AlignState s = *st;
-    const double *v = s_v[warp];
-    if (mode == kEvalFull || mode == kEvalGradient) {
-        s.score = v[0];
-        for (int i = 0; i < 6; ++i) s.g[i] = v[1 + i];
+    if (lane == 0) {
+        const double *v = s_v[warp];
+        if (mode == kEvalFull || mode == kEvalGradient) {
+            s.score = v[0];
+            for (int i = 0; i < 6; ++i) s.g[i] = v[1 + i];
+        }
+        if (mode == kEvalFull || mode == kEvalHessian) {
+            for (int k = 0; k < 36; ++k) s.H[k] = v[7 + k];
+        } else {
+            for (int k = 0; k < 36; ++k) s.H[k] = 0.0;  // computeDerivatives zeroes it (kernel.cpp:667)
+        }
+        s.evals++;
+        s.eval_mode = kEvalNone;
+        advance(s, P);
+        if (s.eval_mode != kEvalNone) atomicAdd(active, 1);
+        if (counters) atomicAdd(&counters->evaluations, 1ull);
     }
-    if (mode == kEvalFull || mode == kEvalHessian) {
-        for (int k = 0; k < 36; ++k) s.H[k] = v[7 + k];
-    } else {
-        for (int k = 0; k < 36; ++k) s.H[k] = 0.0;  // computeDerivatives zeroes it (kernel.cpp:667)
-    }
-    s.evals++;
-    s.eval_mode = kEvalNone;
-    advance(s, P);
-    *st = s;
-    if (s.eval_mode != kEvalNone) atomicAdd(active, 1);
-    if (counters) atomicAdd(&counters->evaluations, 1ull);
+    __syncwarp();
+    copy_state(st, &s, lane);
 }
 
 __global__ void finalize_kernel(const AlignState *__restrict__ states, int B, float *__restrict__ out,
@@ -284,20 +316,30 @@ __global__ void finalize_kernel(const AlignState *__restrict__ states, int B, fl
     if (status) status[b] = st;
 }
 
-// Tile list: ceil(n_b / tile) tiles per alignment, in alignment order.
-__global__ void tile_count_kernel(const int *__restrict__ offsets, int B, int tile, int *__restrict__ tile_begin) {
+// Tile list: ceil(n_b / tile) tiles per alignment, in alignment order; chunk
+// list: ceil(tiles_b / K) chunks per alignment.
+__global__ void tile_count_kernel(const int *__restrict__ offsets, int B, int tile, int K, int *__restrict__ tile_begin,
+                                  int *__restrict__ chunk_begin) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b > B) return;
     if (b == B) {
         tile_begin[B] = 0;
+        chunk_begin[B] = 0;
         return;
     }
-    int n = offsets[b + 1] - offsets[b];
-    tile_begin[b] = n > 0 ? (n + tile - 1) / tile : 0;
+    const int n = offsets[b + 1] - offsets[b];
+    const int t = n > 0 ? (n + tile - 1) / tile : 0;
+    tile_begin[b] = t;
+    chunk_begin[b] = (t + K - 1) / K;
 }
 
-__global__ void scan_small_kernel(int *__restrict__ data, int n, int *__restrict__ total) {
+// Exclusive scan in place of n ints with one block of 1024 threads; block 0
+// scans `a` (total to *ta), block 1 scans `b` (total to *tb).
+__global__ void scan_pair_kernel(int *__restrict__ a, int *__restrict__ ta, int *__restrict__ b, int *__restrict__ tb,
+                                 int n) {
     __shared__ int s_warp[32];
+    int *data = blockIdx.x == 0 ? a : b;
+    int *total = blockIdx.x == 0 ? ta : tb;
     const int t = threadIdx.x, nt = blockDim.x;
     const int chunk = (n + nt - 1) / nt;
     const int lo = min(n, t * chunk), hi = min(n, lo + chunk);
@@ -330,19 +372,27 @@ __global__ void scan_small_kernel(int *__restrict__ data, int n, int *__restrict
     if (total && t == nt - 1) *total = run;
 }
 
-__global__ void tile_fill_kernel(const int *__restrict__ offsets, const int *__restrict__ tile_begin, int B, int tile,
-                                 Tile *__restrict__ tiles) {
+__global__ void tile_fill_kernel(const int *__restrict__ offsets, int B, int tile, int K, TileLists L) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (warp >= B) return;
     const int lo = offsets[warp], hi = offsets[warp + 1];
-    const int t0 = tile_begin[warp], t1 = tile_begin[warp + 1];
+    const int t0 = L.tile_begin[warp], t1 = L.tile_begin[warp + 1];
     for (int t = t0 + lane; t < t1; t += 32) {
         Tile x;
         x.align = warp;
         x.start = lo + (t - t0) * tile;
         x.end = min(hi, x.start + tile);
         x.slot = t;
-        tiles[t] = x;
+        L.tiles[t] = x;
+    }
+    const int c0 = L.chunk_begin[warp], c1 = L.chunk_begin[warp + 1];
+    for (int c = c0 + lane; c < c1; c += 32) {
+        Chunk x;
+        x.align = warp;
+        x.first = t0 + (c - c0) * K;
+        x.end = min(t1, x.first + K);
+        x.pad = 0;
+        L.chunks[c] = x;
     }
 }
 
@@ -372,23 +422,24 @@ int launch_prepare_eval(AlignState *d_state, const double *d_p6, int n, double *
     return (int)cudaGetLastError();
 }
 
-int launch_tiles(const int *d_offsets, int B, int tile, int *d_tile_begin, Tile *d_tiles, int *d_num_tiles,
-                 cudaStream_t st) {
-    tile_count_kernel<<<(B + 1 + 255) / 256, 256, 0, st>>>(d_offsets, B, tile, d_tile_begin);
-    scan_small_kernel<<<1, 1024, 0, st>>>(d_tile_begin, B + 1, d_num_tiles);
-    tile_fill_kernel<<<(B * 32 + 255) / 256, 256, 0, st>>>(d_offsets, d_tile_begin, B, tile, d_tiles);
+int launch_tiles(const int *d_offsets, int B, int tile, int K, const TileLists &L, cudaStream_t st) {
+    tile_count_kernel<<<(B + 1 + 255) / 256, 256, 0, st>>>(d_offsets, B, tile, K, L.tile_begin, L.chunk_begin);
+    scan_pair_kernel<<<2, 1024, 0, st>>>(L.tile_begin, L.num_tiles, L.chunk_begin, L.num_chunks, B + 1);
+    tile_fill_kernel<<<(B * 32 + 255) / 256, 256, 0, st>>>(d_offsets, B, tile, K, L);
     return (int)cudaGetLastError();
 }
 
 int launch_init(AlignState *d_states, const float *d_guesses, const int *d_offsets, int B, const StepParams &P,
                 double *d_exc, cudaStream_t st) {
-    init_kernel<<<(B + 127) / 128, 128, 0, st>>>(d_states, d_guesses, d_offsets, B, P, d_exc);
+    init_kernel<<<(B + kStateWarps - 1) / kStateWarps, 32 * kStateWarps, 0, st>>>(d_states, d_guesses, d_offsets, B,
+                                                                                  P, d_exc);
     return (int)cudaGetLastError();
 }
 
-int launch_step(AlignState *d_states, const double *d_partials, const int *d_tile_begin, double *d_exc, int B,
+int launch_step(AlignState *d_states, const double *d_partials, const int *d_chunk_begin, double *d_exc, int B,
                 const StepParams &P, int *d_active, Counters *d_counters, cudaStream_t st) {
-    step_kernel<<<(B + 3) / 4, 128, 0, st>>>(d_states, d_partials, d_tile_begin, d_exc, B, P, d_active, d_counters);
+    step_kernel<<<(B + kStateWarps - 1) / kStateWarps, 32 * kStateWarps, 0, st>>>(d_states, d_partials, d_chunk_begin,
+                                                                                  d_exc, B, P, d_active, d_counters);
     return (int)cudaGetLastError();
 }
 

@@ -18,11 +18,13 @@ struct StepParams {
     int watchdog_evals;
 };
 
-int launch_tiles(const int *d_offsets, int B, int tile, int *d_tile_begin, Tile *d_tiles, int *d_num_tiles,
-                 cudaStream_t st);
+// Tiles of `tile` points and chunks of up to K tiles for the alignments of a
+// batch (d_offsets: B + 1 point offsets; tile and chunk capacity: total /
+// tile + B + 1).
+int launch_tiles(const int *d_offsets, int B, int tile, int K, const TileLists &L, cudaStream_t st);
 int launch_init(AlignState *d_states, const float *d_guesses, const int *d_offsets, int B, const StepParams &P,
                 double *d_exc, cudaStream_t st);
-int launch_step(AlignState *d_states, const double *d_partials, const int *d_tile_begin, double *d_exc, int B,
+int launch_step(AlignState *d_states, const double *d_partials, const int *d_chunk_begin, double *d_exc, int B,
                 const StepParams &P, int *d_active, Counters *d_counters, cudaStream_t st);
 int launch_prepare_eval(AlignState *d_state, const double *d_p6, int n, double *d_exc, cudaStream_t st);
 int launch_finalize(const AlignState *d_states, int B, float *d_out, int *d_conv, double *d_fit, int *d_status,

@@ -12,10 +12,12 @@ struct EvalArgs {  // (GridDev is in ndt_types.h)
     const float4 *trans;   // optional: already transformed points (then T is not applied)
     const Tile *tiles;
     const int *num_tiles;  // device: number of tiles
+    const Chunk *chunks;   // chunks of tiles (FP32 pass; the FP64 pass uses chunks of 1 tile)
+    const int *num_chunks; // device: number of chunks
     int max_tiles;         // host-side upper bound (grid sizing)
     int tile_size;         // points per tile (must equal the kernel variant's block size)
     AlignState *states;
-    double *partials;      // [tile slot][kPartial]
+    double *partials;      // [chunk][kPartial]
     double *exc;           // [alignment][kPartial] FP64 side sums of flagged voxels (FP32 path)
     double d1, d2;         // Gauss constants (kernel.cpp:1181-1185)
     int compat;
@@ -24,9 +26,10 @@ struct EvalArgs {  // (GridDev is in ndt_types.h)
     unsigned *flag_n;      // queue length (reset by launch_derivatives)
     unsigned flag_cap;     // queue capacity
     int *flag_overflow;    // set when the queue overflowed
-    int *work_counter;     // FP32 pass: next chunk of tiles (reset by launch_derivatives)
-    int chunk_tiles;       // FP32 pass: tiles per chunk
+    int *work_counter;     // FP32 pass: next chunk (reset by launch_derivatives)
 };
+
+constexpr int kChunkTiles = 4;  // tiles per chunk of the FP32 pass (the FP64 pass: 1)
 
 // Per-device set-up (dynamic shared memory opt-in); call with the device current.
 int prepare_derivatives();

@@ -420,62 +420,35 @@ __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(EvalArgs arg
     P.d2 = (float)args.d2;
     P.compat = compat;
 
-    const int nt = *args.num_tiles;
-    const int K = args.chunk_tiles;
+    const int nc = *args.num_chunks;
     for (int k = 0; k < kAcc; ++k) P.acc[k * TILE] = 0.0f;
     if (lane == 0) s_cnt[warp][0] = s_cnt[warp][1] = s_cnt[warp][2] = 0;
     unsigned long long blk_probe = 0, blk_occ = 0, blk_pair = 0, blk_pts = 0, blk_tiles = 0;
-    int cur = -1, run_first = -1, mode = kEvalNone;
     unsigned head = 0, tail = 0;  // deferred ring of this warp (warp-uniform)
     int parity = 0;
 
-    // Ends the current alignment run: evaluates the deferred pairs, then
-    // reduces the block's sums into the run's partial.
-    auto end_run = [&]() {
-        while (tail != head) {
-            const int c = (int)min(32u, tail - head);
-            __syncwarp();
-            eval_deferred(P, ring, head, c);
-            head += c;
-        }
-        head = tail = 0;
-        reduce_run<kW>(sm, s_tot, s_cnt, args.partials + (size_t)run_first * kPartial, kR, compat);
-        __syncthreads();
-        if (lane == 0) s_cnt[warp][0] = s_cnt[warp][1] = s_cnt[warp][2] = 0;
-    };
-
-    // Chunks of K consecutive tiles are handed out dynamically (one atomic per
-    // chunk), so blocks finish together however uneven the alignments are.  A
-    // chunk's partial sums depend only on its tiles, so results do not depend
-    // on which block takes which chunk.
+    // Chunks are handed out dynamically (one atomic per chunk), so blocks
+    // finish together however uneven the alignments are.  A chunk's partial
+    // sums depend only on its own tiles, so results do not depend on which
+    // block takes which chunk.
     for (;;) {
         if (threadIdx.x == 0) s_chunk[parity] = atomicAdd(args.work_counter, 1);
         __syncthreads();
         const int chunk = s_chunk[parity];
         parity ^= 1;
-        const int t_begin = chunk * K;
-        if (t_begin >= nt) break;
-        const int t_end = min(nt, t_begin + K);
-        for (int ti = t_begin; ti < t_end; ++ti) {
+        if (chunk >= nc) break;
+        const Chunk ck = args.chunks[chunk];
+        const AlignState *st = args.states + ck.align;
+        if (threadIdx.x == 0) s_mode = st->eval_mode;
+        if (threadIdx.x < 12) s_T[threadIdx.x] = st->T[threadIdx.x];
+        if (threadIdx.x < kAngle) s_ang[threadIdx.x] = st->angf[threadIdx.x];
+        __syncthreads();
+        const int mode = s_mode;
+        if (mode == kEvalNone) continue;  // s_mode is rewritten only after the next chunk's barrier
+        P.align = ck.align;
+        P.hess = mode != kEvalGradient;
+        for (int ti = ck.first; ti < ck.end; ++ti) {
             const Tile tile = args.tiles[ti];
-            if (tile.align != cur || ti == t_begin) {
-                if (cur >= 0 && mode != kEvalNone) end_run();
-                __syncthreads();
-                const AlignState *st = args.states + tile.align;
-                if (threadIdx.x == 0) s_mode = st->eval_mode;
-                if (threadIdx.x < 12) s_T[threadIdx.x] = st->T[threadIdx.x];
-                if (threadIdx.x < kAngle) s_ang[threadIdx.x] = st->angf[threadIdx.x];
-                __syncthreads();
-                cur = tile.align;
-                run_first = ti;
-                mode = s_mode;
-                P.align = cur;
-                P.hess = mode != kEvalGradient;
-            } else if (mode != kEvalNone && threadIdx.x < kPartial) {
-                args.partials[(size_t)ti * kPartial + threadIdx.x] = 0.0;
-            }
-            if (mode == kEvalNone) continue;
-
             const int i = tile.start + threadIdx.x;
             const bool valid = i < tile.end;
             const float4 x = valid ? args.points[i] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -509,7 +482,7 @@ __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(EvalArgs arg
                             const unsigned code = own[k][lane];
                             const int slot = (int)(code >> 6);
                             if (code & 32u)
-                                queue_flagged(args, cur, i, slot);
+                                queue_flagged(args, ck.align, i, slot);
                             else
                                 add_pair(P, F, slot, px, py, pz);
                         }
@@ -545,9 +518,17 @@ __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(EvalArgs arg
             blk_pts += (unsigned long long)(tile.end - tile.start);
             blk_tiles += 1;
         }
-        // the run of this chunk ends with the chunk
-        if (cur >= 0 && mode != kEvalNone) end_run();
-        cur = -1;
+        // end of the chunk: the deferred pairs, then the block's sums
+        while (tail != head) {
+            const int c = (int)min(32u, tail - head);
+            __syncwarp();
+            eval_deferred(P, ring, head, c);
+            head += c;
+        }
+        head = tail = 0;
+        reduce_run<kW>(sm, s_tot, s_cnt, args.partials + (size_t)chunk * kPartial, kR, compat);
+        __syncthreads();
+        if (lane == 0) s_cnt[warp][0] = s_cnt[warp][1] = s_cnt[warp][2] = 0;
     }
     if (args.counters && lane == 0 && blk_tiles) {
         if (warp == 0) {

@@ -78,6 +78,8 @@ struct ndt_ctx {
     ndt_params prm{};
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;  // host-to-device copies of host-buffer batches
+    std::vector<cudaEvent_t> copy_ev;    // one per copied alignment group
     int num_sms = 148;
     std::string err;
     double d1 = 0, d2 = 0;
@@ -89,6 +91,7 @@ struct ndt_ctx {
     bool have_windows = false;
     int map_points = 0;
     // batch
+    DevBuf chunks, chunk_begin, num_chunks;
     DevBuf points, offsets, guesses, states, tiles, tile_begin, num_tiles, partials, exc, out_T, out_conv, out_fit,
         out_status, active, counters, p6, trans, flag_q, flag_n, flag_overflow, work_counter;
     HostBuf h_offsets, h_active, h_counters, h_out;
@@ -284,7 +287,6 @@ int build_grid(ndt_ctx *c, const float4 *d_map, int m) {
 }
 
 constexpr unsigned kFlagCap = 1u << 20;  // queued pairs with flagged voxels per derivative pass
-constexpr int kChunkTiles = 4;           // tiles per dynamically scheduled chunk of the FP32 pass
 
 int prepare_flag_queue(ndt_ctx *c, EvalArgs &ea) {
     CK(c->flag_q.ensure(sizeof(int4) * kFlagCap));
@@ -297,31 +299,54 @@ int prepare_flag_queue(ndt_ctx *c, EvalArgs &ea) {
     ea.flag_overflow = c->flag_overflow.as<int>();
     CK(c->work_counter.ensure(sizeof(int)));
     ea.work_counter = c->work_counter.as<int>();
-    ea.chunk_tiles = kChunkTiles;
     return NDT_OK;
 }
 
+// Tile and chunk lists for B alignments (capacity max_tiles each); the FP32
+// pass takes chunks of kChunkTiles tiles, the FP64 pass chunks of one tile.
+int prepare_lists(ndt_ctx *c, int B, int max_tiles, TileLists &L) {
+    CK(c->tile_begin.ensure(sizeof(int) * (size_t)(B + 1)));
+    CK(c->tiles.ensure(sizeof(Tile) * (size_t)max_tiles));
+    CK(c->num_tiles.ensure(sizeof(int)));
+    CK(c->chunk_begin.ensure(sizeof(int) * (size_t)(B + 1)));
+    CK(c->chunks.ensure(sizeof(Chunk) * (size_t)max_tiles));
+    CK(c->num_chunks.ensure(sizeof(int)));
+    L.tile_begin = c->tile_begin.as<int>();
+    L.tiles = c->tiles.as<Tile>();
+    L.num_tiles = c->num_tiles.as<int>();
+    L.chunk_begin = c->chunk_begin.as<int>();
+    L.chunks = c->chunks.as<Chunk>();
+    L.num_chunks = c->num_chunks.as<int>();
+    return NDT_OK;
+}
+
+int chunk_tiles(const ndt_ctx *c) { return c->prm.precision == 1 ? 1 : kChunkTiles; }
+
 // Device-side batch: everything already on the device.
+// first = false continues the counters and profiling events of the previous
+// call (alignment groups of one host batch).
 int run_batch(ndt_ctx *c, int B, const float4 *d_points, const int *d_offsets, int total, const float *d_guesses,
-              float *d_out, int *d_conv, double *d_fit, int *d_status) {
+              float *d_out, int *d_conv, double *d_fit, int *d_status, bool first = true) {
     if (!c->have_map) return fail(c, NDT_E_NOMAP, "no map set");
     if (B <= 0 || total < 0) return fail(c, NDT_E_ARG, "empty batch");
     const int tile = c->prm.precision == 1 ? kTile : kDerivVariants[c->variant].tile;
     const int max_tiles = total / tile + B + 1;
     CK(c->states.ensure(sizeof(AlignState) * (size_t)B));
-    CK(c->tile_begin.ensure(sizeof(int) * (size_t)(B + 1)));
-    CK(c->tiles.ensure(sizeof(Tile) * (size_t)max_tiles));
-    CK(c->num_tiles.ensure(sizeof(int)));
+    TileLists L;
+    if (int rc0 = prepare_lists(c, B, max_tiles, L)) return rc0;
     CK(c->partials.ensure(sizeof(double) * kPartial * (size_t)max_tiles));
     CK(c->exc.ensure(sizeof(double) * kPartial * (size_t)B));
     CK(c->active.ensure(sizeof(int)));
     CK(c->counters.ensure(sizeof(Counters)));
     CK(c->h_active.ensure(sizeof(int)));
     cudaStream_t st = c->stream;
-    CK(cudaMemsetAsync(c->counters.p, 0, sizeof(Counters), st));
-    c->ev_used = 0;
+    if (first) {
+        CK(cudaMemsetAsync(c->counters.p, 0, sizeof(Counters), st));
+        c->ev_used = 0;
+        c->last.rounds = 0;
+    }
     long long nl = 0;
-    int rc = launch_tiles(d_offsets, B, tile, c->tile_begin.as<int>(), c->tiles.as<Tile>(), c->num_tiles.as<int>(), st);
+    int rc = launch_tiles(d_offsets, B, tile, chunk_tiles(c), L, st);
     if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_tiles");
     nl += 3;
     const StepParams P = step_params(c->prm);
@@ -334,6 +359,8 @@ int run_batch(ndt_ctx *c, int B, const float4 *d_points, const int *d_offsets, i
     ea.trans = nullptr;
     ea.tiles = c->tiles.as<Tile>();
     ea.num_tiles = c->num_tiles.as<int>();
+    ea.chunks = L.chunks;
+    ea.num_chunks = L.num_chunks;
     ea.max_tiles = max_tiles;
     ea.tile_size = tile;
     ea.states = c->states.as<AlignState>();
@@ -359,7 +386,7 @@ int run_batch(ndt_ctx *c, int B, const float4 *d_points, const int *d_offsets, i
         cudaEvent_t e1 = c->profiling ? next_event(c) : nullptr;
         if (e1) CK(cudaEventRecord(e1, st));
         CK(cudaMemsetAsync(c->active.p, 0, sizeof(int), st));
-        rc = launch_step(c->states.as<AlignState>(), c->partials.as<double>(), c->tile_begin.as<int>(),
+        rc = launch_step(c->states.as<AlignState>(), c->partials.as<double>(), L.chunk_begin,
                          c->exc.as<double>(), B, P, c->active.as<int>(), c->counters.as<Counters>(), st);
         if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_step");
         nl += 1 + (c->prm.precision == 1 ? 1 : kDerivLaunchesFP32);
@@ -376,7 +403,7 @@ int run_batch(ndt_ctx *c, int B, const float4 *d_points, const int *d_offsets, i
     nl += 1;
     c->launches += nl;
     c->last.launches = c->launches;
-    c->last.rounds = rounds;
+    c->last.rounds += rounds;
     return NDT_OK;
 }
 
@@ -410,10 +437,77 @@ int read_counters(ndt_ctx *c) {
     return NDT_OK;
 }
 
-// Host batch: stage scans and guesses into the context's device buffers.
+// Number of alignment groups of a host-buffer batch: each group's points are
+// copied on the copy stream while the compute stream runs the previous
+// group's rounds (and, for the first group, the grid build of a map set just
+// before).  By size: about 2^20 points per group, at most 4 groups (each
+// group repeats the per-round fixed costs, so small groups do not pay).
+int copy_group_count(const ndt_ctx *c, int B, long long total) {
+    int g = c->prm.copy_groups > 0 ? c->prm.copy_groups : (int)std::min<long long>(4, total >> 20);
+    if (g < 1) g = 1;
+    if (g > B) g = B;
+    return g;
+}
+
+// Host batch: offsets (off[0] = 0) and guesses are host arrays; copy(b0, b1,
+// stream) enqueues the host-to-device copy of the points of alignments
+// [b0, b1) into c->points at off[b0].  Alignments are split into groups of
+// about equal point counts; group k's rounds wait only for group k's copy.
+template <class CopyFn>
+int staged_batch(ndt_ctx *c, int B, const int *off, const float *guesses, float *out, int *conv, double *fit,
+                 int *status, CopyFn copy) {
+    const long long total = off[B];
+    cudaStream_t st = c->stream, cs = c->copy_stream;
+    CK(c->points.ensure(sizeof(float4) * (size_t)(total > 0 ? total : 1)));
+    CK(c->offsets.ensure(sizeof(int) * (size_t)(B + 1)));
+    CK(c->guesses.ensure(sizeof(float) * 16 * (size_t)B));
+    CK(c->out_T.ensure(sizeof(float) * 16 * (size_t)B));
+    CK(c->out_conv.ensure(sizeof(int) * (size_t)B));
+    CK(c->out_fit.ensure(sizeof(double) * (size_t)B));
+    CK(c->out_status.ensure(sizeof(int) * (size_t)B));
+    const int G = copy_group_count(c, B, total);
+    while ((int)c->copy_ev.size() < G) {
+        cudaEvent_t e;
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        c->copy_ev.push_back(e);
+    }
+    CK(cudaMemcpyAsync(c->offsets.p, off, sizeof(int) * (size_t)(B + 1), cudaMemcpyHostToDevice, cs));
+    CK(cudaMemcpyAsync(c->guesses.p, guesses, sizeof(float) * 16 * (size_t)B, cudaMemcpyHostToDevice, cs));
+    int b0 = 0;
+    for (int k = 0; k < G; ++k) {
+        // group k ends at the first alignment whose start reaches (k + 1) / G of the points
+        int b1 = B;
+        if (k + 1 < G) {
+            const long long target = total * (k + 1) / G;
+            b1 = b0 + 1;
+            while (b1 < B - (G - 1 - k) && off[b1] < target) ++b1;
+        }
+        if (int rc = copy(b0, b1, cs)) return rc;
+        CK(cudaEventRecord(c->copy_ev[k], cs));
+        CK(cudaStreamWaitEvent(st, c->copy_ev[k], 0));
+        int rc = run_batch(c, b1 - b0, c->points.as<float4>(), c->offsets.as<int>() + b0, off[b1] - off[b0],
+                           c->guesses.as<float>() + 16 * (size_t)b0, c->out_T.as<float>() + 16 * (size_t)b0,
+                           c->out_conv.as<int>() + b0, c->out_fit.as<double>() + b0, c->out_status.as<int>() + b0,
+                           k == 0);
+        if (rc) {
+            cudaStreamSynchronize(cs);
+            return rc;
+        }
+        b0 = b1;
+    }
+    CK(cudaMemcpyAsync(out, c->out_T.p, sizeof(float) * 16 * (size_t)B, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(conv, c->out_conv.p, sizeof(int) * (size_t)B, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(fit, c->out_fit.p, sizeof(double) * (size_t)B, cudaMemcpyDeviceToHost, st));
+    if (status) CK(cudaMemcpyAsync(status, c->out_status.p, sizeof(int) * (size_t)B, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return NDT_OK;
+}
+
+// Host batch of separate scan buffers.
 int host_batch(ndt_ctx *c, int B, const float *const *scans, const int *ns, const float *guesses, float *out,
                int *conv, double *fit, int *status) {
     if (B <= 0 || !scans || !ns || !guesses || !out || !conv || !fit) return fail(c, NDT_E_ARG, "null argument");
+    if (!c->have_map) return fail(c, NDT_E_NOMAP, "no map set");
     CK(c->h_offsets.ensure(sizeof(int) * (size_t)(B + 1)));
     int *off = c->h_offsets.as<int>();
     long long total = 0;
@@ -424,60 +518,30 @@ int host_batch(ndt_ctx *c, int B, const float *const *scans, const int *ns, cons
         if (total > (1LL << 31) - 1) return fail(c, NDT_E_CAPACITY, "batch larger than 2^31 points");
         off[b + 1] = (int)total;
     }
-    cudaStream_t st = c->stream;
-    CK(c->points.ensure(sizeof(float4) * (size_t)(total > 0 ? total : 1)));
-    CK(c->offsets.ensure(sizeof(int) * (size_t)(B + 1)));
-    CK(c->guesses.ensure(sizeof(float) * 16 * (size_t)B));
-    CK(c->out_T.ensure(sizeof(float) * 16 * (size_t)B));
-    CK(c->out_conv.ensure(sizeof(int) * (size_t)B));
-    CK(c->out_fit.ensure(sizeof(double) * (size_t)B));
-    CK(c->out_status.ensure(sizeof(int) * (size_t)B));
-    for (int b = 0; b < B; ++b)
-        if (ns[b] > 0)
-            CK(cudaMemcpyAsync(c->points.as<float4>() + off[b], scans[b], sizeof(float4) * (size_t)ns[b],
-                               cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(c->offsets.p, off, sizeof(int) * (size_t)(B + 1), cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(c->guesses.p, guesses, sizeof(float) * 16 * (size_t)B, cudaMemcpyHostToDevice, st));
-    int rc = run_batch(c, B, c->points.as<float4>(), c->offsets.as<int>(), (int)total, c->guesses.as<float>(),
-                       c->out_T.as<float>(), c->out_conv.as<int>(), c->out_fit.as<double>(), c->out_status.as<int>());
-    if (rc) return rc;
-    CK(cudaMemcpyAsync(out, c->out_T.p, sizeof(float) * 16 * (size_t)B, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(conv, c->out_conv.p, sizeof(int) * (size_t)B, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(fit, c->out_fit.p, sizeof(double) * (size_t)B, cudaMemcpyDeviceToHost, st));
-    if (status) CK(cudaMemcpyAsync(status, c->out_status.p, sizeof(int) * (size_t)B, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    return NDT_OK;
+    return staged_batch(c, B, off, guesses, out, conv, fit, status, [&](int b0, int b1, cudaStream_t cs) -> int {
+        for (int b = b0; b < b1; ++b)
+            if (ns[b] > 0)
+                CK(cudaMemcpyAsync(c->points.as<float4>() + off[b], scans[b], sizeof(float4) * (size_t)ns[b],
+                                   cudaMemcpyHostToDevice, cs));
+        return NDT_OK;
+    });
 }
 
 // Host batch from one packed host buffer.
 int packed_batch(ndt_ctx *c, int B, const float *points, const int *offsets, const float *guesses, float *out,
                  int *conv, double *fit, int *status) {
     if (B <= 0 || !points || !offsets || !guesses || !out || !conv || !fit) return fail(c, NDT_E_ARG, "null argument");
+    if (!c->have_map) return fail(c, NDT_E_NOMAP, "no map set");
     if (offsets[0] != 0) return fail(c, NDT_E_ARG, "offsets[0] must be 0");
     for (int b = 0; b < B; ++b)
         if (offsets[b + 1] < offsets[b]) return fail(c, NDT_E_ARG, "offsets must be non-decreasing");
-    const int total = offsets[B];
-    cudaStream_t st = c->stream;
-    CK(c->points.ensure(sizeof(float4) * (size_t)(total > 0 ? total : 1)));
-    CK(c->offsets.ensure(sizeof(int) * (size_t)(B + 1)));
-    CK(c->guesses.ensure(sizeof(float) * 16 * (size_t)B));
-    CK(c->out_T.ensure(sizeof(float) * 16 * (size_t)B));
-    CK(c->out_conv.ensure(sizeof(int) * (size_t)B));
-    CK(c->out_fit.ensure(sizeof(double) * (size_t)B));
-    CK(c->out_status.ensure(sizeof(int) * (size_t)B));
-    if (total > 0)
-        CK(cudaMemcpyAsync(c->points.p, points, sizeof(float4) * (size_t)total, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(c->offsets.p, offsets, sizeof(int) * (size_t)(B + 1), cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(c->guesses.p, guesses, sizeof(float) * 16 * (size_t)B, cudaMemcpyHostToDevice, st));
-    int rc = run_batch(c, B, c->points.as<float4>(), c->offsets.as<int>(), total, c->guesses.as<float>(),
-                       c->out_T.as<float>(), c->out_conv.as<int>(), c->out_fit.as<double>(), c->out_status.as<int>());
-    if (rc) return rc;
-    CK(cudaMemcpyAsync(out, c->out_T.p, sizeof(float) * 16 * (size_t)B, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(conv, c->out_conv.p, sizeof(int) * (size_t)B, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(fit, c->out_fit.p, sizeof(double) * (size_t)B, cudaMemcpyDeviceToHost, st));
-    if (status) CK(cudaMemcpyAsync(status, c->out_status.p, sizeof(int) * (size_t)B, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    return NDT_OK;
+    return staged_batch(c, B, offsets, guesses, out, conv, fit, status, [&](int b0, int b1, cudaStream_t cs) -> int {
+        const long long n = (long long)offsets[b1] - offsets[b0];
+        if (n > 0)
+            CK(cudaMemcpyAsync(c->points.as<float4>() + offsets[b0], points + 4 * (size_t)offsets[b0],
+                               sizeof(float4) * (size_t)n, cudaMemcpyHostToDevice, cs));
+        return NDT_OK;
+    });
 }
 
 }  // namespace
@@ -547,6 +611,7 @@ int ndt_create(const ndt_params *params, int device, ndt_ctx **out) {
     c->inv_res = exact_reciprocal(c->prm.resolution);
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
     if (e == cudaSuccess) e = (cudaError_t)prepare_derivatives();
     if (e != cudaSuccess) {
@@ -561,17 +626,22 @@ void ndt_destroy(ndt_ctx *c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     DevBuf *bufs[] = {&c->win_off, &c->win_ent, &c->win_ctot, &c->map, &c->index, &c->mean, &c->mean_hi,
-                      &c->mean_lo, &c->icov32, &c->icov64, &c->count, &c->cell, &c->seg_start, &c->seg_cell, &c->scratch, &c->meta, &c->points, &c->offsets, &c->guesses, &c->states,
-                      &c->tiles, &c->tile_begin, &c->num_tiles, &c->partials, &c->exc, &c->out_T, &c->out_conv,
+                      &c->mean_lo, &c->icov32, &c->icov64, &c->count, &c->cell, &c->seg_start, &c->seg_cell,
+                      &c->scratch, &c->meta, &c->points, &c->offsets, &c->guesses, &c->states,
+                      &c->tiles, &c->tile_begin, &c->num_tiles, &c->chunks, &c->chunk_begin, &c->num_chunks,
+                      &c->partials, &c->exc, &c->out_T, &c->out_conv,
                       &c->out_fit, &c->out_status, &c->active, &c->counters, &c->p6, &c->trans,
                       &c->flag_q, &c->flag_n, &c->flag_overflow, &c->work_counter};
     for (DevBuf *b : bufs) b->release();
     HostBuf *hb[] = {&c->h_offsets, &c->h_active, &c->h_counters, &c->h_out};
     for (HostBuf *b : hb) b->release();
     for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
+    for (cudaEvent_t e : c->copy_ev) cudaEventDestroy(e);
     for (cudaEvent_t e : c->grid_ev)
         if (e) cudaEventDestroy(e);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -738,9 +808,8 @@ int ndt_derivatives(ndt_ctx *c, const float *scan, const float *trans, int n, co
     CK(c->trans.ensure(sizeof(float4) * (size_t)n));
     CK(c->offsets.ensure(sizeof(int) * 2));
     CK(c->states.ensure(sizeof(AlignState)));
-    CK(c->tile_begin.ensure(sizeof(int) * 2));
-    CK(c->tiles.ensure(sizeof(Tile) * (size_t)max_tiles));
-    CK(c->num_tiles.ensure(sizeof(int)));
+    TileLists L;
+    if (int rc0 = prepare_lists(c, 1, max_tiles, L)) return rc0;
     CK(c->partials.ensure(sizeof(double) * kPartial * (size_t)max_tiles));
     CK(c->exc.ensure(sizeof(double) * kPartial));
     CK(c->p6.ensure(sizeof(double) * 6));
@@ -754,8 +823,7 @@ int ndt_derivatives(ndt_ctx *c, const float *scan, const float *trans, int n, co
     CK(cudaMemcpyAsync(c->offsets.p, off, sizeof(int) * 2, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(c->p6.p, p6, sizeof(double) * 6, cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(c->counters.p, 0, sizeof(Counters), st));
-    int rc = launch_tiles(c->offsets.as<int>(), 1, tile, c->tile_begin.as<int>(), c->tiles.as<Tile>(),
-                          c->num_tiles.as<int>(), st);
+    int rc = launch_tiles(c->offsets.as<int>(), 1, tile, chunk_tiles(c), L, st);
     if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_tiles");
     rc = launch_prepare_eval(c->states.as<AlignState>(), c->p6.as<double>(), n, c->exc.as<double>(), st);
     if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_prepare_eval");
@@ -765,6 +833,8 @@ int ndt_derivatives(ndt_ctx *c, const float *scan, const float *trans, int n, co
     ea.trans = c->trans.as<float4>();
     ea.tiles = c->tiles.as<Tile>();
     ea.num_tiles = c->num_tiles.as<int>();
+    ea.chunks = L.chunks;
+    ea.num_chunks = L.num_chunks;
     ea.max_tiles = max_tiles;
     ea.tile_size = tile;
     ea.states = c->states.as<AlignState>();
@@ -779,7 +849,7 @@ int ndt_derivatives(ndt_ctx *c, const float *scan, const float *trans, int n, co
     if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_derivatives");
     int nt = 0;
     std::vector<double> part((size_t)max_tiles * kPartial), exc(kPartial);
-    CK(cudaMemcpyAsync(&nt, c->num_tiles.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&nt, c->num_chunks.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     CK(cudaMemcpyAsync(part.data(), c->partials.p, sizeof(double) * kPartial * (size_t)nt, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(exc.data(), c->exc.p, sizeof(double) * kPartial, cudaMemcpyDeviceToHost, st));

@@ -102,7 +102,29 @@ struct Tile {
     int32_t align;
     int32_t start;   // first point (global index into the concatenated scans)
     int32_t end;     // one past the last point
-    int32_t slot;    // partial slot of this tile
+    int32_t slot;    // index of this tile in the tile list
+};
+
+// Up to K consecutive tiles of one alignment, counted from the alignment's
+// first tile: the unit of work the derivative pass hands out, with one
+// partial-sum slot (partials[chunk]).  Chunk boundaries depend only on the
+// alignment's own point count, so an alignment's sums are the same in any
+// batch.
+struct Chunk {
+    int32_t align;
+    int32_t first;   // first tile
+    int32_t end;     // one past the last tile
+    int32_t pad;
+};
+
+// Tile and chunk lists of a batch (device).
+struct TileLists {
+    int *tile_begin;   // B + 1: first tile of each alignment
+    Tile *tiles;
+    int *num_tiles;
+    int *chunk_begin;  // B + 1: first chunk of each alignment
+    Chunk *chunks;
+    int *num_chunks;
 };
 
 }  // namespace ndt

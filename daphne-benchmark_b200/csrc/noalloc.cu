@@ -10,11 +10,11 @@
 // capture).  They set up a context and its map beforehand, then call this as
 // often as they like.
 //
-// Its scratch memory (tile list, one alignment state, per-tile partial sums,
-// the FP64 side queue, counters) is the file-scope array ndt_noalloc_scratch
-// below, sized for at most kNoAllocMaxPoints scan points.  Every GPU that
-// loads this library holds that array (256 KB) until the process
-// exits.  Host code cannot take the array's address directly (in host code
+// Its scratch memory (tile and chunk lists, one alignment state, per-chunk
+// partial sums, the FP64 side queue, counters) is the file-scope array
+// ndt_noalloc_scratch below, sized for at most kNoAllocMaxPoints scan points.
+// Every GPU that loads this library holds that array (at most 256 KB) until
+// the process exits.  Host code cannot take the array's address directly (in host code
 // the symbol is a host-side stand-in); the first call on each device, with
 // that device current, looks the device address up with cudaGetSymbolAddress
 // and caches it -- make that first call before any stream capture.
@@ -39,7 +39,7 @@ namespace {
 
 constexpr int kNoAllocMaxPoints = 65536;
 constexpr int kNoAllocMaxTiles = kNoAllocMaxPoints / 128 + 2;  // smallest tile: 128 points
-constexpr unsigned kNoAllocFlagCap = 4096;
+constexpr unsigned kNoAllocFlagCap = 2048;
 
 // Layout of the scratch array.
 struct NoAllocScratch {
@@ -48,16 +48,20 @@ struct NoAllocScratch {
     int offsets[2];
     int tile_begin[2];
     int num_tiles;
+    int chunk_begin[2];
+    int num_chunks;
     unsigned flag_n;
     int flag_overflow;
     int work_counter;
     double exc[kPartial];
     Tile tiles[kNoAllocMaxTiles];
+    Chunk chunks[kNoAllocMaxTiles];
     int4 flag_q[kNoAllocFlagCap];
     double partials[kNoAllocMaxTiles * kPartial];
 };
 
 constexpr size_t kNoAllocScratchBytes = (sizeof(NoAllocScratch) + 255) & ~(size_t)255;
+static_assert(kNoAllocScratchBytes <= 256 * 1024, "the static scratch is documented as at most 256 KB");
 
 static __device__ __align__(256) unsigned char ndt_noalloc_scratch[kNoAllocScratchBytes];
 
@@ -96,13 +100,13 @@ __global__ void noalloc_setup_kernel(NoAllocScratch *s, Pose6 pose, int n) {
     }
 }
 
-// out[k] = sum over tiles (in tile order) + side sums; out[43] = pairs, or -1
+// out[k] = sum over chunks (in chunk order) + side sums; out[43] = pairs, or -1
 // when the FP64 side queue overflowed.
 __global__ void noalloc_reduce_kernel(const NoAllocScratch *s, double *out) {
     const int k = threadIdx.x;
     if (k >= kPartial) return;
     double v = 0.0;
-    for (int t = 0; t < s->num_tiles; ++t) v += s->partials[(size_t)t * kPartial + k];
+    for (int t = 0; t < s->num_chunks; ++t) v += s->partials[(size_t)t * kPartial + k];
     v += s->exc[k];
     if (k == kPartial - 1 && (s->flag_overflow || s->flag_n > kNoAllocFlagCap)) v = -1.0;
     out[k] = v;
@@ -157,7 +161,14 @@ extern "C" int ndt_derivatives_noalloc(ndt_ctx *ctx, const float *d_scan, const 
     Pose6 pose;
     for (int i = 0; i < 6; ++i) pose.p[i] = p6[i];
     noalloc_setup_kernel<<<1, 64, 0, st>>>(s, pose, n);
-    int rc = launch_tiles(s->offsets, 1, tile, s->tile_begin, s->tiles, &s->num_tiles, st);
+    TileLists L;
+    L.tile_begin = s->tile_begin;
+    L.tiles = s->tiles;
+    L.num_tiles = &s->num_tiles;
+    L.chunk_begin = s->chunk_begin;
+    L.chunks = s->chunks;
+    L.num_chunks = &s->num_chunks;
+    int rc = launch_tiles(s->offsets, 1, tile, v.precision == 1 ? 1 : kChunkTiles, L, st);
     if (rc) {
         ctx_set_error(ctx, cudaGetErrorString((cudaError_t)rc));
         return NDT_E_CUDA;
@@ -168,6 +179,8 @@ extern "C" int ndt_derivatives_noalloc(ndt_ctx *ctx, const float *d_scan, const 
     ea.trans = reinterpret_cast<const float4 *>(d_trans);
     ea.tiles = s->tiles;
     ea.num_tiles = &s->num_tiles;
+    ea.chunks = s->chunks;
+    ea.num_chunks = &s->num_chunks;
     ea.max_tiles = n / tile + 2;
     ea.tile_size = tile;
     ea.states = &s->state;
@@ -182,7 +195,6 @@ extern "C" int ndt_derivatives_noalloc(ndt_ctx *ctx, const float *d_scan, const 
     ea.flag_cap = kNoAllocFlagCap;
     ea.flag_overflow = &s->flag_overflow;
     ea.work_counter = &s->work_counter;
-    ea.chunk_tiles = 4;
     rc = launch_derivatives(ea, v.precision, v.variant, v.sms, st);
     if (rc) {
         ctx_set_error(ctx, cudaGetErrorString((cudaError_t)rc));

@@ -61,7 +61,8 @@ extern "C" {
  */
 typedef struct ndt_params {
     float resolution;              /* voxel edge length [m] (kernel.cpp:38) */
-    float _pad0;
+    int32_t copy_groups;           /* host-buffer batch calls: alignment groups whose host-to-device
+                                      copy overlaps the previous group's rounds (0 = by size) */
     double outlier_ratio;          /* kernel.cpp:37 */
     double step_size;              /* More-Thuente step_max (kernel.cpp:40) */
     double transformation_epsilon; /* step_min = eps/2 and |step| < eps stop (kernel.cpp:56) */
@@ -219,7 +220,7 @@ NDT_API int ndt_derivatives(ndt_ctx *ctx, const float *scan, const float *trans,
  * pose vector for the angle terms); d_out receives 44 doubles: score,
  * gradient[6], Hessian[36] row major, pair count (-1 if more pairs hit
  * degenerate voxels than the side queue holds).  Scratch is one static device
- * array per GPU (256 KB, held until exit), so n is limited to 65536
+ * array per GPU (at most 256 KB, held until exit), so n is limited to 65536
  * (NDT_E_CAPACITY beyond).  The first call on a device looks the array up
  * (cudaGetSymbolAddress); make it before any stream capture.  Work is
  * enqueued on the context stream (call ndt_synchronize before reading

@@ -31,7 +31,7 @@ class NdtParams(C.Structure):
 
     _fields_ = [
         ("resolution", C.c_float),
-        ("_pad0", C.c_float),
+        ("copy_groups", C.c_int32),
         ("outlier_ratio", C.c_double),
         ("step_size", C.c_double),
         ("transformation_epsilon", C.c_double),

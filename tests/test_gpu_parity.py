@@ -187,3 +187,28 @@ def test_corrected_vs_fp64_oracle(pkg, oracle, binding_mod, precision):
         assert dt <= 0.02 and dr <= 0.1, (i, dt, dr)
         assert conv[i] == rconv[i] and status[i] == 0
     print(f"corrected mode, precision {precision}: worst {worst_t:.2e} m, {worst_r:.2e} deg")
+
+
+def test_copy_groups_do_not_change_results(pkg, cases):
+    """Host batches copied in 1, 2 or 3 alignment groups (each group's rounds
+    overlap the next group's copy) give bit-identical poses and the same
+    work counters: every alignment's arithmetic is independent of the batch."""
+    c0 = [c for c in cases if c["config"]["name"] == "s8k"]
+    cfg, scene, _ = _inputs(pkg, c0[0])
+    aligns = [pkg.synth.make_alignment(cfg, scene, i) for i in range(7)]
+    res = []
+    for groups in (1, 2, 3):
+        prm = pkg.ndt.reference_params()
+        prm.copy_groups = groups
+        with pkg.ndt.Context(prm) as ctx:
+            ctx.set_map(scene.map)
+            out, conv, fit, status = ctx.align_batch([a.scan for a in aligns], [a.guess for a in aligns])
+            k = ctx.counters()
+            res.append((out.view(np.uint32).copy(), conv.copy(), fit.copy(), status.copy(),
+                        (k["pairs"], k["probes"], k["occupied_probes"], k["evaluations"])))
+    for r in res[1:]:
+        assert np.array_equal(r[0], res[0][0])
+        assert np.array_equal(r[1], res[0][1])
+        assert np.array_equal(r[2], res[0][2])
+        assert np.array_equal(r[3], res[0][3])
+        assert r[4] == res[0][4]
