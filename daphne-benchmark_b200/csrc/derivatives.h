@@ -29,6 +29,7 @@ struct EvalArgs {  // (GridDev is in ndt_types.h)
     int *work_counter;     // FP32 pass: next chunk (reset by launch_derivatives)
 };
 
+constexpr int kOwn = 27;        // accepted pairs of one point per collect call, at most (3 x 3 x 3 probes)
 constexpr int kChunkTiles = 4;  // tiles per chunk of the FP32 pass (the FP64 pass: 1)
 
 // Per-device set-up (dynamic shared memory opt-in); call with the device current.

@@ -245,7 +245,7 @@ __device__ void pair_fp64_flagged(double *exc, const float *t, float p0f, float 
 // Pairs with a flagged voxel queued by the FP32 pass: (alignment, point,
 // slot).  The point is transformed and its per-point terms recomputed exactly
 // as the FP32 pass does, then the pair is evaluated in FP64.
-__global__ void flagged_kernel(EvalArgs args) {
+__global__ void flagged_kernel(const __grid_constant__ EvalArgs args) {
     const unsigned n = *args.flag_n;
     const unsigned m = n < args.flag_cap ? n : args.flag_cap;
     for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < m; q += gridDim.x * blockDim.x) {
@@ -286,44 +286,48 @@ struct F32Smem {
     uint2 defer[W][kDefer];          // deferred pairs: (slot << 6 | flag << 5, point index)
 };
 
-// Block-wide reduction of the per-lane sums of one alignment run, written as
-// the FP64 partial of the run's first tile; resets the sums.  Warp w reduces
-// the values w, w + W, ...: each lane sums W of the block's lane sums
-// (conflict-free rows of shared memory) with TwoSum compensation, then the
-// warp combines its 32 (sum, error) pairs with shuffles.  Fixed order, so the
-// result does not depend on timing.
+// Block-wide reduction of the per-lane FP32 sums of one chunk into the
+// chunk's FP64 partial; resets the sums.  Warp w reduces the values w,
+// w + W, ...: each lane adds W of the block's lane sums in FP64 (conflict-free
+// rows of shared memory), then the warp adds its 32 lane sums with a fixed
+// shuffle tree, also in FP64 (B200 issues FP64 adds at half the FP32 rate, and
+// the sums of FP32 values stay exact or nearly so).  Fixed order, so the
+// result does not depend on timing.  A chunk in which no warp found a pair
+// writes its zeros directly.
 template <int W>
 __device__ void reduce_run(F32Smem<W> &sm, double *s_tot, const unsigned (*s_cnt)[3], double *out, double kR,
                            bool compat) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     __syncthreads();
+    unsigned np = 0;
+#pragma unroll
+    for (int w = 0; w < W; ++w) np += s_cnt[w][2];
+    if (np == 0) {  // block-uniform
+        if (threadIdx.x < kPartial) out[threadIdx.x] = 0.0;
+        return;
+    }
     for (int k = warp; k < kAcc; k += W) {
-        float s = 0.0f, e = 0.0f;
+        double sum = 0.0;
 #pragma unroll
         for (int r = 0; r < W; ++r) {
             const float v = sm.acc[k][32 * r + lane];
             sm.acc[k][32 * r + lane] = 0.0f;
-            float t, err;
-            two_sum(s, v, t, err);
-            s = t;
-            e = __fadd_rn(e, err);
+            sum += (double)v;
         }
-        warp_two_sum_reduce(s, e);
-        if (lane == 0) s_tot[k] = (double)s + (double)e;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
+        if (lane == 0) s_tot[k] = sum;
     }
     __syncthreads();
     if (threadIdx.x < kPartial) {
         const int k = threadIdx.x;
         double v;
-        if (k < 7) {
+        if (k < 7)
             v = s_tot[k];
-        } else if (k < 43) {
+        else if (k < 43)
             v = h_entry(s_tot, (k - 7) / 6, (k - 7) % 6, kR, compat);
-        } else {
-            unsigned np = 0;
-            for (int w = 0; w < W; ++w) np += s_cnt[w][2];
+        else
             v = (double)np;
-        }
         out[k] = v;
     }
 }
@@ -391,7 +395,7 @@ __device__ __forceinline__ void eval_deferred(const WarpPairs &P, const uint2 *r
 }
 
 template <int TILE, int MINB>
-__global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(EvalArgs args) {
+__global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(const __grid_constant__ EvalArgs args) {
     constexpr int kW = TILE / 32;
     __shared__ float s_T[12];
     __shared__ float s_ang[kAngle];
@@ -430,8 +434,9 @@ __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(EvalArgs arg
     // Chunks are handed out dynamically (one atomic per chunk), so blocks
     // finish together however uneven the alignments are.  A chunk's partial
     // sums depend only on its own tiles, so results do not depend on which
-    // block takes which chunk.
-    for (;;) {
+    // block takes which chunk.  (No block takes more than nc chunks; the
+    // bound only guards against a corrupted counter.)
+    for (int it = 0; it <= nc; ++it) {
         if (threadIdx.x == 0) s_chunk[parity] = atomicAdd(args.work_counter, 1);
         __syncthreads();
         const int chunk = s_chunk[parity];

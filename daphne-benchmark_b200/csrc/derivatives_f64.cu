@@ -87,7 +87,7 @@ __device__ void pair_fp64(AccD &A, const double *x, const double *ang, const dou
 
 constexpr int kTile64 = 256;
 
-__global__ void __launch_bounds__(kTile64, 1) derivative_f64_kernel(EvalArgs args) {
+__global__ void __launch_bounds__(kTile64, 1) derivative_f64_kernel(const __grid_constant__ EvalArgs args) {
     constexpr int kW = kTile64 / 32;
     __shared__ float s_T[12];
     __shared__ double s_ang[kAngle];

@@ -234,11 +234,4 @@ __device__ inline double trial_value(double a_l, double f_l, double g_l, double 
     return (a_u + (a_t - a_u) * (w - g_u - z) / (g_t - g_u + 2 * w));
 }
 
-// Error-free sum of two floats (Knuth TwoSum): s + e == a + b exactly.
-__device__ __forceinline__ void two_sum(float a, float b, float &s, float &e) {
-    s = __fadd_rn(a, b);
-    float bb = __fsub_rn(s, a);
-    e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
-}
-
 }  // namespace ndt

@@ -145,9 +145,10 @@ __device__ __forceinline__ int window_base(const Axis &a, int dim, bool &ok) {
 }
 
 // Where collect_pairs puts the accepted pairs (code = slot << 6 | flag << 5 |
-// lane).  ListSink compacts the warp's pairs into one list (capacity 27 x 32,
-// `n` entries); OwnSink keeps each lane's pairs in its own column,
-// own[k][lane] for k < c (at most kOwn per lane).
+// lane): add() on the windows and dense paths, add_far() on the generic path.
+// ListSink compacts the warp's pairs into one list (capacity 27 x 32, `n`
+// entries); OwnSink keeps each lane's pairs in its own column, own[k][lane]
+// for k < c (at most kOwn per lane).
 struct ListSink {
     unsigned *list;
     int n;
@@ -156,10 +157,9 @@ struct ListSink {
         if (ok) list[n + __popc(bal & lanemask_lt())] = code;
         n += __popc(bal);
     }
+    __device__ __forceinline__ void add_far(bool ok, unsigned code) { add(ok, code); }
     __device__ __forceinline__ bool full() const { return n > kList - 32; }
 };
-
-constexpr int kOwn = 27;  // accepted pairs per lane and collect call, at most
 
 struct OwnSink {
     unsigned (*own)[32];
@@ -167,6 +167,7 @@ struct OwnSink {
     __device__ __forceinline__ void add(bool ok, unsigned code) {
         if (ok) own[c++][threadIdx.x & 31] = code;
     }
+    __device__ __forceinline__ void add_far(bool ok, unsigned code) { add(ok, code); }
     __device__ __forceinline__ bool full() const { return __any_sync(kFull, c >= kOwn); }
 };
 
@@ -178,9 +179,9 @@ struct OwnSink {
 //   windows  the probe-window table (2 offsets + 1 record per occupied cell),
 //            when the table exists and every lane's cells are consecutive;
 //   dense    the 27 dense-index entries in 3 layers of 9 loads, skipping with
-//            warp-uniform branches the layers no lane has in bounds or
-//            occupied, the distance tests of probes no lane occupies and the
-//            appends of probes no lane accepted;
+//            warp-uniform branches the layers and rows no lane has in bounds
+//            or occupied, the distance tests of probes no lane occupies and
+//            the appends of probes no lane accepted;
 //   generic  one probe at a time, the reference's loop as written.
 // The pairs are the reference's on every path; only their order differs.
 template <class Sink>
@@ -263,23 +264,21 @@ __device__ __forceinline__ void collect_pairs(const GridDev &grid, float px, flo
             n_probe += __popc(on_mask);
             n_occ += __popc(occ);
             if (!__any_sync(kFull, occ != 0u)) continue;
-            float4 hi[9];
+            // one row of 3 cells at a time: means, distance tests, appends
 #pragma unroll
-            for (int k = 0; k < 9; ++k)
-                if ((occ >> k) & 1u) hi[k] = __ldg(grid.mean_hi + (v[k] & kSlotMask));
-            unsigned acc = 0;
+            for (int b = 0; b < 3; ++b) {
+                const unsigned row = (occ >> (3 * b)) & 7u;
+                if (!__any_sync(kFull, row != 0u)) continue;
+                float4 hi[3];
 #pragma unroll
-            for (int k = 0; k < 9; ++k) {
-                if (__any_sync(kFull, (occ >> k) & 1u)) {
-                    const bool ok = ((occ >> k) & 1u) && accept(grid, v[k] & kSlotMask, hi[k], px, py, pz, tol);
-                    acc |= (unsigned)ok << k;
+                for (int c = 0; c < 3; ++c)
+                    if ((row >> c) & 1u) hi[c] = __ldg(grid.mean_hi + (v[3 * b + c] & kSlotMask));
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    if (!__any_sync(kFull, (row >> c) & 1u)) continue;
+                    const bool ok = ((row >> c) & 1u) && accept(grid, v[3 * b + c] & kSlotMask, hi[c], px, py, pz, tol);
+                    if (__any_sync(kFull, ok)) sink.add(ok, pair_code(v[3 * b + c], lane));
                 }
-            }
-            if (!__any_sync(kFull, acc != 0u)) continue;
-#pragma unroll
-            for (int k = 0; k < 9; ++k) {
-                const bool ok = (acc >> k) & 1u;
-                if (__any_sync(kFull, ok)) sink.add(ok, pair_code(v[k], lane));
             }
         }
         resume = -1;
@@ -312,25 +311,13 @@ __device__ __forceinline__ void collect_pairs(const GridDev &grid, float px, flo
             ++n_occ;
             ok = accept(grid, v & kSlotMask, __ldg(grid.mean_hi + (v & kSlotMask)), px, py, pz, tol);
         }
-        sink.add(ok, pair_code(v, lane));
+        sink.add_far(ok, pair_code(v, lane));
     }
     resume = -1;
 }
 
 // ---------------------------------------------------------------------------
-// Reduction helpers.
-__device__ __forceinline__ void warp_two_sum_reduce(float &s, float &e) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        float so = __shfl_xor_sync(kFull, s, o);
-        float eo = __shfl_xor_sync(kFull, e, o);
-        float t, err;
-        two_sum(s, so, t, err);
-        s = t;
-        e = __fadd_rn(__fadd_rn(e, eo), err);
-    }
-}
-
+// Partial layout helpers.
 __device__ __forceinline__ int sidx(int i, int j) {  // upper-triangle index, i <= j
     return i * 6 - (i * (i - 1)) / 2 + (j - i);
 }
