@@ -316,30 +316,47 @@ __global__ void finalize_kernel(const AlignState *__restrict__ states, int B, fl
     if (status) status[b] = st;
 }
 
-// Tile list: ceil(n_b / tile) tiles per alignment, in alignment order; chunk
-// list: ceil(tiles_b / K) chunks per alignment.
-__global__ void tile_count_kernel(const int *__restrict__ offsets, int B, int tile, int K, int *__restrict__ tile_begin,
-                                  int *__restrict__ chunk_begin) {
+// Chunk plan of an alignment with t tiles: large chunks of kb tiles over the
+// first tiles, leaving at least 4 small chunks' worth (4 ks tiles, or all of
+// them when t is smaller) for small chunks of ks tiles.
+__device__ __forceinline__ void chunk_plan(int t, int kb, int ks, int &nb, int &ns) {
+    const int keep = min(t, 4 * ks);
+    nb = (t - keep) / kb;
+    const int rest = t - nb * kb;
+    ns = (rest + ks - 1) / ks;
+}
+
+// Tile list: ceil(n_b / tile) tiles per alignment, in alignment order; the
+// large and small chunk counts per alignment.
+__global__ void tile_count_kernel(const int *__restrict__ offsets, int B, int tile, int kb, int ks, TileLists L) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b > B) return;
     if (b == B) {
-        tile_begin[B] = 0;
-        chunk_begin[B] = 0;
+        L.tile_begin[B] = 0;
+        L.big_begin[B] = 0;
+        L.small_begin[B] = 0;
         return;
     }
     const int n = offsets[b + 1] - offsets[b];
     const int t = n > 0 ? (n + tile - 1) / tile : 0;
-    tile_begin[b] = t;
-    chunk_begin[b] = (t + K - 1) / K;
+    int nb, ns;
+    chunk_plan(t, kb, ks, nb, ns);
+    L.tile_begin[b] = t;
+    L.big_begin[b] = nb;
+    L.small_begin[b] = ns;
 }
 
-// Exclusive scan in place of n ints with one block of 1024 threads; block 0
-// scans `a` (total to *ta), block 1 scans `b` (total to *tb).
-__global__ void scan_pair_kernel(int *__restrict__ a, int *__restrict__ ta, int *__restrict__ b, int *__restrict__ tb,
-                                 int n) {
+// Exclusive scans in place of three arrays of n ints, one block of 1024
+// threads per array (block k scans arrays[k], total to *totals[k]).
+struct ScanArgs {
+    int *data[3];
+    int *total[3];
+};
+
+__global__ void scan3_kernel(ScanArgs a, int n) {
     __shared__ int s_warp[32];
-    int *data = blockIdx.x == 0 ? a : b;
-    int *total = blockIdx.x == 0 ? ta : tb;
+    int *data = a.data[blockIdx.x];
+    int *total = a.total[blockIdx.x];
     const int t = threadIdx.x, nt = blockDim.x;
     const int chunk = (n + nt - 1) / nt;
     const int lo = min(n, t * chunk), hi = min(n, lo + chunk);
@@ -372,7 +389,9 @@ __global__ void scan_pair_kernel(int *__restrict__ a, int *__restrict__ ta, int 
     if (total && t == nt - 1) *total = run;
 }
 
-__global__ void tile_fill_kernel(const int *__restrict__ offsets, int B, int tile, int K, TileLists L) {
+// One warp per alignment writes its tiles, its chunks (large ones at the
+// front of the list, small ones after every large one) and its slot range.
+__global__ void tile_fill_kernel(const int *__restrict__ offsets, int B, int tile, int kb, int ks, TileLists L) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (warp >= B) return;
     const int lo = offsets[warp], hi = offsets[warp + 1];
@@ -385,14 +404,29 @@ __global__ void tile_fill_kernel(const int *__restrict__ offsets, int B, int til
         x.slot = t;
         L.tiles[t] = x;
     }
-    const int c0 = L.chunk_begin[warp], c1 = L.chunk_begin[warp + 1];
-    for (int c = c0 + lane; c < c1; c += 32) {
+    const int b0 = L.big_begin[warp], nb = L.big_begin[warp + 1] - b0;
+    const int s0 = L.small_begin[warp], ns = L.small_begin[warp + 1] - s0;
+    const int slot0 = b0 + s0;
+    const int total_big = *L.num_big;
+    if (lane == 0) {
+        L.chunk_begin[warp] = slot0;
+        if (warp == B - 1) L.chunk_begin[B] = *L.num_chunks = slot0 + nb + ns;
+    }
+    for (int j = lane; j < nb + ns; j += 32) {
         Chunk x;
         x.align = warp;
-        x.first = t0 + (c - c0) * K;
-        x.end = min(t1, x.first + K);
-        x.pad = 0;
-        L.chunks[c] = x;
+        int pos;
+        if (j < nb) {
+            x.first = t0 + j * kb;
+            x.end = x.first + kb;
+            pos = b0 + j;
+        } else {
+            x.first = t0 + nb * kb + (j - nb) * ks;
+            x.end = min(t1, x.first + ks);
+            pos = total_big + s0 + (j - nb);
+        }
+        x.slot = slot0 + j;
+        L.chunks[pos] = x;
     }
 }
 
@@ -422,10 +456,17 @@ int launch_prepare_eval(AlignState *d_state, const double *d_p6, int n, double *
     return (int)cudaGetLastError();
 }
 
-int launch_tiles(const int *d_offsets, int B, int tile, int K, const TileLists &L, cudaStream_t st) {
-    tile_count_kernel<<<(B + 1 + 255) / 256, 256, 0, st>>>(d_offsets, B, tile, K, L.tile_begin, L.chunk_begin);
-    scan_pair_kernel<<<2, 1024, 0, st>>>(L.tile_begin, L.num_tiles, L.chunk_begin, L.num_chunks, B + 1);
-    tile_fill_kernel<<<(B * 32 + 255) / 256, 256, 0, st>>>(d_offsets, B, tile, K, L);
+int launch_tiles(const int *d_offsets, int B, int tile, int kb, int ks, const TileLists &L, cudaStream_t st) {
+    tile_count_kernel<<<(B + 1 + 255) / 256, 256, 0, st>>>(d_offsets, B, tile, kb, ks, L);
+    ScanArgs a;
+    a.data[0] = L.tile_begin;
+    a.total[0] = L.num_tiles;
+    a.data[1] = L.big_begin;
+    a.total[1] = L.num_big;
+    a.data[2] = L.small_begin;
+    a.total[2] = nullptr;
+    scan3_kernel<<<3, 1024, 0, st>>>(a, B + 1);
+    tile_fill_kernel<<<(B * 32 + 255) / 256, 256, 0, st>>>(d_offsets, B, tile, kb, ks, L);
     return (int)cudaGetLastError();
 }
 

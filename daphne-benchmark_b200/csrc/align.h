@@ -18,10 +18,10 @@ struct StepParams {
     int watchdog_evals;
 };
 
-// Tiles of `tile` points and chunks of up to K tiles for the alignments of a
-// batch (d_offsets: B + 1 point offsets; tile and chunk capacity: total /
-// tile + B + 1).
-int launch_tiles(const int *d_offsets, int B, int tile, int K, const TileLists &L, cudaStream_t st);
+// Tiles of `tile` points and chunks (large: kb tiles, small: ks tiles) for
+// the alignments of a batch (d_offsets: B + 1 point offsets; tile and chunk
+// capacity: total / tile + B + 1).
+int launch_tiles(const int *d_offsets, int B, int tile, int kb, int ks, const TileLists &L, cudaStream_t st);
 int launch_init(AlignState *d_states, const float *d_guesses, const int *d_offsets, int B, const StepParams &P,
                 double *d_exc, cudaStream_t st);
 int launch_step(AlignState *d_states, const double *d_partials, const int *d_chunk_begin, double *d_exc, int B,

@@ -30,7 +30,8 @@ struct EvalArgs {  // (GridDev is in ndt_types.h)
 };
 
 constexpr int kOwn = 27;        // accepted pairs of one point per collect call, at most (3 x 3 x 3 probes)
-constexpr int kChunkTiles = 4;  // tiles per chunk of the FP32 pass (the FP64 pass: 1)
+constexpr int kChunkBig = 8;    // tiles per large chunk of the FP32 pass (the FP64 pass: 1)
+constexpr int kChunkSmall = 2;  // tiles per small chunk of the FP32 pass (the FP64 pass: 1)
 
 // Per-device set-up (dynamic shared memory opt-in); call with the device current.
 int prepare_derivatives();

@@ -531,7 +531,7 @@ __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(const __grid
             head += c;
         }
         head = tail = 0;
-        reduce_run<kW>(sm, s_tot, s_cnt, args.partials + (size_t)chunk * kPartial, kR, compat);
+        reduce_run<kW>(sm, s_tot, s_cnt, args.partials + (size_t)ck.slot * kPartial, kR, compat);
         __syncthreads();
         if (lane == 0) s_cnt[warp][0] = s_cnt[warp][1] = s_cnt[warp][2] = 0;
     }

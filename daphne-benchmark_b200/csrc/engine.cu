@@ -91,7 +91,7 @@ struct ndt_ctx {
     bool have_windows = false;
     int map_points = 0;
     // batch
-    DevBuf chunks, chunk_begin, num_chunks;
+    DevBuf chunks, chunk_begin, num_chunks, big_begin, small_begin, num_big;
     DevBuf points, offsets, guesses, states, tiles, tile_begin, num_tiles, partials, exc, out_T, out_conv, out_fit,
         out_status, active, counters, p6, trans, flag_q, flag_n, flag_overflow, work_counter;
     HostBuf h_offsets, h_active, h_counters, h_out;
@@ -303,7 +303,8 @@ int prepare_flag_queue(ndt_ctx *c, EvalArgs &ea) {
 }
 
 // Tile and chunk lists for B alignments (capacity max_tiles each); the FP32
-// pass takes chunks of kChunkTiles tiles, the FP64 pass chunks of one tile.
+// pass takes chunks of kChunkBig and kChunkSmall tiles, the FP64 pass chunks
+// of one tile.
 int prepare_lists(ndt_ctx *c, int B, int max_tiles, TileLists &L) {
     CK(c->tile_begin.ensure(sizeof(int) * (size_t)(B + 1)));
     CK(c->tiles.ensure(sizeof(Tile) * (size_t)max_tiles));
@@ -317,10 +318,17 @@ int prepare_lists(ndt_ctx *c, int B, int max_tiles, TileLists &L) {
     L.chunk_begin = c->chunk_begin.as<int>();
     L.chunks = c->chunks.as<Chunk>();
     L.num_chunks = c->num_chunks.as<int>();
+    CK(c->big_begin.ensure(sizeof(int) * (size_t)(B + 1)));
+    CK(c->small_begin.ensure(sizeof(int) * (size_t)(B + 1)));
+    CK(c->num_big.ensure(sizeof(int)));
+    L.big_begin = c->big_begin.as<int>();
+    L.small_begin = c->small_begin.as<int>();
+    L.num_big = c->num_big.as<int>();
     return NDT_OK;
 }
 
-int chunk_tiles(const ndt_ctx *c) { return c->prm.precision == 1 ? 1 : kChunkTiles; }
+int chunk_big(const ndt_ctx *c) { return c->prm.precision == 1 ? 1 : kChunkBig; }
+int chunk_small(const ndt_ctx *c) { return c->prm.precision == 1 ? 1 : kChunkSmall; }
 
 // Device-side batch: everything already on the device.
 // first = false continues the counters and profiling events of the previous
@@ -346,7 +354,7 @@ int run_batch(ndt_ctx *c, int B, const float4 *d_points, const int *d_offsets, i
         c->last.rounds = 0;
     }
     long long nl = 0;
-    int rc = launch_tiles(d_offsets, B, tile, chunk_tiles(c), L, st);
+    int rc = launch_tiles(d_offsets, B, tile, chunk_big(c), chunk_small(c), L, st);
     if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_tiles");
     nl += 3;
     const StepParams P = step_params(c->prm);
@@ -631,6 +639,7 @@ void ndt_destroy(ndt_ctx *c) {
                       &c->mean_lo, &c->icov32, &c->icov64, &c->count, &c->cell, &c->seg_start, &c->seg_cell,
                       &c->scratch, &c->meta, &c->points, &c->offsets, &c->guesses, &c->states,
                       &c->tiles, &c->tile_begin, &c->num_tiles, &c->chunks, &c->chunk_begin, &c->num_chunks,
+                      &c->big_begin, &c->small_begin, &c->num_big,
                       &c->partials, &c->exc, &c->out_T, &c->out_conv,
                       &c->out_fit, &c->out_status, &c->active, &c->counters, &c->p6, &c->trans,
                       &c->flag_q, &c->flag_n, &c->flag_overflow, &c->work_counter};
@@ -823,7 +832,7 @@ int ndt_derivatives(ndt_ctx *c, const float *scan, const float *trans, int n, co
     CK(cudaMemcpyAsync(c->offsets.p, off, sizeof(int) * 2, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(c->p6.p, p6, sizeof(double) * 6, cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(c->counters.p, 0, sizeof(Counters), st));
-    int rc = launch_tiles(c->offsets.as<int>(), 1, tile, chunk_tiles(c), L, st);
+    int rc = launch_tiles(c->offsets.as<int>(), 1, tile, chunk_big(c), chunk_small(c), L, st);
     if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_tiles");
     rc = launch_prepare_eval(c->states.as<AlignState>(), c->p6.as<double>(), n, c->exc.as<double>(), st);
     if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_prepare_eval");

@@ -105,16 +105,18 @@ struct Tile {
     int32_t slot;    // index of this tile in the tile list
 };
 
-// Up to K consecutive tiles of one alignment, counted from the alignment's
-// first tile: the unit of work the derivative pass hands out, with one
-// partial-sum slot (partials[chunk]).  Chunk boundaries depend only on the
-// alignment's own point count, so an alignment's sums are the same in any
-// batch.
+// Consecutive tiles of one alignment: the unit of work the derivative pass
+// hands out, with one partial-sum slot (partials[slot]; an alignment's slots
+// are contiguous, chunk_begin[b] .. chunk_begin[b + 1]).  An alignment's
+// tiles are cut, from its first tile, into large chunks and then a few small
+// ones (the last tiles); the list holds every large chunk of the batch before
+// any small one, so the blocks finish together.  Chunk boundaries depend only
+// on the alignment's own point count, so its sums are the same in any batch.
 struct Chunk {
     int32_t align;
     int32_t first;   // first tile
     int32_t end;     // one past the last tile
-    int32_t pad;
+    int32_t slot;    // partial-sum slot
 };
 
 // Tile and chunk lists of a batch (device).
@@ -122,9 +124,12 @@ struct TileLists {
     int *tile_begin;   // B + 1: first tile of each alignment
     Tile *tiles;
     int *num_tiles;
-    int *chunk_begin;  // B + 1: first chunk of each alignment
-    Chunk *chunks;
+    int *chunk_begin;  // B + 1: first partial slot of each alignment
+    Chunk *chunks;     // large chunks, then small chunks
     int *num_chunks;
+    int *big_begin;    // B + 1: scratch (large chunks before each alignment)
+    int *small_begin;  // B + 1: scratch (small chunks before each alignment)
+    int *num_big;      // total large chunks
 };
 
 }  // namespace ndt

@@ -14,10 +14,11 @@
 // partial sums, the FP64 side queue, counters) is the file-scope array
 // ndt_noalloc_scratch below, sized for at most kNoAllocMaxPoints scan points.
 // Every GPU that loads this library holds that array (at most 256 KB) until
-// the process exits.  Host code cannot take the array's address directly (in host code
-// the symbol is a host-side stand-in); the first call on each device, with
-// that device current, looks the device address up with cudaGetSymbolAddress
-// and caches it -- make that first call before any stream capture.
+// the process exits.  Host code cannot take the array's address directly (in
+// host code the symbol is a host-side stand-in); the first call on each
+// device, with that device current, looks the device address up with
+// cudaGetSymbolAddress and caches it -- make that first call before any
+// stream capture.
 //
 // Every call shares the one array and keeps the previous call's contents:
 // each call clears what must start at zero before it runs, and two calls whose
@@ -50,6 +51,9 @@ struct NoAllocScratch {
     int num_tiles;
     int chunk_begin[2];
     int num_chunks;
+    int big_begin[2];
+    int small_begin[2];
+    int num_big;
     unsigned flag_n;
     int flag_overflow;
     int work_counter;
@@ -168,7 +172,11 @@ extern "C" int ndt_derivatives_noalloc(ndt_ctx *ctx, const float *d_scan, const 
     L.chunk_begin = s->chunk_begin;
     L.chunks = s->chunks;
     L.num_chunks = &s->num_chunks;
-    int rc = launch_tiles(s->offsets, 1, tile, v.precision == 1 ? 1 : kChunkTiles, L, st);
+    L.big_begin = s->big_begin;
+    L.small_begin = s->small_begin;
+    L.num_big = &s->num_big;
+    const bool f64 = v.precision == 1;
+    int rc = launch_tiles(s->offsets, 1, tile, f64 ? 1 : kChunkBig, f64 ? 1 : kChunkSmall, L, st);
     if (rc) {
         ctx_set_error(ctx, cudaGetErrorString((cudaError_t)rc));
         return NDT_E_CUDA;
