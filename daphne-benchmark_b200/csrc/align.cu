@@ -255,6 +255,7 @@ __global__ void step_kernel(AlignState *__restrict__ states, const double *__res
     __shared__ double s_v[kStateWarps][kPartial];
     __shared__ AlignState s_st[kStateWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (counters && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&counters->rounds, 1ull);
     const int b = blockIdx.x * kStateWarps + warp;
     if (b >= B) return;
     AlignState *st = states + b;

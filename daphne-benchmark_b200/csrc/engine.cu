@@ -72,6 +72,30 @@ struct HostBuf {
     }
 };
 
+// Everything one batch enqueues (pointers, sizes, parameters): the key of its
+// cached CUDA graph, compared byte for byte (zero-filled before use).
+struct RunPlan {
+    EvalArgs ea;
+    TileLists L;
+    StepParams P;
+    const int *d_offsets;
+    const float *d_guesses;
+    float *d_out;
+    int *d_conv;
+    double *d_fit;
+    int *d_status;
+    int *active;
+    int *round_no;
+    unsigned long long *dev_launches;
+    int B, tile, kb, ks, max_rounds, precision, variant, sms, fixed;
+};
+
+struct BatchGraph {
+    RunPlan key;
+    cudaGraphExec_t exec;
+    unsigned long long last_use;
+};
+
 }  // namespace
 
 struct ndt_ctx {
@@ -79,6 +103,10 @@ struct ndt_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t copy_stream = nullptr;  // host-to-device copies of host-buffer batches
+    cudaStream_t aux_stream = nullptr;   // capture of the round body of batch graphs
+    bool use_graphs = true;              // device batches as CUDA graphs (when profiling is off)
+    std::vector<BatchGraph> graphs;      // cached batch graphs, least recently used evicted
+    unsigned long long graph_clock = 0;
     std::vector<cudaEvent_t> copy_ev;    // one per copied alignment group
     int num_sms = 148;
     std::string err;
@@ -91,7 +119,7 @@ struct ndt_ctx {
     bool have_windows = false;
     int map_points = 0;
     // batch
-    DevBuf chunks, chunk_begin, num_chunks, big_begin, small_begin, num_big;
+    DevBuf chunks, chunk_begin, num_chunks, big_begin, small_begin, num_big, round_no, dev_launches;
     DevBuf points, offsets, guesses, states, tiles, tile_begin, num_tiles, partials, exc, out_T, out_conv, out_fit,
         out_status, active, counters, p6, trans, flag_q, flag_n, flag_overflow, work_counter;
     HostBuf h_offsets, h_active, h_counters, h_out;
@@ -292,7 +320,6 @@ int prepare_flag_queue(ndt_ctx *c, EvalArgs &ea) {
     CK(c->flag_q.ensure(sizeof(int4) * kFlagCap));
     CK(c->flag_n.ensure(sizeof(unsigned)));
     CK(c->flag_overflow.ensure(sizeof(int)));
-    CK(cudaMemsetAsync(c->flag_overflow.p, 0, sizeof(int), c->stream));
     ea.flag_q = c->flag_q.as<int4>();
     ea.flag_n = c->flag_n.as<unsigned>();
     ea.flag_cap = kFlagCap;
@@ -331,6 +358,150 @@ int chunk_big(const ndt_ctx *c) { return c->prm.precision == 1 ? 1 : kChunkBig; 
 int chunk_small(const ndt_ctx *c) { return c->prm.precision == 1 ? 1 : kChunkSmall; }
 
 // Device-side batch: everything already on the device.
+// Round-loop condition of a batch graph: another round while an alignment
+// asked for an evaluation and the round budget (the evaluation watchdog) is
+// not spent, so the loop always ends.
+__global__ void round_cond_kernel(cudaGraphConditionalHandle h, const int *active, int *round_no, int max_rounds,
+                                  unsigned long long *launches, int per_round) {
+    const int r = ++*round_no;
+    *launches += (unsigned long long)per_round;
+    cudaGraphSetConditional(h, (*active > 0 && r < max_rounds) ? 1u : 0u);
+}
+
+int enqueue_prologue(ndt_ctx *c, const RunPlan &R, cudaStream_t st) {
+    CK(cudaMemsetAsync(R.ea.flag_overflow, 0, sizeof(int), st));
+    CK(cudaMemsetAsync(R.round_no, 0, sizeof(int), st));
+    int rc = launch_tiles(R.d_offsets, R.B, R.tile, R.kb, R.ks, R.L, st);
+    if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_tiles");
+    rc = launch_init(R.ea.states, R.d_guesses, R.d_offsets, R.B, R.P, R.ea.exc, st);
+    if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_init");
+    return NDT_OK;
+}
+
+// One round: the derivative pass, then the step kernel (which counts in
+// *active the alignments that ask for another evaluation).
+int enqueue_round(ndt_ctx *c, const RunPlan &R, cudaStream_t st, bool profile) {
+    cudaEvent_t e0 = profile ? next_event(c) : nullptr;
+    if (e0) CK(cudaEventRecord(e0, st));
+    int rc = launch_derivatives(R.ea, R.precision, R.variant, R.sms, st);
+    if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_derivatives");
+    cudaEvent_t e1 = profile ? next_event(c) : nullptr;
+    if (e1) CK(cudaEventRecord(e1, st));
+    CK(cudaMemsetAsync(R.active, 0, sizeof(int), st));
+    rc = launch_step(R.ea.states, R.ea.partials, R.L.chunk_begin, R.ea.exc, R.B, R.P, R.active, R.ea.counters, st);
+    if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_step");
+    return NDT_OK;
+}
+
+int enqueue_epilogue(ndt_ctx *c, const RunPlan &R, cudaStream_t st) {
+    int rc = launch_finalize(R.ea.states, R.B, R.d_out, R.d_conv, R.d_fit, R.d_status, R.ea.flag_overflow, st);
+    if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_finalize");
+    return NDT_OK;
+}
+
+// Kernel launches of one round (derivative pass + step kernel).
+int round_launches(const RunPlan &R) { return 1 + (R.precision == 1 ? 1 : kDerivLaunchesFP32); }
+
+// The batch as one CUDA graph: prologue, a conditional WHILE node whose body
+// is one round plus round_cond_kernel, epilogue.  Built by stream capture
+// (the round body on the auxiliary stream, into the WHILE node's body graph).
+int build_batch_graph(ndt_ctx *c, const RunPlan &R, cudaGraphExec_t *out) {
+    cudaGraph_t g = nullptr;
+    CK(cudaGraphCreate(&g, 0));
+    cudaStream_t st = c->stream;
+    auto abort_capture = [&](int code) {
+        cudaGraph_t tmp = nullptr;
+        cudaStreamEndCapture(st, &tmp);
+        cudaGraphDestroy(g);
+        return code;
+    };
+    cudaGraphConditionalHandle h;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return cuda_fail(c, e, "cudaGraphConditionalHandleCreate");
+    }
+    e = cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return cuda_fail(c, e, "cudaStreamBeginCaptureToGraph");
+    }
+    if (int rc = enqueue_prologue(c, R, st)) return abort_capture(rc);
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &nd);
+    if (e != cudaSuccess) return abort_capture(cuda_fail(c, e, "cudaStreamGetCaptureInfo"));
+    // (cudaGraphNodeParams has no default constructor: zeroed raw storage)
+    alignas(cudaGraphNodeParams) unsigned char np_raw[sizeof(cudaGraphNodeParams)];
+    std::memset(np_raw, 0, sizeof(np_raw));
+    cudaGraphNodeParams &np = *reinterpret_cast<cudaGraphNodeParams *>(np_raw);
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    e = cudaGraphAddNode(&node, cg, deps, nd, &np);
+    if (e != cudaSuccess) return abort_capture(cuda_fail(c, e, "cudaGraphAddNode (while)"));
+    e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
+    if (e != cudaSuccess) return abort_capture(cuda_fail(c, e, "cudaStreamUpdateCaptureDependencies"));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(c->aux_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return abort_capture(cuda_fail(c, e, "cudaStreamBeginCaptureToGraph (body)"));
+    int rc = enqueue_round(c, R, c->aux_stream, false);
+    if (!rc) {
+        round_cond_kernel<<<1, 1, 0, c->aux_stream>>>(h, R.active, R.round_no, R.max_rounds, R.dev_launches,
+                                                       round_launches(R) + 1);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) rc = cuda_fail(c, e, "round_cond_kernel");
+    }
+    cudaGraph_t body_out = nullptr;
+    e = cudaStreamEndCapture(c->aux_stream, &body_out);
+    if (rc) return abort_capture(rc);
+    if (e != cudaSuccess) return abort_capture(cuda_fail(c, e, "cudaStreamEndCapture (body)"));
+    if (int rc2 = enqueue_epilogue(c, R, st)) return abort_capture(rc2);
+    cudaGraph_t g_out = nullptr;
+    e = cudaStreamEndCapture(st, &g_out);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return cuda_fail(c, e, "cudaStreamEndCapture");
+    }
+    e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate");
+    return NDT_OK;
+}
+
+constexpr size_t kMaxGraphs = 8;  // cached batch graphs per context
+
+int get_batch_graph(ndt_ctx *c, const RunPlan &R, cudaGraphExec_t *out) {
+    ++c->graph_clock;
+    for (BatchGraph &b : c->graphs) {
+        if (std::memcmp(&b.key, &R, sizeof(RunPlan)) == 0) {
+            b.last_use = c->graph_clock;
+            *out = b.exec;
+            return NDT_OK;
+        }
+    }
+    cudaGraphExec_t exec = nullptr;
+    if (int rc = build_batch_graph(c, R, &exec)) return rc;
+    if (c->graphs.size() >= kMaxGraphs) {
+        size_t lru = 0;
+        for (size_t i = 1; i < c->graphs.size(); ++i)
+            if (c->graphs[i].last_use < c->graphs[lru].last_use) lru = i;
+        cudaGraphExecDestroy(c->graphs[lru].exec);
+        c->graphs.erase(c->graphs.begin() + (long)lru);
+    }
+    BatchGraph b;
+    std::memcpy(&b.key, &R, sizeof(RunPlan));
+    b.exec = exec;
+    b.last_use = c->graph_clock;
+    c->graphs.push_back(b);
+    *out = exec;
+    return NDT_OK;
+}
+
 // first = false continues the counters and profiling events of the previous
 // call (alignment groups of one host batch).
 int run_batch(ndt_ctx *c, int B, const float4 *d_points, const int *d_offsets, int total, const float *d_guesses,
@@ -340,35 +511,29 @@ int run_batch(ndt_ctx *c, int B, const float4 *d_points, const int *d_offsets, i
     const int tile = c->prm.precision == 1 ? kTile : kDerivVariants[c->variant].tile;
     const int max_tiles = total / tile + B + 1;
     CK(c->states.ensure(sizeof(AlignState) * (size_t)B));
-    TileLists L;
-    if (int rc0 = prepare_lists(c, B, max_tiles, L)) return rc0;
+    RunPlan R;
+    std::memset(&R, 0, sizeof(R));
+    if (int rc0 = prepare_lists(c, B, max_tiles, R.L)) return rc0;
     CK(c->partials.ensure(sizeof(double) * kPartial * (size_t)max_tiles));
     CK(c->exc.ensure(sizeof(double) * kPartial * (size_t)B));
     CK(c->active.ensure(sizeof(int)));
     CK(c->counters.ensure(sizeof(Counters)));
     CK(c->h_active.ensure(sizeof(int)));
+    CK(c->round_no.ensure(sizeof(int)));
     cudaStream_t st = c->stream;
     if (first) {
         CK(cudaMemsetAsync(c->counters.p, 0, sizeof(Counters), st));
         c->ev_used = 0;
-        c->last.rounds = 0;
     }
-    long long nl = 0;
-    int rc = launch_tiles(d_offsets, B, tile, chunk_big(c), chunk_small(c), L, st);
-    if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_tiles");
-    nl += 3;
-    const StepParams P = step_params(c->prm);
-    rc = launch_init(c->states.as<AlignState>(), d_guesses, d_offsets, B, P, c->exc.as<double>(), st);
-    if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_init");
-    nl += 1;
-    EvalArgs ea;
+    R.P = step_params(c->prm);
+    EvalArgs &ea = R.ea;
     ea.grid = grid_dev(c);
     ea.points = d_points;
     ea.trans = nullptr;
     ea.tiles = c->tiles.as<Tile>();
     ea.num_tiles = c->num_tiles.as<int>();
-    ea.chunks = L.chunks;
-    ea.num_chunks = L.num_chunks;
+    ea.chunks = R.L.chunks;
+    ea.num_chunks = R.L.num_chunks;
     ea.max_tiles = max_tiles;
     ea.tile_size = tile;
     ea.states = c->states.as<AlignState>();
@@ -379,39 +544,53 @@ int run_batch(ndt_ctx *c, int B, const float4 *d_points, const int *d_offsets, i
     ea.compat = c->prm.compat;
     ea.counters = c->counters.as<Counters>();
     if (int rc2 = prepare_flag_queue(c, ea)) return rc2;
+    R.d_offsets = d_offsets;
+    R.d_guesses = d_guesses;
+    R.d_out = d_out;
+    R.d_conv = d_conv;
+    R.d_fit = d_fit;
+    R.d_status = d_status;
+    R.active = c->active.as<int>();
+    R.round_no = c->round_no.as<int>();
+    R.dev_launches = c->dev_launches.as<unsigned long long>();
+    R.B = B;
+    R.tile = tile;
+    R.kb = chunk_big(c);
+    R.ks = chunk_small(c);
+    R.precision = c->prm.precision;
+    R.variant = c->variant;
+    R.sms = c->num_sms;
     // With the reference's line-search test (compat, step_max > step_min)
     // every Newton iteration takes at most one evaluation, so the round count
-    // is fixed and no host polling is needed.
-    const bool fixed = P.compat && (P.step_max - P.step_min) > 0;
-    const int max_rounds = fixed ? P.max_iterations + 3 : P.watchdog_evals + 1;
+    // is fixed.
+    R.fixed = R.P.compat && (R.P.step_max - R.P.step_min) > 0;
+    R.max_rounds = R.fixed ? R.P.max_iterations + 3 : R.P.watchdog_evals + 1;
+
+    if (c->use_graphs && !c->profiling) {
+        // one graph launch: the rounds run on the device until no alignment
+        // asks for an evaluation, with no host synchronisation
+        cudaGraphExec_t exec = nullptr;
+        if (int rc = get_batch_graph(c, R, &exec)) return rc;
+        CK(cudaGraphLaunch(exec, st));
+        c->launches += 5;  // tiles (3), init, finalize; the rounds count themselves on the device
+        return NDT_OK;
+    }
+    long long nl = 0;
+    if (int rc = enqueue_prologue(c, R, st)) return rc;
+    nl += 4;
     const int poll_every = 4;
-    int rounds = 0;
-    for (int r = 0; r < max_rounds; ++r) {
-        cudaEvent_t e0 = c->profiling ? next_event(c) : nullptr;
-        if (e0) CK(cudaEventRecord(e0, st));
-        rc = launch_derivatives(ea, c->prm.precision, c->variant, c->num_sms, st);
-        if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_derivatives");
-        cudaEvent_t e1 = c->profiling ? next_event(c) : nullptr;
-        if (e1) CK(cudaEventRecord(e1, st));
-        CK(cudaMemsetAsync(c->active.p, 0, sizeof(int), st));
-        rc = launch_step(c->states.as<AlignState>(), c->partials.as<double>(), L.chunk_begin,
-                         c->exc.as<double>(), B, P, c->active.as<int>(), c->counters.as<Counters>(), st);
-        if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_step");
-        nl += 1 + (c->prm.precision == 1 ? 1 : kDerivLaunchesFP32);
-        ++rounds;
-        if (!fixed && (r + 1) % poll_every == 0) {
+    for (int r = 0; r < R.max_rounds; ++r) {
+        if (int rc = enqueue_round(c, R, st, c->profiling)) return rc;
+        nl += round_launches(R);
+        if (!R.fixed && (r + 1) % poll_every == 0) {
             CK(cudaMemcpyAsync(c->h_active.p, c->active.p, sizeof(int), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             if (*c->h_active.as<int>() == 0) break;
         }
     }
-    rc = launch_finalize(c->states.as<AlignState>(), B, d_out, d_conv, d_fit, d_status, c->flag_overflow.as<int>(),
-                         st);
-    if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_finalize");
+    if (int rc = enqueue_epilogue(c, R, st)) return rc;
     nl += 1;
     c->launches += nl;
-    c->last.launches = c->launches;
-    c->last.rounds += rounds;
     return NDT_OK;
 }
 
@@ -420,6 +599,10 @@ int read_counters(ndt_ctx *c) {
     CK(cudaMemcpyAsync(c->h_counters.p, c->counters.p, sizeof(Counters), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     const Counters *k = c->h_counters.as<Counters>();
+    c->last.rounds = (int64_t)k->rounds;
+    unsigned long long dl = 0;
+    if (c->dev_launches.p) CK(cudaMemcpy(&dl, c->dev_launches.p, sizeof(dl), cudaMemcpyDeviceToHost));
+    c->last.launches = c->launches + (long long)dl;
     c->last.points = (int64_t)k->points;
     c->last.probes = (int64_t)k->probes;
     c->last.occupied_probes = (int64_t)k->occupied_probes;
@@ -620,6 +803,9 @@ int ndt_create(const ndt_params *params, int device, ndt_ctx **out) {
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = c->dev_launches.ensure(sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(c->dev_launches.p, 0, sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
     if (e == cudaSuccess) e = (cudaError_t)prepare_derivatives();
     if (e != cudaSuccess) {
@@ -639,7 +825,7 @@ void ndt_destroy(ndt_ctx *c) {
                       &c->mean_lo, &c->icov32, &c->icov64, &c->count, &c->cell, &c->seg_start, &c->seg_cell,
                       &c->scratch, &c->meta, &c->points, &c->offsets, &c->guesses, &c->states,
                       &c->tiles, &c->tile_begin, &c->num_tiles, &c->chunks, &c->chunk_begin, &c->num_chunks,
-                      &c->big_begin, &c->small_begin, &c->num_big,
+                      &c->big_begin, &c->small_begin, &c->num_big, &c->round_no, &c->dev_launches,
                       &c->partials, &c->exc, &c->out_T, &c->out_conv,
                       &c->out_fit, &c->out_status, &c->active, &c->counters, &c->p6, &c->trans,
                       &c->flag_q, &c->flag_n, &c->flag_overflow, &c->work_counter};
@@ -650,6 +836,9 @@ void ndt_destroy(ndt_ctx *c) {
     for (cudaEvent_t e : c->copy_ev) cudaEventDestroy(e);
     for (cudaEvent_t e : c->grid_ev)
         if (e) cudaEventDestroy(e);
+    for (BatchGraph &b : c->graphs) cudaGraphExecDestroy(b.exec);
+    c->graphs.clear();
+    if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -707,6 +896,12 @@ int ndt_align_batch_packed(ndt_ctx *c, int B, const float *points, const int *of
     if (!c) return NDT_E_ARG;
     if (int rc = set_device(c)) return rc;
     return packed_batch(c, B, points, offsets, guesses, out, converged, fitness, status);
+}
+
+int ndt_set_batch_graphs(ndt_ctx *c, int on) {
+    if (!c) return NDT_E_ARG;
+    c->use_graphs = on != 0;
+    return NDT_OK;
 }
 
 int ndt_set_profiling(ndt_ctx *c, int on) {

@@ -96,6 +96,7 @@ struct Counters {
     unsigned long long occupied_probes;
     unsigned long long pairs;
     unsigned long long tiles;
+    unsigned long long rounds;  // lockstep rounds (derivative pass + step) of the batch
 };
 
 struct Tile {

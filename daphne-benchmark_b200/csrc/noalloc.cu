@@ -84,7 +84,7 @@ __global__ void noalloc_setup_kernel(NoAllocScratch *s, Pose6 pose, int n) {
     if (t < kPartial) s->exc[t] = 0.0;
     if (t == 0) {
         s->counters.evaluations = s->counters.points = s->counters.probes = 0;
-        s->counters.occupied_probes = s->counters.pairs = s->counters.tiles = 0;
+        s->counters.occupied_probes = s->counters.pairs = s->counters.tiles = s->counters.rounds = 0;
         s->offsets[0] = 0;
         s->offsets[1] = n;
         s->flag_n = 0;

@@ -95,6 +95,7 @@ def lib():
         L.ndt_align_batch_packed.argtypes = [ctxp, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                              C.c_void_p, C.c_void_p, C.c_void_p]
         L.ndt_set_profiling.argtypes = [ctxp, C.c_int]
+        L.ndt_set_batch_graphs.argtypes = [ctxp, C.c_int]
         L.ndt_kernel_variants.argtypes = []
         L.ndt_kernel_variant_shape.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.ndt_set_kernel_variant.argtypes = [ctxp, C.c_int]
@@ -110,7 +111,7 @@ def lib():
                      "ndt_align_batch", "ndt_align_batch_device", "ndt_synchronize", "ndt_get_counters",
                      "ndt_grid_info", "ndt_grid_cells", "ndt_derivatives", "ndt_align_batch_packed",
                      "ndt_set_profiling", "ndt_kernel_variants", "ndt_kernel_variant_shape",
-                     "ndt_set_kernel_variant", "ndt_window_info"):
+                     "ndt_set_kernel_variant", "ndt_window_info", "ndt_set_batch_graphs"):
             getattr(L, name).restype = C.c_int
         _LIB = L
     return _LIB
@@ -251,6 +252,9 @@ class Context:
     def set_map_ptr(self, ptr: int, m: int):
         """Host map by raw pointer (e.g. a pinned torch tensor)."""
         self._check(self.L.ndt_set_map(self.h, C.c_void_p(ptr), m), "ndt_set_map")
+
+    def set_batch_graphs(self, on=True):
+        self._check(self.L.ndt_set_batch_graphs(self.h, int(on)), "ndt_set_batch_graphs")
 
     def set_profiling(self, on=True):
         self._check(self.L.ndt_set_profiling(self.h, int(on)), "ndt_set_profiling")

@@ -175,6 +175,17 @@ NDT_API int ndt_set_profiling(ndt_ctx *ctx, int on);
 NDT_API int ndt_get_counters(ndt_ctx *ctx, ndt_counters *out);
 
 /*
+ * Batch execution as CUDA graphs (default on): each batch call launches one
+ * cached graph (tile lists, initialisation, a device-side loop of rounds that
+ * ends when no alignment asks for another evaluation or the evaluation
+ * watchdog is spent, results), so the host neither polls nor synchronises
+ * between rounds.  Off, or with profiling on, the rounds are launched one by
+ * one from the host (profiling times each derivative pass with events).  No
+ * reference counterpart.
+ */
+NDT_API int ndt_set_batch_graphs(ndt_ctx *ctx, int on);
+
+/*
  * Launch shape of the FP32 derivative pass (points per tile = threads per
  * block, resident blocks per SM).  The autotuner (daphne-benchmark_b200/
  * autotune.py) times every variant on a sample batch and selects one.

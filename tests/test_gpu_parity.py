@@ -212,3 +212,35 @@ def test_copy_groups_do_not_change_results(pkg, cases):
         assert np.array_equal(r[2], res[0][2])
         assert np.array_equal(r[3], res[0][3])
         assert r[4] == res[0][4]
+
+
+@pytest.mark.parametrize("compat", [1, 0])
+def test_batch_graph_equals_host_loop(pkg, compat):
+    """A batch run as one CUDA graph (device-side round loop that stops when no
+    alignment asks for an evaluation) gives bit-identical poses, statuses and
+    work counters to the same batch with every round launched and polled from
+    the host.  Scan sizes differ (1k-6k points), so in corrected mode the
+    alignments finish after different numbers of evaluations."""
+    cfg = pkg.synth.small_config("gr", 30000, 50.0, 20, 4000, seed=51)
+    scene = pkg.synth.make_scene(cfg)
+    aligns = [pkg.synth.make_alignment(cfg, scene, i, n_points=1000 + 700 * i) for i in range(8)]
+    make = pkg.ndt.reference_params if compat else pkg.ndt.corrected_params
+    res = []
+    for graphs in (1, 0):
+        with pkg.ndt.Context(make()) as ctx:
+            ctx.set_batch_graphs(bool(graphs))
+            ctx.set_map(scene.map)
+            for _ in range(2):  # the second call reuses the cached graph
+                out, conv, fit, status = ctx.align_batch([a.scan for a in aligns], [a.guess for a in aligns])
+            k = ctx.counters()
+            res.append((out.view(np.uint32).copy(), conv.copy(), fit.copy(), status.copy(),
+                        {f: k[f] for f in ("evaluations", "pairs", "probes")}, k["rounds"]))
+    (o1, c1, f1, s1, k1, r1), (o0, c0, f0, s0, k0, r0) = res
+    assert np.array_equal(o1, o0) and np.array_equal(c1, c0) and np.array_equal(f1, f0)
+    assert np.array_equal(s1, s0) and (s1 == 0).all()
+    assert k1 == k0
+    # the graph stops at the first round with no active alignment; the host
+    # loop checks every 4 rounds
+    assert 0 < r1 <= r0 <= 1025
+    if compat:
+        assert r1 == r0 == 3
