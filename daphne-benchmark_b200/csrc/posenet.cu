@@ -1,0 +1,653 @@
+// Learned initial pose: a point-feature network (PointNet-style) that reads a
+// scan transformed by its guess and proposes a pose correction, which the
+// plain NDT then refines.  Forward and backward kernels of our own:
+//
+//   per point  u (3)  -> h1 = ReLU(W1 u + b1)        (64,  FP32, CUDA cores)
+//              h1     -> z2 = W2 bf16(h1) + b2       (128, BF16 x BF16 -> FP32 on
+//                                                     the tensor cores: tcgen05.mma,
+//                                                     accumulator in TMEM)
+//              h2 = ReLU(z2); g = max over points (with the argmax point)
+//   per scan   g (128) -> h3 = ReLU(W3 g + b3) (64) -> y = W4 h3 + b4 (6)
+//
+// The network input u is the scan point transformed by the guess into the map
+// frame, centred and scaled by the map's extent (u = (T_guess x - c) / s).
+// y is the pose correction in units of `delta_scale` (see ndt_b200.h).
+//
+// Backward: the max-pool routes the gradient of channel c of scan b to one
+// point (its argmax), so the shared layers' gradient touches at most 128
+// points per scan: a gather, computed on CUDA cores per scan, with the same
+// BF16 operands the forward used (h1 and W2 rounded to BF16).  Per-scan
+// gradients are summed over the batch in scan order (deterministic) and
+// applied with Adam to FP32 master weights; W2 is then re-packed to BF16.
+//
+// Tensor-core tile (one CTA of 128 threads per scan, 128 sampled points per
+// tile): A = bf16(h1) [128 points x 64] and B = W2 [128 outputs x 64], both
+// K-major in shared memory in the interleaved (no-swizzle) core-matrix layout:
+// element (r, k) at (r / 8) * 1024 + (k / 8) * 128 + (r % 8) * 16 + (k % 8) * 2
+// bytes, so a descriptor's leading byte offset (next 8 K-elements) is 128 B
+// and its stride byte offset (next 8 rows) is 1024 B.  Four MMAs of K = 16
+// (start addresses 256 B apart) give D = A B^T, 128 x 128 FP32 in 128 TMEM
+// columns; each warp reads its 32 rows (TMEM lanes) back with tcgen05.ld.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "../../include/ndt_b200.h"
+#include "umma_desc.h"
+
+namespace pn {
+
+constexpr int kH1 = 64, kH2 = 128, kH3 = 64, kOut = 6;
+// FP32 weight blob layout
+constexpr int oW1 = 0, oB1 = oW1 + kH1 * 3, oW2 = oB1 + kH1, oB2 = oW2 + kH2 * kH1, oW3 = oB2 + kH2,
+              oB3 = oW3 + kH3 * kH2, oW4 = oB3 + kH3, oB4 = oW4 + kOut * kH3, kNumW = oB4 + kOut;
+constexpr int kTileRows = 128;                  // points per tensor-core tile (MMA M)
+constexpr int kOperandBytes = kTileRows * kH1 * 2;  // 16 KB per BF16 operand
+constexpr uint32_t kTmemCols = 128;             // FP32 accumulator columns (MMA N)
+constexpr unsigned kWaitLimit = 1u << 26;       // bounded mbarrier wait (error flag when exceeded)
+
+struct Norm {
+    float cx, cy, cz, inv_s;   // input centring and scale
+    float dscale[6];           // pose-correction units
+};
+
+// Byte offset of element (r, k) in an interleaved K-major operand (64 K).
+__host__ __device__ __forceinline__ uint32_t op_offset(int r, int k) {
+    return (uint32_t)((r >> 3) * 1024 + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long pack_max(float v, int idx) {
+    // v >= 0 (after ReLU): its bits order like the value; ties keep the smaller index
+    return ((unsigned long long)__float_as_uint(v) << 32) | (unsigned long long)(0xffffffffu - (unsigned)idx);
+}
+
+// Map-frame feature of point i of the scan: u = (T x - c) * inv_s.
+__device__ __forceinline__ void point_feature(const float *T, float4 x, const Norm &nm, float u[3]) {
+    const float px = T[0] * x.x + T[1] * x.y + T[2] * x.z + T[3];
+    const float py = T[4] * x.x + T[5] * x.y + T[6] * x.z + T[7];
+    const float pz = T[8] * x.x + T[9] * x.y + T[10] * x.z + T[11];
+    u[0] = (px - nm.cx) * nm.inv_s;
+    u[1] = (py - nm.cy) * nm.inv_s;
+    u[2] = (pz - nm.cz) * nm.inv_s;
+}
+
+// Index of the j-th of P sampled points of an n-point scan (evenly strided).
+__device__ __forceinline__ int sample_index(int j, int P, int n) { return (int)(((long long)j * n) / P); }
+
+// ---------------------------------------------------------------------------
+// W2 (FP32 [128][64]) -> BF16 interleaved operand.
+__global__ void pack_w2_kernel(const float *__restrict__ w, uint8_t *__restrict__ w2op) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= kH2 * kH1) return;
+    const int r = t / kH1, k = t % kH1;
+    *reinterpret_cast<__nv_bfloat16 *>(w2op + op_offset(r, k)) = __float2bfloat16_rn(w[oW2 + t]);
+}
+
+// ---------------------------------------------------------------------------
+// Shared layers + max-pool, one CTA per scan.  gmax[b][c] = packed (max
+// value, ~argmax sample index); err is set when an mbarrier wait gives up.
+struct PointArgs {
+    const float4 *points;
+    const int *offsets;
+    const float *guesses;      // B x 16
+    const float *w;            // FP32 weights
+    const uint8_t *w2op;       // BF16 W2 operand (16 KB)
+    unsigned long long *gmax;  // B x 128
+    int *err;
+    Norm nm;
+    int B;
+    int max_points;
+};
+
+__global__ void __launch_bounds__(128, 1) point_kernel(const __grid_constant__ PointArgs a) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t *sA = smem;                                  // 16 KB
+    uint8_t *sB = smem + kOperandBytes;                  // 16 KB
+    float *sW1 = reinterpret_cast<float *>(smem + 2 * kOperandBytes);  // 192 + 64 (b1) + 128 (b2)
+    float *sB1 = sW1 + kH1 * 3;
+    float *sB2 = sB1 + kH1;
+    unsigned long long *sMax = reinterpret_cast<unsigned long long *>(sB2 + kH2);  // 4 x 128
+    uint64_t *sBar = reinterpret_cast<uint64_t *>(sMax + 4 * kH2);
+    uint32_t *sTmem = reinterpret_cast<uint32_t *>(sBar + 1);
+    __shared__ float sT[12];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int b = blockIdx.x;
+    if (b >= a.B) return;  // (grid = B: never taken)
+    const int start = a.offsets[b], n = a.offsets[b + 1] - start;
+    const int P = n < a.max_points ? n : a.max_points;
+
+    // operands and small weights into shared memory
+    for (int i = tid; i < kOperandBytes / 16; i += 128)
+        reinterpret_cast<uint4 *>(sB)[i] = reinterpret_cast<const uint4 *>(a.w2op)[i];
+    for (int i = tid; i < kH1 * 3; i += 128) sW1[i] = a.w[oW1 + i];
+    for (int i = tid; i < kH1; i += 128) sB1[i] = a.w[oB1 + i];
+    for (int i = tid; i < kH2; i += 128) sB2[i] = a.w[oB2 + i];
+    if (tid < 12) sT[tid] = a.guesses[16 * (size_t)b + tid];
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(sBar)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {  // TMEM: 128 columns for the 128 x 128 FP32 accumulator
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(sTmem)),
+                     "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *sTmem;
+
+    const uint32_t idesc = umma::instr_desc_bf16_f32(kTileRows, kH2);
+    unsigned long long run[4];  // this thread's running max of columns 32 * i + lane ... (see below)
+    // per-thread running maxima of all 128 columns live in sMax after each tile:
+    // warp w, lane l keeps columns l, l + 32, l + 64, l + 96 of its 32 rows
+    for (int i = 0; i < 4; ++i) run[i] = 0ull;
+    uint32_t phase = 0;
+    const int tiles = (P + kTileRows - 1) / kTileRows;
+    for (int t = 0; t < tiles; ++t) {
+        // layer 1 for this thread's row (sample j = t * 128 + tid)
+        const int j = t * kTileRows + tid;
+        const bool valid = j < P;
+        float u[3] = {0.f, 0.f, 0.f};
+        if (valid) {
+            const float4 x = a.points[start + sample_index(j, P, n)];
+            point_feature(sT, x, a.nm, u);
+        }
+#pragma unroll
+        for (int kc = 0; kc < kH1 / 8; ++kc) {
+            __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const int k = kc * 8 + e;
+                float v = fmaf(sW1[3 * k], u[0], fmaf(sW1[3 * k + 1], u[1], fmaf(sW1[3 * k + 2], u[2], sB1[k])));
+                v = valid ? fmaxf(v, 0.0f) : 0.0f;
+                h[e] = __float2bfloat16_rn(v);
+            }
+            *reinterpret_cast<uint4 *>(sA + op_offset(tid, kc * 8)) = *reinterpret_cast<const uint4 *>(h);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (tid == 0) {
+#pragma unroll
+            for (int kk = 0; kk < kH1 / 16; ++kk) {
+                const uint64_t da = umma::smem_desc_kmajor_interleaved(smem_u32(sA) + kk * 256, 128, 1024);
+                const uint64_t db = umma::smem_desc_kmajor_interleaved(smem_u32(sB) + kk * 256, 128, 1024);
+                const uint32_t accumulate = kk > 0 ? 1u : 0u;
+                const uint32_t no_mask = 0;  // disable-output-lane mask: all lanes written
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(no_mask), "r"(no_mask), "r"(no_mask),
+                    "r"(no_mask));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(sBar))
+                         : "memory");
+        }
+        // wait for the MMAs (bounded)
+        {
+            uint32_t done = 0;
+            unsigned it = 0;
+            while (!done) {
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                    "selp.b32 %0, 1, 0, p;\n\t}\n"
+                    : "=r"(done)
+                    : "r"(smem_u32(sBar)), "r"(phase)
+                    : "memory");
+                if (!done && ++it > kWaitLimit) {
+                    if (tid == 0) atomicExch(a.err, 1);
+                    break;
+                }
+            }
+            phase ^= 1u;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        // accumulator rows of this warp: row = 32 * warp + lane, 128 columns
+#pragma unroll
+        for (int cq = 0; cq < 4; ++cq) {
+            uint32_t r[32];
+            const uint32_t addr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(32 * cq);
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+                "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                : "r"(addr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            // column c = 32 cq + e of row (this thread's sample j): ReLU(z + b2);
+            // warp max over its 32 rows, lane e keeps column 32 cq + e
+#pragma unroll
+            for (int e = 0; e < 32; ++e) {
+                const float z = __uint_as_float(r[e]) + sB2[32 * cq + e];
+                unsigned long long v = valid ? pack_max(fmaxf(z, 0.0f), j) : 0ull;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+                    v = w > v ? w : v;
+                }
+                if (lane == e) run[cq] = v > run[cq] ? v : run[cq];
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();  // all TMEM reads and sA reads done before the next tile's writes and MMAs
+    }
+    // combine the 4 warps, write the scan's max-pool
+#pragma unroll
+    for (int cq = 0; cq < 4; ++cq) sMax[warp * kH2 + 32 * cq + lane] = run[cq];
+    __syncthreads();
+    {
+        const int c = tid;  // 128 threads, 128 channels
+        unsigned long long m = sMax[c];
+        for (int w = 1; w < 4; ++w) m = sMax[w * kH2 + c] > m ? sMax[w * kH2 + c] : m;
+        a.gmax[(size_t)b * kH2 + c] = m;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+}
+
+// ---------------------------------------------------------------------------
+// Head (forward), loss and backward, one CTA of 128 threads per scan.
+struct HeadArgs {
+    const float4 *points;
+    const int *offsets;
+    const float *guesses;
+    const float *w;
+    const unsigned long long *gmax;
+    const float *target;  // B x 6 (normalised units) or null (inference)
+    float *y;             // B x 6 out (may be null)
+    float *grad_scan;     // B x kNumW per-scan gradients (training) or null
+    float *loss_scan;     // B (training) or null
+    Norm nm;
+    int B;
+    int max_points;
+};
+
+__device__ __forceinline__ float bf16r(float v) { return __bfloat162float(__float2bfloat16_rn(v)); }
+
+__global__ void __launch_bounds__(128) head_kernel(const __grid_constant__ HeadArgs a) {
+    __shared__ float g[kH2], h3[kH3], dy[kOut], dh3[kH3], dg[kH2];
+    __shared__ int arg[kH2];
+    __shared__ float sT[12];
+    const int tid = threadIdx.x, b = blockIdx.x;
+    if (b >= a.B) return;
+    const float *w = a.w;
+    {
+        const unsigned long long m = a.gmax[(size_t)b * kH2 + tid];
+        g[tid] = __uint_as_float((unsigned)(m >> 32));
+        arg[tid] = (int)(0xffffffffu - (unsigned)(m & 0xffffffffu));
+    }
+    if (tid < 12) sT[tid] = a.guesses[16 * (size_t)b + tid];
+    __syncthreads();
+    if (tid < kH3) {
+        float s = w[oB3 + tid];
+        for (int c = 0; c < kH2; ++c) s = fmaf(w[oW3 + tid * kH2 + c], g[c], s);
+        h3[tid] = fmaxf(s, 0.0f);
+    }
+    __syncthreads();
+    if (tid < kOut) {
+        float s = w[oB4 + tid];
+        for (int k = 0; k < kH3; ++k) s = fmaf(w[oW4 + tid * kH3 + k], h3[k], s);
+        if (a.y) a.y[(size_t)b * kOut + tid] = s;
+        if (a.target) dy[tid] = s - a.target[(size_t)b * kOut + tid];
+    }
+    if (!a.grad_scan) return;
+    __syncthreads();
+    // loss_b = sum_i (y_i - t_i)^2 / 6; the batch loss is its mean over scans,
+    // the per-scan gradients are of loss_b (the reduction divides by B)
+    if (tid == 0) {
+        float l = 0.f;
+        for (int i = 0; i < kOut; ++i) l += dy[i] * dy[i];
+        a.loss_scan[b] = l / kOut;
+    }
+    __syncthreads();
+    if (tid < kOut) dy[tid] *= 2.0f / kOut;
+    __syncthreads();
+    float *G = a.grad_scan + (size_t)b * kNumW;
+    // head: W4, b4, dh3 -> W3, b3, dg
+    for (int i = tid; i < kOut * kH3; i += 128) G[oW4 + i] = dy[i / kH3] * h3[i % kH3];
+    if (tid < kOut) G[oB4 + tid] = dy[tid];
+    if (tid < kH3) {
+        float s = 0.f;
+        for (int i = 0; i < kOut; ++i) s = fmaf(w[oW4 + i * kH3 + tid], dy[i], s);
+        dh3[tid] = h3[tid] > 0.0f ? s : 0.0f;
+    }
+    __syncthreads();
+    for (int i = tid; i < kH3 * kH2; i += 128) G[oW3 + i] = dh3[i / kH2] * g[i % kH2];
+    if (tid < kH3) G[oB3 + tid] = dh3[tid];
+    {
+        float s = 0.f;
+        for (int k = 0; k < kH3; ++k) s = fmaf(w[oW3 + k * kH2 + tid], dh3[k], s);
+        dg[tid] = g[tid] > 0.0f ? s : 0.0f;  // max of ReLU outputs: zero max passes no gradient
+    }
+    __syncthreads();
+    // shared layers through the argmax points (BF16 operands as in the forward)
+    const int start = a.offsets[b], n = a.offsets[b + 1] - start;
+    const int P = n < a.max_points ? n : a.max_points;
+    // channel c = tid: dW2[c][k] = dg[c] * bf16(h1[p_c][k]), db2[c] = dg[c]
+    {
+        const int c = tid;
+        const float d = dg[c];
+        float hc[kH1];
+        float u[3] = {0.f, 0.f, 0.f};
+        if (d != 0.0f && P > 0) point_feature(sT, a.points[start + sample_index(arg[c], P, n)], a.nm, u);
+        for (int k = 0; k < kH1; ++k) {
+            const float v = fmaf(w[oW1 + 3 * k], u[0], fmaf(w[oW1 + 3 * k + 1], u[1], fmaf(w[oW1 + 3 * k + 2], u[2],
+                                                                                            w[oB1 + k])));
+            hc[k] = bf16r(fmaxf(v, 0.0f));
+        }
+        for (int k = 0; k < kH1; ++k) G[oW2 + c * kH1 + k] = d * hc[k];
+        G[oB2 + c] = d;
+    }
+    // hidden unit k = tid < 64: over the channels in order,
+    // dz1 = bf16(W2[c][k]) * dg[c] * [h1[p_c][k] > 0]; dW1[k] += dz1 u[p_c]; db1[k] += dz1
+    if (tid < kH1) {
+        const int k = tid;
+        float gw0 = 0.f, gw1 = 0.f, gw2 = 0.f, gb = 0.f;
+        for (int c = 0; c < kH2; ++c) {
+            const float d = dg[c];
+            if (d == 0.0f) continue;
+            float u[3];
+            point_feature(sT, a.points[start + sample_index(arg[c], P, n)], a.nm, u);
+            const float z = fmaf(w[oW1 + 3 * k], u[0], fmaf(w[oW1 + 3 * k + 1], u[1], fmaf(w[oW1 + 3 * k + 2], u[2],
+                                                                                            w[oB1 + k])));
+            if (!(z > 0.0f)) continue;
+            const float dz = bf16r(w[oW2 + c * kH1 + k]) * d;
+            gw0 = fmaf(dz, u[0], gw0);
+            gw1 = fmaf(dz, u[1], gw1);
+            gw2 = fmaf(dz, u[2], gw2);
+            gb += dz;
+        }
+        G[oW1 + 3 * k] = gw0;
+        G[oW1 + 3 * k + 1] = gw1;
+        G[oW1 + 3 * k + 2] = gw2;
+        G[oB1 + k] = gb;
+    }
+}
+
+// Batch gradient (mean of the per-scan gradients, scan order) and loss;
+// optionally an Adam step on the FP32 weights.
+struct AdamArgs {
+    float *w, *m, *v;
+    const float *grad_scan;
+    const float *loss_scan;
+    float *grad;   // kNumW out (batch gradient)
+    float *loss;   // 1 out
+    int B;
+    float lr, beta1, beta2, eps, bc1, bc2;  // bc = 1 - beta^t
+    int update;
+};
+
+__global__ void reduce_adam_kernel(const __grid_constant__ AdamArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        float l = 0.f;
+        for (int b = 0; b < a.B; ++b) l += a.loss_scan[b];
+        *a.loss = l / a.B;
+    }
+    if (i >= kNumW) return;
+    float s = 0.f;
+    for (int b = 0; b < a.B; ++b) s += a.grad_scan[(size_t)b * kNumW + i];
+    const float gi = s / a.B;
+    a.grad[i] = gi;
+    if (!a.update) return;
+    const float m = a.beta1 * a.m[i] + (1.0f - a.beta1) * gi;
+    const float v = a.beta2 * a.v[i] + (1.0f - a.beta2) * gi * gi;
+    a.m[i] = m;
+    a.v[i] = v;
+    a.w[i] -= a.lr * (m / a.bc1) / (sqrtf(v / a.bc2) + a.eps);
+}
+
+}  // namespace pn
+
+// ---------------------------------------------------------------------------
+// C ABI
+struct ndt_mlp {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    float *w = nullptr, *m = nullptr, *v = nullptr, *grad = nullptr, *loss = nullptr;
+    uint8_t *w2op = nullptr;
+    int *err = nullptr;
+    unsigned long long *gmax = nullptr;
+    float *grad_scan = nullptr, *loss_scan = nullptr;
+    size_t cap_b = 0;
+    int step = 0;
+    pn::Norm nm{};
+    std::string msg;
+};
+
+namespace {
+
+int mlp_fail(ndt_mlp *c, cudaError_t e, const char *what) {
+    if (c) c->msg = std::string(what) + ": " + cudaGetErrorString(e);
+    return NDT_E_CUDA;
+}
+
+#define MCK(call)                                               \
+    do {                                                        \
+        cudaError_t e_ = (call);                                \
+        if (e_ != cudaSuccess) return mlp_fail(c, e_, #call);   \
+    } while (0)
+
+constexpr size_t kPointSmem = 2 * pn::kOperandBytes + (pn::kH1 * 3 + pn::kH1 + pn::kH2) * 4 + 4 * pn::kH2 * 8 + 64;
+// keep at most 4 CTAs per SM, so that 4 x 128 TMEM columns fit
+constexpr size_t kPointSmemAlloc = kPointSmem < 48 * 1024 ? 48 * 1024 : kPointSmem;
+
+int ensure_batch(ndt_mlp *c, int B) {
+    if ((size_t)B <= c->cap_b) return NDT_OK;
+    cudaFree(c->gmax);
+    cudaFree(c->grad_scan);
+    cudaFree(c->loss_scan);
+    c->gmax = nullptr;
+    c->grad_scan = c->loss_scan = nullptr;
+    c->cap_b = 0;
+    MCK(cudaMalloc(&c->gmax, sizeof(unsigned long long) * pn::kH2 * (size_t)B));
+    MCK(cudaMalloc(&c->grad_scan, sizeof(float) * pn::kNumW * (size_t)B));
+    MCK(cudaMalloc(&c->loss_scan, sizeof(float) * (size_t)B));
+    c->cap_b = (size_t)B;
+    return NDT_OK;
+}
+
+int run_forward(ndt_mlp *c, int B, const float *d_points, const int *d_offsets, const float *d_guesses,
+                int max_points) {
+    if (int rc = ensure_batch(c, B)) return rc;
+    pn::PointArgs a;
+    a.points = reinterpret_cast<const float4 *>(d_points);
+    a.offsets = d_offsets;
+    a.guesses = d_guesses;
+    a.w = c->w;
+    a.w2op = c->w2op;
+    a.gmax = c->gmax;
+    a.err = c->err;
+    a.nm = c->nm;
+    a.B = B;
+    a.max_points = max_points;
+    pn::point_kernel<<<B, 128, kPointSmemAlloc, c->stream>>>(a);
+    MCK(cudaGetLastError());
+    return NDT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ndt_mlp_num_weights(void) { return pn::kNumW; }
+
+int ndt_mlp_create(int device, ndt_mlp **out) {
+    if (!out) return NDT_E_ARG;
+    *out = nullptr;
+    ndt_mlp *c = new ndt_mlp();
+    c->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&c->w, sizeof(float) * pn::kNumW);
+    if (e == cudaSuccess) e = cudaMalloc(&c->m, sizeof(float) * pn::kNumW);
+    if (e == cudaSuccess) e = cudaMalloc(&c->v, sizeof(float) * pn::kNumW);
+    if (e == cudaSuccess) e = cudaMalloc(&c->grad, sizeof(float) * pn::kNumW);
+    if (e == cudaSuccess) e = cudaMalloc(&c->loss, sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&c->w2op, pn::kOperandBytes);
+    if (e == cudaSuccess) e = cudaMalloc(&c->err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(c->err, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(c->m, 0, sizeof(float) * pn::kNumW);
+    if (e == cudaSuccess) e = cudaMemset(c->v, 0, sizeof(float) * pn::kNumW);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(pn::point_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPointSmemAlloc);
+    if (e != cudaSuccess) {
+        ndt_mlp_destroy(c);
+        return NDT_E_CUDA;
+    }
+    for (int i = 0; i < 6; ++i) c->nm.dscale[i] = 1.0f;
+    c->nm.inv_s = 1.0f;
+    *out = c;
+    return NDT_OK;
+}
+
+void ndt_mlp_destroy(ndt_mlp *c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    void *bufs[] = {c->w, c->m, c->v, c->grad, c->loss, c->w2op, c->err, c->gmax, c->grad_scan, c->loss_scan};
+    for (void *p : bufs)
+        if (p) cudaFree(p);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char *ndt_mlp_last_error(const ndt_mlp *c) { return c ? c->msg.c_str() : "null network"; }
+
+int ndt_mlp_set_input_frame(ndt_mlp *c, const float center3[3], float scale, const float delta_scale6[6]) {
+    if (!c || !center3 || !delta_scale6 || !(scale > 0.0f)) return NDT_E_ARG;
+    c->nm.cx = center3[0];
+    c->nm.cy = center3[1];
+    c->nm.cz = center3[2];
+    c->nm.inv_s = 1.0f / scale;
+    for (int i = 0; i < 6; ++i) c->nm.dscale[i] = delta_scale6[i];
+    return NDT_OK;
+}
+
+int ndt_mlp_set_weights(ndt_mlp *c, const float *w, int n) {
+    if (!c || !w || n != pn::kNumW) return NDT_E_ARG;
+    MCK(cudaSetDevice(c->device));
+    MCK(cudaMemcpyAsync(c->w, w, sizeof(float) * pn::kNumW, cudaMemcpyHostToDevice, c->stream));
+    MCK(cudaMemsetAsync(c->m, 0, sizeof(float) * pn::kNumW, c->stream));
+    MCK(cudaMemsetAsync(c->v, 0, sizeof(float) * pn::kNumW, c->stream));
+    pn::pack_w2_kernel<<<(pn::kH2 * pn::kH1 + 255) / 256, 256, 0, c->stream>>>(c->w, c->w2op);
+    MCK(cudaGetLastError());
+    MCK(cudaStreamSynchronize(c->stream));
+    c->step = 0;
+    return NDT_OK;
+}
+
+int ndt_mlp_get_weights(ndt_mlp *c, float *w, int n) {
+    if (!c || !w || n != pn::kNumW) return NDT_E_ARG;
+    MCK(cudaSetDevice(c->device));
+    MCK(cudaMemcpyAsync(w, c->w, sizeof(float) * pn::kNumW, cudaMemcpyDeviceToHost, c->stream));
+    MCK(cudaStreamSynchronize(c->stream));
+    return NDT_OK;
+}
+
+int ndt_mlp_forward_device(ndt_mlp *c, int B, const float *d_points, const int *d_offsets, const float *d_guesses,
+                           int max_points, float *d_y6) {
+    if (!c || B <= 0 || !d_points || !d_offsets || !d_guesses || !d_y6 || max_points <= 0) return NDT_E_ARG;
+    MCK(cudaSetDevice(c->device));
+    if (int rc = run_forward(c, B, d_points, d_offsets, d_guesses, max_points)) return rc;
+    pn::HeadArgs h;
+    std::memset(&h, 0, sizeof(h));
+    h.points = reinterpret_cast<const float4 *>(d_points);
+    h.offsets = d_offsets;
+    h.guesses = d_guesses;
+    h.w = c->w;
+    h.gmax = c->gmax;
+    h.y = d_y6;
+    h.nm = c->nm;
+    h.B = B;
+    h.max_points = max_points;
+    pn::head_kernel<<<B, 128, 0, c->stream>>>(h);
+    MCK(cudaGetLastError());
+    return NDT_OK;
+}
+
+int ndt_mlp_train_step_device(ndt_mlp *c, int B, const float *d_points, const int *d_offsets, const float *d_guesses,
+                              const float *d_target6, int max_points, float lr, int update, float *h_loss,
+                              float *h_grad) {
+    if (!c || B <= 0 || !d_points || !d_offsets || !d_guesses || !d_target6 || max_points <= 0) return NDT_E_ARG;
+    MCK(cudaSetDevice(c->device));
+    if (int rc = run_forward(c, B, d_points, d_offsets, d_guesses, max_points)) return rc;
+    pn::HeadArgs h;
+    std::memset(&h, 0, sizeof(h));
+    h.points = reinterpret_cast<const float4 *>(d_points);
+    h.offsets = d_offsets;
+    h.guesses = d_guesses;
+    h.w = c->w;
+    h.gmax = c->gmax;
+    h.target = d_target6;
+    h.grad_scan = c->grad_scan;
+    h.loss_scan = c->loss_scan;
+    h.nm = c->nm;
+    h.B = B;
+    h.max_points = max_points;
+    pn::head_kernel<<<B, 128, 0, c->stream>>>(h);
+    MCK(cudaGetLastError());
+    if (update) ++c->step;
+    pn::AdamArgs a;
+    a.w = c->w;
+    a.m = c->m;
+    a.v = c->v;
+    a.grad_scan = c->grad_scan;
+    a.loss_scan = c->loss_scan;
+    a.grad = c->grad;
+    a.loss = c->loss;
+    a.B = B;
+    a.lr = lr;
+    a.beta1 = 0.9f;
+    a.beta2 = 0.999f;
+    a.eps = 1e-8f;
+    a.bc1 = 1.0f - std::pow(0.9f, (float)(c->step > 0 ? c->step : 1));
+    a.bc2 = 1.0f - std::pow(0.999f, (float)(c->step > 0 ? c->step : 1));
+    a.update = update;
+    pn::reduce_adam_kernel<<<(pn::kNumW + 255) / 256, 256, 0, c->stream>>>(a);
+    MCK(cudaGetLastError());
+    if (update) {
+        pn::pack_w2_kernel<<<(pn::kH2 * pn::kH1 + 255) / 256, 256, 0, c->stream>>>(c->w, c->w2op);
+        MCK(cudaGetLastError());
+    }
+    if (h_loss) MCK(cudaMemcpyAsync(h_loss, c->loss, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    if (h_grad) MCK(cudaMemcpyAsync(h_grad, c->grad, sizeof(float) * pn::kNumW, cudaMemcpyDeviceToHost, c->stream));
+    if (h_loss || h_grad) MCK(cudaStreamSynchronize(c->stream));
+    return NDT_OK;
+}
+
+int ndt_mlp_maxpool_device(ndt_mlp *c, unsigned long long *d_out, int B) {
+    if (!c || !d_out || B <= 0 || (size_t)B > c->cap_b) return NDT_E_ARG;
+    MCK(cudaMemcpyAsync(d_out, c->gmax, sizeof(unsigned long long) * pn::kH2 * (size_t)B,
+                        cudaMemcpyDeviceToDevice, c->stream));
+    return NDT_OK;
+}
+
+int ndt_mlp_synchronize(ndt_mlp *c, int *tc_error) {
+    if (!c) return NDT_E_ARG;
+    MCK(cudaStreamSynchronize(c->stream));
+    int e = 0;
+    MCK(cudaMemcpy(&e, c->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (tc_error) *tc_error = e;
+    return NDT_OK;
+}
+
+void *ndt_mlp_stream(ndt_mlp *c) { return c ? (void *)c->stream : nullptr; }
+
+}  // extern "C"

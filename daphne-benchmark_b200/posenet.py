@@ -1,0 +1,168 @@
+"""Learned initial pose: Python side of the point-feature network
+(csrc/posenet.cu, include/ndt_b200.h `ndt_mlp_*`).
+
+`PoseNet` owns the network's device weights and its stream; the forward and
+training calls take device pointers (torch CUDA tensors here).  The pose
+helpers convert between 4x4 transforms and the pose vector of the corrected
+NDT parametrisation T = Trans(x, y, z) Rx(roll) Ry(pitch) Rz(yaw), in which
+the network's correction is expressed.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import ndt as _ndt
+
+H1, H2, H3, OUT = 64, 128, 64, 6
+DELTA_SCALE = np.array([1.0, 1.0, 0.1, 0.02, 0.02, 0.1], np.float32)  # m, m, m, rad, rad, rad
+
+
+def _lib():
+    L = _ndt.lib()
+    if not getattr(L, "_pn_ready", False):
+        p = C.c_void_p
+        L.ndt_mlp_num_weights.restype = C.c_int
+        L.ndt_mlp_create.argtypes = [C.c_int, C.POINTER(p)]
+        L.ndt_mlp_destroy.argtypes = [p]
+        L.ndt_mlp_destroy.restype = None
+        L.ndt_mlp_last_error.argtypes = [p]
+        L.ndt_mlp_last_error.restype = C.c_char_p
+        L.ndt_mlp_set_input_frame.argtypes = [p, C.POINTER(C.c_float), C.c_float, C.POINTER(C.c_float)]
+        L.ndt_mlp_set_weights.argtypes = [p, C.POINTER(C.c_float), C.c_int]
+        L.ndt_mlp_get_weights.argtypes = [p, C.POINTER(C.c_float), C.c_int]
+        L.ndt_mlp_forward_device.argtypes = [p, C.c_int, p, p, p, C.c_int, p]
+        L.ndt_mlp_train_step_device.argtypes = [p, C.c_int, p, p, p, p, C.c_int, C.c_float, C.c_int,
+                                                C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.ndt_mlp_maxpool_device.argtypes = [p, p, C.c_int]
+        L.ndt_mlp_synchronize.argtypes = [p, C.POINTER(C.c_int)]
+        L.ndt_mlp_stream.argtypes = [p]
+        L.ndt_mlp_stream.restype = p
+        for n in ("ndt_mlp_create", "ndt_mlp_set_input_frame", "ndt_mlp_set_weights", "ndt_mlp_get_weights",
+                  "ndt_mlp_forward_device", "ndt_mlp_train_step_device", "ndt_mlp_maxpool_device",
+                  "ndt_mlp_synchronize"):
+            getattr(L, n).restype = C.c_int
+        L._pn_ready = True
+    return L
+
+
+def num_weights():
+    return _lib().ndt_mlp_num_weights()
+
+
+def _f32p(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class PoseNet:
+    """Device weights, Adam state and stream of one network."""
+
+    def __init__(self, device=0, center=(0.0, 0.0, 0.0), scale=1.0, delta_scale=DELTA_SCALE):
+        self.L = _lib()
+        h = C.c_void_p()
+        rc = self.L.ndt_mlp_create(device, C.byref(h))
+        if rc != 0:
+            raise _ndt.NdtError(f"ndt_mlp_create failed ({rc})")
+        self.h = h
+        self.n_w = self.L.ndt_mlp_num_weights()
+        self.delta_scale = np.asarray(delta_scale, np.float32)
+        self.set_input_frame(center, scale, self.delta_scale)
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise _ndt.NdtError(f"{what}: {self.L.ndt_mlp_last_error(self.h).decode()}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.ndt_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_input_frame(self, center, scale, delta_scale):
+        c = np.ascontiguousarray(center, np.float32)
+        d = np.ascontiguousarray(delta_scale, np.float32)
+        self.center, self.scale = c, float(scale)
+        self._check(self.L.ndt_mlp_set_input_frame(self.h, _f32p(c), float(scale), _f32p(d)), "set_input_frame")
+
+    def set_weights(self, w):
+        w = np.ascontiguousarray(w, np.float32)
+        assert w.size == self.n_w
+        self._check(self.L.ndt_mlp_set_weights(self.h, _f32p(w), self.n_w), "set_weights")
+
+    def get_weights(self):
+        w = np.zeros(self.n_w, np.float32)
+        self._check(self.L.ndt_mlp_get_weights(self.h, _f32p(w), self.n_w), "get_weights")
+        return w
+
+    def forward(self, B, d_points, d_offsets, d_guesses, d_y, max_points=1024):
+        self._check(self.L.ndt_mlp_forward_device(self.h, B, C.c_void_p(d_points), C.c_void_p(d_offsets),
+                                                  C.c_void_p(d_guesses), max_points, C.c_void_p(d_y)), "forward")
+
+    def train_step(self, B, d_points, d_offsets, d_guesses, d_target, lr=1e-3, update=True, max_points=1024,
+                   want_grad=False):
+        loss = np.zeros(1, np.float32)
+        grad = np.zeros(self.n_w, np.float32) if want_grad else None
+        self._check(self.L.ndt_mlp_train_step_device(self.h, B, C.c_void_p(d_points), C.c_void_p(d_offsets),
+                                                     C.c_void_p(d_guesses), C.c_void_p(d_target), max_points,
+                                                     float(lr), int(update), _f32p(loss),
+                                                     _f32p(grad) if grad is not None else None), "train_step")
+        return float(loss[0]), grad
+
+    def maxpool(self, d_out, B):
+        self._check(self.L.ndt_mlp_maxpool_device(self.h, C.c_void_p(d_out), B), "maxpool")
+
+    def synchronize(self):
+        e = C.c_int()
+        self._check(self.L.ndt_mlp_synchronize(self.h, C.byref(e)), "synchronize")
+        if e.value:
+            raise _ndt.NdtError("tensor-core wait gave up (mbarrier wait limit)")
+
+    @property
+    def stream(self):
+        return self.L.ndt_mlp_stream(self.h)
+
+
+# ---------------------------------------------------------------------------
+# Pose vectors of the corrected parametrisation T = Trans Rx(a) Ry(b) Rz(c).
+def pose_from_matrix(T):
+    T = np.asarray(T, np.float64).reshape(4, 4)
+    R = T[:3, :3]
+    b = np.arcsin(np.clip(R[0, 2], -1.0, 1.0))
+    a = np.arctan2(-R[1, 2], R[2, 2])
+    c = np.arctan2(-R[0, 1], R[0, 0])
+    return np.array([T[0, 3], T[1, 3], T[2, 3], a, b, c])
+
+
+def matrix_from_pose(p):
+    x, y, z, a, b, c = [float(v) for v in p]
+    ca, sa, cb, sb, cc, sc = np.cos(a), np.sin(a), np.cos(b), np.sin(b), np.cos(c), np.sin(c)
+    Rx = np.array([[1, 0, 0], [0, ca, -sa], [0, sa, ca]])
+    Ry = np.array([[cb, 0, sb], [0, 1, 0], [-sb, 0, cb]])
+    Rz = np.array([[cc, -sc, 0], [sc, cc, 0], [0, 0, 1]])
+    T = np.eye(4)
+    T[:3, :3] = Rx @ Ry @ Rz
+    T[:3, 3] = [x, y, z]
+    return T
+
+
+def wrap_angle(a):
+    return (np.asarray(a) + np.pi) % (2 * np.pi) - np.pi
+
+
+def correction_target(guess16, converged16, delta_scale=DELTA_SCALE):
+    """Normalised pose correction from a guess to a converged pose."""
+    d = pose_from_matrix(converged16) - pose_from_matrix(guess16)
+    d[3:] = wrap_angle(d[3:])
+    return (d / delta_scale).astype(np.float32)
+
+
+def apply_correction(guess16, y, delta_scale=DELTA_SCALE):
+    """The proposed 4x4 (float32, row major) from a guess and a network output."""
+    p = pose_from_matrix(guess16) + np.asarray(y, np.float64) * delta_scale
+    return matrix_from_pose(p).astype(np.float32).reshape(16)

@@ -240,6 +240,44 @@ NDT_API int ndt_derivatives(ndt_ctx *ctx, const float *scan, const float *trans,
 NDT_API int ndt_derivatives_noalloc(ndt_ctx *ctx, const float *d_scan, const float *d_trans, int n,
                                     const double p6[6], double *d_out);
 
+/*
+ * Learned initial pose (no counterpart in the reference): a point-feature
+ * network that reads a scan transformed by its guess and proposes a pose
+ * correction for the NDT to refine.  Per point u (3) -> 64 -> 128 (shared
+ * layers, ReLU; the 64 -> 128 layer in BF16 on the tensor cores with FP32
+ * accumulation), max-pool over up to max_points evenly strided points of the
+ * scan, then 128 -> 64 -> 6.  u = (T_guess x - center) / scale; the output y
+ * is the correction of the pose vector (x, y, z, roll, pitch, yaw of the
+ * corrected parametrisation T = Trans Rx Ry Rz) in units of delta_scale6.
+ * Weights: ndt_mlp_num_weights() FP32 values (W1[64][3], b1[64], W2[128][64],
+ * b2[128], W3[64][128], b3[64], W4[6][64], b4[6]).  All arrays passed to the
+ * *_device calls are device pointers; work is ordered on the network's own
+ * stream (ndt_mlp_stream).  ndt_mlp_synchronize reports a tensor-core wait
+ * that gave up (*tc_error != 0; the outputs are then invalid).
+ */
+typedef struct ndt_mlp ndt_mlp;
+NDT_API int ndt_mlp_num_weights(void);
+NDT_API int ndt_mlp_create(int device, ndt_mlp **out);
+NDT_API void ndt_mlp_destroy(ndt_mlp *mlp);
+NDT_API const char *ndt_mlp_last_error(const ndt_mlp *mlp);
+NDT_API int ndt_mlp_set_input_frame(ndt_mlp *mlp, const float center3[3], float scale, const float delta_scale6[6]);
+NDT_API int ndt_mlp_set_weights(ndt_mlp *mlp, const float *w, int n);  /* host array; resets Adam state */
+NDT_API int ndt_mlp_get_weights(ndt_mlp *mlp, float *w, int n);        /* host array */
+/* y6: B x 6 corrections (normalised units) for B scans (points: float4, offsets: B + 1, guesses: B x 16). */
+NDT_API int ndt_mlp_forward_device(ndt_mlp *mlp, int B, const float *d_points, const int *d_offsets,
+                                   const float *d_guesses, int max_points, float *d_y6);
+/* One training step on B scans with targets (B x 6, normalised units): loss = mean over scans of
+ * mean over the 6 outputs of (y - target)^2.  update = 1 applies Adam (lr, beta 0.9 / 0.999) to the
+ * weights; update = 0 only computes.  h_loss (1 float) and h_grad (num_weights floats, the batch
+ * gradient) are optional host outputs. */
+NDT_API int ndt_mlp_train_step_device(ndt_mlp *mlp, int B, const float *d_points, const int *d_offsets,
+                                      const float *d_guesses, const float *d_target6, int max_points, float lr,
+                                      int update, float *h_loss, float *h_grad);
+/* Max-pool of the last forward: B x 128 packed (float bits << 32 | 0xffffffff - argmax sample). */
+NDT_API int ndt_mlp_maxpool_device(ndt_mlp *mlp, unsigned long long *d_out, int B);
+NDT_API int ndt_mlp_synchronize(ndt_mlp *mlp, int *tc_error);
+NDT_API void *ndt_mlp_stream(ndt_mlp *mlp);
+
 #ifdef __cplusplus
 }
 #endif
