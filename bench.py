@@ -504,6 +504,165 @@ def run_ours(args, pkg, world, rank, local):
     return 0
 
 
+def run_learned(args, pkg, world, rank, local):
+    """Learned-init vs plain batched NDT (corrected NDT) on a config's
+    alignments: the network is trained first (untimed) on pairs the plain NDT
+    labels on the same map; then both pipelines run the whole batch, timed
+    with the wall clock around synchronised steps (the learned one includes
+    its proposal passes, the judge's two score passes and its host round
+    trips)."""
+    import torch
+    import posenet_ref
+    torch.cuda.set_device(local)
+    if rank != 0:
+        return 0
+    L, ndt, synth = pkg.learned, pkg.ndt, pkg.synth
+    cfg = synth.CONFIGS[args.config]
+    scene = synth.make_scene(cfg)
+    ctx = ndt.Context(ndt.corrected_params(cfg.resolution), device=local)
+    ctx.set_map(scene.map)
+    t0 = time.perf_counter()
+    pairs = L.make_pairs(cfg, scene, args.train_scans, 25, cfg.dt, cfg.dyaw_deg, seed=7, fine_frac=0.5)
+    t_pairs = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    L.label_scans(ctx, torch, pairs)
+    t_label = time.perf_counter() - t0
+    net = pkg.posenet.PoseNet(device=local, center=(0.0, 0.0, 0.0), scale=4.0)
+    net.set_weights(posenet_ref.init_weights(1))
+    t0 = time.perf_counter()
+    losses = L.train(net, torch, pairs, epochs=args.train_epochs, batch=256, lr=2e-3)
+    t_train = time.perf_counter() - t0
+    aligns = [synth.make_alignment(cfg, scene, i) for i in range(cfg.aligns)]
+    dev = L.DeviceScans(torch, [a.scan for a in aligns])
+    pts, offs, total = dev.batch(np.arange(len(aligns)))
+    guesses = np.stack([a.guess for a in aligns])
+    truths = np.stack([a.truth for a in aligns])
+    B = len(aligns)
+
+    def plain():
+        return L.ndt_align_device(ctx, torch, pts, offs, total, guesses)
+
+    def learned():
+        return L.learned_align(ctx, net, torch, pts, offs, total, guesses, passes=3)
+
+    res = {}
+    for name, fn in (("plain", plain), ("learned", learned)):
+        for _ in range(args.warmup):
+            fn()
+        times, out = [], None
+        for _ in range(args.steps):
+            out, t = L.timed(fn, torch)
+            times.append(t)
+        dt, dr = L.pose_errors(out[0], truths)
+        ok = (dt <= 0.02) & (dr <= 0.1)
+        res[name] = {"aligns_per_s": B * args.steps / sum(times), "ms_per_step": 1e3 * sum(times) / args.steps,
+                     "within_2cm_0.1deg_of_truth": float(ok.mean()),
+                     "median_translation_error_m": float(np.median(dt)),
+                     "aligns_per_s_within_2cm_0.1deg_of_truth": float(ok.mean()) * B * args.steps / sum(times),
+                     "converged": float(np.mean(out[1] != 0))}
+        if name == "learned":
+            res[name]["used_proposal"] = float(np.mean(out[4]))
+    # accuracy of the refinement against the FP64 oracle from the same start
+    # poses, on a sample (the oracle is the CPU restatement)
+    import binding
+    n_acc = min(B, args.oracle_sample)
+    orc = binding.Oracle()
+    prop = guesses
+    for _ in range(3):
+        prop, _ = L.propose(net, torch, pts, offs, prop)
+    s_p = L.score(ctx, torch, pts, offs, total, prop)
+    s_g = L.score(ctx, torch, pts, offs, total, guesses)
+    starts = np.where((s_p >= s_g)[:, None], prop, guesses).astype(np.float32)
+    acc = {}
+    for name, st in (("plain", guesses), ("learned", starts)):
+        gpu = L.ndt_align_device(ctx, torch, pts, offs, total, st)[0][:n_acc]
+        ref, _, _, _ = orc.align_batch(binding.corrected_params(cfg.resolution), [a.scan for a in aligns[:n_acc]],
+                                       list(st[:n_acc]), scene.map)
+        e_t = np.linalg.norm(gpu.reshape(-1, 4, 4)[:, :3, 3] - ref.reshape(-1, 4, 4)[:, :3, 3], axis=1)
+        e_r = np.array([rot_deg(gpu[i], ref[i]) for i in range(n_acc)])
+        acc[name] = {"alignments": n_acc, "within_2cm_0.1deg": int(np.sum((e_t <= 0.02) & (e_r <= 0.1))),
+                     "max_translation_m": float(e_t.max()), "max_rotation_deg": float(e_r.max())}
+    ratio = res["learned"]["aligns_per_s"] / res["plain"]["aligns_per_s"]
+    ratio_ok = (res["learned"]["aligns_per_s_within_2cm_0.1deg_of_truth"] /
+                max(1e-9, res["plain"]["aligns_per_s_within_2cm_0.1deg_of_truth"]))
+    line = {
+        "metric": METRIC, "value": res["learned"]["aligns_per_s"], "unit": "aligns/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["learned"]["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32 pair terms, fp64 solve/line search; network bf16 x bf16 -> fp32 (tensor cores)",
+        "data": "synthetic (seeded plane + walls generator)",
+        "config": {"workload": f"{cfg.name}: {cfg.map_points}-point map ({cfg.area:.0f} x {cfg.area:.0f} m, "
+                               f"{cfg.walls} walls), {B} alignments, scans {cfg.scan_min}-{cfg.scan_max} points, "
+                               f"resolution {cfg.resolution} m, guesses +-{cfg.dt} m / +-{cfg.dyaw_deg} deg",
+                   "mode": "corrected", "learned": "3 network passes, NDT judge (score at proposal vs guess), "
+                                                  "NDT refinement"},
+        "plain": res["plain"], "learned": res["learned"],
+        "learned_vs_plain_aligns_per_s": ratio,
+        "learned_vs_plain_aligns_per_s_within_2cm_0.1deg_of_truth": ratio_ok,
+        "accuracy_vs_fp64_oracle": acc,
+        "training": {"pairs": int(pairs.keep.sum()), "scans": args.train_scans, "epochs": args.train_epochs,
+                     "pair_generation_s": t_pairs, "ndt_labelling_s": t_label, "gpu_training_s": t_train,
+                     "loss_first_last": [float(losses[:50].mean()), float(losses[-50:].mean())]},
+        "timing": "wall clock around synchronised steps (host round trips of the learned pipeline included)",
+    }
+    print(json.dumps(line))
+    net.close()
+    ctx.close()
+    return 0
+
+
+def run_posenet(args, pkg, local):
+    """Throughput of the network kernels alone: forward (inference) over B
+    scans of 512 sampled points and one training step over 256 scans, CUDA
+    events on the network's stream; the shared 64 -> 128 layer's FLOPs
+    against the measured dense BF16 peak."""
+    import torch
+    import posenet_ref
+    torch.cuda.set_device(local)
+    B, P = args.posenet_scans, 512
+    rng = np.random.default_rng(0)
+    pts = np.ones((B * P, 4), np.float32)
+    pts[:, :3] = rng.uniform(-40, 40, (B * P, 3))
+    offs = (np.arange(B + 1) * P).astype(np.int32)
+    g = np.tile(np.eye(4, dtype=np.float32).reshape(1, 16), (B, 1))
+    tgt = rng.normal(0, 1, (B, 6)).astype(np.float32)
+    d = {k: torch.from_numpy(v).cuda() for k, v in dict(p=pts, o=offs, g=g, t=tgt).items()}
+    y = torch.zeros((B, 6), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    net = pkg.posenet.PoseNet(device=local, scale=4.0)
+    net.set_weights(posenet_ref.init_weights(1))
+    st = torch.cuda.ExternalStream(net.stream)
+    out = {}
+    for name, fn in (("forward", lambda: net.forward(B, d["p"].data_ptr(), d["o"].data_ptr(), d["g"].data_ptr(),
+                                                       y.data_ptr(), P)),
+                     ("train_step_256", lambda: net.train_step(256, d["p"].data_ptr(), d["o"].data_ptr(),
+                                                               d["g"].data_ptr(), d["t"].data_ptr(), lr=1e-4,
+                                                               update=True, max_points=P))):
+        for _ in range(args.warmup):
+            fn()
+        net.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(args.steps):
+            fn()
+        e1.record(st)
+        e1.synchronize()
+        net.synchronize()
+        out[name] = e0.elapsed_time(e1) / args.steps
+    flops = 2.0 * B * P * 128 * 64
+    peak = None
+    pk = ROOT / "MEASURED_PEAKS.json"
+    if pk.exists():
+        peak = json.loads(pk.read_text()).get("bf16_tflops")
+    tf = flops / (out["forward"] / 1e3) / 1e12
+    print(json.dumps({"workload": f"point network: {B} scans x {P} points", "forward_ms": out["forward"],
+                      "train_step_256_ms": out["train_step_256"],
+                      "shared_layer_tflops": tf, "bf16_peak_tflops": peak,
+                      "frac_of_bf16_peak": (tf / peak) if peak else None}))
+    net.close()
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -521,11 +680,22 @@ def main(argv=None):
                     help="e2e: alignment groups whose host-to-device copy overlaps compute (0 = by size)")
     ap.add_argument("--graphs", type=int, choices=[0, 1], default=1,
                     help="1: each batch is one CUDA graph with a device-side round loop (default)")
+    ap.add_argument("--posenet", action="store_true", help="time the network kernels alone")
+    ap.add_argument("--posenet-scans", type=int, default=4096)
+    ap.add_argument("--learned", action="store_true",
+                    help="learned-init vs plain batched NDT (trains the network first; use --config c4 or c5)")
+    ap.add_argument("--train-scans", type=int, default=8000)
+    ap.add_argument("--train-epochs", type=int, default=30)
+    ap.add_argument("--oracle-sample", type=int, default=64)
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     pkg = load_pkg()
     world, rank, local = dist_setup()
+    if args.posenet and args.impl != "reference":
+        return run_posenet(args, pkg, local)
+    if args.learned and args.impl != "reference":
+        return run_learned(args, pkg, world, rank, local)
     if args.impl == "reference":
         return run_reference_arm(args, pkg, world, rank)
     return run_ours(args, pkg, world, rank, local)

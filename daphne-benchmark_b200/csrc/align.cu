@@ -485,6 +485,23 @@ int launch_step(AlignState *d_states, const double *d_partials, const int *d_chu
     return (int)cudaGetLastError();
 }
 
+// score[b] = the alignment's NDT score (sum over its chunk partials in chunk
+// order, plus its FP64 side sum) after one derivative pass.
+__global__ void score_kernel(const double *__restrict__ partials, const int *__restrict__ chunk_begin,
+                             const double *__restrict__ exc, int B, double *__restrict__ score) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B) return;
+    double v = 0.0;
+    for (int c = chunk_begin[b]; c < chunk_begin[b + 1]; ++c) v += partials[(size_t)c * kPartial];
+    score[b] = v + exc[(size_t)b * kPartial];
+}
+
+int launch_score(const double *d_partials, const int *d_chunk_begin, const double *d_exc, int B, double *d_score,
+                 cudaStream_t st) {
+    score_kernel<<<(B + 127) / 128, 128, 0, st>>>(d_partials, d_chunk_begin, d_exc, B, d_score);
+    return (int)cudaGetLastError();
+}
+
 int launch_finalize(const AlignState *d_states, int B, float *d_out, int *d_conv, double *d_fit, int *d_status,
                     const int *d_overflow, cudaStream_t st) {
     finalize_kernel<<<(B + 127) / 128, 128, 0, st>>>(d_states, B, d_out, d_conv, d_fit, d_status, d_overflow);

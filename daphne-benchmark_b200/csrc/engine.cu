@@ -898,6 +898,63 @@ int ndt_align_batch_packed(ndt_ctx *c, int B, const float *points, const int *of
     return packed_batch(c, B, points, offsets, guesses, out, converged, fitness, status);
 }
 
+int ndt_score_batch_device(ndt_ctx *c, int B, const float *d_points, const int *d_offsets, int total_points,
+                           const float *d_poses, double *d_score) {
+    if (!c || !d_points || !d_offsets || !d_poses || !d_score) return fail(c, NDT_E_ARG, "null argument");
+    if (int rc = set_device(c)) return rc;
+    if (!c->have_map) return fail(c, NDT_E_NOMAP, "no map set");
+    if (B <= 0 || total_points < 0) return fail(c, NDT_E_ARG, "empty batch");
+    const int tile = c->prm.precision == 1 ? kTile : kDerivVariants[c->variant].tile;
+    const int max_tiles = total_points / tile + B + 1;
+    CK(c->states.ensure(sizeof(AlignState) * (size_t)B));
+    RunPlan R;
+    std::memset(&R, 0, sizeof(R));
+    if (int rc0 = prepare_lists(c, B, max_tiles, R.L)) return rc0;
+    CK(c->partials.ensure(sizeof(double) * kPartial * (size_t)max_tiles));
+    CK(c->exc.ensure(sizeof(double) * kPartial * (size_t)B));
+    CK(c->counters.ensure(sizeof(Counters)));
+    CK(c->round_no.ensure(sizeof(int)));
+    cudaStream_t st = c->stream;
+    CK(cudaMemsetAsync(c->counters.p, 0, sizeof(Counters), st));
+    c->ev_used = 0;
+    R.P = step_params(c->prm);
+    EvalArgs &ea = R.ea;
+    ea.grid = grid_dev(c);
+    ea.points = (const float4 *)d_points;
+    ea.trans = nullptr;
+    ea.tiles = c->tiles.as<Tile>();
+    ea.num_tiles = c->num_tiles.as<int>();
+    ea.chunks = R.L.chunks;
+    ea.num_chunks = R.L.num_chunks;
+    ea.max_tiles = max_tiles;
+    ea.tile_size = tile;
+    ea.states = c->states.as<AlignState>();
+    ea.partials = c->partials.as<double>();
+    ea.exc = c->exc.as<double>();
+    ea.d1 = c->d1;
+    ea.d2 = c->d2;
+    ea.compat = c->prm.compat;
+    ea.counters = c->counters.as<Counters>();
+    if (int rc2 = prepare_flag_queue(c, ea)) return rc2;
+    R.d_offsets = d_offsets;
+    R.d_guesses = d_poses;
+    R.round_no = c->round_no.as<int>();
+    R.B = B;
+    R.tile = tile;
+    R.kb = chunk_big(c);
+    R.ks = chunk_small(c);
+    R.precision = c->prm.precision;
+    R.variant = c->variant;
+    R.sms = c->num_sms;
+    if (int rc = enqueue_prologue(c, R, st)) return rc;
+    int rc = launch_derivatives(R.ea, R.precision, R.variant, R.sms, st);
+    if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_derivatives");
+    rc = launch_score(R.ea.partials, R.L.chunk_begin, R.ea.exc, B, d_score, st);
+    if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_score");
+    c->launches += 4 + (R.precision == 1 ? 1 : kDerivLaunchesFP32) + 1;
+    return NDT_OK;
+}
+
 int ndt_set_batch_graphs(ndt_ctx *c, int on) {
     if (!c) return NDT_E_ARG;
     c->use_graphs = on != 0;

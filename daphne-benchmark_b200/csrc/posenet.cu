@@ -21,13 +21,14 @@
 // applied with Adam to FP32 master weights; W2 is then re-packed to BF16.
 //
 // Tensor-core tile (one CTA of 128 threads per scan, 128 sampled points per
-// tile): A = bf16(h1) [128 points x 64] and B = W2 [128 outputs x 64], both
+// tile): A = W2 [128 outputs x 64] and B = bf16(h1) [128 points x 64], both
 // K-major in shared memory in the interleaved (no-swizzle) core-matrix layout:
 // element (r, k) at (r / 8) * 1024 + (k / 8) * 128 + (r % 8) * 16 + (k % 8) * 2
 // bytes, so a descriptor's leading byte offset (next 8 K-elements) is 128 B
 // and its stride byte offset (next 8 rows) is 1024 B.  Four MMAs of K = 16
-// (start addresses 256 B apart) give D = A B^T, 128 x 128 FP32 in 128 TMEM
-// columns; each warp reads its 32 rows (TMEM lanes) back with tcgen05.ld.
+// (start addresses 256 B apart) give D = A B^T (channels x points), 128 x 128
+// FP32 in 128 TMEM columns; thread c reads its channel's row (TMEM lane c)
+// back with tcgen05.ld and keeps the running maximum over the points.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -112,8 +113,7 @@ __global__ void __launch_bounds__(128, 1) point_kernel(const __grid_constant__ P
     float *sW1 = reinterpret_cast<float *>(smem + 2 * kOperandBytes);  // 192 + 64 (b1) + 128 (b2)
     float *sB1 = sW1 + kH1 * 3;
     float *sB2 = sB1 + kH1;
-    unsigned long long *sMax = reinterpret_cast<unsigned long long *>(sB2 + kH2);  // 4 x 128
-    uint64_t *sBar = reinterpret_cast<uint64_t *>(sMax + 4 * kH2);
+    uint64_t *sBar = reinterpret_cast<uint64_t *>(sB2 + kH2);  // 8-byte aligned (offset 32768 + 1536)
     uint32_t *sTmem = reinterpret_cast<uint32_t *>(sBar + 1);
     __shared__ float sT[12];
 
@@ -145,15 +145,18 @@ __global__ void __launch_bounds__(128, 1) point_kernel(const __grid_constant__ P
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *sTmem;
 
-    const uint32_t idesc = umma::instr_desc_bf16_f32(kTileRows, kH2);
-    unsigned long long run[4];  // this thread's running max of columns 32 * i + lane ... (see below)
-    // per-thread running maxima of all 128 columns live in sMax after each tile:
-    // warp w, lane l keeps columns l, l + 32, l + 64, l + 96 of its 32 rows
-    for (int i = 0; i < 4; ++i) run[i] = 0ull;
+    // D = W2 h1^T: 128 channels (TMEM lanes; thread 32 warp + lane owns
+    // channel c) x 128 points of the tile (columns).  The max-pool is then a
+    // per-thread reduction over its own row; bias and ReLU are monotonic, so
+    // they apply once to the final maximum.
+    const uint32_t idesc = umma::instr_desc_bf16_f32(kH2, kTileRows);
+    const int c = tid;
+    float best = -INFINITY;
+    int best_j = 0;
     uint32_t phase = 0;
     const int tiles = (P + kTileRows - 1) / kTileRows;
     for (int t = 0; t < tiles; ++t) {
-        // layer 1 for this thread's row (sample j = t * 128 + tid)
+        // layer 1 for this thread's point (sample j = t * 128 + tid), row tid of the h1 operand
         const int j = t * kTileRows + tid;
         const bool valid = j < P;
         float u[3] = {0.f, 0.f, 0.f};
@@ -180,8 +183,9 @@ __global__ void __launch_bounds__(128, 1) point_kernel(const __grid_constant__ P
         if (tid == 0) {
 #pragma unroll
             for (int kk = 0; kk < kH1 / 16; ++kk) {
-                const uint64_t da = umma::smem_desc_kmajor_interleaved(smem_u32(sA) + kk * 256, 128, 1024);
-                const uint64_t db = umma::smem_desc_kmajor_interleaved(smem_u32(sB) + kk * 256, 128, 1024);
+                // A = W2 (channels x K), B = h1 (points x K), both K-major
+                const uint64_t da = umma::smem_desc_kmajor_interleaved(smem_u32(sB) + kk * 256, 128, 1024);
+                const uint64_t db = umma::smem_desc_kmajor_interleaved(smem_u32(sA) + kk * 256, 128, 1024);
                 const uint32_t accumulate = kk > 0 ? 1u : 0u;
                 const uint32_t no_mask = 0;  // disable-output-lane mask: all lanes written
                 asm volatile(
@@ -213,11 +217,12 @@ __global__ void __launch_bounds__(128, 1) point_kernel(const __grid_constant__ P
             phase ^= 1u;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        // accumulator rows of this warp: row = 32 * warp + lane, 128 columns
+        // this channel's 128 values: columns 32 q .. 32 q + 31 = points t * 128 + column
+        const int nvalid = min(kTileRows, P - t * kTileRows);
 #pragma unroll
-        for (int cq = 0; cq < 4; ++cq) {
+        for (int q = 0; q < 4; ++q) {
             uint32_t r[32];
-            const uint32_t addr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(32 * cq);
+            const uint32_t addr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(32 * q);
             asm volatile(
                 "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
                 "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
@@ -229,32 +234,24 @@ __global__ void __launch_bounds__(128, 1) point_kernel(const __grid_constant__ P
                   "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
                 : "r"(addr));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            // column c = 32 cq + e of row (this thread's sample j): ReLU(z + b2);
-            // warp max over its 32 rows, lane e keeps column 32 cq + e
 #pragma unroll
             for (int e = 0; e < 32; ++e) {
-                const float z = __uint_as_float(r[e]) + sB2[32 * cq + e];
-                unsigned long long v = valid ? pack_max(fmaxf(z, 0.0f), j) : 0ull;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
-                    v = w > v ? w : v;
+                const int col = 32 * q + e;
+                const float z = __uint_as_float(r[e]);
+                if (col < nvalid && z > best) {  // strict: the smallest index among equal maxima
+                    best = z;
+                    best_j = t * kTileRows + col;
                 }
-                if (lane == e) run[cq] = v > run[cq] ? v : run[cq];
             }
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();  // all TMEM reads and sA reads done before the next tile's writes and MMAs
+        __syncthreads();  // all TMEM reads and operand reads done before the next tile's writes and MMAs
     }
-    // combine the 4 warps, write the scan's max-pool
-#pragma unroll
-    for (int cq = 0; cq < 4; ++cq) sMax[warp * kH2 + 32 * cq + lane] = run[cq];
-    __syncthreads();
     {
-        const int c = tid;  // 128 threads, 128 channels
-        unsigned long long m = sMax[c];
-        for (int w = 1; w < 4; ++w) m = sMax[w * kH2 + c] > m ? sMax[w * kH2 + c] : m;
-        a.gmax[(size_t)b * kH2 + c] = m;
+        // g_c = ReLU(max_p z + b2_c); a zero maximum routes no gradient: report sample 0
+        float g = P > 0 ? fmaxf(best + sB2[c], 0.0f) : 0.0f;
+        const int j = g > 0.0f ? best_j : 0;
+        a.gmax[(size_t)b * kH2 + c] = P > 0 ? pack_max(g, j) : 0ull;
     }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (warp == 0)
@@ -444,7 +441,7 @@ int mlp_fail(ndt_mlp *c, cudaError_t e, const char *what) {
         if (e_ != cudaSuccess) return mlp_fail(c, e_, #call);   \
     } while (0)
 
-constexpr size_t kPointSmem = 2 * pn::kOperandBytes + (pn::kH1 * 3 + pn::kH1 + pn::kH2) * 4 + 4 * pn::kH2 * 8 + 64;
+constexpr size_t kPointSmem = 2 * pn::kOperandBytes + (pn::kH1 * 3 + pn::kH1 + pn::kH2) * 4 + 64;
 // keep at most 4 CTAs per SM, so that 4 x 128 TMEM columns fit
 constexpr size_t kPointSmemAlloc = kPointSmem < 48 * 1024 ? 48 * 1024 : kPointSmem;
 

@@ -96,6 +96,8 @@ def lib():
                                              C.c_void_p, C.c_void_p, C.c_void_p]
         L.ndt_set_profiling.argtypes = [ctxp, C.c_int]
         L.ndt_set_batch_graphs.argtypes = [ctxp, C.c_int]
+        L.ndt_score_batch_device.argtypes = [ctxp, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                             C.c_void_p]
         L.ndt_kernel_variants.argtypes = []
         L.ndt_kernel_variant_shape.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.ndt_set_kernel_variant.argtypes = [ctxp, C.c_int]
@@ -111,7 +113,8 @@ def lib():
                      "ndt_align_batch", "ndt_align_batch_device", "ndt_synchronize", "ndt_get_counters",
                      "ndt_grid_info", "ndt_grid_cells", "ndt_derivatives", "ndt_align_batch_packed",
                      "ndt_set_profiling", "ndt_kernel_variants", "ndt_kernel_variant_shape",
-                     "ndt_set_kernel_variant", "ndt_window_info", "ndt_set_batch_graphs"):
+                     "ndt_set_kernel_variant", "ndt_window_info", "ndt_set_batch_graphs",
+                     "ndt_score_batch_device"):
             getattr(L, name).restype = C.c_int
         _LIB = L
     return _LIB
@@ -252,6 +255,12 @@ class Context:
     def set_map_ptr(self, ptr: int, m: int):
         """Host map by raw pointer (e.g. a pinned torch tensor)."""
         self._check(self.L.ndt_set_map(self.h, C.c_void_p(ptr), m), "ndt_set_map")
+
+    def score_batch_device(self, B, d_points, d_offsets, total, d_poses, d_score):
+        """NDT score of B scans at B poses (device pointers), into d_score (B doubles)."""
+        self._check(self.L.ndt_score_batch_device(self.h, B, C.c_void_p(d_points), C.c_void_p(d_offsets), total,
+                                                  C.c_void_p(d_poses), C.c_void_p(d_score)),
+                    "ndt_score_batch_device")
 
     def set_batch_graphs(self, on=True):
         self._check(self.L.ndt_set_batch_graphs(self.h, int(on)), "ndt_set_batch_graphs")

@@ -166,3 +166,43 @@ def apply_correction(guess16, y, delta_scale=DELTA_SCALE):
     """The proposed 4x4 (float32, row major) from a guess and a network output."""
     p = pose_from_matrix(guess16) + np.asarray(y, np.float64) * delta_scale
     return matrix_from_pose(p).astype(np.float32).reshape(16)
+
+
+def poses_from_matrices(T):
+    """Vectorised pose_from_matrix: (B, 16) or (B, 4, 4) -> (B, 6)."""
+    T = np.asarray(T, np.float64).reshape(-1, 4, 4)
+    b = np.arcsin(np.clip(T[:, 0, 2], -1.0, 1.0))
+    a = np.arctan2(-T[:, 1, 2], T[:, 2, 2])
+    c = np.arctan2(-T[:, 0, 1], T[:, 0, 0])
+    return np.stack([T[:, 0, 3], T[:, 1, 3], T[:, 2, 3], a, b, c], 1)
+
+
+def matrices_from_poses(p):
+    """Vectorised matrix_from_pose: (B, 6) -> (B, 16) float32."""
+    p = np.asarray(p, np.float64)
+    a, b, c = p[:, 3], p[:, 4], p[:, 5]
+    ca, sa, cb, sb, cc, sc = np.cos(a), np.sin(a), np.cos(b), np.sin(b), np.cos(c), np.sin(c)
+    T = np.zeros((len(p), 4, 4))
+    # Rx(a) Ry(b) Rz(c)
+    T[:, 0, 0] = cb * cc
+    T[:, 0, 1] = -cb * sc
+    T[:, 0, 2] = sb
+    T[:, 1, 0] = ca * sc + sa * sb * cc
+    T[:, 1, 1] = ca * cc - sa * sb * sc
+    T[:, 1, 2] = -sa * cb
+    T[:, 2, 0] = sa * sc - ca * sb * cc
+    T[:, 2, 1] = sa * cc + ca * sb * sc
+    T[:, 2, 2] = ca * cb
+    T[:, :3, 3] = p[:, :3]
+    T[:, 3, 3] = 1.0
+    return T.astype(np.float32).reshape(-1, 16)
+
+
+def correction_targets(guesses16, converged16, delta_scale=DELTA_SCALE):
+    d = poses_from_matrices(converged16) - poses_from_matrices(guesses16)
+    d[:, 3:] = wrap_angle(d[:, 3:])
+    return (d / delta_scale).astype(np.float32)
+
+
+def apply_corrections(guesses16, y, delta_scale=DELTA_SCALE):
+    return matrices_from_poses(poses_from_matrices(guesses16) + np.asarray(y, np.float64) * delta_scale)

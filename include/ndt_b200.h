@@ -186,6 +186,16 @@ NDT_API int ndt_get_counters(ndt_ctx *ctx, ndt_counters *out);
 NDT_API int ndt_set_batch_graphs(ndt_ctx *ctx, int on);
 
 /*
+ * NDT score of B scans at given poses (one derivative pass, no iteration):
+ * d_score[b] = the score of computeDerivatives (kernel.cpp:651-705; the
+ * corrected mode's objective when compat = 0), higher = better fit.  Device
+ * arrays as ndt_align_batch_device (d_poses: B x 16 row major).  Used to judge
+ * a learned pose proposal against the raw guess.  No reference counterpart.
+ */
+NDT_API int ndt_score_batch_device(ndt_ctx *ctx, int B, const float *d_points, const int *d_offsets,
+                                   int total_points, const float *d_poses, double *d_score);
+
+/*
  * Launch shape of the FP32 derivative pass (points per tile = threads per
  * block, resident blocks per SM).  The autotuner (daphne-benchmark_b200/
  * autotune.py) times every variant on a sample batch and selects one.
