@@ -410,6 +410,60 @@ __global__ void reduce_adam_kernel(const __grid_constant__ AdamArgs a) {
     a.w[i] -= a.lr * (m / a.bc1) / (sqrtf(v / a.bc2) + a.eps);
 }
 
+// Pose vector (x, y, z, roll, pitch, yaw) of T = Trans Rx Ry Rz and back, FP64.
+__device__ __forceinline__ void pose_of(const float *T, double p[6]) {
+    p[0] = T[3];
+    p[1] = T[7];
+    p[2] = T[11];
+    p[3] = atan2(-(double)T[6], (double)T[10]);
+    p[4] = asin(fmin(1.0, fmax(-1.0, (double)T[2])));
+    p[5] = atan2(-(double)T[1], (double)T[0]);
+}
+
+__device__ __forceinline__ void matrix_of(const double p[6], float *T) {
+    double sa, ca, sb, cb, sc, cc;
+    sincos(p[3], &sa, &ca);
+    sincos(p[4], &sb, &cb);
+    sincos(p[5], &sc, &cc);
+    T[0] = (float)(cb * cc);
+    T[1] = (float)(-cb * sc);
+    T[2] = (float)sb;
+    T[3] = (float)p[0];
+    T[4] = (float)(ca * sc + sa * sb * cc);
+    T[5] = (float)(ca * cc - sa * sb * sc);
+    T[6] = (float)(-sa * cb);
+    T[7] = (float)p[1];
+    T[8] = (float)(sa * sc - ca * sb * cc);
+    T[9] = (float)(sa * cc + ca * sb * sc);
+    T[10] = (float)(ca * cb);
+    T[11] = (float)p[2];
+    T[12] = T[13] = T[14] = 0.0f;
+    T[15] = 1.0f;
+}
+
+// proposal = T(pose(guess) + y * dscale)
+__global__ void apply_kernel(const float *__restrict__ guesses, const float *__restrict__ y, Norm nm, int B,
+                             float *__restrict__ out) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B) return;
+    double p[6];
+    pose_of(guesses + 16 * (size_t)b, p);
+    for (int i = 0; i < 6; ++i) p[i] += (double)y[6 * (size_t)b + i] * (double)nm.dscale[i];
+    matrix_of(p, out + 16 * (size_t)b);
+}
+
+// The NDT's judgement: start from the proposal where its score is at least
+// the raw guess's, from the guess otherwise.
+__global__ void judge_kernel(const float *__restrict__ prop, const float *__restrict__ guess,
+                             const double *__restrict__ s_prop, const double *__restrict__ s_guess, int B,
+                             float *__restrict__ start, int *__restrict__ used) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B) return;
+    const bool u = s_prop[b] >= s_guess[b];
+    for (int k = 0; k < 16; ++k) start[16 * (size_t)b + k] = u ? prop[16 * (size_t)b + k] : guess[16 * (size_t)b + k];
+    if (used) used[b] = u ? 1 : 0;
+}
+
 }  // namespace pn
 
 // ---------------------------------------------------------------------------
@@ -417,6 +471,7 @@ __global__ void reduce_adam_kernel(const __grid_constant__ AdamArgs a) {
 struct ndt_mlp {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;  // created with the network; `stream` may be a caller's
     float *w = nullptr, *m = nullptr, *v = nullptr, *grad = nullptr, *loss = nullptr;
     uint8_t *w2op = nullptr;
     int *err = nullptr;
@@ -491,7 +546,8 @@ int ndt_mlp_create(int device, ndt_mlp **out) {
     ndt_mlp *c = new ndt_mlp();
     c->device = device;
     cudaError_t e = cudaSetDevice(device);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+    c->stream = c->own_stream;
     if (e == cudaSuccess) e = cudaMalloc(&c->w, sizeof(float) * pn::kNumW);
     if (e == cudaSuccess) e = cudaMalloc(&c->m, sizeof(float) * pn::kNumW);
     if (e == cudaSuccess) e = cudaMalloc(&c->v, sizeof(float) * pn::kNumW);
@@ -521,7 +577,7 @@ void ndt_mlp_destroy(ndt_mlp *c) {
     void *bufs[] = {c->w, c->m, c->v, c->grad, c->loss, c->w2op, c->err, c->gmax, c->grad_scan, c->loss_scan};
     for (void *p : bufs)
         if (p) cudaFree(p);
-    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
 }
 
@@ -646,5 +702,37 @@ int ndt_mlp_synchronize(ndt_mlp *c, int *tc_error) {
 }
 
 void *ndt_mlp_stream(ndt_mlp *c) { return c ? (void *)c->stream : nullptr; }
+
+int ndt_mlp_set_stream(ndt_mlp *c, void *stream) {
+    if (!c) return NDT_E_ARG;
+    MCK(cudaStreamSynchronize(c->stream));
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    return NDT_OK;
+}
+
+int ndt_mlp_propose_device(ndt_mlp *c, int B, const float *d_points, const int *d_offsets, const float *d_guesses,
+                           int max_points, int passes, float *d_y6, float *d_prop16) {
+    if (!c || B <= 0 || !d_points || !d_offsets || !d_guesses || !d_y6 || !d_prop16 || max_points <= 0 || passes < 1)
+        return NDT_E_ARG;
+    MCK(cudaSetDevice(c->device));
+    const float *g = d_guesses;
+    for (int k = 0; k < passes; ++k) {
+        if (int rc = ndt_mlp_forward_device(c, B, d_points, d_offsets, g, max_points, d_y6)) return rc;
+        pn::apply_kernel<<<(B + 127) / 128, 128, 0, c->stream>>>(g, d_y6, c->nm, B, d_prop16);
+        MCK(cudaGetLastError());
+        g = d_prop16;  // the next pass reads the previous proposal (in place: each thread reads its own row first)
+    }
+    return NDT_OK;
+}
+
+int ndt_mlp_judge_device(ndt_mlp *c, int B, const float *d_prop16, const float *d_guesses, const double *d_score_prop,
+                         const double *d_score_guess, float *d_start16, int *d_used) {
+    if (!c || B <= 0 || !d_prop16 || !d_guesses || !d_score_prop || !d_score_guess || !d_start16) return NDT_E_ARG;
+    MCK(cudaSetDevice(c->device));
+    pn::judge_kernel<<<(B + 127) / 128, 128, 0, c->stream>>>(d_prop16, d_guesses, d_score_prop, d_score_guess, B,
+                                                             d_start16, d_used);
+    MCK(cudaGetLastError());
+    return NDT_OK;
+}
 
 }  // extern "C"

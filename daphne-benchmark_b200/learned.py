@@ -207,6 +207,54 @@ def score(ctx, torch, pts, offs, total, poses_np):
     return s.cpu().numpy()
 
 
+class LearnedBatch:
+    """Device buffers of the learned pipeline for one batch; run() enqueues
+    proposal passes, the two score passes, the judge and the refinement on the
+    NDT context's stream (the network is put on that stream), with one
+    synchronisation at the end."""
+
+    def __init__(self, ctx, net, torch, pts, offs, total, guesses_np, max_points=512, passes=3):
+        B = len(guesses_np)
+        self.ctx, self.net, self.torch = ctx, net, torch
+        self.pts, self.offs, self.total, self.B = pts, offs, total, B
+        self.max_points, self.passes = max_points, passes
+        f32 = dict(dtype=torch.float32, device="cuda")
+        self.g = torch.from_numpy(np.ascontiguousarray(guesses_np, np.float32)).cuda()
+        self.y = torch.zeros((B, 6), **f32)
+        self.prop = torch.zeros((B, 16), **f32)
+        self.start = torch.zeros((B, 16), **f32)
+        self.s_p = torch.zeros(B, dtype=torch.float64, device="cuda")
+        self.s_g = torch.zeros(B, dtype=torch.float64, device="cuda")
+        self.used = torch.zeros(B, dtype=torch.int32, device="cuda")
+        self.out = torch.zeros((B, 16), **f32)
+        self.conv = torch.zeros(B, dtype=torch.int32, device="cuda")
+        self.fit = torch.zeros(B, dtype=torch.float64, device="cuda")
+        self.st = torch.zeros(B, dtype=torch.int32, device="cuda")
+        torch.cuda.current_stream().synchronize()
+        net.set_stream(ctx.stream)
+
+    def run(self):
+        n, c, B = self.net, self.ctx, self.B
+        n.propose_device(B, self.pts.data_ptr(), self.offs.data_ptr(), self.g.data_ptr(), self.y.data_ptr(),
+                         self.prop.data_ptr(), self.passes, self.max_points)
+        c.score_batch_device(B, self.pts.data_ptr(), self.offs.data_ptr(), self.total, self.prop.data_ptr(),
+                             self.s_p.data_ptr())
+        c.score_batch_device(B, self.pts.data_ptr(), self.offs.data_ptr(), self.total, self.g.data_ptr(),
+                             self.s_g.data_ptr())
+        n.judge_device(B, self.prop.data_ptr(), self.g.data_ptr(), self.s_p.data_ptr(), self.s_g.data_ptr(),
+                       self.start.data_ptr(), self.used.data_ptr())
+        c.align_batch_device(B, self.pts.data_ptr(), self.offs.data_ptr(), self.total, self.start.data_ptr(),
+                             self.out.data_ptr(), self.conv.data_ptr(), self.fit.data_ptr(), self.st.data_ptr())
+        c.synchronize()
+
+    def results(self):
+        return (self.out.cpu().numpy(), self.conv.cpu().numpy(), self.fit.cpu().numpy(), self.st.cpu().numpy(),
+                self.used.cpu().numpy() != 0, self.prop.cpu().numpy(), self.start.cpu().numpy())
+
+    def close(self):
+        self.net.set_stream(None)
+
+
 def learned_align(ctx, net, torch, pts, offs, total, guesses_np, max_points=512, passes=1):
     """Proposal (the network applied `passes` times, each pass to the previous
     proposal) -> judge -> refine.  Returns (out, conv, fit, status, used_proposal)."""

@@ -39,9 +39,12 @@ def _lib():
         L.ndt_mlp_synchronize.argtypes = [p, C.POINTER(C.c_int)]
         L.ndt_mlp_stream.argtypes = [p]
         L.ndt_mlp_stream.restype = p
+        L.ndt_mlp_set_stream.argtypes = [p, p]
+        L.ndt_mlp_propose_device.argtypes = [p, C.c_int, p, p, p, C.c_int, C.c_int, p, p]
+        L.ndt_mlp_judge_device.argtypes = [p, C.c_int, p, p, p, p, p, p]
         for n in ("ndt_mlp_create", "ndt_mlp_set_input_frame", "ndt_mlp_set_weights", "ndt_mlp_get_weights",
                   "ndt_mlp_forward_device", "ndt_mlp_train_step_device", "ndt_mlp_maxpool_device",
-                  "ndt_mlp_synchronize"):
+                  "ndt_mlp_synchronize", "ndt_mlp_set_stream", "ndt_mlp_propose_device", "ndt_mlp_judge_device"):
             getattr(L, n).restype = C.c_int
         L._pn_ready = True
     return L
@@ -122,6 +125,20 @@ class PoseNet:
         self._check(self.L.ndt_mlp_synchronize(self.h, C.byref(e)), "synchronize")
         if e.value:
             raise _ndt.NdtError("tensor-core wait gave up (mbarrier wait limit)")
+
+    def set_stream(self, stream):
+        """Run on a caller's stream (an int handle, e.g. Context.stream), or its own (None)."""
+        self._check(self.L.ndt_mlp_set_stream(self.h, C.c_void_p(stream) if stream else None), "set_stream")
+
+    def propose_device(self, B, d_points, d_offsets, d_guesses, d_y, d_prop, passes=3, max_points=512):
+        self._check(self.L.ndt_mlp_propose_device(self.h, B, C.c_void_p(d_points), C.c_void_p(d_offsets),
+                                                  C.c_void_p(d_guesses), max_points, passes, C.c_void_p(d_y),
+                                                  C.c_void_p(d_prop)), "propose")
+
+    def judge_device(self, B, d_prop, d_guesses, d_s_prop, d_s_guess, d_start, d_used=0):
+        self._check(self.L.ndt_mlp_judge_device(self.h, B, C.c_void_p(d_prop), C.c_void_p(d_guesses),
+                                                C.c_void_p(d_s_prop), C.c_void_p(d_s_guess), C.c_void_p(d_start),
+                                                C.c_void_p(d_used) if d_used else None), "judge")
 
     @property
     def stream(self):

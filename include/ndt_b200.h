@@ -287,6 +287,19 @@ NDT_API int ndt_mlp_train_step_device(ndt_mlp *mlp, int B, const float *d_points
 NDT_API int ndt_mlp_maxpool_device(ndt_mlp *mlp, unsigned long long *d_out, int B);
 NDT_API int ndt_mlp_synchronize(ndt_mlp *mlp, int *tc_error);
 NDT_API void *ndt_mlp_stream(ndt_mlp *mlp);
+/* Run the network's work on a caller's stream (e.g. ndt_stream of an NDT context, so that proposals, the
+ * judge's scores and the refinement are ordered without host synchronisation); NULL = its own stream. */
+NDT_API int ndt_mlp_set_stream(ndt_mlp *mlp, void *stream);
+/* Proposals: `passes` times, y = network(scan at the current pose) and pose <- T(pose(current) + y *
+ * delta_scale), starting from the guesses; d_prop16 receives the last poses (B x 16), d_y6 the last y. */
+NDT_API int ndt_mlp_propose_device(ndt_mlp *mlp, int B, const float *d_points, const int *d_offsets,
+                                   const float *d_guesses, int max_points, int passes, float *d_y6,
+                                   float *d_prop16);
+/* The NDT judge: d_start16[b] = proposal b where d_score_prop[b] >= d_score_guess[b] (scores of
+ * ndt_score_batch_device), the raw guess otherwise; d_used[b] (optional) = 1 where the proposal won. */
+NDT_API int ndt_mlp_judge_device(ndt_mlp *mlp, int B, const float *d_prop16, const float *d_guesses,
+                                 const double *d_score_prop, const double *d_score_guess, float *d_start16,
+                                 int *d_used);
 
 #ifdef __cplusplus
 }

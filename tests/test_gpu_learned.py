@@ -52,6 +52,16 @@ def test_learned_initial_pose_beats_plain(pkg, binding_mod):
           f"within 2 cm / 0.1 deg of truth: plain {ok_plain:.3f}, learned {ok_learned:.3f}")
     assert np.median(p_dt) < 0.6 * np.median(g_dt)
     assert ok_learned >= ok_plain + 0.15
+    # the same pipeline enqueued on one stream with device-side proposals and judge
+    lb = L.LearnedBatch(ctx, net, torch, pts, offs, total, guesses, passes=3)
+    lb.run()
+    d_out, d_conv, _, d_st, d_used, _, _ = lb.results()
+    lb.close()
+    d_dt, d_dr = L.pose_errors(d_out, truths)
+    ok_device = np.mean((d_dt <= 0.02) & (d_dr <= 0.1))
+    assert (d_st == 0).all()
+    assert ok_device >= ok_plain + 0.15
+    assert abs(ok_device - ok_learned) <= 0.05
     # the refinement from the chosen starts against the FP64 oracle (sample)
     s_p = L.score(ctx, torch, pts, offs, total, prop)
     s_g = L.score(ctx, torch, pts, offs, total, guesses)
