@@ -518,6 +518,9 @@ def run_learned(args, pkg, world, rank, local):
         return 0
     L, ndt, synth = pkg.learned, pkg.ndt, pkg.synth
     cfg = synth.CONFIGS[args.config]
+    big = cfg.map_points > 1_000_000
+    args.train_scans = args.train_scans or (16000 if big else 8000)
+    args.train_epochs = args.train_epochs or (60 if big else 30)
     scene = synth.make_scene(cfg)
     ctx = ndt.Context(ndt.corrected_params(cfg.resolution), device=local)
     ctx.set_map(scene.map)
@@ -706,8 +709,8 @@ def main(argv=None):
     ap.add_argument("--posenet-scans", type=int, default=4096)
     ap.add_argument("--learned", action="store_true",
                     help="learned-init vs plain batched NDT (trains the network first; use --config c4 or c5)")
-    ap.add_argument("--train-scans", type=int, default=8000)
-    ap.add_argument("--train-epochs", type=int, default=30)
+    ap.add_argument("--train-scans", type=int, default=0, help="0: 8000 (c4), 16000 (c5)")
+    ap.add_argument("--train-epochs", type=int, default=0, help="0: 30 (c4), 60 (c5)")
     ap.add_argument("--oracle-sample", type=int, default=64)
     args = ap.parse_args(argv)
     if args.warmup < 3:

@@ -260,11 +260,15 @@ int build_grid(ndt_ctx *c, const float4 *d_map, int m) {
         if (!c->grid_ev[1]) CK(cudaEventCreate(&c->grid_ev[1]));
         CK(cudaEventRecord(c->grid_ev[0], c->stream));
     }
-    CK(c->scratch.ensure(ndt::grid_scratch_bytes(m)));
+    {
+        void *old = c->scratch.p;
+        CK(c->scratch.ensure(ndt::grid_scratch_bytes(m)));
+        if (c->scratch.p != old) CK((cudaError_t)grid_scratch_init(c->scratch.p, c->stream));
+    }
     CK(c->meta.ensure(sizeof(GridMeta)));
     int rc = grid_bbox(d_map, m, c->prm.resolution, c->meta.as<GridMeta>(), c->scratch.p, c->stream);
     if (rc) return cuda_fail(c, (cudaError_t)rc, "grid_bbox");
-    c->launches += 2;
+    c->launches += 1;
     CK(cudaMemcpyAsync(&c->meta_host, c->meta.p, sizeof(GridMeta), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     if (c->meta_host.error == 2) return fail(c, NDT_E_ARG, "map has non-finite coordinates");

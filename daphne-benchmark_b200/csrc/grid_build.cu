@@ -28,6 +28,11 @@ constexpr int kThreads = 256;
 constexpr int kItems = 8;                       // items per thread in the sort / segment tiles
 constexpr int kSortTile = kThreads * kItems;    // 2048
 constexpr int kWarps = kThreads / 32;
+constexpr int kMaxDigits = 1 << 10;             // radix digits of one pass, at most
+// Scratch layout: [bounding-box partials (6 x 1024 floats) + its 2 counters,
+// which must stay zero between builds] [sort and segment buffers].
+constexpr size_t kBboxFlagsOffset = sizeof(float) * 6 * 1024;
+constexpr size_t kBboxBytes = kBboxFlagsOffset + 256;
 
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;
@@ -38,8 +43,12 @@ __device__ __forceinline__ unsigned lanemask_lt() {
 // ---------------------------------------------------------------------------
 // Bounding box.  min/max are exact in any order; NaN/inf points are counted
 // and make the build fail (the reference's behaviour there is undefined).
-__global__ void bbox_partial_kernel(const float4 *__restrict__ map, int m, float *__restrict__ part,
-                                    int *__restrict__ nonfinite) {
+// One kernel: block partial min/max, then the last block to finish (atomic
+// ticket) reduces the partials and computes the grid geometry with the
+// reference's float arithmetic (kernel.cpp:1305-1322).  *flags = {ticket,
+// non-finite}: zero on entry, reset to zero by the last block.
+__global__ void bbox_kernel(const float4 *__restrict__ map, int m, float *__restrict__ part, int *__restrict__ flags,
+                            float res, GridMeta *__restrict__ meta) {
     float mn0 = FLT_MAX, mn1 = FLT_MAX, mn2 = FLT_MAX;
     float mx0 = -FLT_MAX, mx1 = -FLT_MAX, mx2 = -FLT_MAX;
     int bad = 0;
@@ -61,36 +70,39 @@ __global__ void bbox_partial_kernel(const float4 *__restrict__ map, int m, float
         mx2 = fmaxf(mx2, __shfl_xor_sync(0xffffffffu, mx2, o));
     }
     __shared__ float s[kWarps][6];
+    __shared__ int s_last;
     int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (lane == 0) {
         s[w][0] = mn0; s[w][1] = mn1; s[w][2] = mn2;
         s[w][3] = mx0; s[w][4] = mx1; s[w][5] = mx2;
     }
-    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(nonfinite, 1);
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flags + 1, 1);
     if (threadIdx.x < 6) {
         float v = s[0][threadIdx.x];
         for (int k = 1; k < kWarps; ++k)
             v = threadIdx.x < 3 ? fminf(v, s[k][threadIdx.x]) : fmaxf(v, s[k][threadIdx.x]);
         part[6 * blockIdx.x + threadIdx.x] = v;
     }
-}
-
-// kernel.cpp:1318-1322: min -= 0.01f, max += 0.01f, dim = (max - min) / res + 1
-// (float arithmetic, truncated to int).
-__global__ void bbox_final_kernel(const float *__restrict__ part, int nblk, float res,
-                                  const int *__restrict__ nonfinite, GridMeta *__restrict__ meta) {
-    // min/max of the block partials (exact in any order), then the
-    // reference's float arithmetic on one thread
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(flags, 1) == (int)gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    // min/max of the block partials (exact in any order)
+    const int nblk = gridDim.x;
     float v[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
     for (int b = threadIdx.x; b < nblk; b += blockDim.x)
-        for (int k = 0; k < 6; ++k) v[k] = k < 3 ? fminf(v[k], part[6 * b + k]) : fmaxf(v[k], part[6 * b + k]);
+        for (int k = 0; k < 6; ++k) {
+            const float x = __ldcg(part + 6 * b + k);
+            v[k] = k < 3 ? fminf(v[k], x) : fmaxf(v[k], x);
+        }
     for (int o = 16; o > 0; o >>= 1)
         for (int k = 0; k < 6; ++k) {
             float u = __shfl_xor_sync(0xffffffffu, v[k], o);
             v[k] = k < 3 ? fminf(v[k], u) : fmaxf(v[k], u);
         }
-    __shared__ float s[kWarps][6];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __syncthreads();
     if (lane == 0)
         for (int k = 0; k < 6; ++k) s[w][k] = v[k];
     __syncthreads();
@@ -100,7 +112,7 @@ __global__ void bbox_final_kernel(const float *__restrict__ part, int nblk, floa
     GridMeta g;
     g.res = res;
     g.occupied = 0;
-    g.error = *nonfinite ? 2 : 0;
+    g.error = atomicAdd(flags + 1, 0) ? 2 : 0;
     long long G = 1;
     for (int e = 0; e < 3; ++e) {
         g.minv[e] = v[e] - 0.01f;
@@ -115,6 +127,8 @@ __global__ void bbox_final_kernel(const float *__restrict__ part, int nblk, floa
     }
     g.G = G;
     *meta = g;
+    flags[0] = 0;
+    flags[1] = 0;
 }
 
 // Dense cell id of each map point (linearizeCoord, kernel.cpp:236-244).
@@ -152,40 +166,64 @@ __global__ void radix_upsweep_kernel(const uint32_t *__restrict__ keys, int n, i
     for (int d = threadIdx.x; d < nb; d += blockDim.x) hist[d * gridDim.x + blockIdx.x] = s_hist[d];
 }
 
-// Exclusive scan of n ints in place with one block of 1024 threads; each
-// thread owns a contiguous chunk.  *total (optional) receives the sum.
-__global__ void scan_single_block_kernel(int *__restrict__ data, int n, int *__restrict__ total) {
+// Exclusive scan of n ints in place with one block of 1024 threads; *total
+// (optional) receives the sum.  Tiles of 8192 ints are staged in shared
+// memory with coalesced loads and stores; each thread scans 8 consecutive
+// values (two 16-byte shared loads), the block scans the thread sums, and a
+// carry links the tiles.
+__global__ void __launch_bounds__(1024) scan_single_block_kernel(int *__restrict__ data, int n,
+                                                                 int *__restrict__ total) {
+    constexpr int kT = 1024, kI = 8, kTileN = kT * kI;
+    __shared__ __align__(16) int s_data[kTileN];
     __shared__ int s_warp[32];
-    const int t = threadIdx.x, nt = blockDim.x;
-    const int chunk = (n + nt - 1) / nt;
-    const int lo = min(n, t * chunk), hi = min(n, lo + chunk);
-    int sum = 0;
-    for (int i = lo; i < hi; ++i) sum += data[i];
-    int lane = t & 31, w = t >> 5;
-    int incl = sum;
-    for (int o = 1; o < 32; o <<= 1) {
-        int v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-    }
-    if (lane == 31) s_warp[w] = incl;
-    __syncthreads();
-    if (w == 0) {
-        int v = (lane < (nt >> 5)) ? s_warp[lane] : 0;
-        int inc2 = v;
+    __shared__ int s_carry;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    if (t == 0) s_carry = 0;
+    for (int base = 0; base < n; base += kTileN) {
+        for (int i = t; i < kTileN; i += kT) s_data[i] = base + i < n ? data[base + i] : 0;
+        __syncthreads();
+        const int4 a = reinterpret_cast<const int4 *>(s_data)[2 * t];
+        const int4 b = reinterpret_cast<const int4 *>(s_data)[2 * t + 1];
+        const int v[kI] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+        int sum = 0;
+#pragma unroll
+        for (int k = 0; k < kI; ++k) sum += v[k];
+        int incl = sum;
+#pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            int u = __shfl_up_sync(0xffffffffu, inc2, o);
-            if (lane >= o) inc2 += u;
+            const int u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += u;
         }
-        s_warp[lane] = inc2 - v;
+        if (lane == 31) s_warp[w] = incl;
+        const int carry = s_carry;
+        __syncthreads();
+        if (w == 0) {
+            const int x = s_warp[lane];
+            int inc2 = x;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, inc2, o);
+                if (lane >= o) inc2 += u;
+            }
+            s_warp[lane] = inc2 - x;
+            if (lane == 31) s_carry = carry + inc2;
+        }
+        __syncthreads();
+        int run = carry + s_warp[w] + incl - sum;
+        int o[kI];
+#pragma unroll
+        for (int k = 0; k < kI; ++k) {
+            o[k] = run;
+            run += v[k];
+        }
+        reinterpret_cast<int4 *>(s_data)[2 * t] = make_int4(o[0], o[1], o[2], o[3]);
+        reinterpret_cast<int4 *>(s_data)[2 * t + 1] = make_int4(o[4], o[5], o[6], o[7]);
+        __syncthreads();
+        for (int i = t; i < kTileN; i += kT)
+            if (base + i < n) data[base + i] = s_data[i];
+        __syncthreads();
     }
-    __syncthreads();
-    int run = s_warp[w] + incl - sum;
-    for (int i = lo; i < hi; ++i) {
-        int v = data[i];
-        data[i] = run;
-        run += v;
-    }
-    if (total && t == nt - 1) *total = run;
+    if (total && t == 0) *total = s_carry;
 }
 
 // Stable scatter: warp w of a block owns items [base + w*256, base + w*256 + 256)
@@ -328,9 +366,10 @@ __device__ bool write_records(int s, const double *mu, const double *C, GridBuff
 // (G = dense cell count), inverted by adjugate (invertMatrix, :1277-1300).
 __global__ void cell_finalize_compat_kernel(const float4 *__restrict__ map, const uint32_t *__restrict__ order,
                                             const int *__restrict__ seg_start, const uint32_t *__restrict__ seg_cell,
-                                            const int *__restrict__ nseg, int n, const GridMeta *__restrict__ meta,
+                                            const int *__restrict__ nseg, int n, GridMeta *__restrict__ meta,
                                             GridBuffers buf) {
     const int K = *nseg;
+    if (blockIdx.x == 0 && threadIdx.x == 0) meta->occupied = K;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= K) return;
     const int lo = seg_start[s], hi = (s + 1 < K) ? seg_start[s + 1] : n;
@@ -424,8 +463,10 @@ __device__ void jacobi3(double A[3][3], double V[3][3], double w[3]) {
 __global__ void cell_finalize_corrected_kernel(const float4 *__restrict__ map, const uint32_t *__restrict__ order,
                                                const int *__restrict__ seg_start,
                                                const uint32_t *__restrict__ seg_cell, const int *__restrict__ nseg,
-                                               int n, int min_points, double eig_ratio, GridBuffers buf) {
+                                               int n, int min_points, double eig_ratio, GridMeta *__restrict__ meta,
+                                               GridBuffers buf) {
     const int K = *nseg;
+    if (blockIdx.x == 0 && threadIdx.x == 0) meta->occupied = K;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= K) return;
     const int lo = seg_start[s], hi = (s + 1 < K) ? seg_start[s + 1] : n;
@@ -550,10 +591,6 @@ __global__ void window_fill_kernel(const int32_t *__restrict__ index, const floa
     });
 }
 
-__global__ void store_occupied_kernel(const int *__restrict__ nseg, GridMeta *__restrict__ meta) {
-    if (threadIdx.x == 0) meta->occupied = *nseg;
-}
-
 inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
 
 }  // namespace
@@ -563,9 +600,9 @@ size_t grid_scratch_bytes(int m) {
     size_t nblk = (size_t)div_up(m, kSortTile);
     size_t b = 0;
     b += 4 * sizeof(uint32_t) * (size_t)m;   // keys/vals ping-pong
-    b += sizeof(int) * 256 * nblk + 64;      // radix histogram
+    b += sizeof(int) * kMaxDigits * nblk + 256;  // radix histogram (digits up to 10 bits)
     b += sizeof(int) * (nblk + 1) + 64;      // segment block counts
-    b += sizeof(float) * 6 * 1024 + 64;      // bbox partials
+    b += kBboxBytes;                         // bbox partials and counters
     b += 4 * 64;                             // small scalars
     return b + 4096;
 }
@@ -573,13 +610,16 @@ size_t grid_scratch_bytes(int m) {
 int grid_bbox(const float4 *d_map, int m, float res, GridMeta *d_meta, void *scratch, cudaStream_t st) {
     char *p = (char *)scratch;
     float *part = (float *)p;
-    int *nonfinite = (int *)(p + sizeof(float) * 6 * 1024);
+    int *flags = (int *)(p + kBboxFlagsOffset);  // zeroed by grid_scratch_init, left at zero
     int nblk = div_up(m, kThreads);
     if (nblk > 1024) nblk = 1024;
-    cudaMemsetAsync(nonfinite, 0, sizeof(int), st);
-    bbox_partial_kernel<<<nblk, kThreads, 0, st>>>(d_map, m, part, nonfinite);
-    bbox_final_kernel<<<1, kThreads, 0, st>>>(part, nblk, res, nonfinite, d_meta);
+    bbox_kernel<<<nblk, kThreads, 0, st>>>(d_map, m, part, flags, res, d_meta);
     return (int)cudaGetLastError();
+}
+
+int grid_scratch_init(void *scratch, cudaStream_t st) {
+    int *flags = (int *)((char *)scratch + kBboxFlagsOffset);
+    return (int)cudaMemsetAsync(flags, 0, 2 * sizeof(int), st);
 }
 
 int64_t window_count(const GridMeta &g) {
@@ -605,7 +645,7 @@ int grid_windows(const GridMeta &meta_host, const int32_t *index, const float4 *
 int grid_build(const float4 *d_map, int m, const GridMeta &meta_host, GridMeta *d_meta, const NdtGridOptions &opt,
                GridBuffers buf, void *scratch, cudaStream_t st, int *launches) {
     const int nblk = div_up(m, kSortTile);
-    char *p = (char *)scratch;
+    char *p = (char *)scratch + kBboxBytes;  // after the bounding-box region
     auto take = [&](size_t bytes) {
         char *r = p;
         p += (bytes + 255) & ~(size_t)255;
@@ -615,7 +655,7 @@ int grid_build(const float4 *d_map, int m, const GridMeta &meta_host, GridMeta *
     uint32_t *v0 = (uint32_t *)take(sizeof(uint32_t) * (size_t)m);
     uint32_t *k1 = (uint32_t *)take(sizeof(uint32_t) * (size_t)m);
     uint32_t *v1 = (uint32_t *)take(sizeof(uint32_t) * (size_t)m);
-    int *hist = (int *)take(sizeof(int) * 256 * (size_t)nblk);
+    int *hist = (int *)take(sizeof(int) * (size_t)kMaxDigits * (size_t)nblk);
     int *segc = (int *)take(sizeof(int) * (size_t)(nblk + 1));
     int *nseg = (int *)take(sizeof(int));
     int nl = 0;
@@ -623,11 +663,13 @@ int grid_build(const float4 *d_map, int m, const GridMeta &meta_host, GridMeta *
     cudaMemsetAsync(buf.index, 0xff, sizeof(int32_t) * (size_t)meta_host.G, st);
     cell_key_kernel<<<div_up(m, kThreads), kThreads, 0, st>>>(d_map, m, d_meta, k0, v0);
     ++nl;
-    // digit width: passes = ceil(bits / 8), width = ceil(bits / passes)
+    // digit width: passes = ceil(bits / 8), width = ceil(bits / passes).  (Wider
+    // digits save a pass but make the one-block histogram scan longer than the
+    // pass: 9-bit digits over 196 blocks were slower on a 400k-point map.)
     int bits = 1;
     while (bits < 31 && (1LL << bits) < meta_host.G) ++bits;
     int passes = (bits + 7) / 8;
-    int width = (bits + passes - 1) / passes;
+    int width = (bits + passes - 1) / passes;  // <= 8 <= log2(kMaxDigits)
     int shift = 0;
     for (int ps = 0; ps < passes; ++ps) {
         int w = width;
@@ -653,11 +695,10 @@ int grid_build(const float4 *d_map, int m, const GridMeta &meta_host, GridMeta *
     } else {
         cell_finalize_corrected_kernel<<<div_up(m, 128), 128, 0, st>>>(d_map, v0, buf.seg_start, buf.seg_cell,
                                                                        nseg, m, opt.min_points, opt.eigen_ratio,
-                                                                       buf);
+                                                                       d_meta, buf);
     }
-    store_occupied_kernel<<<1, 32, 0, st>>>(nseg, d_meta);
-    nl += 2;
-    if (launches) *launches += nl + 2;
+    nl += 1;
+    if (launches) *launches += nl;
     return (int)cudaGetLastError();
 }
 

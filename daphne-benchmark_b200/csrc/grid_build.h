@@ -49,6 +49,8 @@ int grid_windows(const GridMeta &meta_host, const int32_t *index, const float4 *
                  cudaStream_t st, int *launches);
 
 size_t grid_scratch_bytes(int m);
+// Zeroes the scratch's bounding-box counters (once, after the scratch is allocated).
+int grid_scratch_init(void *scratch, cudaStream_t st);
 
 // Phase 1: bounding box and dims into *d_meta (the caller reads it back to
 // size the dense index table).
