@@ -642,6 +642,59 @@ int grid_windows(const GridMeta &meta_host, const int32_t *index, const float4 *
     return (int)cudaGetLastError();
 }
 
+int sort_segments(SortBuffers &b, int n, int bits, int32_t *seg_start, uint32_t *seg_key, cudaStream_t st) {
+    const int nblk = div_up(n, kSortTile);
+    int nl = 0;
+    // digit width: passes = ceil(bits / 8), width = ceil(bits / passes).  (Wider
+    // digits save a pass but make the one-block histogram scan longer than the
+    // pass: 9-bit digits over 196 blocks were slower on a 400k-point map.)
+    int passes = (bits + 7) / 8;
+    int width = (bits + passes - 1) / passes;  // <= 8 <= log2(kMaxDigits)
+    int shift = 0;
+    for (int ps = 0; ps < passes; ++ps) {
+        int w = width;
+        if (shift + w > bits) w = bits - shift;
+        size_t smem_up = sizeof(int) << w;
+        size_t smem_dn = sizeof(int) * kWarps << w;
+        radix_upsweep_kernel<<<nblk, kThreads, smem_up, st>>>(b.k0, n, shift, w, b.hist);
+        scan_single_block_kernel<<<1, 1024, 0, st>>>(b.hist, nblk << w, nullptr);
+        radix_downsweep_kernel<<<nblk, kThreads, smem_dn, st>>>(b.k0, b.v0, b.k1, b.v1, n, shift, w, b.hist);
+        nl += 3;
+        uint32_t *t = b.k0; b.k0 = b.k1; b.k1 = t;
+        t = b.v0; b.v0 = b.v1; b.v1 = t;
+        shift += w;
+    }
+    seg_count_kernel<<<nblk, kThreads, 0, st>>>(b.k0, n, b.segc);
+    scan_single_block_kernel<<<1, 1024, 0, st>>>(b.segc, nblk, b.nseg);
+    seg_write_kernel<<<nblk, kThreads, 0, st>>>(b.k0, n, b.segc, seg_start, seg_key);
+    nl += 3;
+    return nl;
+}
+
+size_t sort_scratch_bytes(int n) {
+    const size_t nblk = (size_t)div_up(n, kSortTile);
+    return 4 * sizeof(uint32_t) * (size_t)n + sizeof(int) * kMaxDigits * nblk + sizeof(int) * (nblk + 1) + 8 * 256;
+}
+
+SortBuffers sort_buffers(void *scratch, int n) {
+    const size_t nblk = (size_t)div_up(n, kSortTile);
+    char *p = (char *)scratch;
+    auto take = [&](size_t bytes) {
+        char *r = p;
+        p += (bytes + 255) & ~(size_t)255;
+        return (void *)r;
+    };
+    SortBuffers b;
+    b.k0 = (uint32_t *)take(sizeof(uint32_t) * (size_t)n);
+    b.v0 = (uint32_t *)take(sizeof(uint32_t) * (size_t)n);
+    b.k1 = (uint32_t *)take(sizeof(uint32_t) * (size_t)n);
+    b.v1 = (uint32_t *)take(sizeof(uint32_t) * (size_t)n);
+    b.hist = (int *)take(sizeof(int) * (size_t)kMaxDigits * nblk);
+    b.segc = (int *)take(sizeof(int) * (nblk + 1));
+    b.nseg = (int *)take(sizeof(int));
+    return b;
+}
+
 int grid_build(const float4 *d_map, int m, const GridMeta &meta_host, GridMeta *d_meta, const NdtGridOptions &opt,
                GridBuffers buf, void *scratch, cudaStream_t st, int *launches) {
     const int nblk = div_up(m, kSortTile);
@@ -663,31 +716,11 @@ int grid_build(const float4 *d_map, int m, const GridMeta &meta_host, GridMeta *
     cudaMemsetAsync(buf.index, 0xff, sizeof(int32_t) * (size_t)meta_host.G, st);
     cell_key_kernel<<<div_up(m, kThreads), kThreads, 0, st>>>(d_map, m, d_meta, k0, v0);
     ++nl;
-    // digit width: passes = ceil(bits / 8), width = ceil(bits / passes).  (Wider
-    // digits save a pass but make the one-block histogram scan longer than the
-    // pass: 9-bit digits over 196 blocks were slower on a 400k-point map.)
     int bits = 1;
     while (bits < 31 && (1LL << bits) < meta_host.G) ++bits;
-    int passes = (bits + 7) / 8;
-    int width = (bits + passes - 1) / passes;  // <= 8 <= log2(kMaxDigits)
-    int shift = 0;
-    for (int ps = 0; ps < passes; ++ps) {
-        int w = width;
-        if (shift + w > bits) w = bits - shift;
-        size_t smem_up = sizeof(int) << w;
-        size_t smem_dn = sizeof(int) * kWarps << w;
-        radix_upsweep_kernel<<<nblk, kThreads, smem_up, st>>>(k0, m, shift, w, hist);
-        scan_single_block_kernel<<<1, 1024, 0, st>>>(hist, nblk << w, nullptr);
-        radix_downsweep_kernel<<<nblk, kThreads, smem_dn, st>>>(k0, v0, k1, v1, m, shift, w, hist);
-        nl += 3;
-        uint32_t *t = k0; k0 = k1; k1 = t;
-        t = v0; v0 = v1; v1 = t;
-        shift += w;
-    }
-    seg_count_kernel<<<nblk, kThreads, 0, st>>>(k0, m, segc);
-    scan_single_block_kernel<<<1, 1024, 0, st>>>(segc, nblk, nseg);
-    seg_write_kernel<<<nblk, kThreads, 0, st>>>(k0, m, segc, buf.seg_start, buf.seg_cell);
-    nl += 3;
+    SortBuffers sb{k0, v0, k1, v1, hist, segc, nseg};
+    nl += sort_segments(sb, m, bits, buf.seg_start, buf.seg_cell, st);
+    v0 = sb.v0;
     // at most m segments: launch for m, kernels read the true count
     if (opt.compat) {
         cell_finalize_compat_kernel<<<div_up(m, 128), 128, 0, st>>>(d_map, v0, buf.seg_start, buf.seg_cell, nseg,

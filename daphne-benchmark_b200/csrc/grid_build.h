@@ -48,6 +48,19 @@ int64_t window_count(const GridMeta &g);  // W = (dim_x + 2)(dim_y + 2)(dim_z + 
 int grid_windows(const GridMeta &meta_host, const int32_t *index, const float4 *mean_hi, WindowBuffers wb,
                  cudaStream_t st, int *launches);
 
+// Stable LSD radix sort of n (key, value) pairs on the low `bits` key bits,
+// then the segments of equal keys: seg_start[s] = first sorted position of
+// segment s, seg_key[s] = its key, *b.nseg = segment count (device).  After
+// the call b.k0 / b.v0 hold the sorted keys and values.  Returns the number of
+// kernel launches.
+struct SortBuffers {
+    uint32_t *k0, *v0, *k1, *v1;
+    int *hist, *segc, *nseg;
+};
+size_t sort_scratch_bytes(int n);
+SortBuffers sort_buffers(void *scratch, int n);
+int sort_segments(SortBuffers &b, int n, int bits, int32_t *seg_start, uint32_t *seg_key, cudaStream_t st);
+
 size_t grid_scratch_bytes(int m);
 // Zeroes the scratch's bounding-box counters (once, after the scratch is allocated).
 int grid_scratch_init(void *scratch, cudaStream_t st);

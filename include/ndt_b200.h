@@ -301,6 +301,29 @@ NDT_API int ndt_mlp_judge_device(ndt_mlp *mlp, int B, const float *d_prop16, con
                                  const double *d_score_prop, const double *d_score_guess, float *d_start16,
                                  int *d_used);
 
+/*
+ * Scan pre-filter (no counterpart in the reference kernel: it is the
+ * voxel-grid downsampling that produces the "filtered scan" inputs of the
+ * align call upstream).  For each of B scans (d_points: float4 x, y, z,
+ * intensity; d_offsets: B + 1 prefix offsets, d_offsets[B] = total_points)
+ * the points with finite x, y, z fall into leaves (floor(x * r),
+ * floor(y * r), floor(z * r)), r = 1 / leaf and each product rounded to float; every
+ * occupied leaf yields one point, the mean of its points (all four
+ * components, summed in double precision in input order, rounded to float).
+ * A scan's output points are ordered by leaf, x fastest, then y, then z.
+ * d_out: room for total_points float4; d_out_offsets: B + 1 output offsets;
+ * *out_total (host) = number of output points.  NDT_E_CAPACITY when a scan
+ * spans 2^31 leaves or more, or the batch 2^31 - 1 leaves or more.  The call
+ * blocks until the result is ready (it reads the key range back once).
+ */
+typedef struct ndt_filter ndt_filter;
+NDT_API int ndt_filter_create(int device, ndt_filter **out);
+NDT_API void ndt_filter_destroy(ndt_filter *f);
+NDT_API const char *ndt_filter_last_error(const ndt_filter *f);
+NDT_API void *ndt_filter_stream(ndt_filter *f);
+NDT_API int ndt_voxel_filter_device(ndt_filter *f, int B, const float *d_points, const int *d_offsets,
+                                    int total_points, float leaf, float *d_out, int *d_out_offsets, int *out_total);
+
 #ifdef __cplusplus
 }
 #endif
