@@ -166,21 +166,22 @@ __global__ void radix_upsweep_kernel(const uint32_t *__restrict__ keys, int n, i
     for (int d = threadIdx.x; d < nb; d += blockDim.x) hist[d * gridDim.x + blockIdx.x] = s_hist[d];
 }
 
-// Exclusive scan of n ints in place with one block of 1024 threads; *total
-// (optional) receives the sum.  Tiles of 8192 ints are staged in shared
-// memory with coalesced loads and stores; each thread scans 8 consecutive
-// values (two 16-byte shared loads), the block scans the thread sums, and a
-// carry links the tiles.
-__global__ void __launch_bounds__(1024) scan_single_block_kernel(int *__restrict__ data, int n,
-                                                                 int *__restrict__ total) {
-    constexpr int kT = 1024, kI = 8, kTileN = kT * kI;
+// Exclusive scan of data[begin, end) in place by one block of 1024 threads,
+// starting from `carry`; returns the running total (carry + sum) in every
+// thread.  Tiles of 8192 ints are staged in shared memory with coalesced
+// loads and stores; each thread scans 8 consecutive values (two 16-byte
+// shared loads), the block scans the thread sums, and a carry links the tiles.
+constexpr int kScanThreads = 1024, kScanItems = 8, kScanTile = kScanThreads * kScanItems;
+
+__device__ int block_scan_range(int *__restrict__ data, int begin, int end, int carry_in) {
+    constexpr int kT = kScanThreads, kI = kScanItems, kTileN = kScanTile;
     __shared__ __align__(16) int s_data[kTileN];
     __shared__ int s_warp[32];
     __shared__ int s_carry;
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-    if (t == 0) s_carry = 0;
-    for (int base = 0; base < n; base += kTileN) {
-        for (int i = t; i < kTileN; i += kT) s_data[i] = base + i < n ? data[base + i] : 0;
+    if (t == 0) s_carry = carry_in;
+    for (int base = begin; base < end; base += kTileN) {
+        for (int i = t; i < kTileN; i += kT) s_data[i] = base + i < end ? data[base + i] : 0;
         __syncthreads();
         const int4 a = reinterpret_cast<const int4 *>(s_data)[2 * t];
         const int4 b = reinterpret_cast<const int4 *>(s_data)[2 * t + 1];
@@ -220,11 +221,65 @@ __global__ void __launch_bounds__(1024) scan_single_block_kernel(int *__restrict
         reinterpret_cast<int4 *>(s_data)[2 * t + 1] = make_int4(o[4], o[5], o[6], o[7]);
         __syncthreads();
         for (int i = t; i < kTileN; i += kT)
-            if (base + i < n) data[base + i] = s_data[i];
+            if (base + i < end) data[base + i] = s_data[i];
         __syncthreads();
     }
-    if (total && t == 0) *total = s_carry;
+    return s_carry;
 }
+
+// Exclusive scan of n ints in place with one block; *total (optional)
+// receives the sum.
+__global__ void __launch_bounds__(kScanThreads) scan_single_block_kernel(int *__restrict__ data, int n,
+                                                                         int *__restrict__ total) {
+    const int run = block_scan_range(data, 0, n, 0);
+    if (total && threadIdx.x == 0) *total = run;
+}
+
+// Multi-block form for long arrays: part[b] = sum of tile b (8192 ints) ...
+__global__ void __launch_bounds__(kScanThreads) scan_tile_sum_kernel(const int *__restrict__ data, int n,
+                                                                     int *__restrict__ part) {
+    __shared__ int s_warp[32];
+    const int base = blockIdx.x * kScanTile;
+    int sum = 0;
+    for (int i = threadIdx.x; i < kScanTile; i += kScanThreads)
+        if (base + i < n) sum += data[base + i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = sum;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        sum = s_warp[threadIdx.x];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        if (threadIdx.x == 0) part[blockIdx.x] = sum;
+    }
+}
+
+// ... then, after part is scanned, tile b scans itself from carry part[b].
+__global__ void __launch_bounds__(kScanThreads) scan_tile_kernel(int *__restrict__ data, int n,
+                                                                 const int *__restrict__ part) {
+    const int base = blockIdx.x * kScanTile;
+    const int end = base + kScanTile < n ? base + kScanTile : n;
+    block_scan_range(data, base, end, part[blockIdx.x]);
+}
+
+// Arrays of at most this many ints are scanned by one block (one launch);
+// longer ones by tiles (three launches, part holds one int per tile).
+constexpr int kSingleScanMax = 8 * kScanTile;
+
+int scan_exclusive(int *data, int n, int *total, int *part, cudaStream_t st) {
+    if (n <= kSingleScanMax) {
+        scan_single_block_kernel<<<1, kScanThreads, 0, st>>>(data, n, total);
+        return 1;
+    }
+    const int tiles = (n + kScanTile - 1) / kScanTile;
+    scan_tile_sum_kernel<<<tiles, kScanThreads, 0, st>>>(data, n, part);
+    scan_single_block_kernel<<<1, kScanThreads, 0, st>>>(part, tiles, total);
+    scan_tile_kernel<<<tiles, kScanThreads, 0, st>>>(data, n, part);
+    return 3;
+}
+
+size_t scan_part_ints(size_t n) { return (n + kScanTile - 1) / kScanTile + 1; }
 
 // Stable scatter: warp w of a block owns items [base + w*256, base + w*256 + 256)
 // in 8 chunks of 32 consecutive items; ranks inside a chunk come from
@@ -597,14 +652,7 @@ inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
 
 // ---------------------------------------------------------------------------
 size_t grid_scratch_bytes(int m) {
-    size_t nblk = (size_t)div_up(m, kSortTile);
-    size_t b = 0;
-    b += 4 * sizeof(uint32_t) * (size_t)m;   // keys/vals ping-pong
-    b += sizeof(int) * kMaxDigits * nblk + 256;  // radix histogram (digits up to 10 bits)
-    b += sizeof(int) * (nblk + 1) + 64;      // segment block counts
-    b += kBboxBytes;                         // bbox partials and counters
-    b += 4 * 64;                             // small scalars
-    return b + 4096;
+    return kBboxBytes + sort_scratch_bytes(m) + 4096;  // bbox partials and counters, sort buffers
 }
 
 int grid_bbox(const float4 *d_map, int m, float res, GridMeta *d_meta, void *scratch, cudaStream_t st) {
@@ -657,23 +705,24 @@ int sort_segments(SortBuffers &b, int n, int bits, int32_t *seg_start, uint32_t 
         size_t smem_up = sizeof(int) << w;
         size_t smem_dn = sizeof(int) * kWarps << w;
         radix_upsweep_kernel<<<nblk, kThreads, smem_up, st>>>(b.k0, n, shift, w, b.hist);
-        scan_single_block_kernel<<<1, 1024, 0, st>>>(b.hist, nblk << w, nullptr);
+        nl += scan_exclusive(b.hist, nblk << w, nullptr, b.part, st);
         radix_downsweep_kernel<<<nblk, kThreads, smem_dn, st>>>(b.k0, b.v0, b.k1, b.v1, n, shift, w, b.hist);
-        nl += 3;
+        nl += 2;
         uint32_t *t = b.k0; b.k0 = b.k1; b.k1 = t;
         t = b.v0; b.v0 = b.v1; b.v1 = t;
         shift += w;
     }
     seg_count_kernel<<<nblk, kThreads, 0, st>>>(b.k0, n, b.segc);
-    scan_single_block_kernel<<<1, 1024, 0, st>>>(b.segc, nblk, b.nseg);
+    nl += scan_exclusive(b.segc, nblk, b.nseg, b.part, st);
     seg_write_kernel<<<nblk, kThreads, 0, st>>>(b.k0, n, b.segc, seg_start, seg_key);
-    nl += 3;
+    nl += 2;
     return nl;
 }
 
 size_t sort_scratch_bytes(int n) {
     const size_t nblk = (size_t)div_up(n, kSortTile);
-    return 4 * sizeof(uint32_t) * (size_t)n + sizeof(int) * kMaxDigits * nblk + sizeof(int) * (nblk + 1) + 8 * 256;
+    return 4 * sizeof(uint32_t) * (size_t)n + sizeof(int) * kMaxDigits * nblk + sizeof(int) * (nblk + 1) +
+           sizeof(int) * scan_part_ints((size_t)kMaxDigits * nblk) + 8 * 256;
 }
 
 SortBuffers sort_buffers(void *scratch, int n) {
@@ -692,35 +741,23 @@ SortBuffers sort_buffers(void *scratch, int n) {
     b.hist = (int *)take(sizeof(int) * (size_t)kMaxDigits * nblk);
     b.segc = (int *)take(sizeof(int) * (nblk + 1));
     b.nseg = (int *)take(sizeof(int));
+    b.part = (int *)take(sizeof(int) * scan_part_ints((size_t)kMaxDigits * nblk));
     return b;
 }
 
 int grid_build(const float4 *d_map, int m, const GridMeta &meta_host, GridMeta *d_meta, const NdtGridOptions &opt,
                GridBuffers buf, void *scratch, cudaStream_t st, int *launches) {
-    const int nblk = div_up(m, kSortTile);
-    char *p = (char *)scratch + kBboxBytes;  // after the bounding-box region
-    auto take = [&](size_t bytes) {
-        char *r = p;
-        p += (bytes + 255) & ~(size_t)255;
-        return (void *)r;
-    };
-    uint32_t *k0 = (uint32_t *)take(sizeof(uint32_t) * (size_t)m);
-    uint32_t *v0 = (uint32_t *)take(sizeof(uint32_t) * (size_t)m);
-    uint32_t *k1 = (uint32_t *)take(sizeof(uint32_t) * (size_t)m);
-    uint32_t *v1 = (uint32_t *)take(sizeof(uint32_t) * (size_t)m);
-    int *hist = (int *)take(sizeof(int) * (size_t)kMaxDigits * (size_t)nblk);
-    int *segc = (int *)take(sizeof(int) * (size_t)(nblk + 1));
-    int *nseg = (int *)take(sizeof(int));
+    SortBuffers sb = sort_buffers((char *)scratch + kBboxBytes, m);  // after the bounding-box region
     int nl = 0;
 
     cudaMemsetAsync(buf.index, 0xff, sizeof(int32_t) * (size_t)meta_host.G, st);
-    cell_key_kernel<<<div_up(m, kThreads), kThreads, 0, st>>>(d_map, m, d_meta, k0, v0);
+    cell_key_kernel<<<div_up(m, kThreads), kThreads, 0, st>>>(d_map, m, d_meta, sb.k0, sb.v0);
     ++nl;
     int bits = 1;
     while (bits < 31 && (1LL << bits) < meta_host.G) ++bits;
-    SortBuffers sb{k0, v0, k1, v1, hist, segc, nseg};
     nl += sort_segments(sb, m, bits, buf.seg_start, buf.seg_cell, st);
-    v0 = sb.v0;
+    const uint32_t *v0 = sb.v0;
+    const int *nseg = sb.nseg;
     // at most m segments: launch for m, kernels read the true count
     if (opt.compat) {
         cell_finalize_compat_kernel<<<div_up(m, 128), 128, 0, st>>>(d_map, v0, buf.seg_start, buf.seg_cell, nseg,

@@ -55,7 +55,7 @@ int grid_windows(const GridMeta &meta_host, const int32_t *index, const float4 *
 // kernel launches.
 struct SortBuffers {
     uint32_t *k0, *v0, *k1, *v1;
-    int *hist, *segc, *nseg;
+    int *hist, *segc, *nseg, *part;
 };
 size_t sort_scratch_bytes(int n);
 SortBuffers sort_buffers(void *scratch, int n);

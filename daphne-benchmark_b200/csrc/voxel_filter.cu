@@ -51,98 +51,221 @@ struct ScanGeom {
     long long d[3];   // leaf extent per axis
 };
 
-// Leaf bounding box and key range of scan b (one block per scan).  range[b]
-// = dx * dy * dz (0 for a scan without finite points); err |= 1 when a range
-// exceeds 2^31.
-__global__ void scan_box_kernel(const float4 *__restrict__ pts, const int *__restrict__ offsets, float r,
-                                ScanGeom *__restrict__ geom, int *__restrict__ range, int *__restrict__ err) {
-    const int b = blockIdx.x;
-    const int s = offsets[b], e = offsets[b + 1];
-    long long mn[3] = {LLONG_MAX, LLONG_MAX, LLONG_MAX}, mx[3] = {LLONG_MIN, LLONG_MIN, LLONG_MIN};
-    for (int i = s + threadIdx.x; i < e; i += blockDim.x) {
-        const float4 p = pts[i];
-        if (!finite3(p)) continue;
-        const long long q[3] = {leaf_of(p.x, r), leaf_of(p.y, r), leaf_of(p.z, r)};
-        for (int k = 0; k < 3; ++k) {
-            mn[k] = q[k] < mn[k] ? q[k] : mn[k];
-            mx[k] = q[k] > mx[k] ? q[k] : mx[k];
-        }
+// Scan of point (or key) i: the last b in [0, B) with first[b] <= i, for a
+// non-decreasing first[] (point offsets, or key bases: with empty scans the
+// search lands on the scan that owns i).
+__device__ __forceinline__ int owner(const int *__restrict__ first, int B, int i) {
+    int lo = 0, hi = B;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(first + mid) <= i) lo = mid; else hi = mid;
     }
-    __shared__ long long s_mn[3][kThreads], s_mx[3][kThreads];
+    return lo;
+}
+
+constexpr int kBoxWarpPoints = 1024;  // points per warp in the box pass
+
+// Leaf bounding boxes: box[6 b .. 6 b + 5] = min x, y, z, max x, y, z leaf
+// index of scan b's finite points, by 64-bit atomics (order-independent).
+// Each warp walks kBoxWarpPoints consecutive points 32 at a time and keeps a
+// per-lane box while the points stay in one scan; a step that crosses a scan
+// boundary flushes it and settles its points one by one.
+__device__ __forceinline__ void box_flush(long long *__restrict__ box, int b, long long (&mn)[3],
+                                          long long (&mx)[3]) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const long long a = __shfl_xor_sync(0xffffffffu, mn[k], o);
+            const long long c = __shfl_xor_sync(0xffffffffu, mx[k], o);
+            mn[k] = a < mn[k] ? a : mn[k];
+            mx[k] = c > mx[k] ? c : mx[k];
+        }
+    if ((threadIdx.x & 31) == 0 && mn[0] <= mx[0])
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            atomicMin(box + 6 * b + k, mn[k]);
+            atomicMax(box + 6 * b + 3 + k, mx[k]);
+        }
+#pragma unroll
     for (int k = 0; k < 3; ++k) {
-        s_mn[k][threadIdx.x] = mn[k];
-        s_mx[k][threadIdx.x] = mx[k];
+        mn[k] = LLONG_MAX;
+        mx[k] = LLONG_MIN;
     }
+}
+
+__global__ void box_kernel(const float4 *__restrict__ pts, const int *__restrict__ offsets, int B, int n, float r,
+                           long long *__restrict__ box) {
+    const int lane = threadIdx.x & 31;
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long w0l = gw * kBoxWarpPoints;
+    if (w0l >= n) return;
+    const int w0 = (int)w0l, w1 = n - w0 < kBoxWarpPoints ? n : w0 + kBoxWarpPoints;
+    int cur = owner(offsets, B, w0);
+    int hi = __ldg(offsets + cur + 1);
+    long long mn[3] = {LLONG_MAX, LLONG_MAX, LLONG_MAX}, mx[3] = {LLONG_MIN, LLONG_MIN, LLONG_MIN};
+    for (int base = w0; base < w1; base += 32) {
+        const int i = base + lane;
+        const int last = base + 31 < w1 ? base + 31 : w1 - 1;
+        float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+        bool ok = i < w1;
+        if (ok) {
+            p = pts[i];
+            ok = finite3(p);
+        }
+        long long q[3] = {0, 0, 0};
+        if (ok) {
+            q[0] = leaf_of(p.x, r);
+            q[1] = leaf_of(p.y, r);
+            q[2] = leaf_of(p.z, r);
+        }
+        if (last < hi) {  // warp-uniform: the whole step lies in scan cur
+            if (ok)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    mn[k] = q[k] < mn[k] ? q[k] : mn[k];
+                    mx[k] = q[k] > mx[k] ? q[k] : mx[k];
+                }
+        } else {
+            box_flush(box, cur, mn, mx);
+            if (ok) {
+                const int b = owner(offsets, B, i);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    atomicMin(box + 6 * b + k, q[k]);
+                    atomicMax(box + 6 * b + 3 + k, q[k]);
+                }
+            }
+            if (base + 32 < w1) {
+                cur = owner(offsets, B, base + 32);
+                hi = __ldg(offsets + cur + 1);
+            }
+        }
+    }
+    box_flush(box, cur, mn, mx);
+}
+
+__global__ void box_init_kernel(long long *__restrict__ box, int B) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 6 * B; i += gridDim.x * blockDim.x)
+        box[i] = (i % 6) < 3 ? LLONG_MAX : LLONG_MIN;
+}
+
+// One block: per scan its geometry and key range (dx * dy * dz, 0 without
+// finite points), the exclusive scan of the ranges into key bases
+// (base[B] = total), and the box reset for the next call.  flags[0] |= 1 when
+// a scan spans 2^31 leaves or more, |= 2 when the batch spans 2^31 - 1 or
+// more; flags[1] = total.
+constexpr int kRangeThreads = 1024;
+
+__global__ void __launch_bounds__(kRangeThreads) range_kernel(long long *__restrict__ box, int B,
+                                                              ScanGeom *__restrict__ geom, int *__restrict__ base,
+                                                              int *__restrict__ flags) {
+    __shared__ long long s_sum[kRangeThreads];
+    const int t = threadIdx.x;
+    const int per = (B + kRangeThreads - 1) / kRangeThreads;
+    const int b0 = t * per, b1 = b0 + per < B ? b0 + per : B;
+    long long local = 0;
+    int err = 0;
+    for (int b = b0; b < b1; ++b) {
+        ScanGeom g;
+        long long span = 0;
+        const long long *bx = box + 6 * b;
+        if (bx[0] <= bx[3]) {
+            span = 1;
+            for (int k = 0; k < 3; ++k) {
+                g.lo[k] = bx[k];
+                g.d[k] = bx[3 + k] - bx[k] + 1;
+                span = (span > (1LL << 31) / g.d[k]) ? (1LL << 32) : span * g.d[k];
+            }
+        } else {
+            for (int k = 0; k < 3; ++k) {
+                g.lo[k] = 0;
+                g.d[k] = 1;
+            }
+        }
+        if (span >= (1LL << 31)) {
+            err |= 1;
+            span = 0;
+        }
+        geom[b] = g;
+        base[b] = (int)span;  // the range for now; the scan below makes it a base
+        local += span;
+        for (int k = 0; k < 6; ++k) box[6 * b + k] = k < 3 ? LLONG_MAX : LLONG_MIN;
+    }
+    s_sum[t] = local;
     __syncthreads();
-    if (threadIdx.x != 0) return;
-    for (int t = 1; t < (int)blockDim.x; ++t)
-        for (int k = 0; k < 3; ++k) {
-            mn[k] = s_mn[k][t] < mn[k] ? s_mn[k][t] : mn[k];
-            mx[k] = s_mx[k][t] > mx[k] ? s_mx[k][t] : mx[k];
-        }
-    ScanGeom g;
-    long long span = 0;
-    if (mn[0] <= mx[0]) {
-        span = 1;
-        for (int k = 0; k < 3; ++k) {
-            g.lo[k] = mn[k];
-            g.d[k] = mx[k] - mn[k] + 1;
-            span = (span > (1LL << 31) / g.d[k]) ? (1LL << 32) : span * g.d[k];
-        }
-    } else {
-        for (int k = 0; k < 3; ++k) {
-            g.lo[k] = 0;
-            g.d[k] = 1;
-        }
+    for (int o = 1; o < kRangeThreads; o <<= 1) {  // inclusive Hillis-Steele scan
+        const long long v = t >= o ? s_sum[t - o] : 0;
+        __syncthreads();
+        s_sum[t] += v;
+        __syncthreads();
     }
-    if (span >= (1LL << 31)) {
-        atomicOr(err, 1);
-        span = 0;
+    long long run = s_sum[t] - local;
+    const long long total = s_sum[kRangeThreads - 1];
+    const long long cap = 0x7fffffffLL;
+    for (int b = b0; b < b1; ++b) {
+        const int span = base[b];
+        base[b] = (int)(run < cap ? run : cap);
+        run += span;
     }
-    geom[b] = g;
-    range[b] = (int)span;
+    if (err) atomicOr(flags, 1);
+    if (t == 0) {
+        if (total >= cap) atomicOr(flags, 2);
+        base[B] = (int)(total < cap ? total : cap);
+        flags[1] = (int)(total < cap ? total : cap);
+    }
 }
 
 // key = base[scan] + local leaf key (x fastest); non-finite points get the
 // key of the batch's end (sorted last, dropped); val = point index.
 __global__ void key_kernel(const float4 *__restrict__ pts, const int *__restrict__ offsets, int B, float r,
                            const ScanGeom *__restrict__ geom, const int *__restrict__ base, int total_keys, int n,
-                           uint32_t *__restrict__ keys, uint32_t *__restrict__ vals, int *__restrict__ scan_of) {
+                           uint32_t *__restrict__ keys, uint32_t *__restrict__ vals) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    // scan of point i: binary search in offsets
-    int lo = 0, hi = B;
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (offsets[mid] <= i) lo = mid; else hi = mid;
-    }
     const float4 p = pts[i];
     uint32_t k = (uint32_t)total_keys;
     if (finite3(p)) {
-        const ScanGeom &g = geom[lo];
+        const int b = owner(offsets, B, i);
+        const ScanGeom &g = geom[b];
         const long long qx = leaf_of(p.x, r) - g.lo[0], qy = leaf_of(p.y, r) - g.lo[1], qz = leaf_of(p.z, r) - g.lo[2];
-        k = (uint32_t)(base[lo] + (int)(qx + g.d[0] * (qy + g.d[1] * qz)));
+        k = (uint32_t)(base[b] + (int)(qx + g.d[0] * (qy + g.d[1] * qz)));
     }
     keys[i] = k;
     vals[i] = (uint32_t)i;
-    scan_of[i] = lo;
 }
 
 // One thread per segment: the FP64 mean of its points in input order (the
 // stable sort keeps that order within a segment), written to out[s], and one
 // count for its scan.  Segments are in key order (scan, then leaf) and the
 // segment of dropped points, if any, is the last, so s is the output index.
+// Points are loaded four at a time ahead of the (sequential) sums.
 __global__ void mean_kernel(const float4 *__restrict__ pts, const uint32_t *__restrict__ order,
                             const int32_t *__restrict__ seg_start, const uint32_t *__restrict__ seg_key,
-                            const int *__restrict__ nseg, int n, uint32_t drop_key, const int *__restrict__ scan_of,
-                            float4 *__restrict__ out, int *__restrict__ count) {
+                            const int *__restrict__ nseg, int n, uint32_t drop_key, const int *__restrict__ base,
+                            int B, float4 *__restrict__ out, int *__restrict__ count) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     const int K = *nseg;
-    if (s >= K || seg_key[s] == drop_key) return;
+    if (s >= K) return;
+    const uint32_t key = seg_key[s];
+    if (key == drop_key) return;
     const int a = seg_start[s], e = s + 1 < K ? seg_start[s + 1] : n;
     double sx = 0, sy = 0, sz = 0, sw = 0;
-    for (int j = a; j < e; ++j) {
-        const float4 p = pts[order[j]];
+    int j = a;
+    for (; j + 4 <= e; j += 4) {
+        float4 p[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) p[u] = pts[__ldg(order + j + u)];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            sx += (double)p[u].x;
+            sy += (double)p[u].y;
+            sz += (double)p[u].z;
+            sw += (double)p[u].w;
+        }
+    }
+    for (; j < e; ++j) {
+        const float4 p = pts[__ldg(order + j)];
         sx += (double)p.x;
         sy += (double)p.y;
         sz += (double)p.z;
@@ -150,24 +273,34 @@ __global__ void mean_kernel(const float4 *__restrict__ pts, const uint32_t *__re
     }
     const double c = (double)(e - a);
     out[s] = make_float4((float)(sx / c), (float)(sy / c), (float)(sz / c), (float)(sw / c));
-    atomicAdd(count + scan_of[order[a]], 1);
+    atomicAdd(count + owner(base, B, (int)key), 1);
 }
 
-// Exclusive scan of n ints in place (one thread; n is the scan count + 1);
-// *total = the sum, err |= 2 when it reaches 2^31 - 1.
-__global__ void scan_small_kernel(int *__restrict__ data, int n, int *__restrict__ total, int *__restrict__ err) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    long long run = 0;
-    for (int i = 0; i < n; ++i) {
-        const long long v = data[i];
-        data[i] = (int)(run < 0x7fffffffLL ? run : 0x7fffffffLL);
+// Exclusive scan of n ints in place by one block (n = the scan count + 1:
+// counts in, output offsets out); *total = the sum.
+__global__ void __launch_bounds__(kRangeThreads) offsets_kernel(int *__restrict__ data, int n,
+                                                                int *__restrict__ total) {
+    __shared__ int s_sum[kRangeThreads];
+    const int t = threadIdx.x;
+    const int per = (n + kRangeThreads - 1) / kRangeThreads;
+    const int i0 = t * per, i1 = i0 + per < n ? i0 + per : n;
+    int local = 0;
+    for (int i = i0; i < i1; ++i) local += data[i];
+    s_sum[t] = local;
+    __syncthreads();
+    for (int o = 1; o < kRangeThreads; o <<= 1) {
+        const int v = t >= o ? s_sum[t - o] : 0;
+        __syncthreads();
+        s_sum[t] += v;
+        __syncthreads();
+    }
+    int run = s_sum[t] - local;
+    for (int i = i0; i < i1; ++i) {
+        const int v = data[i];
+        data[i] = run;
         run += v;
     }
-    if (run >= 0x7fffffffLL) {
-        if (err) atomicOr(err, 2);
-        run = 0x7fffffffLL;
-    }
-    if (total) *total = (int)run;
+    if (t == kRangeThreads - 1) *total = s_sum[t];
 }
 
 }  // namespace vf
@@ -196,7 +329,9 @@ struct Buf {
 struct ndt_filter {
     int device = 0;
     cudaStream_t stream = nullptr;
-    Buf geom, range, err, keys_scratch, scan_of, seg_start, seg_key, total;
+    Buf geom, base, flags, box, sort_scratch, seg_start, seg_key;
+    int box_cap = 0;
+    int *h_flags = nullptr;  // pinned: error flags, key total, output total
     std::string msg;
 };
 
@@ -209,8 +344,9 @@ int ndt_filter_create(int device, ndt_filter **out) {
     f->device = device;
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&f->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&f->h_flags, sizeof(int) * 4);
     if (e != cudaSuccess) {
-        delete f;
+        ndt_filter_destroy(f);
         return NDT_E_CUDA;
     }
     *out = f;
@@ -224,6 +360,7 @@ void ndt_filter_destroy(ndt_filter *f) {
         cudaStreamSynchronize(f->stream);
         cudaStreamDestroy(f->stream);
     }
+    if (f->h_flags) cudaFreeHost(f->h_flags);
     delete f;
 }
 
@@ -252,25 +389,33 @@ int ndt_voxel_filter_device(ndt_filter *f, int B, const float *d_points, const i
     const int n = total_points;
     const float r = 1.0f / leaf;
     FCK(f->geom.ensure(sizeof(vf::ScanGeom) * (size_t)B));
-    FCK(f->range.ensure(sizeof(int) * (size_t)(B + 1)));
-    FCK(f->err.ensure(sizeof(int) * 2));
-    FCK(cudaMemsetAsync(f->err.p, 0, sizeof(int) * 2, st));
-    int *range = (int *)f->range.p;
-    int *err = (int *)f->err.p;
-    vf::scan_box_kernel<<<B, vf::kThreads, 0, st>>>((const float4 *)d_points, d_offsets, r, (vf::ScanGeom *)f->geom.p,
-                                                    range, err);
+    FCK(f->base.ensure(sizeof(int) * (size_t)(B + 1)));
+    FCK(f->flags.ensure(sizeof(int) * 4));
+    if (f->box_cap < B) {  // the range pass resets the boxes it read; a fresh buffer is set once
+        FCK(f->box.ensure(sizeof(long long) * 6 * (size_t)B));
+        vf::box_init_kernel<<<(6 * B + 255) / 256, 256, 0, st>>>((long long *)f->box.p, B);
+        FCK(cudaGetLastError());
+        f->box_cap = B;
+    }
+    long long *box = (long long *)f->box.p;
+    int *base = (int *)f->base.p;
+    int *flags = (int *)f->flags.p;
+    FCK(cudaMemsetAsync(flags, 0, sizeof(int) * 4, st));
+    if (n > 0) {
+        const long long warps = ((long long)n + vf::kBoxWarpPoints - 1) / vf::kBoxWarpPoints;
+        vf::box_kernel<<<(unsigned)((warps * 32 + vf::kThreads - 1) / vf::kThreads), vf::kThreads, 0, st>>>(
+            (const float4 *)d_points, d_offsets, B, n, r, box);
+        FCK(cudaGetLastError());
+    }
+    vf::range_kernel<<<1, vf::kRangeThreads, 0, st>>>(box, B, (vf::ScanGeom *)f->geom.p, base, flags);
     FCK(cudaGetLastError());
-    FCK(cudaMemsetAsync(range + B, 0, sizeof(int), st));
-    vf::scan_small_kernel<<<1, 1, 0, st>>>(range, B + 1, err + 1, err);  // range -> base, total keys
-    FCK(cudaGetLastError());
-    int h[2] = {0, 0};
-    FCK(cudaMemcpyAsync(h, err, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));
+    FCK(cudaMemcpyAsync(f->h_flags, flags, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));
     FCK(cudaStreamSynchronize(st));
-    if (h[0]) {
-        f->msg = (h[0] & 1) ? "a scan spans 2^31 leaves or more" : "the batch spans 2^31 - 1 leaves or more";
+    if (f->h_flags[0]) {
+        f->msg = (f->h_flags[0] & 1) ? "a scan spans 2^31 leaves or more" : "the batch spans 2^31 - 1 leaves or more";
         return NDT_E_CAPACITY;
     }
-    const int total_keys = h[1];  // key total_keys marks the dropped points
+    const int total_keys = f->h_flags[1];  // key total_keys marks the dropped points
     if (n == 0) {
         FCK(cudaMemsetAsync(d_out_offsets, 0, sizeof(int) * (size_t)(B + 1), st));
         FCK(cudaStreamSynchronize(st));
@@ -279,27 +424,26 @@ int ndt_voxel_filter_device(ndt_filter *f, int B, const float *d_points, const i
     }
     int bits = 1;
     while (bits < 32 && (1LL << bits) <= (long long)total_keys) ++bits;
-    FCK(f->keys_scratch.ensure(ndt::sort_scratch_bytes(n)));
-    FCK(f->scan_of.ensure(sizeof(int) * (size_t)n));
+    FCK(f->sort_scratch.ensure(ndt::sort_scratch_bytes(n)));
     FCK(f->seg_start.ensure(sizeof(int32_t) * (size_t)n));
     FCK(f->seg_key.ensure(sizeof(uint32_t) * (size_t)n));
-    ndt::SortBuffers sb = ndt::sort_buffers(f->keys_scratch.p, n);
-    vf::key_kernel<<<(n + vf::kThreads - 1) / vf::kThreads, vf::kThreads, 0, st>>>(
-        (const float4 *)d_points, d_offsets, B, r, (const vf::ScanGeom *)f->geom.p, range, total_keys, n, sb.k0, sb.v0,
-        (int *)f->scan_of.p);
+    ndt::SortBuffers sb = ndt::sort_buffers(f->sort_scratch.p, n);
+    const unsigned pblk = (unsigned)((n + vf::kThreads - 1) / vf::kThreads);
+    vf::key_kernel<<<pblk, vf::kThreads, 0, st>>>((const float4 *)d_points, d_offsets, B, r,
+                                                  (const vf::ScanGeom *)f->geom.p, base, total_keys, n, sb.k0, sb.v0);
     FCK(cudaGetLastError());
     ndt::sort_segments(sb, n, bits, (int32_t *)f->seg_start.p, (uint32_t *)f->seg_key.p, st);
     FCK(cudaGetLastError());
     FCK(cudaMemsetAsync(d_out_offsets, 0, sizeof(int) * (size_t)(B + 1), st));
-    vf::mean_kernel<<<(n + vf::kThreads - 1) / vf::kThreads, vf::kThreads, 0, st>>>(
-        (const float4 *)d_points, sb.v0, (const int32_t *)f->seg_start.p, (const uint32_t *)f->seg_key.p, sb.nseg, n,
-        (uint32_t)total_keys, (const int *)f->scan_of.p, (float4 *)d_out, d_out_offsets);
+    vf::mean_kernel<<<pblk, vf::kThreads, 0, st>>>((const float4 *)d_points, sb.v0, (const int32_t *)f->seg_start.p,
+                                                   (const uint32_t *)f->seg_key.p, sb.nseg, n, (uint32_t)total_keys,
+                                                   base, B, (float4 *)d_out, d_out_offsets);
     FCK(cudaGetLastError());
-    FCK(f->total.ensure(sizeof(int)));
-    vf::scan_small_kernel<<<1, 1, 0, st>>>(d_out_offsets, B + 1, (int *)f->total.p, nullptr);
+    vf::offsets_kernel<<<1, vf::kRangeThreads, 0, st>>>(d_out_offsets, B + 1, flags + 2);
     FCK(cudaGetLastError());
-    FCK(cudaMemcpyAsync(out_total, f->total.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    FCK(cudaMemcpyAsync(f->h_flags + 2, flags + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
     FCK(cudaStreamSynchronize(st));
+    *out_total = f->h_flags[2];
     return NDT_OK;
 }
 

@@ -206,6 +206,24 @@ def make_alignment(cfg: Config, scene: Scene, index: int, n_points: int | None =
     return Alignment(scan=scan, guess=guess.astype(np.float32).reshape(16), truth=truth)
 
 
+def make_raw_scan(cfg: Config, scene: Scene, index: int, n_points: int, radius: float = 60.0,
+                  sigma: float = 0.02) -> np.ndarray:
+    """An unfiltered scan of alignment `index`'s sensor pose: n_points surface
+    samples within `radius` in the sensor frame, in sweep order (by azimuth),
+    intensity uniform in [0, 255) -- the input of the voxel-grid pre-filter."""
+    rng = np.random.default_rng([cfg.seed, 3, index])
+    W = cfg.area
+    sx, sy = (rng.random(2) - 0.5) * (W / 2.0)
+    world = _scan_world(rng, scene, sx, sy, n_points, radius, sigma)
+    px, py = world[:, 0] - sx, world[:, 1] - sy
+    scan = np.empty((n_points, 4), dtype=np.float32)
+    scan[:, 0] = px.astype(np.float32)
+    scan[:, 1] = py.astype(np.float32)
+    scan[:, 2] = world[:, 2].astype(np.float32)
+    scan[:, 3] = (rng.random(n_points) * 255.0).astype(np.float32)
+    return scan[np.argsort(np.arctan2(py, px), kind="stable")]
+
+
 def leaf_order(scan, leaf=2.0):
     """Point order of a voxel-grid filtered scan: by 2 m leaf index, x fastest.
 
