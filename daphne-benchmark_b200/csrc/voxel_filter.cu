@@ -13,13 +13,14 @@
 //     float (x, y, z and the fourth component alike);
 //   * a scan's output points are ordered by leaf, x fastest, then y, then z.
 //
-// Device pipeline for B scans: per scan the leaf bounding box (one block per
-// scan) and its leaf-key range; an exclusive scan of the ranges gives every
-// scan a disjoint key interval, so one 32-bit key per point (scan interval
-// base + local leaf key) orders points by scan, then leaf; one stable radix
-// sort and segmentation of all points (shared with the voxel-grid build);
-// per segment the FP64 mean in input order; per-scan output counts by atomic
-// increments of integers (order-independent), scanned into output offsets.
+// Device pipeline for B scans: the leaf bounding box of every scan (warps
+// over the packed points, 64-bit atomics) and its leaf-key range; an
+// exclusive scan of the ranges gives every scan a disjoint key interval, so
+// one 32-bit key per point (scan interval base + local leaf key) orders
+// points by scan, then leaf; one stable radix sort and segmentation of all
+// points (shared with the voxel-grid build); the points gathered into key
+// order; per segment the FP64 mean in input order; output offsets by lower
+// bounds of the scans' key bases in the sorted segment keys.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -235,37 +236,28 @@ __global__ void key_kernel(const float4 *__restrict__ pts, const int *__restrict
     vals[i] = (uint32_t)i;
 }
 
+// sorted[j] = pts[order[j]]: the points in key order (one thread per point,
+// so the random reads are all in flight at once; writes coalesced).
+__global__ void gather_kernel(const float4 *__restrict__ pts, const uint32_t *__restrict__ order, int n,
+                              float4 *__restrict__ sorted) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) sorted[j] = pts[__ldg(order + j)];
+}
+
 // One thread per segment: the FP64 mean of its points in input order (the
-// stable sort keeps that order within a segment), written to out[s], and one
-// count for its scan.  Segments are in key order (scan, then leaf) and the
-// segment of dropped points, if any, is the last, so s is the output index.
-// Points are loaded four at a time ahead of the (sequential) sums.
-__global__ void mean_kernel(const float4 *__restrict__ pts, const uint32_t *__restrict__ order,
-                            const int32_t *__restrict__ seg_start, const uint32_t *__restrict__ seg_key,
-                            const int *__restrict__ nseg, int n, uint32_t drop_key, const int *__restrict__ base,
-                            int B, float4 *__restrict__ out, int *__restrict__ count) {
+// stable sort keeps that order within a segment), written to out[s].
+// Segments are in key order (scan, then leaf) and the segment of dropped
+// points, if any, is the last, so s is the output index.
+__global__ void mean_kernel(const float4 *__restrict__ sorted, const int32_t *__restrict__ seg_start,
+                            const uint32_t *__restrict__ seg_key, const int *__restrict__ nseg, int n,
+                            uint32_t drop_key, float4 *__restrict__ out) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     const int K = *nseg;
-    if (s >= K) return;
-    const uint32_t key = seg_key[s];
-    if (key == drop_key) return;
+    if (s >= K || seg_key[s] == drop_key) return;
     const int a = seg_start[s], e = s + 1 < K ? seg_start[s + 1] : n;
     double sx = 0, sy = 0, sz = 0, sw = 0;
-    int j = a;
-    for (; j + 4 <= e; j += 4) {
-        float4 p[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) p[u] = pts[__ldg(order + j + u)];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            sx += (double)p[u].x;
-            sy += (double)p[u].y;
-            sz += (double)p[u].z;
-            sw += (double)p[u].w;
-        }
-    }
-    for (; j < e; ++j) {
-        const float4 p = pts[__ldg(order + j)];
+    for (int j = a; j < e; ++j) {
+        const float4 p = sorted[j];
         sx += (double)p.x;
         sy += (double)p.y;
         sz += (double)p.z;
@@ -273,34 +265,23 @@ __global__ void mean_kernel(const float4 *__restrict__ pts, const uint32_t *__re
     }
     const double c = (double)(e - a);
     out[s] = make_float4((float)(sx / c), (float)(sy / c), (float)(sz / c), (float)(sw / c));
-    atomicAdd(count + owner(base, B, (int)key), 1);
 }
 
-// Exclusive scan of n ints in place by one block (n = the scan count + 1:
-// counts in, output offsets out); *total = the sum.
-__global__ void __launch_bounds__(kRangeThreads) offsets_kernel(int *__restrict__ data, int n,
-                                                                int *__restrict__ total) {
-    __shared__ int s_sum[kRangeThreads];
-    const int t = threadIdx.x;
-    const int per = (n + kRangeThreads - 1) / kRangeThreads;
-    const int i0 = t * per, i1 = i0 + per < n ? i0 + per : n;
-    int local = 0;
-    for (int i = i0; i < i1; ++i) local += data[i];
-    s_sum[t] = local;
-    __syncthreads();
-    for (int o = 1; o < kRangeThreads; o <<= 1) {
-        const int v = t >= o ? s_sum[t - o] : 0;
-        __syncthreads();
-        s_sum[t] += v;
-        __syncthreads();
+// Output offsets without atomics: scan b's leaves are the segments with keys
+// in [base[b], base[b + 1]), so out_off[b] = the number of segments with a
+// key below base[b] (a lower bound in the sorted segment keys), b = 0 .. B
+// (base[B] = the key total = the dropped points' key).
+__global__ void offsets_kernel(const uint32_t *__restrict__ seg_key, const int *__restrict__ nseg,
+                               const int *__restrict__ base, int B, int *__restrict__ out_off) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b > B) return;
+    const uint32_t k = (uint32_t)base[b];
+    int lo = 0, hi = *nseg;  // first index in [lo, hi] with seg_key >= k
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (seg_key[mid] < k) lo = mid + 1; else hi = mid;
     }
-    int run = s_sum[t] - local;
-    for (int i = i0; i < i1; ++i) {
-        const int v = data[i];
-        data[i] = run;
-        run += v;
-    }
-    if (t == kRangeThreads - 1) *total = s_sum[t];
+    out_off[b] = lo;
 }
 
 }  // namespace vf
@@ -329,7 +310,7 @@ struct Buf {
 struct ndt_filter {
     int device = 0;
     cudaStream_t stream = nullptr;
-    Buf geom, base, flags, box, sort_scratch, seg_start, seg_key;
+    Buf geom, base, flags, box, sort_scratch, seg_start, seg_key, sorted;
     int box_cap = 0;
     int *h_flags = nullptr;  // pinned: error flags, key total, output total
     std::string msg;
@@ -427,6 +408,7 @@ int ndt_voxel_filter_device(ndt_filter *f, int B, const float *d_points, const i
     FCK(f->sort_scratch.ensure(ndt::sort_scratch_bytes(n)));
     FCK(f->seg_start.ensure(sizeof(int32_t) * (size_t)n));
     FCK(f->seg_key.ensure(sizeof(uint32_t) * (size_t)n));
+    FCK(f->sorted.ensure(sizeof(float4) * (size_t)n));
     ndt::SortBuffers sb = ndt::sort_buffers(f->sort_scratch.p, n);
     const unsigned pblk = (unsigned)((n + vf::kThreads - 1) / vf::kThreads);
     vf::key_kernel<<<pblk, vf::kThreads, 0, st>>>((const float4 *)d_points, d_offsets, B, r,
@@ -434,14 +416,14 @@ int ndt_voxel_filter_device(ndt_filter *f, int B, const float *d_points, const i
     FCK(cudaGetLastError());
     ndt::sort_segments(sb, n, bits, (int32_t *)f->seg_start.p, (uint32_t *)f->seg_key.p, st);
     FCK(cudaGetLastError());
-    FCK(cudaMemsetAsync(d_out_offsets, 0, sizeof(int) * (size_t)(B + 1), st));
-    vf::mean_kernel<<<pblk, vf::kThreads, 0, st>>>((const float4 *)d_points, sb.v0, (const int32_t *)f->seg_start.p,
+    vf::gather_kernel<<<pblk, vf::kThreads, 0, st>>>((const float4 *)d_points, sb.v0, n, (float4 *)f->sorted.p);
+    vf::mean_kernel<<<pblk, vf::kThreads, 0, st>>>((const float4 *)f->sorted.p, (const int32_t *)f->seg_start.p,
                                                    (const uint32_t *)f->seg_key.p, sb.nseg, n, (uint32_t)total_keys,
-                                                   base, B, (float4 *)d_out, d_out_offsets);
+                                                   (float4 *)d_out);
+    vf::offsets_kernel<<<(B + 1 + vf::kThreads - 1) / vf::kThreads, vf::kThreads, 0, st>>>(
+        (const uint32_t *)f->seg_key.p, sb.nseg, base, B, d_out_offsets);
     FCK(cudaGetLastError());
-    vf::offsets_kernel<<<1, vf::kRangeThreads, 0, st>>>(d_out_offsets, B + 1, flags + 2);
-    FCK(cudaGetLastError());
-    FCK(cudaMemcpyAsync(f->h_flags + 2, flags + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
+    FCK(cudaMemcpyAsync(f->h_flags + 2, d_out_offsets + B, sizeof(int), cudaMemcpyDeviceToHost, st));
     FCK(cudaStreamSynchronize(st));
     *out_total = f->h_flags[2];
     return NDT_OK;
