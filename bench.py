@@ -789,6 +789,81 @@ def run_filter(args, pkg, local):
     return 0
 
 
+def run_append(args, pkg, local):
+    """Map growth: the configuration's map grown by --append-scans aligned
+    scans (each scan in the map frame at its true pose, as the mapping
+    pipeline appends it), one ndt_map_append_device call per scan, against
+    rebuilding the grid of the grown map with ndt_set_map_device.  Every few
+    appends the grid is checked against the rebuild (grid cells bit for bit).
+    CUDA events on the context stream around each call (the append reads one
+    bounding box back to the host, so the time includes that round trip)."""
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    synth = pkg.synth
+    cfg = synth.CONFIGS[args.config]
+    scene = synth.make_scene(cfg)
+    K = args.append_scans
+    scans = []
+    for i in range(K + args.warmup):
+        a = synth.make_alignment(cfg, scene, 10000 + i)
+        w = np.ones_like(a.scan)
+        w[:, :3] = (a.scan[:, :3].astype(np.float64) @ a.truth[:3, :3].T + a.truth[:3, 3]).astype(np.float32)
+        scans.append(w)
+    warm, scans = scans[:args.warmup], scans[args.warmup:]
+    grown = np.concatenate([scene.map] + scans)
+    d_all = torch.from_numpy(np.ascontiguousarray(grown)).to(dev)
+    d_warm = [torch.from_numpy(np.ascontiguousarray(w)).to(dev) for w in warm]
+    M = scene.map.shape[0]
+    sizes = [s.shape[0] for s in scans]
+    starts = np.concatenate([[M], M + np.cumsum(sizes)]).astype(np.int64)
+    prm = pkg.ndt.reference_params(cfg.resolution)
+    inc = pkg.ndt.Context(prm, device=local)
+    full = pkg.ndt.Context(prm, device=local)
+    st_i = torch.cuda.ExternalStream(inc.stream, device=dev)
+    st_f = torch.cuda.ExternalStream(full.stream, device=dev)
+    torch.cuda.synchronize()
+
+    def timed(st, fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        fn()
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    # warm both paths (allocations sized for the grown map, first launches)
+    inc.set_map_device(d_all.data_ptr(), len(grown))
+    full.set_map_device(d_all.data_ptr(), len(grown))
+    inc.set_map_device(d_all.data_ptr(), M)
+    for w in d_warm:
+        inc.map_append_device(w.data_ptr(), w.shape[0])
+    inc.set_map_device(d_all.data_ptr(), M)
+    t_app, t_full, incremental = [], [], 0
+    for i in range(K):
+        m, k = int(starts[i]), sizes[i]
+        bbox_before = inc.grid_info()[0].copy()
+        t_app.append(timed(st_i, lambda: inc.map_append_device(d_all.data_ptr() + 16 * m, k)))
+        incremental += int(np.array_equal(inc.grid_info()[0], bbox_before))
+        t_full.append(timed(st_f, lambda: full.set_map_device(d_all.data_ptr(), m + k)))
+        if i % 8 == 0 or i == K - 1:
+            a, b = inc.grid_cells(), full.grid_cells()
+            oa, ob = np.argsort(a[0]), np.argsort(b[0])
+            for x, y in zip(a, b):
+                if not np.array_equal(np.asarray(x)[oa].view(np.uint8), np.asarray(y)[ob].view(np.uint8)):
+                    raise SystemExit(f"append {i}: grid differs from the rebuild")
+    ta, tf = statistics.median(t_app), statistics.median(t_full)
+    print(json.dumps({"workload": f"map growth: {args.config} map ({M} points, resolution {cfg.resolution:g} m) + "
+                                  f"{K} aligned scans ({min(sizes)}-{max(sizes)} points)",
+                      "append_ms_median": ta, "rebuild_ms_median": tf, "speedup": tf / ta,
+                      "appends_incremental": incremental, "appends": K, "final_map_points": int(starts[-1]),
+                      "append_ms": [round(x, 4) for x in t_app], "rebuild_ms": [round(x, 4) for x in t_full],
+                      "grids_equal": True}), flush=True)
+    inc.close()
+    full.close()
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -814,6 +889,8 @@ def main(argv=None):
     ap.add_argument("--train-epochs", type=int, default=0, help="0: 30 (c4), 60 (c5)")
     ap.add_argument("--oracle-sample", type=int, default=64)
     ap.add_argument("--filter", action="store_true", help="time the scan pre-filter (voxel-grid downsampling)")
+    ap.add_argument("--append", action="store_true", help="time map growth (ndt_map_append) against rebuilds")
+    ap.add_argument("--append-scans", type=int, default=32)
     ap.add_argument("--filter-scans", type=int, default=256)
     ap.add_argument("--filter-points", type=int, default=65536)
     args = ap.parse_args(argv)
@@ -827,6 +904,8 @@ def main(argv=None):
         return run_learned(args, pkg, world, rank, local)
     if args.filter and args.impl != "reference":
         return run_filter(args, pkg, local)
+    if args.append and args.impl != "reference":
+        return run_append(args, pkg, local)
     if args.impl == "reference":
         return run_reference_arm(args, pkg, world, rank)
     return run_ours(args, pkg, world, rank, local)

@@ -27,15 +27,41 @@ namespace {
 struct DevBuf {
     void *p = nullptr;
     size_t cap = 0;
+    // Contents are not kept.  A buffer that has to grow takes half as much
+    // again, so that a slowly growing size (a map grown scan by scan)
+    // reallocates only now and then.
     cudaError_t ensure(size_t bytes) {
         if (bytes <= cap && p) return cudaSuccess;
+        const bool regrow = p != nullptr;
         if (p) cudaFree(p);
         p = nullptr;
         cap = 0;
         size_t want = bytes < 256 ? 256 : bytes;
+        if (regrow) want += want / 2;
         cudaError_t e = cudaMalloc(&p, want);
         if (e == cudaSuccess) cap = want;
         return e;
+    }
+    // Grows to at least `bytes` keeping the first `keep` bytes (copied on
+    // stream st, which is synchronised before the old buffer is freed).
+    cudaError_t grow_keep(size_t bytes, size_t keep, cudaStream_t st) {
+        if (bytes <= cap && p) return cudaSuccess;
+        void *fresh = nullptr;
+        const size_t want = bytes + bytes / 2;
+        cudaError_t e = cudaMalloc(&fresh, want);
+        if (e != cudaSuccess) return e;
+        if (p && keep) {
+            e = cudaMemcpyAsync(fresh, p, keep < cap ? keep : cap, cudaMemcpyDeviceToDevice, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) {
+                cudaFree(fresh);
+                return e;
+            }
+        }
+        if (p) cudaFree(p);
+        p = fresh;
+        cap = want;
+        return cudaSuccess;
     }
     void release() {
         if (p) cudaFree(p);
@@ -112,12 +138,20 @@ struct ndt_ctx {
     std::string err;
     double d1 = 0, d2 = 0;
     // grid
-    DevBuf map, index, mean, mean_hi, mean_lo, icov32, icov64, count, cell, seg_start, seg_cell, scratch, meta;
+    DevBuf map, index, slot_of, mean, mean_hi, mean_lo, icov32, icov64, count, cell, seg_start, seg_cell, scratch, meta;
     DevBuf win_off, win_ent, win_ctot;
     GridMeta meta_host{};
     bool have_map = false;
     bool have_windows = false;
     int map_points = 0;
+    // map growth (ndt_map_append): the current map's points on the device
+    // (the context's own buffer `map`, or the caller's for ndt_set_map_device),
+    // its cell-sorted pairs (in the build scratch, or in sorted_keys / _order
+    // [sorted_in]) and the append's own scratch
+    const float4 *map_src = nullptr;
+    ndt::SortedMap sorted{nullptr, nullptr};
+    int sorted_in = -1;  // -1: in `scratch`, else the index of the buffer pair
+    DevBuf sorted_keys[2], sorted_order[2], append_scratch, meta_tmp;
     // batch
     DevBuf chunks, chunk_begin, num_chunks, big_begin, small_begin, num_big, round_no, dev_launches;
     DevBuf points, offsets, guesses, states, tiles, tile_begin, num_tiles, partials, exc, out_T, out_conv, out_fit,
@@ -207,6 +241,7 @@ GridBuffers grid_buffers(ndt_ctx *c) {
     b.cell = c->cell.as<int32_t>();
     b.seg_start = c->seg_start.as<int32_t>();
     b.seg_cell = c->seg_cell.as<uint32_t>();
+    b.slot_of = c->slot_of.as<int32_t>();
     return b;
 }
 
@@ -248,6 +283,59 @@ constexpr long long kMaxWindowEntries = 1LL << 28;  // window entries (16 B each
 
 // Grid build from a device-resident map (any device pointer valid on the
 // context's stream for the duration of the call).
+// Probe-window table of the finished dense index: W + 1 offsets and at most
+// 27 entries per usable voxel (skipped when it would not fit, or with
+// dense_probe set).
+int build_windows(ndt_ctx *c, int m) {
+    const size_t G = (size_t)c->meta_host.G;
+    const long long W = (long long)window_count(c->meta_host);
+    const long long ent_cap = 27LL * (long long)std::min<size_t>((size_t)m, G);
+    c->have_windows = false;
+    if (!c->prm.dense_probe && W < kMaxWindows && ent_cap < kMaxWindowEntries) {
+        CK(c->win_off.ensure(sizeof(int32_t) * (size_t)(W + 1)));
+        CK(c->win_ent.ensure(sizeof(float4) * (size_t)ent_cap));
+        CK(c->win_ctot.ensure(sizeof(int32_t) * (size_t)(W / 256 + 2)));
+        WindowBuffers wb;
+        wb.off = c->win_off.as<int32_t>();
+        wb.ent = c->win_ent.as<float4>();
+        wb.ctot = c->win_ctot.as<int32_t>();
+        int nl = 0;
+        int rc = grid_windows(c->meta_host, c->index.as<int32_t>(), c->mean_hi.as<float4>(), wb, c->stream, &nl);
+        if (rc) return cuda_fail(c, (cudaError_t)rc, "grid_windows");
+        c->launches += nl;
+        c->have_windows = true;
+    }
+    return NDT_OK;
+}
+
+// Per-voxel record buffers for m slots, keeping the first `keep` slots.
+int grow_records(ndt_ctx *c, int m, int keep) {
+    cudaStream_t st = c->stream;
+    const size_t n = (size_t)m, k = (size_t)keep;
+    CK(c->mean.grow_keep(sizeof(double4) * n, sizeof(double4) * k, st));
+    CK(c->mean_hi.grow_keep(sizeof(float4) * n, sizeof(float4) * k, st));
+    CK(c->mean_lo.grow_keep(sizeof(float4) * n, sizeof(float4) * k, st));
+    CK(c->icov32.grow_keep(2 * sizeof(float4) * n, 2 * sizeof(float4) * k, st));
+    CK(c->icov64.grow_keep(9 * sizeof(double) * n, 9 * sizeof(double) * k, st));
+    CK(c->count.grow_keep(sizeof(int32_t) * n, sizeof(int32_t) * k, st));
+    CK(c->cell.grow_keep(sizeof(int32_t) * n, sizeof(int32_t) * k, st));
+    return NDT_OK;
+}
+
+// Per-voxel record buffers for a map of m points.
+int ensure_records(ndt_ctx *c, int m) {
+    CK(c->mean.ensure(sizeof(double4) * (size_t)m));
+    CK(c->mean_hi.ensure(sizeof(float4) * (size_t)m));
+    CK(c->mean_lo.ensure(sizeof(float4) * (size_t)m));
+    CK(c->icov32.ensure(2 * sizeof(float4) * (size_t)m));
+    CK(c->icov64.ensure(9 * sizeof(double) * (size_t)m));
+    CK(c->count.ensure(sizeof(int32_t) * (size_t)m));
+    CK(c->cell.ensure(sizeof(int32_t) * (size_t)m));
+    CK(c->seg_start.ensure(sizeof(int32_t) * (size_t)m));
+    CK(c->seg_cell.ensure(sizeof(uint32_t) * (size_t)m));
+    return NDT_OK;
+}
+
 int build_grid(ndt_ctx *c, const float4 *d_map, int m) {
     if (m <= 0) return fail(c, NDT_E_ARG, "map must have at least one point");
     // voxel slots travel in 26 bits of a packed pair code (slot << 6 | flag << 5 | lane)
@@ -275,44 +363,24 @@ int build_grid(ndt_ctx *c, const float4 *d_map, int m) {
     if (c->meta_host.error) return fail(c, NDT_E_GRID, "voxel grid does not fit 32-bit cell indices");
     const size_t G = (size_t)c->meta_host.G;
     CK(c->index.ensure(sizeof(int32_t) * G));
-    CK(c->mean.ensure(sizeof(double4) * (size_t)m));
-    CK(c->mean_hi.ensure(sizeof(float4) * (size_t)m));
-    CK(c->mean_lo.ensure(sizeof(float4) * (size_t)m));
-    CK(c->icov32.ensure(2 * sizeof(float4) * (size_t)m));
-    CK(c->icov64.ensure(9 * sizeof(double) * (size_t)m));
-    CK(c->count.ensure(sizeof(int32_t) * (size_t)m));
-    CK(c->cell.ensure(sizeof(int32_t) * (size_t)m));
-    CK(c->seg_start.ensure(sizeof(int32_t) * (size_t)m));
-    CK(c->seg_cell.ensure(sizeof(uint32_t) * (size_t)m));
+    CK(c->slot_of.ensure(sizeof(int32_t) * G));
+    if (int rc0 = ensure_records(c, m)) return rc0;
     NdtGridOptions opt;
     opt.compat = c->prm.compat;
     opt.min_points = c->prm.min_points_per_voxel;
     opt.eigen_ratio = c->prm.eigen_ratio;
     int nl = 0;
-    rc = grid_build(d_map, m, c->meta_host, c->meta.as<GridMeta>(), opt, grid_buffers(c), c->scratch.p, c->stream, &nl);
+    rc = grid_build(d_map, m, c->meta_host, c->meta.as<GridMeta>(), opt, grid_buffers(c), c->scratch.p, c->stream, &nl,
+                    &c->sorted);
     if (rc) return cuda_fail(c, (cudaError_t)rc, "grid_build");
     c->launches += nl;
-    // probe-window table: W + 1 offsets and at most 27 entries per usable voxel
-    const long long W = (long long)window_count(c->meta_host);
-    const long long ent_cap = 27LL * (long long)std::min<size_t>((size_t)m, G);
-    if (!c->prm.dense_probe && W < kMaxWindows && ent_cap < kMaxWindowEntries) {
-        CK(c->win_off.ensure(sizeof(int32_t) * (size_t)(W + 1)));
-        CK(c->win_ent.ensure(sizeof(float4) * (size_t)ent_cap));
-        CK(c->win_ctot.ensure(sizeof(int32_t) * (size_t)(W / 256 + 2)));
-        WindowBuffers wb;
-        wb.off = c->win_off.as<int32_t>();
-        wb.ent = c->win_ent.as<float4>();
-        wb.ctot = c->win_ctot.as<int32_t>();
-        nl = 0;
-        rc = grid_windows(c->meta_host, c->index.as<int32_t>(), c->mean_hi.as<float4>(), wb, c->stream, &nl);
-        if (rc) return cuda_fail(c, (cudaError_t)rc, "grid_windows");
-        c->launches += nl;
-        c->have_windows = true;
-    }
+    c->sorted_in = -1;
+    if (int rc2 = build_windows(c, m)) return rc2;
     if (c->profiling) {
         CK(cudaEventRecord(c->grid_ev[1], c->stream));
         c->grid_timed = true;
     }
+    c->map_src = d_map;
     c->have_map = true;
     c->map_points = m;
     return NDT_OK;
@@ -871,6 +939,95 @@ int ndt_set_map_device(ndt_ctx *c, const float *d_map, int m) {
     if (int rc = set_device(c)) return rc;
     return build_grid(c, (const float4 *)d_map, m);
 }
+
+// Appends k points (host or device) to the current map and brings the grid up
+// to date: incrementally (merge of the new points' sorted cells into the
+// map's, then the voxel records) when they lie inside the old points'
+// bounding box, else by a full build of the grown map.  Either way the grid
+// equals ndt_set_map of the whole grown map.
+int map_append(ndt_ctx *c, const float *pts, int k, bool host) {
+    if (!c) return NDT_E_ARG;
+    if (k < 0 || (k > 0 && !pts)) return fail(c, NDT_E_ARG, "null points or negative count");
+    if (int rc = set_device(c)) return rc;
+    if (!c->have_map || !c->map_src) return fail(c, NDT_E_NOMAP, "no map set");
+    if (k == 0) return NDT_OK;
+    const int m = c->map_points;
+    const long long nl_total = (long long)m + k;
+    if (nl_total >= (1LL << 25)) return fail(c, NDT_E_CAPACITY, "map larger than 2^25 points");
+    const int n = (int)nl_total;
+    cudaStream_t st = c->stream;
+    // 1. the grown map in the context's own buffer (grown by half again when full)
+    const size_t need = sizeof(float4) * (size_t)n;
+    if (c->map_src != c->map.as<float4>() || c->map.cap < need) {
+        void *fresh = nullptr;
+        const size_t want = std::max(need + need / 2, (size_t)4096);
+        CK(cudaMalloc(&fresh, want));
+        cudaError_t e = cudaMemcpyAsync(fresh, c->map_src, sizeof(float4) * (size_t)m, cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            cudaFree(fresh);
+            return cuda_fail(c, e, "copy of the map");
+        }
+        c->map.release();
+        c->map.p = fresh;
+        c->map.cap = want;
+        c->map_src = c->map.as<float4>();
+    }
+    float4 *map = c->map.as<float4>();
+    CK(cudaMemcpyAsync(map + m, pts, sizeof(float4) * (size_t)k,
+                       host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
+    // 2. the new points' bounding box against the old points'
+    CK(c->meta_tmp.ensure(sizeof(GridMeta)));
+    int rc = grid_bbox(map + m, k, c->prm.resolution, c->meta_tmp.as<GridMeta>(), c->scratch.p, st);
+    if (rc) return cuda_fail(c, (cudaError_t)rc, "grid_bbox");
+    c->launches += 1;
+    GridMeta nm;
+    CK(cudaMemcpyAsync(&nm, c->meta_tmp.p, sizeof(GridMeta), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (nm.error == 2) return fail(c, NDT_E_ARG, "appended points have non-finite coordinates");
+    bool inside = true;
+    for (int e = 0; e < 3; ++e)
+        if (!(nm.raw_min[e] >= c->meta_host.raw_min[e] && nm.raw_max[e] <= c->meta_host.raw_max[e])) inside = false;
+    if (!inside) return build_grid(c, map, n);
+    // 3. incremental: merge, the touched cells' records, windows
+    c->have_map = false;
+    c->grid_timed = false;
+    if (c->profiling) {
+        if (!c->grid_ev[0]) CK(cudaEventCreate(&c->grid_ev[0]));
+        if (!c->grid_ev[1]) CK(cudaEventCreate(&c->grid_ev[1]));
+        CK(cudaEventRecord(c->grid_ev[0], st));
+    }
+    if (int rc0 = grow_records(c, n, m)) return rc0;
+    const int out = c->sorted_in == 0 ? 1 : 0;
+    CK(c->sorted_keys[out].ensure(sizeof(uint32_t) * (size_t)n));
+    CK(c->sorted_order[out].ensure(sizeof(uint32_t) * (size_t)n));
+    CK(c->append_scratch.ensure(ndt::append_scratch_bytes(k)));
+    NdtGridOptions opt;
+    opt.compat = c->prm.compat;
+    opt.min_points = c->prm.min_points_per_voxel;
+    opt.eigen_ratio = c->prm.eigen_ratio;
+    int nl = 0;
+    rc = grid_append(map, m, k, c->meta_host, c->meta.as<GridMeta>(), opt, grid_buffers(c), c->sorted,
+                     c->sorted_keys[out].as<uint32_t>(), c->sorted_order[out].as<uint32_t>(), c->append_scratch.p, st,
+                     &nl);
+    if (rc) return cuda_fail(c, (cudaError_t)rc, "grid_append");
+    c->launches += nl;
+    c->sorted.keys = c->sorted_keys[out].as<uint32_t>();
+    c->sorted.order = c->sorted_order[out].as<uint32_t>();
+    c->sorted_in = out;
+    if (int rc2 = build_windows(c, n)) return rc2;
+    if (c->profiling) {
+        CK(cudaEventRecord(c->grid_ev[1], st));
+        c->grid_timed = true;
+    }
+    c->have_map = true;
+    c->map_points = n;
+    return NDT_OK;
+}
+
+int ndt_map_append(ndt_ctx *c, const float *points, int k) { return map_append(c, points, k, true); }
+
+int ndt_map_append_device(ndt_ctx *c, const float *d_points, int k) { return map_append(c, d_points, k, false); }
 
 int ndt_align(ndt_ctx *c, const float *scan, int n, const float guess16[16], float out16[16], int *converged,
               double *fitness) {

@@ -115,6 +115,8 @@ __global__ void bbox_kernel(const float4 *__restrict__ map, int m, float *__rest
     g.error = atomicAdd(flags + 1, 0) ? 2 : 0;
     long long G = 1;
     for (int e = 0; e < 3; ++e) {
+        g.raw_min[e] = v[e];
+        g.raw_max[e] = v[3 + e];
         g.minv[e] = v[e] - 0.01f;
         g.maxv[e] = v[3 + e] + 0.01f;
         float d = (g.maxv[e] - g.minv[e]) / res + 1;
@@ -133,7 +135,7 @@ __global__ void bbox_kernel(const float4 *__restrict__ map, int m, float *__rest
 
 // Dense cell id of each map point (linearizeCoord, kernel.cpp:236-244).
 __global__ void cell_key_kernel(const float4 *__restrict__ map, int m, const GridMeta *__restrict__ meta,
-                                uint32_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+                                uint32_t *__restrict__ keys, uint32_t *__restrict__ vals, int index_offset = 0) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m) return;
     const GridMeta g = *meta;
@@ -143,7 +145,38 @@ __global__ void cell_key_kernel(const float4 *__restrict__ map, int m, const Gri
     int iy = (int)((p.y - g.minv[1]) / g.res);
     int iz = (int)((p.z - g.minv[2]) / g.res);
     keys[i] = (uint32_t)(ix + g.dim[0] * (iy + g.dim[1] * iz));
-    vals[i] = (uint32_t)i;
+    vals[i] = (uint32_t)(i + index_offset);
+}
+
+// Stable merge of two key-sorted (key, value) runs, run a first on equal
+// keys: element t of a lands at t + #{b keys < key}, element j of b at
+// j + #{a keys <= key} (binary searches; each output position is written
+// once).
+__global__ void merge_kernel(const uint32_t *__restrict__ ka, const uint32_t *__restrict__ va, int na,
+                             const uint32_t *__restrict__ kb, const uint32_t *__restrict__ vb, int nb,
+                             uint32_t *__restrict__ ko, uint32_t *__restrict__ vo) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= na + nb) return;
+    if (t < na) {
+        const uint32_t key = ka[t];
+        int lo = 0, hi = nb;  // first b key >= key
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (__ldg(kb + mid) < key) lo = mid + 1; else hi = mid;
+        }
+        ko[t + lo] = key;
+        vo[t + lo] = va[t];
+    } else {
+        const int j = t - na;
+        const uint32_t key = kb[j];
+        int lo = 0, hi = na;  // first a key > key
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (__ldg(ka + mid) <= key) lo = mid + 1; else hi = mid;
+        }
+        ko[j + lo] = key;
+        vo[j + lo] = vb[j];
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -419,15 +452,8 @@ __device__ bool write_records(int s, const double *mu, const double *C, GridBuff
 // the float products x_r * x_c; then mean = sum / N and
 //   S_rc = ((S_rc - 2 (sum_r mean_c)) / G + mean_r mean_c) * ((G - 1) / N)
 // (G = dense cell count), inverted by adjugate (invertMatrix, :1277-1300).
-__global__ void cell_finalize_compat_kernel(const float4 *__restrict__ map, const uint32_t *__restrict__ order,
-                                            const int *__restrict__ seg_start, const uint32_t *__restrict__ seg_cell,
-                                            const int *__restrict__ nseg, int n, GridMeta *__restrict__ meta,
-                                            GridBuffers buf) {
-    const int K = *nseg;
-    if (blockIdx.x == 0 && threadIdx.x == 0) meta->occupied = K;
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= K) return;
-    const int lo = seg_start[s], hi = (s + 1 < K) ? seg_start[s + 1] : n;
+__device__ void compat_cell(const float4 *__restrict__ map, const uint32_t *__restrict__ order, int lo, int hi,
+                            double Gd, int s, uint32_t cell_id, GridBuffers buf) {
     double sum[3] = {0.0, 0.0, 0.0};
     double S[9] = {0.0, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0, 0.0, 0.0};
     int cnt = 0;
@@ -443,7 +469,6 @@ __global__ void cell_finalize_compat_kernel(const float4 *__restrict__ map, cons
 #pragma unroll
             for (int c = 0; c < 3; ++c) S[3 * r + c] += (double)(v[r] * v[c]);
     }
-    const double Gd = (double)meta->G;
     double mu[3];
     for (int e = 0; e < 3; ++e) mu[e] = sum[e] / cnt;
 #pragma unroll
@@ -472,8 +497,21 @@ __global__ void cell_finalize_compat_kernel(const float4 *__restrict__ map, cons
     for (int k = 0; k < 9; ++k) C[k] = t[k] * inv_det;
     const bool flag = write_records(s, mu, C, buf);
     buf.count[s] = cnt;
-    buf.cell[s] = (int)seg_cell[s];
-    buf.index[seg_cell[s]] = s | (flag ? kSlotFlag : 0);
+    buf.cell[s] = (int)cell_id;
+    buf.index[cell_id] = s | (flag ? kSlotFlag : 0);
+    buf.slot_of[cell_id] = s;
+}
+
+__global__ void cell_finalize_compat_kernel(const float4 *__restrict__ map, const uint32_t *__restrict__ order,
+                                            const int *__restrict__ seg_start, const uint32_t *__restrict__ seg_cell,
+                                            const int *__restrict__ nseg, int n, GridMeta *__restrict__ meta,
+                                            GridBuffers buf) {
+    const int K = *nseg;
+    if (blockIdx.x == 0 && threadIdx.x == 0) meta->occupied = K;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= K) return;
+    const int lo = seg_start[s], hi = (s + 1 < K) ? seg_start[s + 1] : n;
+    compat_cell(map, order, lo, hi, (double)meta->G, s, seg_cell[s], buf);
 }
 
 // Symmetric 3x3 eigen-decomposition by cyclic Jacobi rotations (V columns =
@@ -515,20 +553,21 @@ __device__ void jacobi3(double A[3][3], double V[3][3], double w[3]) {
 // Corrected voxel: mean, centred covariance / (N - 1), usable only with at
 // least min_points points, eigenvalues floored at eig_ratio * max, inverse
 // as V diag(1 / w) V^T.
-__global__ void cell_finalize_corrected_kernel(const float4 *__restrict__ map, const uint32_t *__restrict__ order,
-                                               const int *__restrict__ seg_start,
-                                               const uint32_t *__restrict__ seg_cell, const int *__restrict__ nseg,
-                                               int n, int min_points, double eig_ratio, GridMeta *__restrict__ meta,
-                                               GridBuffers buf) {
-    const int K = *nseg;
-    if (blockIdx.x == 0 && threadIdx.x == 0) meta->occupied = K;
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= K) return;
-    const int lo = seg_start[s], hi = (s + 1 < K) ? seg_start[s + 1] : n;
+__device__ void corrected_cell(const float4 *__restrict__ map, const uint32_t *__restrict__ order, int lo, int hi,
+                               int min_points, double eig_ratio, int s, uint32_t cell_id, GridBuffers buf) {
     const int cnt = hi - lo;
     buf.count[s] = cnt;
-    buf.cell[s] = (int)seg_cell[s];
-    if (cnt < min_points || cnt < 2) return;
+    buf.cell[s] = (int)cell_id;
+    buf.slot_of[cell_id] = s;
+    // a cell that is not usable has index -1; its records read NaN
+    const double qnan = __longlong_as_double(0x7ff8000000000000LL);
+    const double nan3[3] = {qnan, qnan, qnan};
+    const double nan9[9] = {qnan, qnan, qnan, qnan, qnan, qnan, qnan, qnan, qnan};
+    if (cnt < min_points || cnt < 2) {
+        write_records(s, nan3, nan9, buf);
+        buf.index[cell_id] = -1;
+        return;
+    }
     double sum[3] = {0.0, 0.0, 0.0};
     for (int j = lo; j < hi; ++j) {
         float4 p = map[order[j]];
@@ -551,12 +590,20 @@ __global__ void cell_finalize_corrected_kernel(const float4 *__restrict__ map, c
     double V[3][3], w[3];
     jacobi3(A, V, w);
     double wmax = fmax(w[0], fmax(w[1], w[2]));
-    if (!(wmax > 0.0) || !isfinite(wmax)) return;
+    if (!(wmax > 0.0) || !isfinite(wmax)) {
+        write_records(s, nan3, nan9, buf);
+        buf.index[cell_id] = -1;
+        return;
+    }
     double floor_v = eig_ratio * wmax;
     double inv_w[3];
     for (int e = 0; e < 3; ++e) {
         double we = w[e] < floor_v ? floor_v : w[e];
-        if (!(we > 0.0)) return;
+        if (!(we > 0.0)) {
+            write_records(s, nan3, nan9, buf);
+            buf.index[cell_id] = -1;
+            return;
+        }
         inv_w[e] = 1.0 / we;
     }
     double C[9];
@@ -564,7 +611,68 @@ __global__ void cell_finalize_corrected_kernel(const float4 *__restrict__ map, c
         for (int q = 0; q < 3; ++q)
             C[3 * r + q] = V[r][0] * inv_w[0] * V[q][0] + V[r][1] * inv_w[1] * V[q][1] + V[r][2] * inv_w[2] * V[q][2];
     const bool flag = write_records(s, mu, C, buf);
-    buf.index[seg_cell[s]] = s | (flag ? kSlotFlag : 0);
+    buf.index[cell_id] = s | (flag ? kSlotFlag : 0);
+}
+
+__global__ void cell_finalize_corrected_kernel(const float4 *__restrict__ map, const uint32_t *__restrict__ order,
+                                               const int *__restrict__ seg_start,
+                                               const uint32_t *__restrict__ seg_cell, const int *__restrict__ nseg,
+                                               int n, int min_points, double eig_ratio, GridMeta *__restrict__ meta,
+                                               GridBuffers buf) {
+    const int K = *nseg;
+    if (blockIdx.x == 0 && threadIdx.x == 0) meta->occupied = K;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= K) return;
+    const int lo = seg_start[s], hi = (s + 1 < K) ? seg_start[s + 1] : n;
+    corrected_cell(map, order, lo, hi, min_points, eig_ratio, s, seg_cell[s], buf);
+}
+
+// Map growth, touched cells only.  new_keys: the appended points' cell keys,
+// sorted; keys / order: all points' sorted (cell, point) pairs.  Pass 1:
+// fresh[j] = 1 where j is the first of its key and the cell has no slot yet;
+// k_old = the slot count before the append.
+__global__ void append_mark_kernel(const uint32_t *__restrict__ new_keys, int k, const int32_t *__restrict__ slot_of,
+                                   const GridMeta *__restrict__ meta, int *__restrict__ fresh,
+                                   int *__restrict__ k_old) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j == 0) *k_old = meta->occupied;
+    if (j >= k) return;
+    const uint32_t key = new_keys[j];
+    const bool first = j == 0 || new_keys[j - 1] != key;
+    fresh[j] = (first && slot_of[key] < 0) ? 1 : 0;
+}
+
+// Pass 2 (fresh[] exclusively scanned, *n_fresh its total): every touched
+// cell, one thread per first key, is recomputed from all its points in the
+// sorted order (the same arithmetic as the build, so the records equal a
+// full build's); new cells take slots k_old, k_old + 1, ... in key order.
+__global__ void append_cells_kernel(const float4 *__restrict__ map, const uint32_t *__restrict__ new_keys, int k,
+                                    const uint32_t *__restrict__ keys, const uint32_t *__restrict__ order, int n,
+                                    const int *__restrict__ fresh, const int *__restrict__ n_fresh,
+                                    const int *__restrict__ k_old, int compat, int min_points, double eig_ratio,
+                                    GridMeta *__restrict__ meta, GridBuffers buf) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j == 0) meta->occupied = *k_old + *n_fresh;
+    if (j >= k) return;
+    const uint32_t key = new_keys[j];
+    if (j > 0 && new_keys[j - 1] == key) return;
+    const int old_slot = buf.slot_of[key];
+    const int s = old_slot >= 0 ? old_slot : *k_old + fresh[j];
+    int lo = 0, hi = n;  // first key >= key
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(keys + mid) < key) lo = mid + 1; else hi = mid;
+    }
+    const int first = lo;
+    hi = n;  // first key > key
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(keys + mid) <= key) lo = mid + 1; else hi = mid;
+    }
+    if (compat)
+        compat_cell(map, order, first, lo, (double)meta->G, s, key, buf);
+    else
+        corrected_cell(map, order, first, lo, min_points, eig_ratio, s, key, buf);
 }
 
 // ---------------------------------------------------------------------------
@@ -690,7 +798,7 @@ int grid_windows(const GridMeta &meta_host, const int32_t *index, const float4 *
     return (int)cudaGetLastError();
 }
 
-int sort_segments(SortBuffers &b, int n, int bits, int32_t *seg_start, uint32_t *seg_key, cudaStream_t st) {
+int radix_sort_pairs(SortBuffers &b, int n, int bits, cudaStream_t st) {
     const int nblk = div_up(n, kSortTile);
     int nl = 0;
     // digit width: passes = ceil(bits / 8), width = ceil(bits / passes).  (Wider
@@ -712,11 +820,21 @@ int sort_segments(SortBuffers &b, int n, int bits, int32_t *seg_start, uint32_t 
         t = b.v0; b.v0 = b.v1; b.v1 = t;
         shift += w;
     }
-    seg_count_kernel<<<nblk, kThreads, 0, st>>>(b.k0, n, b.segc);
-    nl += scan_exclusive(b.segc, nblk, b.nseg, b.part, st);
-    seg_write_kernel<<<nblk, kThreads, 0, st>>>(b.k0, n, b.segc, seg_start, seg_key);
-    nl += 2;
     return nl;
+}
+
+int segment_sorted(const uint32_t *keys, int n, int *segc, int *nseg, int *part, int32_t *seg_start,
+                   uint32_t *seg_key, cudaStream_t st) {
+    const int nblk = div_up(n, kSortTile);
+    seg_count_kernel<<<nblk, kThreads, 0, st>>>(keys, n, segc);
+    int nl = scan_exclusive(segc, nblk, nseg, part, st);
+    seg_write_kernel<<<nblk, kThreads, 0, st>>>(keys, n, segc, seg_start, seg_key);
+    return nl + 2;
+}
+
+int sort_segments(SortBuffers &b, int n, int bits, int32_t *seg_start, uint32_t *seg_key, cudaStream_t st) {
+    int nl = radix_sort_pairs(b, n, bits, st);
+    return nl + segment_sorted(b.k0, n, b.segc, b.nseg, b.part, seg_start, seg_key, st);
 }
 
 size_t sort_scratch_bytes(int n) {
@@ -745,29 +863,80 @@ SortBuffers sort_buffers(void *scratch, int n) {
     return b;
 }
 
+// Key bits of the dense cell ids.
+int key_bits(const GridMeta &meta_host) {
+    int bits = 1;
+    while (bits < 31 && (1LL << bits) < meta_host.G) ++bits;
+    return bits;
+}
+
+// Per-voxel records from the sorted order (one launch).
+int grid_finalize(const float4 *d_map, const uint32_t *order, int m, const int *nseg, GridMeta *d_meta,
+                  const NdtGridOptions &opt, GridBuffers buf, cudaStream_t st) {
+    // at most m segments: launch for m, kernels read the true count
+    if (opt.compat) {
+        cell_finalize_compat_kernel<<<div_up(m, 128), 128, 0, st>>>(d_map, order, buf.seg_start, buf.seg_cell, nseg,
+                                                                    m, d_meta, buf);
+    } else {
+        cell_finalize_corrected_kernel<<<div_up(m, 128), 128, 0, st>>>(d_map, order, buf.seg_start, buf.seg_cell,
+                                                                       nseg, m, opt.min_points, opt.eigen_ratio,
+                                                                       d_meta, buf);
+    }
+    return 1;
+}
+
 int grid_build(const float4 *d_map, int m, const GridMeta &meta_host, GridMeta *d_meta, const NdtGridOptions &opt,
-               GridBuffers buf, void *scratch, cudaStream_t st, int *launches) {
+               GridBuffers buf, void *scratch, cudaStream_t st, int *launches, SortedMap *sorted) {
     SortBuffers sb = sort_buffers((char *)scratch + kBboxBytes, m);  // after the bounding-box region
     int nl = 0;
 
     cudaMemsetAsync(buf.index, 0xff, sizeof(int32_t) * (size_t)meta_host.G, st);
+    cudaMemsetAsync(buf.slot_of, 0xff, sizeof(int32_t) * (size_t)meta_host.G, st);
     cell_key_kernel<<<div_up(m, kThreads), kThreads, 0, st>>>(d_map, m, d_meta, sb.k0, sb.v0);
     ++nl;
-    int bits = 1;
-    while (bits < 31 && (1LL << bits) < meta_host.G) ++bits;
-    nl += sort_segments(sb, m, bits, buf.seg_start, buf.seg_cell, st);
-    const uint32_t *v0 = sb.v0;
-    const int *nseg = sb.nseg;
-    // at most m segments: launch for m, kernels read the true count
-    if (opt.compat) {
-        cell_finalize_compat_kernel<<<div_up(m, 128), 128, 0, st>>>(d_map, v0, buf.seg_start, buf.seg_cell, nseg,
-                                                                    m, d_meta, buf);
-    } else {
-        cell_finalize_corrected_kernel<<<div_up(m, 128), 128, 0, st>>>(d_map, v0, buf.seg_start, buf.seg_cell,
-                                                                       nseg, m, opt.min_points, opt.eigen_ratio,
-                                                                       d_meta, buf);
+    nl += sort_segments(sb, m, key_bits(meta_host), buf.seg_start, buf.seg_cell, st);
+    nl += grid_finalize(d_map, sb.v0, m, sb.nseg, d_meta, opt, buf, st);
+    if (sorted) {
+        sorted->keys = sb.k0;
+        sorted->order = sb.v0;
     }
-    nl += 1;
+    if (launches) *launches += nl;
+    return (int)cudaGetLastError();
+}
+
+size_t append_scratch_bytes(int k) {
+    return sort_scratch_bytes(k) + sizeof(int) * ((size_t)k + 1) + sizeof(int) * scan_part_ints((size_t)k) + 8 * 256;
+}
+
+int grid_append(const float4 *d_map, int m_old, int k, const GridMeta &meta_host, GridMeta *d_meta,
+                const NdtGridOptions &opt, GridBuffers buf, SortedMap old_sorted, uint32_t *keys_out,
+                uint32_t *order_out, void *scratch, cudaStream_t st, int *launches) {
+    const int n = m_old + k;
+    char *p = (char *)scratch;
+    auto take = [&](size_t bytes) {
+        char *r = p;
+        p += (bytes + 255) & ~(size_t)255;
+        return (void *)r;
+    };
+    SortBuffers sb = sort_buffers(take(sort_scratch_bytes(k)), k);
+    int *fresh = (int *)take(sizeof(int) * (size_t)k);
+    int *small = (int *)take(2 * sizeof(int));  // n_fresh, k_old
+    int *part = (int *)take(sizeof(int) * scan_part_ints((size_t)k));
+    int nl = 0;
+    // the new points' keys (point indices m_old ...), stably sorted
+    cell_key_kernel<<<div_up(k, kThreads), kThreads, 0, st>>>(d_map + m_old, k, d_meta, sb.k0, sb.v0, m_old);
+    ++nl;
+    nl += radix_sort_pairs(sb, k, key_bits(meta_host), st);
+    // merged with the map's sorted pairs: the stable sort of all n points
+    merge_kernel<<<div_up(n, kThreads), kThreads, 0, st>>>(old_sorted.keys, old_sorted.order, m_old, sb.k0, sb.v0,
+                                                           k, keys_out, order_out);
+    // the touched cells: new slots in key order, records from all their points
+    append_mark_kernel<<<div_up(k, kThreads), kThreads, 0, st>>>(sb.k0, k, buf.slot_of, d_meta, fresh, small + 1);
+    nl += 2;
+    nl += scan_exclusive(fresh, k, small, part, st);
+    append_cells_kernel<<<div_up(k, 128), 128, 0, st>>>(d_map, sb.k0, k, keys_out, order_out, n, fresh, small, small + 1,
+                                                        opt.compat, opt.min_points, opt.eigen_ratio, d_meta, buf);
+    ++nl;
     if (launches) *launches += nl;
     return (int)cudaGetLastError();
 }

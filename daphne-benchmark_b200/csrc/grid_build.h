@@ -20,6 +20,7 @@ struct GridBuffers {
     int32_t *cell;       // slot -> dense cell id
     int32_t *seg_start;  // slot -> first position in the sorted order
     uint32_t *seg_cell;  // slot -> dense cell id (sort output)
+    int32_t *slot_of;    // G dense cell -> its slot, usable or not (-1 = no points)
 };
 
 struct NdtGridOptions {
@@ -60,6 +61,19 @@ struct SortBuffers {
 size_t sort_scratch_bytes(int n);
 SortBuffers sort_buffers(void *scratch, int n);
 int sort_segments(SortBuffers &b, int n, int bits, int32_t *seg_start, uint32_t *seg_key, cudaStream_t st);
+// The two halves: the radix passes alone (b.k0 / b.v0 sorted afterwards), and
+// the segments of sorted keys (segc: ceil(n / 2048) + 1 ints, part: the
+// multi-block scan's tile sums).
+int radix_sort_pairs(SortBuffers &b, int n, int bits, cudaStream_t st);
+int segment_sorted(const uint32_t *keys, int n, int *segc, int *nseg, int *part, int32_t *seg_start,
+                   uint32_t *seg_key, cudaStream_t st);
+
+// The map's points sorted by dense cell (key) and, within a cell, by point
+// index: what the last build or append left, the input of the next append.
+struct SortedMap {
+    const uint32_t *keys;
+    const uint32_t *order;
+};
 
 size_t grid_scratch_bytes(int m);
 // Zeroes the scratch's bounding-box counters (once, after the scratch is allocated).
@@ -69,8 +83,26 @@ int grid_scratch_init(void *scratch, cudaStream_t st);
 // size the dense index table).
 int grid_bbox(const float4 *d_map, int m, float res, GridMeta *d_meta, void *scratch, cudaStream_t st);
 
-// Phase 2: keys, stable sort, segments, per-voxel records.
+// Phase 2: keys, stable sort, segments, per-voxel records.  *sorted (optional)
+// receives the sorted (cell, point) pairs, which stay valid in the scratch
+// until the next build.
 int grid_build(const float4 *d_map, int m, const GridMeta &meta_host, GridMeta *d_meta, const NdtGridOptions &opt,
-               GridBuffers buf, void *scratch, cudaStream_t st, int *launches);
+               GridBuffers buf, void *scratch, cudaStream_t st, int *launches, SortedMap *sorted = nullptr);
+
+// Incremental map growth: the map's points [0, m_old) were built into the
+// grid (same meta: the appended points lie inside the old points' bounding
+// box) and sorted as old_sorted; points [m_old, m_old + k) of d_map are new.
+// Their keys are sorted and merged with old_sorted (old first on equal keys:
+// exactly the stable sort of all m_old + k points) into keys_out / order_out
+// (capacity m_old + k).  Only the cells the new points fall in are recomputed,
+// each from all its points in that order with the build's arithmetic, so the
+// records equal a full build's bit for bit; cells new to the grid take the
+// next slots (slot numbers may differ from a full build's; the records per
+// cell do not).  The record arrays must hold m_old + k slots with the old
+// slots kept.  Scratch: append_scratch_bytes(k).
+size_t append_scratch_bytes(int k);
+int grid_append(const float4 *d_map, int m_old, int k, const GridMeta &meta_host, GridMeta *d_meta,
+                const NdtGridOptions &opt, GridBuffers buf, SortedMap old_sorted, uint32_t *keys_out,
+                uint32_t *order_out, void *scratch, cudaStream_t st, int *launches);
 
 }  // namespace ndt

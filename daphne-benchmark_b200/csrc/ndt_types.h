@@ -36,6 +36,8 @@ enum Phase : int32_t {
 struct GridMeta {
     float minv[3];
     float maxv[3];
+    float raw_min[3];  // min / max of the map points themselves (minv = raw_min - 0.01f, maxv = raw_max + 0.01f)
+    float raw_max[3];
     int32_t dim[3];
     float res;
     int64_t G;         // dense cell count

@@ -86,6 +86,8 @@ def lib():
         L.ndt_last_error.restype = C.c_char_p
         L.ndt_set_map.argtypes = [ctxp, C.c_void_p, C.c_int]
         L.ndt_set_map_device.argtypes = [ctxp, C.c_void_p, C.c_int]
+        L.ndt_map_append.argtypes = [ctxp, C.c_void_p, C.c_int]
+        L.ndt_map_append_device.argtypes = [ctxp, C.c_void_p, C.c_int]
         L.ndt_align.argtypes = [ctxp, _f32p, C.c_int, _f32p, _f32p, C.POINTER(C.c_int), C.POINTER(C.c_double)]
         L.ndt_align_with_map.argtypes = [ctxp, _f32p, C.c_int, _f32p, _f32p, C.c_int, _f32p, C.POINTER(C.c_int),
                                          C.POINTER(C.c_double)]
@@ -109,7 +111,8 @@ def lib():
         L.ndt_grid_cells.argtypes = [ctxp, C.c_int, _i32p, _i32p, _f64p, _f64p]
         L.ndt_window_info.argtypes = [ctxp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
         L.ndt_derivatives.argtypes = [ctxp, _f32p, _f32p, C.c_int, _f64p, C.POINTER(C.c_double), _f64p, _f64p]
-        for name in ("ndt_create", "ndt_set_map", "ndt_set_map_device", "ndt_align", "ndt_align_with_map",
+        for name in ("ndt_create", "ndt_set_map", "ndt_set_map_device", "ndt_map_append", "ndt_map_append_device",
+                     "ndt_align", "ndt_align_with_map",
                      "ndt_align_batch", "ndt_align_batch_device", "ndt_synchronize", "ndt_get_counters",
                      "ndt_grid_info", "ndt_grid_cells", "ndt_derivatives", "ndt_align_batch_packed",
                      "ndt_set_profiling", "ndt_kernel_variants", "ndt_kernel_variant_shape",
@@ -199,6 +202,16 @@ class Context:
 
     def set_map_device(self, ptr: int, m: int):
         self._check(self.L.ndt_set_map_device(self.h, C.c_void_p(ptr), m), "ndt_set_map_device")
+
+    def map_append(self, points):
+        """Grows the map by `points` (host array); the grid then equals set_map of the grown map."""
+        points = _f32(points)
+        self._check(self.L.ndt_map_append(self.h, points.ctypes.data if len(points) else None, points.shape[0]),
+                    "ndt_map_append")
+
+    def map_append_device(self, ptr: int, k: int):
+        """Same, with the points on the device (raw pointer)."""
+        self._check(self.L.ndt_map_append_device(self.h, C.c_void_p(ptr), k), "ndt_map_append_device")
 
     def align(self, scan, guess):
         scan = _f32(scan)

@@ -99,6 +99,21 @@ NDT_API int ndt_set_map(ndt_ctx *ctx, const float *map, int m);
 NDT_API int ndt_set_map_device(ndt_ctx *ctx, const float *d_map, int m);
 
 /*
+ * Map growth (ndt_mapping's map grows by the aligned scans it appends; each
+ * reference test case carries its map, kernel.cpp:210-229).  Appends k points
+ * (HOST pointer, or DEVICE pointer for the _device form) to the current map;
+ * the grid afterwards is the one ndt_set_map builds for the whole grown map,
+ * bit for bit.  When the new points lie inside the bounding box of the map's
+ * points the update is incremental: the new points' cells are sorted and
+ * merged into the map's sorted cells and the voxel records recomputed, with no
+ * new sort of the whole map; otherwise the grid is rebuilt.  The context keeps
+ * its own copy of the grown map: after ndt_set_map_device the caller's map
+ * buffer must still hold the map when the first append is made.
+ */
+NDT_API int ndt_map_append(ndt_ctx *ctx, const float *points, int k);
+NDT_API int ndt_map_append_device(ndt_ctx *ctx, const float *d_points, int k);
+
+/*
  * One alignment with host buffers: the partial_points_callback call
  * (kernel.cpp:1405-1414) against the map set by ndt_set_map.
  * out16 = final transformation, *converged, *fitness (NDT score per point;
