@@ -864,6 +864,65 @@ def run_append(args, pkg, local):
     return 0
 
 
+def run_dat(args, pkg, local):
+    """The input file on the fast path: a c2-shaped ndt_input.dat (--dat-cases
+    test cases, each with its 8000-point scan, guess and the 400k-point map, as
+    the format stores it) written to a temporary directory, then (1) opened
+    (mmap + index + map comparison), (2) aligned with ndt_dat_align (chunks
+    that share a map, uploads by DMA from the registered mapping), against (3)
+    a case-by-case loop of ndt_set_map + ndt_align from the parsed arrays and
+    (4) parsing the file into arrays (numpy, datfile.read_input).  Wall clock,
+    file in the page cache; results of (2) and (3) are compared bit for bit."""
+    import shutil
+    import tempfile
+    import torch
+    torch.cuda.set_device(local)
+    synth = pkg.synth
+    cfg = synth.CONFIGS["c2"]
+    scene = synth.make_scene(cfg)
+    T = args.dat_cases
+    al = [synth.make_alignment(cfg, scene, i) for i in range(T)]
+    tmp = tempfile.mkdtemp(prefix="ndt_dat_")
+    try:
+        path = pathlib.Path(tmp) / "ndt_input.dat"
+        pkg.datfile.write_input(path, [(a.guess, a.scan, scene.map) for a in al])
+        size = path.stat().st_size
+        prm = pkg.ndt.reference_params(cfg.resolution)
+        ctx = pkg.ndt.Context(prm, device=local)
+        t0 = time.perf_counter()
+        cases = pkg.datfile.read_input(path)
+        t_parse = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        f = pkg.ndt.DatFile(path)
+        t_open = time.perf_counter() - t0
+        for _ in range(args.warmup):
+            out, conv, fit, status = f.align(ctx)
+        reps = max(1, args.steps)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            out, conv, fit, status = f.align(ctx)
+        t_align = (time.perf_counter() - t0) / reps
+        # case by case through the single-alignment call (the reference's run loop, kernel.cpp:1425-1429)
+        loop_out = np.zeros((T, 16), np.float32)
+        t0 = time.perf_counter()
+        for i, (g, sc, mp) in enumerate(cases):
+            ctx.set_map(mp)
+            loop_out[i] = ctx.align(sc, g)[0]
+        t_loop = time.perf_counter() - t0
+        same = bool(np.array_equal(loop_out.view(np.uint32), out.view(np.uint32)))
+        f.close()
+        ctx.close()
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    print(json.dumps({"workload": f"ndt_input.dat: {T} test cases of c2 (8000-point scan + 400000-point map each), "
+                                  f"{size / 1e6:.0f} MB, file in the page cache",
+                      "open_ms": t_open * 1e3, "open_gbs": size / t_open / 1e9,
+                      "dat_align_ms": t_align * 1e3, "dat_aligns_per_s": T / t_align,
+                      "case_loop_ms": t_loop * 1e3, "case_loop_aligns_per_s": T / t_loop,
+                      "numpy_parse_ms": t_parse * 1e3, "results_equal_case_loop": same}), flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -891,6 +950,8 @@ def main(argv=None):
     ap.add_argument("--filter", action="store_true", help="time the scan pre-filter (voxel-grid downsampling)")
     ap.add_argument("--append", action="store_true", help="time map growth (ndt_map_append) against rebuilds")
     ap.add_argument("--append-scans", type=int, default=32)
+    ap.add_argument("--dat", action="store_true", help="time the input-file fast path (ndt_dat_*)")
+    ap.add_argument("--dat-cases", type=int, default=64)
     ap.add_argument("--filter-scans", type=int, default=256)
     ap.add_argument("--filter-points", type=int, default=65536)
     args = ap.parse_args(argv)
@@ -906,6 +967,8 @@ def main(argv=None):
         return run_filter(args, pkg, local)
     if args.append and args.impl != "reference":
         return run_append(args, pkg, local)
+    if args.dat and args.impl != "reference":
+        return run_dat(args, pkg, local)
     if args.impl == "reference":
         return run_reference_arm(args, pkg, world, rank)
     return run_ours(args, pkg, world, rank, local)

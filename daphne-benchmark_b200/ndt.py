@@ -322,3 +322,82 @@ class Context:
         self._check(self.L.ndt_derivatives(self.h, scan, trans, scan.shape[0], np.ascontiguousarray(p6, np.float64),
                                            C.byref(score), g, H), "ndt_derivatives")
         return score.value, g, H.reshape(6, 6)
+
+
+class DatFile:
+    """An ndt_input.dat opened on the fast path (include/ndt_b200.h ndt_dat_*):
+    memory-mapped and indexed once; `case(i)` gives copies of a test case's
+    arrays, `relation(i)` how its map relates to the previous case's
+    (MAP_NEW / MAP_SAME / MAP_GROWN), `align(ctx, first, count)` runs the
+    cases through the library in chunks that share a map."""
+
+    MAP_NEW, MAP_SAME, MAP_GROWN = 0, 1, 2
+
+    def __init__(self, path):
+        self.L = lib()
+        L = self.L
+        if not getattr(L, "_dat_ready", False):
+            p = C.c_void_p
+            L.ndt_dat_open.argtypes = [C.c_char_p, C.POINTER(p)]
+            L.ndt_dat_close.argtypes = [p]
+            L.ndt_dat_close.restype = None
+            L.ndt_dat_last_error.argtypes = [p]
+            L.ndt_dat_last_error.restype = C.c_char_p
+            L.ndt_dat_count.argtypes = [p]
+            fp = C.POINTER(C.POINTER(C.c_float))
+            L.ndt_dat_case.argtypes = [p, C.c_int, fp, fp, C.POINTER(C.c_int), fp, C.POINTER(C.c_int)]
+            L.ndt_dat_map_relation.argtypes = [p, C.c_int]
+            L.ndt_dat_align.argtypes = [p, p, C.c_int, C.c_int, p, p, p, p]
+            for n in ("ndt_dat_open", "ndt_dat_count", "ndt_dat_case", "ndt_dat_map_relation", "ndt_dat_align"):
+                getattr(L, n).restype = C.c_int
+            L._dat_ready = True
+        h = C.c_void_p()
+        rc = L.ndt_dat_open(str(path).encode(), C.byref(h))
+        self.h = h
+        if rc != 0:
+            msg = L.ndt_dat_last_error(h).decode() if h else ""
+            self.close()
+            raise NdtError(f"ndt_dat_open: {ERRORS.get(rc, rc)}: {msg}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.ndt_dat_close(self.h)
+            self.h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __len__(self):
+        return self.L.ndt_dat_count(self.h)
+
+    def case(self, i):
+        g, sc, mp = (C.POINTER(C.c_float)(), C.POINTER(C.c_float)(), C.POINTER(C.c_float)())
+        n, m = C.c_int(), C.c_int()
+        if self.L.ndt_dat_case(self.h, i, C.byref(g), C.byref(sc), C.byref(n), C.byref(mp), C.byref(m)) != 0:
+            raise IndexError(i)
+        arr = lambda ptr, k: np.ctypeslib.as_array(ptr, (k,)).copy() if k else np.zeros(0, np.float32)
+        return arr(g, 16), arr(sc, 4 * n.value).reshape(-1, 4), arr(mp, 4 * m.value).reshape(-1, 4)
+
+    def relation(self, i):
+        return self.L.ndt_dat_map_relation(self.h, i)
+
+    def align(self, ctx, first=0, count=None):
+        count = len(self) - first if count is None else count
+        out = np.zeros((max(count, 1), 16), np.float32)
+        conv = np.zeros(max(count, 1), np.int32)
+        fit = np.zeros(max(count, 1), np.float64)
+        status = np.zeros(max(count, 1), np.int32)
+        rc = self.L.ndt_dat_align(ctx.h, self.h, first, count, out.ctypes.data, conv.ctypes.data, fit.ctypes.data,
+                                  status.ctypes.data)
+        if rc != 0:
+            raise NdtError(f"ndt_dat_align: {ERRORS.get(rc, rc)}: {self.L.ndt_dat_last_error(self.h).decode()}")
+        return out[:count], conv[:count], fit[:count], status[:count]

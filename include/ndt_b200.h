@@ -317,6 +317,37 @@ NDT_API int ndt_mlp_judge_device(ndt_mlp *mlp, int B, const float *d_prop16, con
                                  int *d_used);
 
 /*
+ * The input file on the fast path (replaces the reference's one-value-at-a-
+ * time reads of ndt_input.dat, parseInitGuess / parseFilteredScan,
+ * kernel.cpp:143-173, read_next_testcases :192-229; same format).
+ * ndt_dat_open maps the file read-only and indexes its test cases (a
+ * truncated or malformed file gives NDT_E_ARG; *out is set even then, so that
+ * ndt_dat_last_error can say why; close it with ndt_dat_close).
+ * ndt_dat_case returns pointers into the mapping (valid until close).
+ * ndt_dat_map_relation tells how case i's map relates to case i - 1's.
+ * ndt_dat_align aligns cases [first, first + count) as the reference's run
+ * loop would (each scan against its own case's map) and returns the results
+ * in case order: the mapping is registered with the driver, so scans and maps
+ * go to the device by asynchronous DMA from it; cases are aligned in chunks
+ * of cases that share a map, the next chunk's upload overlapping the current
+ * chunk's alignments; a map equal to the previous one reuses the grid, one
+ * that extends it grows the grid (ndt_map_append), any other is built.
+ */
+#define NDT_DAT_MAP_NEW 0    /* a map unlike the previous case's */
+#define NDT_DAT_MAP_SAME 1   /* byte-identical to the previous case's map */
+#define NDT_DAT_MAP_GROWN 2  /* the previous case's map followed by more points */
+typedef struct ndt_dat ndt_dat;
+NDT_API int ndt_dat_open(const char *path, ndt_dat **out);
+NDT_API void ndt_dat_close(ndt_dat *dat);
+NDT_API const char *ndt_dat_last_error(const ndt_dat *dat);
+NDT_API int ndt_dat_count(const ndt_dat *dat);
+NDT_API int ndt_dat_case(const ndt_dat *dat, int i, const float **guess16, const float **scan, int *n,
+                         const float **map, int *m);
+NDT_API int ndt_dat_map_relation(const ndt_dat *dat, int i);
+NDT_API int ndt_dat_align(ndt_ctx *ctx, ndt_dat *dat, int first, int count, float *out16, int *converged,
+                          double *fitness, int *status);
+
+/*
  * Scan pre-filter (no counterpart in the reference kernel: it is the
  * voxel-grid downsampling that produces the "filtered scan" inputs of the
  * align call upstream).  For each of B scans (d_points: float4 x, y, z,
