@@ -5,4 +5,4 @@ include/ndt_b200.h (`ndt`), the synthetic workload generator (`synth`) and the
 DAPHNE .dat format (`datfile`).  The compute path is the CUDA library built
 from csrc/ into _build/libndt_b200.so; there is no CPU fallback.
 """
-from . import autotune, datfile, learned, ndt, posenet, shard, synth, voxel_filter  # noqa: F401
+from . import autotune, datfile, ec, learned, ndt, posenet, shard, synth, voxel_filter  # noqa: F401

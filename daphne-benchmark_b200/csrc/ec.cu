@@ -1,0 +1,414 @@
+// Euclidean clustering on the GPU: the radius search and cluster extraction of
+// DAPHNE's euclidean_cluster kernel (extractEuclideanClusters / extract,
+// src/CPU/euclidean_cluster/kernel.cpp:562-647; its CUDA port builds an N x N
+// boolean distance matrix, src/Cuda/euclidean_cluster/kernel.cu:506-560), and
+// the host side of segmentByDistance / clusterAndColor (:652-814) around it.
+//
+// The reference grows each cluster breadth-first from its smallest
+// unprocessed point through all points whose float squared distance
+// dx*dx + dy*dy + dz*dz (each product and sum rounded) is <= r*r (float): the
+// clusters are the connected components of that graph, in order of their
+// smallest point index, each listed in ascending index order; those with
+// [min, max] points are kept and ordered by size with std::sort over reverse
+// iterators.
+//
+// Here: points are sorted into cells of edge r * (1 + 1e-4) (cell indices in
+// FP64, so an accepted pair is never more than one cell apart on any axis;
+// at most 2^28 cells per cloud) with the voxel-grid
+// build's stable radix sort; one thread per point tests the points of the 27
+// surrounding cells with the same float operations and joins accepted pairs
+// in a lock-free union-find whose roots are always the component's smallest
+// index (the larger root is linked under the smaller by atomicCAS); after a
+// final compression every label is its component's smallest index.  The host
+// groups the indices by label (ascending, so clusters come out in the
+// reference's order), filters by size and applies the same std::sort.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "../../include/ndt_b200.h"
+#include "grid_build.h"
+
+namespace ec {
+
+constexpr int kThreads = 256;
+constexpr int kUnionLimit = 1 << 20;  // CAS retries of one union (never reached in practice; flags an error)
+
+struct Geom {
+    float minv[3];
+    float cell;
+    int dim[3];
+};
+
+// Cell index in FP64 (the difference of two floats is exact there), so that
+// cell boundaries move by no more than ~1e-16 cells: with cells 1e-4 wider
+// than the radius, points of an accepted pair are at most one cell apart.
+__device__ __forceinline__ int cell_of(float v, float minv, float cell, int dim) {
+    int c = (int)(((double)v - (double)minv) / (double)cell);
+    return c < 0 ? 0 : (c >= dim ? dim - 1 : c);
+}
+
+__global__ void key_kernel(const float4 *__restrict__ pts, int n, Geom g, uint32_t *__restrict__ keys,
+                           uint32_t *__restrict__ vals, int *__restrict__ parent) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = pts[i];
+    const int cx = cell_of(p.x, g.minv[0], g.cell, g.dim[0]);
+    const int cy = cell_of(p.y, g.minv[1], g.cell, g.dim[1]);
+    const int cz = cell_of(p.z, g.minv[2], g.cell, g.dim[2]);
+    keys[i] = (uint32_t)(cx + g.dim[0] * (cy + g.dim[1] * cz));
+    vals[i] = (uint32_t)i;
+    parent[i] = i;
+}
+
+// cell -> first sorted position of its points (segment s), or -1
+__global__ void cell_index_kernel(const int32_t *__restrict__ seg_start, const uint32_t *__restrict__ seg_key,
+                                  const int *__restrict__ nseg, int *__restrict__ cell_first) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < *nseg) cell_first[seg_key[s]] = s;
+}
+
+__device__ __forceinline__ int find_root(int *parent, int x) {
+    for (int it = 0; it < kUnionLimit; ++it) {
+        const int p = atomicAdd(parent + x, 0);
+        if (p == x) return x;
+        const int gp = atomicAdd(parent + p, 0);
+        if (gp != p) atomicCAS(parent + x, p, gp);  // path halving (any interleaving keeps parents valid)
+        x = p;
+    }
+    return -1;
+}
+
+__device__ __forceinline__ void unite(int *parent, int a, int b, int *err) {
+    for (int it = 0; it < kUnionLimit; ++it) {
+        a = find_root(parent, a);
+        b = find_root(parent, b);
+        if (a < 0 || b < 0) break;
+        if (a == b) return;
+        if (a > b) {
+            const int t = a;
+            a = b;
+            b = t;
+        }
+        // link the larger root under the smaller: roots stay component minima
+        if (atomicCAS(parent + b, b, a) == b) return;
+    }
+    atomicOr(err, 1);
+}
+
+// One thread per point i (in sorted order, so a warp's points share cells):
+// the points j > i of the 27 surrounding cells within the radius.
+__global__ void join_kernel(const float4 *__restrict__ pts, const uint32_t *__restrict__ order,
+                            const uint32_t *__restrict__ keys, int n, const int32_t *__restrict__ seg_start,
+                            const int *__restrict__ nseg, const int *__restrict__ cell_first, Geom g, float r2,
+                            int *__restrict__ parent, int *__restrict__ err) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int i = (int)order[t];
+    const float4 p = pts[i];
+    const uint32_t key = keys[t];
+    const int cx = (int)(key % (uint32_t)g.dim[0]);
+    const int cy = (int)((key / (uint32_t)g.dim[0]) % (uint32_t)g.dim[1]);
+    const int cz = (int)(key / ((uint32_t)g.dim[0] * (uint32_t)g.dim[1]));
+    const int K = *nseg;
+    for (int dz = -1; dz <= 1; ++dz) {
+        const int z = cz + dz;
+        if (z < 0 || z >= g.dim[2]) continue;
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int y = cy + dy;
+            if (y < 0 || y >= g.dim[1]) continue;
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int x = cx + dx;
+                if (x < 0 || x >= g.dim[0]) continue;
+                const int s = cell_first[x + g.dim[0] * (y + g.dim[1] * z)];
+                if (s < 0) continue;
+                const int e = s + 1 < K ? seg_start[s + 1] : n;
+                for (int u = seg_start[s]; u < e; ++u) {
+                    const int j = (int)order[u];
+                    if (j <= i) continue;
+                    const float4 q = pts[j];
+                    const float ex = __fsub_rn(q.x, p.x), ey = __fsub_rn(q.y, p.y), ez = __fsub_rn(q.z, p.z);
+                    const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey)), __fmul_rn(ez, ez));
+                    if (d2 <= r2) unite(parent, i, j, err);
+                }
+            }
+        }
+    }
+}
+
+__global__ void label_kernel(int *__restrict__ parent, int n, int *__restrict__ err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int r = find_root(parent, i);
+    if (r < 0) atomicOr(err, 2);
+    parent[i] = r;
+}
+
+}  // namespace ec
+
+struct ndt_ec {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    void *pts = nullptr, *scratch = nullptr, *parent = nullptr, *seg_start = nullptr, *seg_key = nullptr,
+         *cell_first = nullptr, *flags = nullptr;
+    size_t pts_cap = 0, scratch_cap = 0, parent_cap = 0, seg_start_cap = 0, seg_key_cap = 0, cell_cap = 0;
+    float4 *h_pts = nullptr;  // pinned staging
+    int *h_labels = nullptr;
+    size_t h_cap = 0;
+};
+
+namespace {
+
+constexpr long long kMaxCells = 1LL << 28;  // dense cell table (4 B per cell) of one cloud, at most
+
+int fail(ndt_ec *h, int code, const std::string &msg) {
+    if (h) h->err = msg;
+    return code;
+}
+
+cudaError_t ensure(void **p, size_t *cap, size_t bytes) {
+    if (*p && *cap >= bytes) return cudaSuccess;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    const size_t want = std::max(bytes + bytes / 2, (size_t)256);
+    cudaError_t e = cudaMalloc(p, want);
+    if (e == cudaSuccess) *cap = want;
+    return e;
+}
+
+#define ECK(call)                                                                             \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) return fail(h, NDT_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// Component labels (smallest index of each point's component) of n points.
+int labels_of(ndt_ec *h, const float *xyz, int n, float tolerance, std::vector<int> &labels) {
+    labels.assign(n, 0);
+    if (n == 0) return NDT_OK;
+    cudaStream_t st = h->stream;
+    if (h->h_cap < (size_t)n) {
+        if (h->h_pts) cudaFreeHost(h->h_pts);
+        if (h->h_labels) cudaFreeHost(h->h_labels);
+        h->h_pts = nullptr;
+        h->h_labels = nullptr;
+        h->h_cap = 0;
+        const size_t want = (size_t)n + n / 2;
+        ECK(cudaMallocHost((void **)&h->h_pts, sizeof(float4) * want));
+        ECK(cudaMallocHost((void **)&h->h_labels, sizeof(int) * want));
+        h->h_cap = want;
+    }
+    float mn[3] = {std::numeric_limits<float>::max(), std::numeric_limits<float>::max(),
+                   std::numeric_limits<float>::max()};
+    float mx[3] = {-mn[0], -mn[1], -mn[2]};
+    for (int i = 0; i < n; ++i) {
+        const float *q = xyz + 3 * (size_t)i;
+        if (!std::isfinite(q[0]) || !std::isfinite(q[1]) || !std::isfinite(q[2]))
+            return fail(h, NDT_E_ARG, "non-finite point coordinates");
+        h->h_pts[i] = make_float4(q[0], q[1], q[2], 0.0f);
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = std::min(mn[k], q[k]);
+            mx[k] = std::max(mx[k], q[k]);
+        }
+    }
+    ec::Geom g;
+    g.cell = tolerance * 1.0001f;  // cells a little wider than the radius
+    long long G = 1;
+    for (int k = 0; k < 3; ++k) {
+        g.minv[k] = mn[k];
+        const double d = std::floor(((double)mx[k] - (double)mn[k]) / (double)g.cell) + 1.0;
+        if (!(d >= 1.0 && d < 2147483647.0)) return fail(h, NDT_E_CAPACITY, "the cloud spans too many cells");
+        g.dim[k] = (int)d;
+        G *= g.dim[k];
+    }
+    if (G > kMaxCells) return fail(h, NDT_E_CAPACITY, "the cloud spans more than 2^28 cells of the tolerance");
+    const float r2 = tolerance * tolerance;
+    int bits = 1;
+    while (bits < 31 && (1LL << bits) < G) ++bits;
+    ECK(ensure(&h->pts, &h->pts_cap, sizeof(float4) * (size_t)n));
+    ECK(ensure(&h->scratch, &h->scratch_cap, ndt::sort_scratch_bytes(n)));
+    ECK(ensure(&h->parent, &h->parent_cap, sizeof(int) * (size_t)n));
+    ECK(ensure(&h->seg_start, &h->seg_start_cap, sizeof(int) * (size_t)n));
+    ECK(ensure(&h->seg_key, &h->seg_key_cap, sizeof(int) * (size_t)n));
+    ECK(ensure(&h->cell_first, &h->cell_cap, sizeof(int) * (size_t)G));
+    size_t fcap = 0;
+    if (!h->flags) ECK(ensure(&h->flags, &fcap, 256));
+    float4 *d_pts = (float4 *)h->pts;
+    int *parent = (int *)h->parent, *err = (int *)h->flags;
+    ECK(cudaMemcpyAsync(d_pts, h->h_pts, sizeof(float4) * (size_t)n, cudaMemcpyHostToDevice, st));
+    ECK(cudaMemsetAsync(err, 0, sizeof(int), st));
+    ECK(cudaMemsetAsync(h->cell_first, 0xff, sizeof(int) * (size_t)G, st));
+    ndt::SortBuffers sb = ndt::sort_buffers(h->scratch, n);
+    const unsigned blocks = (unsigned)((n + ec::kThreads - 1) / ec::kThreads);
+    ec::key_kernel<<<blocks, ec::kThreads, 0, st>>>(d_pts, n, g, sb.k0, sb.v0, parent);
+    ndt::sort_segments(sb, n, bits, (int32_t *)h->seg_start, (uint32_t *)h->seg_key, st);
+    ec::cell_index_kernel<<<blocks, ec::kThreads, 0, st>>>((const int32_t *)h->seg_start, (const uint32_t *)h->seg_key,
+                                                           sb.nseg, (int *)h->cell_first);
+    ec::join_kernel<<<blocks, ec::kThreads, 0, st>>>(d_pts, sb.v0, sb.k0, n, (const int32_t *)h->seg_start, sb.nseg,
+                                                     (const int *)h->cell_first, g, r2, parent, err);
+    ec::label_kernel<<<blocks, ec::kThreads, 0, st>>>(parent, n, err);
+    ECK(cudaGetLastError());
+    ECK(cudaMemcpyAsync(h->h_labels, parent, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, st));
+    int e = 0;
+    ECK(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    ECK(cudaStreamSynchronize(st));
+    if (e) return fail(h, NDT_E_CUDA, "union-find retry limit reached");
+    std::memcpy(labels.data(), h->h_labels, sizeof(int) * (size_t)n);
+    return NDT_OK;
+}
+
+// The reference's clusters from component labels: components in order of
+// their smallest index, indices ascending, sizes in [lo, hi], then ordered by
+// size with std::sort over reverse iterators (extract, kernel.cpp:635-647).
+void clusters_of(const std::vector<int> &labels, int lo, int hi, std::vector<std::vector<int>> &out) {
+    const int n = (int)labels.size();
+    std::vector<int> size(n, 0), slot(n, -1);
+    for (int i = 0; i < n; ++i) ++size[labels[i]];
+    out.clear();
+    for (int i = 0; i < n; ++i)
+        if (labels[i] == i && size[i] >= lo && size[i] <= hi) {
+            slot[i] = (int)out.size();
+            out.emplace_back();
+            out.back().reserve(size[i]);
+        }
+    for (int i = 0; i < n; ++i)
+        if (slot[labels[i]] >= 0) out[slot[labels[i]]].push_back(i);
+    std::sort(out.rbegin(), out.rend(),
+              [](const std::vector<int> &a, const std::vector<int> &b) { return a.size() < b.size(); });
+}
+
+}  // namespace
+
+extern "C" {
+
+int ndt_ec_create(int device, ndt_ec **out) {
+    if (!out) return NDT_E_ARG;
+    *out = nullptr;
+    ndt_ec *h = new ndt_ec();
+    h->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete h;
+        return NDT_E_CUDA;
+    }
+    *out = h;
+    return NDT_OK;
+}
+
+void ndt_ec_destroy(ndt_ec *h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (void *p : {h->pts, h->scratch, h->parent, h->seg_start, h->seg_key, h->cell_first, h->flags})
+        if (p) cudaFree(p);
+    if (h->h_pts) cudaFreeHost(h->h_pts);
+    if (h->h_labels) cudaFreeHost(h->h_labels);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+const char *ndt_ec_last_error(const ndt_ec *h) { return h ? h->err.c_str() : "null handle"; }
+
+int ndt_ec_labels(ndt_ec *h, const float *xyz, int n, float tolerance, int *labels) {
+    if (!h || n < 0 || (n > 0 && (!xyz || !labels)) || !(tolerance > 0.0f) || !std::isfinite(tolerance))
+        return fail(h, NDT_E_ARG, "bad argument");
+    ECK(cudaSetDevice(h->device));
+    std::vector<int> lab;
+    if (int rc = labels_of(h, xyz, n, tolerance, lab)) return rc;
+    if (n) std::memcpy(labels, lab.data(), sizeof(int) * (size_t)n);
+    return NDT_OK;
+}
+
+int ndt_ec_extract(ndt_ec *h, const float *xyz, int n, float tolerance, int min_size, int max_size,
+                   int *num_clusters, int *cluster_offsets, int *cluster_indices) {
+    if (!h || n < 0 || (n > 0 && !xyz) || !num_clusters || !cluster_offsets || !cluster_indices ||
+        !(tolerance > 0.0f) || !std::isfinite(tolerance))
+        return fail(h, NDT_E_ARG, "bad argument");
+    ECK(cudaSetDevice(h->device));
+    std::vector<int> lab;
+    if (int rc = labels_of(h, xyz, n, tolerance, lab)) return rc;
+    std::vector<std::vector<int>> cl;
+    clusters_of(lab, min_size, max_size, cl);
+    int pos = 0;
+    cluster_offsets[0] = 0;
+    for (size_t c = 0; c < cl.size(); ++c) {
+        std::memcpy(cluster_indices + pos, cl[c].data(), sizeof(int) * cl[c].size());
+        pos += (int)cl[c].size();
+        cluster_offsets[c + 1] = pos;
+    }
+    *num_clusters = (int)cl.size();
+    return NDT_OK;
+}
+
+// segmentByDistance (kernel.cpp:767-814) with clusterAndColor (:652-765):
+// five rings of distance from the sensor (< 15, 30, 45, 60 m, beyond) with
+// tolerances 0.5, 1.1, 1.6, 2.3 and 2.6f, clusters of 20 to 100000 points.
+int ndt_ec_segment(ndt_ec *h, const float *xyz, int n, float *out_xyz, int *out_n, double *boxes, int *num_boxes,
+                   double *centroids, int *num_centroids) {
+    if (!h || n < 0 || (n > 0 && !xyz) || !out_xyz || !out_n || !boxes || !num_boxes || !centroids ||
+        !num_centroids)
+        return fail(h, NDT_E_ARG, "bad argument");
+    ECK(cudaSetDevice(h->device));
+    const double tol[5] = {0.5, 1.1, 1.6, 2.3, 2.6f};
+    std::vector<float> ring[5];
+    for (int i = 0; i < n; ++i) {
+        const float x = xyz[3 * (size_t)i], y = xyz[3 * (size_t)i + 1];
+        const float d = std::sqrt(x * x + y * y);
+        const int r = d < 15 ? 0 : (d < 30 ? 1 : (d < 45 ? 2 : (d < 60 ? 3 : 4)));
+        ring[r].insert(ring[r].end(), xyz + 3 * (size_t)i, xyz + 3 * (size_t)i + 3);
+    }
+    int np = 0, nb = 0, nc = 0;
+    std::vector<int> lab;
+    std::vector<std::vector<int>> cl;
+    for (int r = 0; r < 5; ++r) {
+        const std::vector<float> &c = ring[r];
+        const int m = (int)(c.size() / 3);
+        if (m == 0) continue;
+        if (int rc = labels_of(h, c.data(), m, (float)tol[r], lab)) return rc;
+        clusters_of(lab, 20, 100000, cl);
+        for (const std::vector<int> &idx : cl) {
+            double cen[3] = {0.0, 0.0, 0.0};
+            float lo[3] = {std::numeric_limits<float>::max(), std::numeric_limits<float>::max(),
+                           std::numeric_limits<float>::max()};
+            float hi[3] = {-lo[0], -lo[1], -lo[2]};
+            for (int i : idx) {
+                const float *p = &c[3 * (size_t)i];
+                for (int k = 0; k < 3; ++k) {
+                    out_xyz[3 * (size_t)np + k] = p[k];
+                    cen[k] += p[k];
+                    if (p[k] < lo[k]) lo[k] = p[k];
+                    if (p[k] > hi[k]) hi[k] = p[k];
+                }
+                ++np;
+            }
+            for (int k = 0; k < 3; ++k) cen[k] /= idx.size();
+            const float l = hi[0] - lo[0], w = hi[1] - lo[1], ht = hi[2] - lo[2];
+            const double dim[3] = {l < 0 ? -1 * l : l, w < 0 ? -1 * w : w, ht < 0 ? -1 * ht : ht};
+            if (dim[0] > 0 && dim[1] > 0 && dim[2] > 0 && dim[0] < 15 && dim[1] > 0 && dim[1] < 15 && hi[2] > -1.5 &&
+                lo[2] > -1.5 && lo[2] < 1.0) {
+                // position, orientation (x, y, z, w; the yaw is not estimated here: identity), dimensions
+                const double b[10] = {lo[0] + l / 2, lo[1] + w / 2, lo[2] + ht / 2, 0.0, 0.0, 0.0, 1.0,
+                                      dim[0], dim[1], dim[2]};
+                std::memcpy(boxes + 10 * (size_t)nb, b, sizeof(b));
+                ++nb;
+                std::memcpy(centroids + 3 * (size_t)nc, cen, sizeof(cen));
+                ++nc;
+            }
+        }
+    }
+    *out_n = np;
+    *num_boxes = nb;
+    *num_centroids = nc;
+    return NDT_OK;
+}
+
+}  // extern "C"

@@ -370,6 +370,37 @@ NDT_API void *ndt_filter_stream(ndt_filter *f);
 NDT_API int ndt_voxel_filter_device(ndt_filter *f, int B, const float *d_points, const int *d_offsets,
                                     int total_points, float leaf, float *d_out, int *d_out_offsets, int *out_total);
 
+/*
+ * Euclidean clustering (DAPHNE's euclidean_cluster kernel, whose radius
+ * search builds an N x N distance matrix: src/CPU/euclidean_cluster/
+ * kernel.cpp:512-647, CUDA port src/Cuda/euclidean_cluster/kernel.cu:506-560).
+ * xyz: n points, 3 floats each (HOST).  Two points are neighbours when the
+ * float dx*dx + dy*dy + dz*dz is <= tolerance * tolerance, as there; clusters
+ * are the connected components.  ndt_ec_labels gives each point the smallest
+ * index of its cluster.  ndt_ec_extract gives extract()'s clusters
+ * (:635-647): sizes in [min_size, max_size], ordered as the reference orders
+ * them, each point list ascending; cluster c is cluster_indices
+ * [cluster_offsets[c], cluster_offsets[c + 1]) (capacities: n + 1 and n).
+ * ndt_ec_segment runs segmentByDistance (:767-814): five distance rings with
+ * their tolerances, clusters of 20..100000 points, and returns the clustered
+ * points (out_xyz, capacity 3n floats; the reference colours them all
+ * r, g, b = 10, 20, 30), the boxes that pass the reference's size filter (10
+ * doubles each: position xyz, orientation xyzw, dimensions xyz; capacity 10n)
+ * and their centroids (3 doubles each; capacity 3n).  The box yaw (the
+ * reference's minimum-area-rectangle pose estimate) is not computed: the
+ * orientation is the identity.  NDT_E_CAPACITY when a cloud spans more than
+ * 2^28 cells of the tolerance.
+ */
+typedef struct ndt_ec ndt_ec;
+NDT_API int ndt_ec_create(int device, ndt_ec **out);
+NDT_API void ndt_ec_destroy(ndt_ec *ec);
+NDT_API const char *ndt_ec_last_error(const ndt_ec *ec);
+NDT_API int ndt_ec_labels(ndt_ec *ec, const float *xyz, int n, float tolerance, int *labels);
+NDT_API int ndt_ec_extract(ndt_ec *ec, const float *xyz, int n, float tolerance, int min_size, int max_size,
+                           int *num_clusters, int *cluster_offsets, int *cluster_indices);
+NDT_API int ndt_ec_segment(ndt_ec *ec, const float *xyz, int n, float *out_xyz, int *out_n, double *boxes,
+                           int *num_boxes, double *centroids, int *num_centroids);
+
 #ifdef __cplusplus
 }
 #endif
