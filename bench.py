@@ -923,6 +923,43 @@ def run_dat(args, pkg, local):
     return 0
 
 
+def run_ec(args, pkg, local):
+    """Euclidean clustering (segmentByDistance) on the reference's own five
+    point clouds (tests/golden/ec_cases.npz, ~10k points each): the GPU path
+    (ndt_ec_segment, host arrays in and out) against the reference kernel
+    compiled from its own source (oracle/_ref/libref_ec.so, one thread),
+    wall clock per cloud; outputs compared with the reference's rule."""
+    import torch
+    import ec_ref
+    torch.cuda.set_device(local)
+    gold = np.load(ROOT / "tests" / "golden" / "ec_cases.npz")
+    clouds = [gold[f"in{i}"] for i in range(int(gold["cases"]))]
+    h = pkg.ec.EuclideanClusters(local)
+    for _ in range(args.warmup):
+        for c in clouds:
+            h.segment(c)
+    reps = max(1, args.steps)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        outs = [h.segment(c) for c in clouds]
+    t_gpu = (time.perf_counter() - t0) / (reps * len(clouds))
+    line = {"workload": f"euclidean clustering: the reference's {len(clouds)} clouds "
+                        f"({min(map(len, clouds))}-{max(map(len, clouds))} points), 5 distance rings",
+            "gpu_ms_per_cloud": t_gpu * 1e3, "gpu_clouds_per_s": 1.0 / t_gpu}
+    if ec_ref.Reference.available():
+        ref = ec_ref.Reference()
+        t0 = time.perf_counter()
+        refs = [ref.segment(c) for c in clouds]
+        t_ref = (time.perf_counter() - t0) / len(clouds)
+        ok = all(ec_ref.check(o[0], ec_ref.boxes10_to_8(o[1]), o[2], r[0], ec_ref.boxes10_to_8(r[1]), r[2])[0]
+                 for o, r in zip(outs, refs))
+        line.update({"reference_ms_per_cloud": t_ref * 1e3, "speedup": t_ref / t_gpu, "reference_rule_passed": ok,
+                     "reference": "src/CPU/euclidean_cluster compiled from its own source, 1 thread"})
+    print(json.dumps(line), flush=True)
+    h.close()
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -952,6 +989,7 @@ def main(argv=None):
     ap.add_argument("--append-scans", type=int, default=32)
     ap.add_argument("--dat", action="store_true", help="time the input-file fast path (ndt_dat_*)")
     ap.add_argument("--dat-cases", type=int, default=64)
+    ap.add_argument("--ec", action="store_true", help="time euclidean clustering on the reference's clouds")
     ap.add_argument("--filter-scans", type=int, default=256)
     ap.add_argument("--filter-points", type=int, default=65536)
     args = ap.parse_args(argv)
@@ -969,6 +1007,8 @@ def main(argv=None):
         return run_append(args, pkg, local)
     if args.dat and args.impl != "reference":
         return run_dat(args, pkg, local)
+    if args.ec and args.impl != "reference":
+        return run_ec(args, pkg, local)
     if args.impl == "reference":
         return run_reference_arm(args, pkg, world, rank)
     return run_ours(args, pkg, world, rank, local)

@@ -15,8 +15,8 @@
 // Here: points are sorted into cells of edge r * (1 + 1e-4) (cell indices in
 // FP64, so an accepted pair is never more than one cell apart on any axis;
 // at most 2^28 cells per cloud) with the voxel-grid
-// build's stable radix sort; one thread per point tests the points of the 27
-// surrounding cells with the same float operations and joins accepted pairs
+// build's stable radix sort; one thread per point and neighbour cell tests
+// that cell's points with the same float operations and joins accepted pairs
 // in a lock-free union-find whose roots are always the component's smallest
 // index (the larger root is linked under the smaller by atomicCAS); after a
 // final compression every label is its component's smallest index.  The host
@@ -74,70 +74,69 @@ __global__ void cell_index_kernel(const int32_t *__restrict__ seg_start, const u
     if (s < *nseg) cell_first[seg_key[s]] = s;
 }
 
+// Union-find over parent[] with parent[v] <= v for every v (a root links
+// under a smaller one only), so every chain strictly decreases and a root is
+// its component's smallest index.  Reads are volatile (other threads link and
+// shorten concurrently); path halving stores a valid ancestor, so any
+// interleaving keeps the invariant.
 __device__ __forceinline__ int find_root(int *parent, int x) {
+    volatile int *p = parent;
     for (int it = 0; it < kUnionLimit; ++it) {
-        const int p = atomicAdd(parent + x, 0);
-        if (p == x) return x;
-        const int gp = atomicAdd(parent + p, 0);
-        if (gp != p) atomicCAS(parent + x, p, gp);  // path halving (any interleaving keeps parents valid)
-        x = p;
+        const int up = p[x];
+        if (up == x) return x;
+        const int up2 = p[up];
+        if (up2 != up) p[x] = up2;
+        x = up;
     }
     return -1;
 }
 
-__device__ __forceinline__ void unite(int *parent, int a, int b, int *err) {
-    for (int it = 0; it < kUnionLimit; ++it) {
-        a = find_root(parent, a);
-        b = find_root(parent, b);
-        if (a < 0 || b < 0) break;
-        if (a == b) return;
-        if (a > b) {
-            const int t = a;
-            a = b;
-            b = t;
-        }
-        // link the larger root under the smaller: roots stay component minima
-        if (atomicCAS(parent + b, b, a) == b) return;
-    }
-    atomicOr(err, 1);
-}
-
-// One thread per point i (in sorted order, so a warp's points share cells):
-// the points j > i of the 27 surrounding cells within the radius.
+// One thread per (point i, neighbour cell): blockIdx.y picks the cell offset
+// (27 of them), x walks the points in sorted order, so a warp's points share
+// cells and read the same neighbours.  The thread tests the points j > i of
+// its cell; i's root is found at the first accepted pair and kept; a pair
+// whose roots already agree costs the reads of j's chain, a merge one
+// atomicCAS (the larger root under the smaller).
 __global__ void join_kernel(const float4 *__restrict__ pts, const uint32_t *__restrict__ order,
                             const uint32_t *__restrict__ keys, int n, const int32_t *__restrict__ seg_start,
                             const int *__restrict__ nseg, const int *__restrict__ cell_first, Geom g, float r2,
                             int *__restrict__ parent, int *__restrict__ err) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
+    const int off = blockIdx.y;  // 9 dz + 3 dy + dx, each in {0, 1, 2}
+    const uint32_t key = keys[t];
+    const int x = (int)(key % (uint32_t)g.dim[0]) + off % 3 - 1;
+    const int y = (int)((key / (uint32_t)g.dim[0]) % (uint32_t)g.dim[1]) + (off / 3) % 3 - 1;
+    const int z = (int)(key / ((uint32_t)g.dim[0] * (uint32_t)g.dim[1])) + off / 9 - 1;
+    if (x < 0 || x >= g.dim[0] || y < 0 || y >= g.dim[1] || z < 0 || z >= g.dim[2]) return;
+    const int s = cell_first[x + g.dim[0] * (y + g.dim[1] * z)];
+    if (s < 0) return;
     const int i = (int)order[t];
     const float4 p = pts[i];
-    const uint32_t key = keys[t];
-    const int cx = (int)(key % (uint32_t)g.dim[0]);
-    const int cy = (int)((key / (uint32_t)g.dim[0]) % (uint32_t)g.dim[1]);
-    const int cz = (int)(key / ((uint32_t)g.dim[0] * (uint32_t)g.dim[1]));
-    const int K = *nseg;
-    for (int dz = -1; dz <= 1; ++dz) {
-        const int z = cz + dz;
-        if (z < 0 || z >= g.dim[2]) continue;
-        for (int dy = -1; dy <= 1; ++dy) {
-            const int y = cy + dy;
-            if (y < 0 || y >= g.dim[1]) continue;
-            for (int dx = -1; dx <= 1; ++dx) {
-                const int x = cx + dx;
-                if (x < 0 || x >= g.dim[0]) continue;
-                const int s = cell_first[x + g.dim[0] * (y + g.dim[1] * z)];
-                if (s < 0) continue;
-                const int e = s + 1 < K ? seg_start[s + 1] : n;
-                for (int u = seg_start[s]; u < e; ++u) {
-                    const int j = (int)order[u];
-                    if (j <= i) continue;
-                    const float4 q = pts[j];
-                    const float ex = __fsub_rn(q.x, p.x), ey = __fsub_rn(q.y, p.y), ez = __fsub_rn(q.z, p.z);
-                    const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey)), __fmul_rn(ez, ez));
-                    if (d2 <= r2) unite(parent, i, j, err);
-                }
+    const int e = s + 1 < *nseg ? seg_start[s + 1] : n;
+    int ri = -2;  // not looked up yet
+    for (int u = seg_start[s]; u < e; ++u) {
+        const int j = (int)order[u];
+        if (j <= i) continue;
+        const float4 q = pts[j];
+        const float ex = __fsub_rn(q.x, p.x), ey = __fsub_rn(q.y, p.y), ez = __fsub_rn(q.z, p.z);
+        const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey)), __fmul_rn(ez, ez));
+        if (!(d2 <= r2)) continue;
+        if (ri == -2) ri = find_root(parent, i);
+        int rj = find_root(parent, j);
+        int it = 0;
+        for (; it < kUnionLimit && ri >= 0 && rj >= 0 && ri != rj; ++it) {
+            const int lo = ri < rj ? ri : rj, hi = ri < rj ? rj : ri;
+            if (atomicCAS(parent + hi, hi, lo) == hi) {
+                ri = lo;
+                break;
             }
+            ri = find_root(parent, ri);  // hi was linked meanwhile
+            rj = find_root(parent, rj);
+        }
+        if (ri < 0 || rj < 0 || it == kUnionLimit) {
+            atomicOr(err, 1);
+            return;
         }
     }
 }
@@ -252,8 +251,8 @@ int labels_of(ndt_ec *h, const float *xyz, int n, float tolerance, std::vector<i
     ndt::sort_segments(sb, n, bits, (int32_t *)h->seg_start, (uint32_t *)h->seg_key, st);
     ec::cell_index_kernel<<<blocks, ec::kThreads, 0, st>>>((const int32_t *)h->seg_start, (const uint32_t *)h->seg_key,
                                                            sb.nseg, (int *)h->cell_first);
-    ec::join_kernel<<<blocks, ec::kThreads, 0, st>>>(d_pts, sb.v0, sb.k0, n, (const int32_t *)h->seg_start, sb.nseg,
-                                                     (const int *)h->cell_first, g, r2, parent, err);
+    ec::join_kernel<<<dim3(blocks, 27), ec::kThreads, 0, st>>>(d_pts, sb.v0, sb.k0, n, (const int32_t *)h->seg_start,
+                                                               sb.nseg, (const int *)h->cell_first, g, r2, parent, err);
     ec::label_kernel<<<blocks, ec::kThreads, 0, st>>>(parent, n, err);
     ECK(cudaGetLastError());
     ECK(cudaMemcpyAsync(h->h_labels, parent, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, st));
