@@ -40,10 +40,19 @@ namespace ec {
 constexpr int kThreads = 256;
 constexpr int kUnionLimit = 1 << 20;  // CAS retries of one union (never reached in practice; flags an error)
 
-struct Geom {
-    float minv[3];
-    float cell;
-    int dim[3];
+constexpr int kMaxParts = 8;  // clouds clustered in one pass (segmentByDistance: its 5 rings)
+
+// Geometry of the clouds of one pass: part p's points are [off[p], off[p + 1])
+// of the concatenation, its cells have edge cell[p] from minv[p] with dims
+// dim[p], and its cell keys are base[p] + x + dx (y + dy z).
+struct Parts {
+    int np;
+    int off[kMaxParts + 1];
+    long long base[kMaxParts + 1];
+    float minv[kMaxParts][3];
+    float cell[kMaxParts];
+    float r2[kMaxParts];
+    int dim[kMaxParts][3];
 };
 
 // Cell index in FP64 (the difference of two floats is exact there), so that
@@ -54,15 +63,24 @@ __device__ __forceinline__ int cell_of(float v, float minv, float cell, int dim)
     return c < 0 ? 0 : (c >= dim ? dim - 1 : c);
 }
 
-__global__ void key_kernel(const float4 *__restrict__ pts, int n, Geom g, uint32_t *__restrict__ keys,
-                           uint32_t *__restrict__ vals, int *__restrict__ parent) {
+// The part of point t (or of key k): the last p with first[p] <= t.
+template <class T>
+__device__ __forceinline__ int part_of(const T *first, int np, long long t) {
+    int p = 0;
+    while (p + 1 < np && (long long)first[p + 1] <= t) ++p;
+    return p;
+}
+
+__global__ void key_kernel(const float4 *__restrict__ pts, int n, const __grid_constant__ Parts P,
+                           uint32_t *__restrict__ keys, uint32_t *__restrict__ vals, int *__restrict__ parent) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const int q = part_of(P.off, P.np, i);
     const float4 p = pts[i];
-    const int cx = cell_of(p.x, g.minv[0], g.cell, g.dim[0]);
-    const int cy = cell_of(p.y, g.minv[1], g.cell, g.dim[1]);
-    const int cz = cell_of(p.z, g.minv[2], g.cell, g.dim[2]);
-    keys[i] = (uint32_t)(cx + g.dim[0] * (cy + g.dim[1] * cz));
+    const int cx = cell_of(p.x, P.minv[q][0], P.cell[q], P.dim[q][0]);
+    const int cy = cell_of(p.y, P.minv[q][1], P.cell[q], P.dim[q][1]);
+    const int cz = cell_of(p.z, P.minv[q][2], P.cell[q], P.dim[q][2]);
+    keys[i] = (uint32_t)(P.base[q] + cx + (long long)P.dim[q][0] * (cy + (long long)P.dim[q][1] * cz));
     vals[i] = (uint32_t)i;
     parent[i] = i;
 }
@@ -94,32 +112,36 @@ __device__ __forceinline__ int find_root(int *parent, int x) {
 // One thread per (point i, neighbour cell): blockIdx.y picks the cell offset
 // (27 of them), x walks the points in sorted order, so a warp's points share
 // cells and read the same neighbours.  The thread tests the points j > i of
-// its cell; i's root is found at the first accepted pair and kept; a pair
-// whose roots already agree costs the reads of j's chain, a merge one
-// atomicCAS (the larger root under the smaller).
+// its cell (cells never cross parts); i's root is found at the first accepted
+// pair and kept; a pair whose roots already agree costs the reads of j's
+// chain, a merge one atomicCAS (the larger root under the smaller).
 __global__ void join_kernel(const float4 *__restrict__ pts, const uint32_t *__restrict__ order,
                             const uint32_t *__restrict__ keys, int n, const int32_t *__restrict__ seg_start,
-                            const int *__restrict__ nseg, const int *__restrict__ cell_first, Geom g, float r2,
-                            int *__restrict__ parent, int *__restrict__ err) {
+                            const int *__restrict__ nseg, const int *__restrict__ cell_first,
+                            const __grid_constant__ Parts P, int *__restrict__ parent, int *__restrict__ err) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     const int off = blockIdx.y;  // 9 dz + 3 dy + dx, each in {0, 1, 2}
-    const uint32_t key = keys[t];
-    const int x = (int)(key % (uint32_t)g.dim[0]) + off % 3 - 1;
-    const int y = (int)((key / (uint32_t)g.dim[0]) % (uint32_t)g.dim[1]) + (off / 3) % 3 - 1;
-    const int z = (int)(key / ((uint32_t)g.dim[0] * (uint32_t)g.dim[1])) + off / 9 - 1;
-    if (x < 0 || x >= g.dim[0] || y < 0 || y >= g.dim[1] || z < 0 || z >= g.dim[2]) return;
-    const int s = cell_first[x + g.dim[0] * (y + g.dim[1] * z)];
+    const long long key = keys[t];
+    const int q = part_of(P.base, P.np, key);
+    const long long local = key - P.base[q];
+    const int dx0 = P.dim[q][0], dy0 = P.dim[q][1], dz0 = P.dim[q][2];
+    const int x = (int)(local % dx0) + off % 3 - 1;
+    const int y = (int)((local / dx0) % dy0) + (off / 3) % 3 - 1;
+    const int z = (int)(local / ((long long)dx0 * dy0)) + off / 9 - 1;
+    if (x < 0 || x >= dx0 || y < 0 || y >= dy0 || z < 0 || z >= dz0) return;
+    const int s = cell_first[P.base[q] + x + (long long)dx0 * (y + (long long)dy0 * z)];
     if (s < 0) return;
     const int i = (int)order[t];
     const float4 p = pts[i];
+    const float r2 = P.r2[q];
     const int e = s + 1 < *nseg ? seg_start[s + 1] : n;
     int ri = -2;  // not looked up yet
     for (int u = seg_start[s]; u < e; ++u) {
         const int j = (int)order[u];
         if (j <= i) continue;
-        const float4 q = pts[j];
-        const float ex = __fsub_rn(q.x, p.x), ey = __fsub_rn(q.y, p.y), ez = __fsub_rn(q.z, p.z);
+        const float4 qj = pts[j];
+        const float ex = __fsub_rn(qj.x, p.x), ey = __fsub_rn(qj.y, p.y), ez = __fsub_rn(qj.z, p.z);
         const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey)), __fmul_rn(ez, ez));
         if (!(d2 <= r2)) continue;
         if (ri == -2) ri = find_root(parent, i);
@@ -189,78 +211,98 @@ cudaError_t ensure(void **p, size_t *cap, size_t bytes) {
         if (e_ != cudaSuccess) return fail(h, NDT_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-// Component labels (smallest index of each point's component) of n points.
-int labels_of(ndt_ec *h, const float *xyz, int n, float tolerance, std::vector<int> &labels) {
-    labels.assign(n, 0);
-    if (n == 0) return NDT_OK;
+// Component labels of up to kMaxParts clouds in one pass: labels[p][i] is the
+// smallest index within cloud p of point i's component (clouds never join).
+int labels_of(ndt_ec *h, const std::vector<const float *> &xyz, const std::vector<int> &n,
+              const std::vector<float> &tolerance, std::vector<std::vector<int>> &labels) {
+    const int np = (int)xyz.size();
+    labels.assign(np, std::vector<int>());
+    ec::Parts P;
+    std::memset(&P, 0, sizeof(P));
+    P.np = np;
+    long long total = 0, cells = 0;
+    for (int q = 0; q < np; ++q) {
+        P.off[q] = (int)total;
+        P.base[q] = cells;
+        total += n[q];
+        labels[q].assign(n[q], 0);
+        float mn[3] = {0.0f, 0.0f, 0.0f}, mx[3] = {0.0f, 0.0f, 0.0f};
+        for (int i = 0; i < n[q]; ++i) {
+            const float *v = xyz[q] + 3 * (size_t)i;
+            if (!std::isfinite(v[0]) || !std::isfinite(v[1]) || !std::isfinite(v[2]))
+                return fail(h, NDT_E_ARG, "non-finite point coordinates");
+            for (int k = 0; k < 3; ++k) {
+                mn[k] = i ? std::min(mn[k], v[k]) : v[k];
+                mx[k] = i ? std::max(mx[k], v[k]) : v[k];
+            }
+        }
+        P.cell[q] = tolerance[q] * 1.0001f;  // cells a little wider than the radius
+        P.r2[q] = tolerance[q] * tolerance[q];
+        long long G = 1;
+        for (int k = 0; k < 3; ++k) {
+            P.minv[q][k] = mn[k];
+            const double d = std::floor(((double)mx[k] - (double)mn[k]) / (double)P.cell[q]) + 1.0;
+            if (!(d >= 1.0 && d < 2147483647.0)) return fail(h, NDT_E_CAPACITY, "a cloud spans too many cells");
+            P.dim[q][k] = (int)d;
+            G *= P.dim[q][k];
+            if (G > kMaxCells) break;
+        }
+        cells += n[q] ? G : 0;
+        if (cells > kMaxCells) return fail(h, NDT_E_CAPACITY, "the clouds span more than 2^28 cells of the tolerance");
+    }
+    P.off[np] = (int)total;
+    P.base[np] = cells;
+    const int N = (int)total;
+    if (N == 0) return NDT_OK;
     cudaStream_t st = h->stream;
-    if (h->h_cap < (size_t)n) {
+    if (h->h_cap < (size_t)N) {
         if (h->h_pts) cudaFreeHost(h->h_pts);
         if (h->h_labels) cudaFreeHost(h->h_labels);
         h->h_pts = nullptr;
         h->h_labels = nullptr;
         h->h_cap = 0;
-        const size_t want = (size_t)n + n / 2;
+        const size_t want = (size_t)N + N / 2;
         ECK(cudaMallocHost((void **)&h->h_pts, sizeof(float4) * want));
         ECK(cudaMallocHost((void **)&h->h_labels, sizeof(int) * want));
         h->h_cap = want;
     }
-    float mn[3] = {std::numeric_limits<float>::max(), std::numeric_limits<float>::max(),
-                   std::numeric_limits<float>::max()};
-    float mx[3] = {-mn[0], -mn[1], -mn[2]};
-    for (int i = 0; i < n; ++i) {
-        const float *q = xyz + 3 * (size_t)i;
-        if (!std::isfinite(q[0]) || !std::isfinite(q[1]) || !std::isfinite(q[2]))
-            return fail(h, NDT_E_ARG, "non-finite point coordinates");
-        h->h_pts[i] = make_float4(q[0], q[1], q[2], 0.0f);
-        for (int k = 0; k < 3; ++k) {
-            mn[k] = std::min(mn[k], q[k]);
-            mx[k] = std::max(mx[k], q[k]);
+    for (int q = 0; q < np; ++q)
+        for (int i = 0; i < n[q]; ++i) {
+            const float *v = xyz[q] + 3 * (size_t)i;
+            h->h_pts[P.off[q] + i] = make_float4(v[0], v[1], v[2], 0.0f);
         }
-    }
-    ec::Geom g;
-    g.cell = tolerance * 1.0001f;  // cells a little wider than the radius
-    long long G = 1;
-    for (int k = 0; k < 3; ++k) {
-        g.minv[k] = mn[k];
-        const double d = std::floor(((double)mx[k] - (double)mn[k]) / (double)g.cell) + 1.0;
-        if (!(d >= 1.0 && d < 2147483647.0)) return fail(h, NDT_E_CAPACITY, "the cloud spans too many cells");
-        g.dim[k] = (int)d;
-        G *= g.dim[k];
-    }
-    if (G > kMaxCells) return fail(h, NDT_E_CAPACITY, "the cloud spans more than 2^28 cells of the tolerance");
-    const float r2 = tolerance * tolerance;
     int bits = 1;
-    while (bits < 31 && (1LL << bits) < G) ++bits;
-    ECK(ensure(&h->pts, &h->pts_cap, sizeof(float4) * (size_t)n));
-    ECK(ensure(&h->scratch, &h->scratch_cap, ndt::sort_scratch_bytes(n)));
-    ECK(ensure(&h->parent, &h->parent_cap, sizeof(int) * (size_t)n));
-    ECK(ensure(&h->seg_start, &h->seg_start_cap, sizeof(int) * (size_t)n));
-    ECK(ensure(&h->seg_key, &h->seg_key_cap, sizeof(int) * (size_t)n));
-    ECK(ensure(&h->cell_first, &h->cell_cap, sizeof(int) * (size_t)G));
+    while (bits < 31 && (1LL << bits) < cells) ++bits;
+    ECK(ensure(&h->pts, &h->pts_cap, sizeof(float4) * (size_t)N));
+    ECK(ensure(&h->scratch, &h->scratch_cap, ndt::sort_scratch_bytes(N)));
+    ECK(ensure(&h->parent, &h->parent_cap, sizeof(int) * (size_t)N));
+    ECK(ensure(&h->seg_start, &h->seg_start_cap, sizeof(int) * (size_t)N));
+    ECK(ensure(&h->seg_key, &h->seg_key_cap, sizeof(int) * (size_t)N));
+    ECK(ensure(&h->cell_first, &h->cell_cap, sizeof(int) * (size_t)cells));
     size_t fcap = 0;
     if (!h->flags) ECK(ensure(&h->flags, &fcap, 256));
     float4 *d_pts = (float4 *)h->pts;
     int *parent = (int *)h->parent, *err = (int *)h->flags;
-    ECK(cudaMemcpyAsync(d_pts, h->h_pts, sizeof(float4) * (size_t)n, cudaMemcpyHostToDevice, st));
+    ECK(cudaMemcpyAsync(d_pts, h->h_pts, sizeof(float4) * (size_t)N, cudaMemcpyHostToDevice, st));
     ECK(cudaMemsetAsync(err, 0, sizeof(int), st));
-    ECK(cudaMemsetAsync(h->cell_first, 0xff, sizeof(int) * (size_t)G, st));
-    ndt::SortBuffers sb = ndt::sort_buffers(h->scratch, n);
-    const unsigned blocks = (unsigned)((n + ec::kThreads - 1) / ec::kThreads);
-    ec::key_kernel<<<blocks, ec::kThreads, 0, st>>>(d_pts, n, g, sb.k0, sb.v0, parent);
-    ndt::sort_segments(sb, n, bits, (int32_t *)h->seg_start, (uint32_t *)h->seg_key, st);
+    ECK(cudaMemsetAsync(h->cell_first, 0xff, sizeof(int) * (size_t)cells, st));
+    ndt::SortBuffers sb = ndt::sort_buffers(h->scratch, N);
+    const unsigned blocks = (unsigned)((N + ec::kThreads - 1) / ec::kThreads);
+    ec::key_kernel<<<blocks, ec::kThreads, 0, st>>>(d_pts, N, P, sb.k0, sb.v0, parent);
+    ndt::sort_segments(sb, N, bits, (int32_t *)h->seg_start, (uint32_t *)h->seg_key, st);
     ec::cell_index_kernel<<<blocks, ec::kThreads, 0, st>>>((const int32_t *)h->seg_start, (const uint32_t *)h->seg_key,
                                                            sb.nseg, (int *)h->cell_first);
-    ec::join_kernel<<<dim3(blocks, 27), ec::kThreads, 0, st>>>(d_pts, sb.v0, sb.k0, n, (const int32_t *)h->seg_start,
-                                                               sb.nseg, (const int *)h->cell_first, g, r2, parent, err);
-    ec::label_kernel<<<blocks, ec::kThreads, 0, st>>>(parent, n, err);
+    ec::join_kernel<<<dim3(blocks, 27), ec::kThreads, 0, st>>>(d_pts, sb.v0, sb.k0, N, (const int32_t *)h->seg_start,
+                                                               sb.nseg, (const int *)h->cell_first, P, parent, err);
+    ec::label_kernel<<<blocks, ec::kThreads, 0, st>>>(parent, N, err);
     ECK(cudaGetLastError());
-    ECK(cudaMemcpyAsync(h->h_labels, parent, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, st));
+    ECK(cudaMemcpyAsync(h->h_labels, parent, sizeof(int) * (size_t)N, cudaMemcpyDeviceToHost, st));
     int e = 0;
     ECK(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
     ECK(cudaStreamSynchronize(st));
     if (e) return fail(h, NDT_E_CUDA, "union-find retry limit reached");
-    std::memcpy(labels.data(), h->h_labels, sizeof(int) * (size_t)n);
+    for (int q = 0; q < np; ++q)
+        for (int i = 0; i < n[q]; ++i) labels[q][i] = h->h_labels[P.off[q] + i] - P.off[q];
     return NDT_OK;
 }
 
@@ -321,9 +363,9 @@ int ndt_ec_labels(ndt_ec *h, const float *xyz, int n, float tolerance, int *labe
     if (!h || n < 0 || (n > 0 && (!xyz || !labels)) || !(tolerance > 0.0f) || !std::isfinite(tolerance))
         return fail(h, NDT_E_ARG, "bad argument");
     ECK(cudaSetDevice(h->device));
-    std::vector<int> lab;
-    if (int rc = labels_of(h, xyz, n, tolerance, lab)) return rc;
-    if (n) std::memcpy(labels, lab.data(), sizeof(int) * (size_t)n);
+    std::vector<std::vector<int>> lab;
+    if (int rc = labels_of(h, {xyz}, {n}, {tolerance}, lab)) return rc;
+    if (n) std::memcpy(labels, lab[0].data(), sizeof(int) * (size_t)n);
     return NDT_OK;
 }
 
@@ -333,10 +375,10 @@ int ndt_ec_extract(ndt_ec *h, const float *xyz, int n, float tolerance, int min_
         !(tolerance > 0.0f) || !std::isfinite(tolerance))
         return fail(h, NDT_E_ARG, "bad argument");
     ECK(cudaSetDevice(h->device));
-    std::vector<int> lab;
-    if (int rc = labels_of(h, xyz, n, tolerance, lab)) return rc;
+    std::vector<std::vector<int>> lab;
+    if (int rc = labels_of(h, {xyz}, {n}, {tolerance}, lab)) return rc;
     std::vector<std::vector<int>> cl;
-    clusters_of(lab, min_size, max_size, cl);
+    clusters_of(lab[0], min_size, max_size, cl);
     int pos = 0;
     cluster_offsets[0] = 0;
     for (size_t c = 0; c < cl.size(); ++c) {
@@ -366,14 +408,21 @@ int ndt_ec_segment(ndt_ec *h, const float *xyz, int n, float *out_xyz, int *out_
         ring[r].insert(ring[r].end(), xyz + 3 * (size_t)i, xyz + 3 * (size_t)i + 3);
     }
     int np = 0, nb = 0, nc = 0;
-    std::vector<int> lab;
+    std::vector<const float *> parts;
+    std::vector<int> sizes;
+    std::vector<float> tols;
+    for (int r = 0; r < 5; ++r) {
+        parts.push_back(ring[r].data());
+        sizes.push_back((int)(ring[r].size() / 3));
+        tols.push_back((float)tol[r]);
+    }
+    std::vector<std::vector<int>> lab;
+    if (int rc = labels_of(h, parts, sizes, tols, lab)) return rc;  // all rings in one pass
     std::vector<std::vector<int>> cl;
     for (int r = 0; r < 5; ++r) {
         const std::vector<float> &c = ring[r];
-        const int m = (int)(c.size() / 3);
-        if (m == 0) continue;
-        if (int rc = labels_of(h, c.data(), m, (float)tol[r], lab)) return rc;
-        clusters_of(lab, 20, 100000, cl);
+        if (sizes[r] == 0) continue;
+        clusters_of(lab[r], 20, 100000, cl);
         for (const std::vector<int> &idx : cl) {
             double cen[3] = {0.0, 0.0, 0.0};
             float lo[3] = {std::numeric_limits<float>::max(), std::numeric_limits<float>::max(),
