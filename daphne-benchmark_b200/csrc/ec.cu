@@ -38,6 +38,7 @@
 namespace ec {
 
 constexpr int kThreads = 256;
+constexpr int kSplit = 4;  // threads per (point, neighbour cell): dense cells are shared out
 constexpr int kUnionLimit = 1 << 20;  // CAS retries of one union (never reached in practice; flags an error)
 
 constexpr int kMaxParts = 8;  // clouds clustered in one pass (segmentByDistance: its 5 rings)
@@ -109,8 +110,9 @@ __device__ __forceinline__ int find_root(int *parent, int x) {
     return -1;
 }
 
-// One thread per (point i, neighbour cell): blockIdx.y picks the cell offset
-// (27 of them), x walks the points in sorted order, so a warp's points share
+// kSplit threads per (point i, neighbour cell): blockIdx.y picks the cell
+// offset (27 of them) and the thread's share of the cell's points (every
+// kSplit-th), x walks the points in sorted order, so a warp's points share
 // cells and read the same neighbours.  The thread tests the points j > i of
 // its cell (cells never cross parts); i's root is found at the first accepted
 // pair and kept; a pair whose roots already agree costs the reads of j's
@@ -121,7 +123,8 @@ __global__ void join_kernel(const float4 *__restrict__ pts, const uint32_t *__re
                             const __grid_constant__ Parts P, int *__restrict__ parent, int *__restrict__ err) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
-    const int off = blockIdx.y;  // 9 dz + 3 dy + dx, each in {0, 1, 2}
+    const int off = blockIdx.y / kSplit;  // 9 dz + 3 dy + dx, each in {0, 1, 2}
+    const int part = blockIdx.y % kSplit;  // this thread's share of the cell: every kSplit-th point
     const long long key = keys[t];
     const int q = part_of(P.base, P.np, key);
     const long long local = key - P.base[q];
@@ -137,7 +140,7 @@ __global__ void join_kernel(const float4 *__restrict__ pts, const uint32_t *__re
     const float r2 = P.r2[q];
     const int e = s + 1 < *nseg ? seg_start[s + 1] : n;
     int ri = -2;  // not looked up yet
-    for (int u = seg_start[s]; u < e; ++u) {
+    for (int u = seg_start[s] + part; u < e; u += kSplit) {
         const int j = (int)order[u];
         if (j <= i) continue;
         const float4 qj = pts[j];
@@ -292,8 +295,8 @@ int labels_of(ndt_ec *h, const std::vector<const float *> &xyz, const std::vecto
     ndt::sort_segments(sb, N, bits, (int32_t *)h->seg_start, (uint32_t *)h->seg_key, st);
     ec::cell_index_kernel<<<blocks, ec::kThreads, 0, st>>>((const int32_t *)h->seg_start, (const uint32_t *)h->seg_key,
                                                            sb.nseg, (int *)h->cell_first);
-    ec::join_kernel<<<dim3(blocks, 27), ec::kThreads, 0, st>>>(d_pts, sb.v0, sb.k0, N, (const int32_t *)h->seg_start,
-                                                               sb.nseg, (const int *)h->cell_first, P, parent, err);
+    ec::join_kernel<<<dim3(blocks, 27 * ec::kSplit), ec::kThreads, 0, st>>>(
+        d_pts, sb.v0, sb.k0, N, (const int32_t *)h->seg_start, sb.nseg, (const int *)h->cell_first, P, parent, err);
     ec::label_kernel<<<blocks, ec::kThreads, 0, st>>>(parent, N, err);
     ECK(cudaGetLastError());
     ECK(cudaMemcpyAsync(h->h_labels, parent, sizeof(int) * (size_t)N, cudaMemcpyDeviceToHost, st));
