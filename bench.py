@@ -379,9 +379,10 @@ def run_ours(args, pkg, world, rank, local):
     h_status = torch.zeros(B, dtype=torch.int32).pin_memory()
 
     def host_step():
-        ctx.set_map_ptr(h_map.data_ptr(), M)
-        ctx.align_batch_packed_ptr(B, h_pts.data_ptr(), h_off.data_ptr(), h_g.data_ptr(), h_out.data_ptr(),
-                                   h_conv.data_ptr(), h_fit.data_ptr(), h_status.data_ptr())
+        # the batched align call with its map, as the reference's align call takes the map every time
+        ctx.align_batch_packed_with_map_ptr(h_map.data_ptr(), M, B, h_pts.data_ptr(), h_off.data_ptr(),
+                                            h_g.data_ptr(), h_out.data_ptr(), h_conv.data_ptr(), h_fit.data_ptr(),
+                                            h_status.data_ptr())
 
     # warm-up: at least W steps and at least E2E_WARM_S seconds -- the
     # host-to-device path of a freshly started process takes about a second of
@@ -486,7 +487,8 @@ def run_ours(args, pkg, world, rank, local):
                 "pinned_h2d_gbs": round(h2d_gbs, 1),
                 "copy_groups": prm.copy_groups or "by size",
                 "warmup_steps": n_warm,
-                "path": "ndt_set_map + ndt_align_batch_packed (C ABI), pinned host buffers"},
+                "path": "ndt_align_batch_packed_with_map (C ABI: map + packed scans, the grid build overlapping "
+                        "the scans' copies), pinned host buffers"},
         "roofline": roofline,
         "cpu_baseline": cpu,
         "clocks": clk,

@@ -716,9 +716,17 @@ int copy_group_count(const ndt_ctx *c, int B, long long total) {
 // stream) enqueues the host-to-device copy of the points of alignments
 // [b0, b1) into c->points at off[b0].  Alignments are split into groups of
 // about equal point counts; group k's rounds wait only for group k's copy.
-template <class CopyFn>
+// A host batch in copy groups: every group's points are copied on the copy
+// stream (all copies enqueued first, one event each), then each group's
+// rounds run on the compute stream once its event has fired, so the copies
+// of later groups overlap the rounds of earlier ones.  `before_copies` and
+// `before_runs` (optional) run before the copies are enqueued and before the
+// first group's rounds: the map of ndt_align_batch_packed_with_map is
+// uploaded in the first and built in the second, so its grid build overlaps
+// the scans' copies.
+template <class CopyFn, class PreFn, class MidFn>
 int staged_batch(ndt_ctx *c, int B, const int *off, const float *guesses, float *out, int *conv, double *fit,
-                 int *status, CopyFn copy) {
+                 int *status, CopyFn copy, PreFn before_copies, MidFn before_runs) {
     const long long total = off[B];
     cudaStream_t st = c->stream, cs = c->copy_stream;
     CK(c->points.ensure(sizeof(float4) * (size_t)(total > 0 ? total : 1)));
@@ -734,19 +742,32 @@ int staged_batch(ndt_ctx *c, int B, const int *off, const float *guesses, float 
         CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         c->copy_ev.push_back(e);
     }
+    // group k ends at the first alignment whose start reaches (k + 1) / G of the points
+    std::vector<int> bound(G + 1, 0);
+    bound[G] = B;
+    for (int k = 0; k + 1 < G; ++k) {
+        const long long target = total * (k + 1) / G;
+        int b1 = bound[k] + 1;
+        while (b1 < B - (G - 1 - k) && off[b1] < target) ++b1;
+        bound[k + 1] = b1;
+    }
+    if (int rc = before_copies()) return rc;
     CK(cudaMemcpyAsync(c->offsets.p, off, sizeof(int) * (size_t)(B + 1), cudaMemcpyHostToDevice, cs));
     CK(cudaMemcpyAsync(c->guesses.p, guesses, sizeof(float) * 16 * (size_t)B, cudaMemcpyHostToDevice, cs));
-    int b0 = 0;
     for (int k = 0; k < G; ++k) {
-        // group k ends at the first alignment whose start reaches (k + 1) / G of the points
-        int b1 = B;
-        if (k + 1 < G) {
-            const long long target = total * (k + 1) / G;
-            b1 = b0 + 1;
-            while (b1 < B - (G - 1 - k) && off[b1] < target) ++b1;
-        }
-        if (int rc = copy(b0, b1, cs)) return rc;
+        if (int rc = copy(bound[k], bound[k + 1], cs)) return rc;
         CK(cudaEventRecord(c->copy_ev[k], cs));
+    }
+    if (int rc = before_runs()) {
+        cudaStreamSynchronize(cs);
+        return rc;
+    }
+    if (!c->have_map) {
+        cudaStreamSynchronize(cs);
+        return fail(c, NDT_E_NOMAP, "no map set");
+    }
+    for (int k = 0; k < G; ++k) {
+        const int b0 = bound[k], b1 = bound[k + 1];
         CK(cudaStreamWaitEvent(st, c->copy_ev[k], 0));
         int rc = run_batch(c, b1 - b0, c->points.as<float4>(), c->offsets.as<int>() + b0, off[b1] - off[b0],
                            c->guesses.as<float>() + 16 * (size_t)b0, c->out_T.as<float>() + 16 * (size_t)b0,
@@ -756,7 +777,6 @@ int staged_batch(ndt_ctx *c, int B, const int *off, const float *guesses, float 
             cudaStreamSynchronize(cs);
             return rc;
         }
-        b0 = b1;
     }
     CK(cudaMemcpyAsync(out, c->out_T.p, sizeof(float) * 16 * (size_t)B, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(conv, c->out_conv.p, sizeof(int) * (size_t)B, cudaMemcpyDeviceToHost, st));
@@ -765,6 +785,8 @@ int staged_batch(ndt_ctx *c, int B, const int *off, const float *guesses, float 
     CK(cudaStreamSynchronize(st));
     return NDT_OK;
 }
+
+int no_hook() { return NDT_OK; }
 
 // Host batch of separate scan buffers.
 int host_batch(ndt_ctx *c, int B, const float *const *scans, const int *ns, const float *guesses, float *out,
@@ -787,24 +809,34 @@ int host_batch(ndt_ctx *c, int B, const float *const *scans, const int *ns, cons
                 CK(cudaMemcpyAsync(c->points.as<float4>() + off[b], scans[b], sizeof(float4) * (size_t)ns[b],
                                    cudaMemcpyHostToDevice, cs));
         return NDT_OK;
-    });
+    }, no_hook, no_hook);
 }
 
-// Host batch from one packed host buffer.
+// Host batch from one packed host buffer; with map != nullptr the batch's map
+// comes along (uploaded first, built while the scans are copied).
 int packed_batch(ndt_ctx *c, int B, const float *points, const int *offsets, const float *guesses, float *out,
-                 int *conv, double *fit, int *status) {
+                 int *conv, double *fit, int *status, const float *map = nullptr, int m = 0) {
     if (B <= 0 || !points || !offsets || !guesses || !out || !conv || !fit) return fail(c, NDT_E_ARG, "null argument");
-    if (!c->have_map) return fail(c, NDT_E_NOMAP, "no map set");
+    if (!map && !c->have_map) return fail(c, NDT_E_NOMAP, "no map set");
+    if (map && m <= 0) return fail(c, NDT_E_ARG, "empty map");
     if (offsets[0] != 0) return fail(c, NDT_E_ARG, "offsets[0] must be 0");
     for (int b = 0; b < B; ++b)
         if (offsets[b + 1] < offsets[b]) return fail(c, NDT_E_ARG, "offsets must be non-decreasing");
+    auto upload_map = [&]() -> int {
+        if (!map) return NDT_OK;
+        c->have_map = false;
+        CK(c->map.ensure(sizeof(float4) * (size_t)m));
+        CK(cudaMemcpyAsync(c->map.p, map, sizeof(float4) * (size_t)m, cudaMemcpyHostToDevice, c->stream));
+        return NDT_OK;
+    };
+    auto build_map = [&]() -> int { return map ? build_grid(c, c->map.as<float4>(), m) : NDT_OK; };
     return staged_batch(c, B, offsets, guesses, out, conv, fit, status, [&](int b0, int b1, cudaStream_t cs) -> int {
         const long long n = (long long)offsets[b1] - offsets[b0];
         if (n > 0)
             CK(cudaMemcpyAsync(c->points.as<float4>() + offsets[b0], points + 4 * (size_t)offsets[b0],
                                sizeof(float4) * (size_t)n, cudaMemcpyHostToDevice, cs));
         return NDT_OK;
-    });
+    }, upload_map, build_map);
 }
 
 }  // namespace
@@ -1057,6 +1089,14 @@ int ndt_align_batch_packed(ndt_ctx *c, int B, const float *points, const int *of
     if (!c) return NDT_E_ARG;
     if (int rc = set_device(c)) return rc;
     return packed_batch(c, B, points, offsets, guesses, out, converged, fitness, status);
+}
+
+int ndt_align_batch_packed_with_map(ndt_ctx *c, const float *map, int m, int B, const float *points,
+                                    const int *offsets, const float *guesses, float *out, int *converged,
+                                    double *fitness, int *status) {
+    if (!c || !map) return fail(c, NDT_E_ARG, "null argument");
+    if (int rc = set_device(c)) return rc;
+    return packed_batch(c, B, points, offsets, guesses, out, converged, fitness, status, map, m);
 }
 
 int ndt_score_batch_device(ndt_ctx *c, int B, const float *d_points, const int *d_offsets, int total_points,

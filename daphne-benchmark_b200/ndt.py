@@ -96,6 +96,8 @@ def lib():
                                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ndt_align_batch_packed.argtypes = [ctxp, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                              C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ndt_align_batch_packed_with_map.argtypes = [ctxp, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ndt_set_profiling.argtypes = [ctxp, C.c_int]
         L.ndt_set_batch_graphs.argtypes = [ctxp, C.c_int]
         L.ndt_score_batch_device.argtypes = [ctxp, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
@@ -115,6 +117,7 @@ def lib():
                      "ndt_align", "ndt_align_with_map",
                      "ndt_align_batch", "ndt_align_batch_device", "ndt_synchronize", "ndt_get_counters",
                      "ndt_grid_info", "ndt_grid_cells", "ndt_derivatives", "ndt_align_batch_packed",
+                     "ndt_align_batch_packed_with_map",
                      "ndt_set_profiling", "ndt_kernel_variants", "ndt_kernel_variant_shape",
                      "ndt_set_kernel_variant", "ndt_window_info", "ndt_set_batch_graphs",
                      "ndt_score_batch_device"):
@@ -264,6 +267,14 @@ class Context:
                                                   C.c_void_p(guesses), C.c_void_p(out), C.c_void_p(conv),
                                                   C.c_void_p(fit), C.c_void_p(status) if status else None),
                     "ndt_align_batch_packed")
+
+    def align_batch_packed_with_map_ptr(self, map_ptr, m, B, points, offsets, guesses, out, conv, fit, status=0):
+        """The batch with its map (raw host pointers, e.g. pinned torch tensors); the map's grid stays set."""
+        self._check(self.L.ndt_align_batch_packed_with_map(self.h, C.c_void_p(map_ptr), m, B, C.c_void_p(points),
+                                                           C.c_void_p(offsets), C.c_void_p(guesses),
+                                                           C.c_void_p(out), C.c_void_p(conv), C.c_void_p(fit),
+                                                           C.c_void_p(status) if status else None),
+                    "ndt_align_batch_packed_with_map")
 
     def set_map_ptr(self, ptr: int, m: int):
         """Host map by raw pointer (e.g. a pinned torch tensor)."""

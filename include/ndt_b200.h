@@ -162,6 +162,18 @@ NDT_API int ndt_align_batch_packed(ndt_ctx *ctx, int B, const float *points, con
                                    const float *guesses, float *out, int *converged, double *fitness,
                                    int *status);
 
+/*
+ * The same with the batch's map, as the reference's align call takes the map
+ * every time (partial_points_callback(scan, guess, map), kernel.cpp:1405,
+ * which rebuilds the grid: ndt_align, :1375-1392): map = m float[4] points
+ * (HOST).  The map is uploaded first and its grid built while the scans are
+ * copied, so the build overlaps the copies; the grid then stays set as after
+ * ndt_set_map.
+ */
+NDT_API int ndt_align_batch_packed_with_map(ndt_ctx *ctx, const float *map, int m, int B, const float *points,
+                                            const int *offsets, const float *guesses, float *out, int *converged,
+                                            double *fitness, int *status);
+
 /* The context's CUDA stream (cudaStream_t), for callers that time or order work. */
 NDT_API void *ndt_stream(ndt_ctx *ctx);
 

@@ -244,3 +244,41 @@ def test_batch_graph_equals_host_loop(pkg, compat):
     assert 0 < r1 <= r0 <= 1025
     if compat:
         assert r1 == r0 == 3
+
+
+@pytest.mark.parametrize("groups", [1, 3])
+def test_batch_with_map_equals_set_map_then_batch(pkg, cases, groups):
+    """ndt_align_batch_packed_with_map (the map built while the scans are
+    copied) gives the results of ndt_set_map + ndt_align_batch_packed bit for
+    bit, and leaves that map's grid set."""
+    torch = pytest.importorskip("torch")
+    c0 = [c for c in cases if c["config"]["name"] == "s8k"]
+    cfg, scene, _ = _inputs(pkg, c0[0])
+    aligns = [pkg.synth.make_alignment(cfg, scene, i) for i in range(7)]
+    offs = np.zeros(len(aligns) + 1, np.int32)
+    offs[1:] = np.cumsum([len(a.scan) for a in aligns])
+    pts = np.ascontiguousarray(np.concatenate([a.scan for a in aligns]))
+    g = np.ascontiguousarray(np.stack([a.guess for a in aligns]).astype(np.float32))
+    B = len(aligns)
+    prm = pkg.ndt.reference_params()
+    prm.copy_groups = groups
+    res = []
+    for with_map in (False, True):
+        out = np.zeros((B, 16), np.float32)
+        conv = np.zeros(B, np.int32)
+        fit = np.zeros(B, np.float64)
+        st = np.zeros(B, np.int32)
+        with pkg.ndt.Context(prm) as ctx:
+            if with_map:
+                mp = np.ascontiguousarray(scene.map)
+                ctx.align_batch_packed_with_map_ptr(mp.ctypes.data, len(mp), B, pts.ctypes.data, offs.ctypes.data,
+                                                    g.ctypes.data, out.ctypes.data, conv.ctypes.data, fit.ctypes.data,
+                                                    st.ctypes.data)
+                again = ctx.align_batch([a.scan for a in aligns], g)  # the grid stays set
+                assert np.array_equal(again[0].view(np.uint32), out.view(np.uint32))
+            else:
+                ctx.set_map(scene.map)
+                ctx.align_batch_packed(pts, offs, g, out, conv, fit, st)
+        res.append((out.view(np.uint32).copy(), conv, fit, st))
+    for a, b in zip(res[0], res[1]):
+        assert np.array_equal(a, b)
