@@ -42,7 +42,7 @@ struct DerivVariant {
     int tile;
     int min_blocks;
 };
-constexpr int kNumDerivVariants = 5;
+constexpr int kNumDerivVariants = 7;
 extern const DerivVariant kDerivVariants[kNumDerivVariants];
 
 // precision 0 = FP32 pair arithmetic (launch shape `variant`), 1 = FP64

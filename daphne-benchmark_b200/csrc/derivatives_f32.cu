@@ -560,7 +560,7 @@ void launch_one(const EvalArgs &args, int blocks, cudaStream_t st) {
 }  // namespace
 
 const DerivVariant kDerivVariants[kNumDerivVariants] = {
-    {256, 2}, {256, 1}, {128, 4}, {128, 3}, {256, 3},
+    {256, 2}, {256, 1}, {128, 4}, {128, 3}, {256, 3}, {128, 5}, {128, 6},
 };
 
 int prepare_derivatives() {
@@ -570,6 +570,8 @@ int prepare_derivatives() {
     if ((r = prepare_one<128, 4>()) != cudaSuccess) e = r;
     if ((r = prepare_one<128, 3>()) != cudaSuccess) e = r;
     if ((r = prepare_one<256, 3>()) != cudaSuccess) e = r;
+    if ((r = prepare_one<128, 5>()) != cudaSuccess) e = r;
+    if ((r = prepare_one<128, 6>()) != cudaSuccess) e = r;
     return (int)e;
 }
 
@@ -588,6 +590,8 @@ int launch_derivatives(const EvalArgs &args, int precision, int variant, int sms
         case 1: launch_one<256, 1>(args, blocks, st); break;
         case 2: launch_one<128, 4>(args, blocks, st); break;
         case 3: launch_one<128, 3>(args, blocks, st); break;
+        case 5: launch_one<128, 5>(args, blocks, st); break;
+        case 6: launch_one<128, 6>(args, blocks, st); break;
         default: launch_one<256, 3>(args, blocks, st); break;
     }
     flagged_kernel<<<sms, 128, 0, st>>>(args);
