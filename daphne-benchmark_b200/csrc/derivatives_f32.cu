@@ -397,6 +397,7 @@ __device__ __forceinline__ void eval_deferred(const WarpPairs &P, const uint2 *r
 template <int TILE, int MINB>
 __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(const __grid_constant__ EvalArgs args) {
     constexpr int kW = TILE / 32;
+    static_assert(TILE >= kPartial, "the partial is written by one thread per entry");
     __shared__ float s_T[12];
     __shared__ float s_ang[kAngle];
     __shared__ int s_mode;
@@ -446,7 +447,7 @@ __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(const __grid
         const AlignState *st = args.states + ck.align;
         if (threadIdx.x == 0) s_mode = st->eval_mode;
         if (threadIdx.x < 12) s_T[threadIdx.x] = st->T[threadIdx.x];
-        if (threadIdx.x < kAngle) s_ang[threadIdx.x] = st->angf[threadIdx.x];
+        for (int k = threadIdx.x; k < kAngle; k += TILE) s_ang[k] = st->angf[k];
         __syncthreads();
         const int mode = s_mode;
         if (mode == kEvalNone) continue;  // s_mode is rewritten only after the next chunk's barrier
