@@ -41,7 +41,7 @@ constexpr int kThreads = 256;
 constexpr int kSplit = 4;  // threads per (point, neighbour cell): dense cells are shared out
 constexpr int kUnionLimit = 1 << 20;  // CAS retries of one union (never reached in practice; flags an error)
 
-constexpr int kMaxParts = 8;  // clouds clustered in one pass (segmentByDistance: its 5 rings)
+constexpr int kMaxParts = 40;  // clouds clustered in one pass (segmentByDistance: 5 rings of up to 8 clouds)
 
 // Geometry of the clouds of one pass: part p's points are [off[p], off[p + 1])
 // of the concatenation, its cells have edge cell[p] from minv[p] with dims
@@ -67,9 +67,12 @@ __device__ __forceinline__ int cell_of(float v, float minv, float cell, int dim)
 // The part of point t (or of key k): the last p with first[p] <= t.
 template <class T>
 __device__ __forceinline__ int part_of(const T *first, int np, long long t) {
-    int p = 0;
-    while (p + 1 < np && (long long)first[p + 1] <= t) ++p;
-    return p;
+    int lo = 0, hi = np;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if ((long long)first[mid] <= t) lo = mid; else hi = mid;
+    }
+    return lo;
 }
 
 __global__ void key_kernel(const float4 *__restrict__ pts, int n, const __grid_constant__ Parts P,
@@ -396,69 +399,107 @@ int ndt_ec_extract(ndt_ec *h, const float *xyz, int n, float tolerance, int min_
 // segmentByDistance (kernel.cpp:767-814) with clusterAndColor (:652-765):
 // five rings of distance from the sensor (< 15, 30, 45, 60 m, beyond) with
 // tolerances 0.5, 1.1, 1.6, 2.3 and 2.6f, clusters of 20 to 100000 points.
+// Clouds [c0, c1) of a packed batch in one GPU pass; outputs appended at the
+// running counts np / nb.
+namespace {
+int segment_clouds(ndt_ec *h, const float *xyz, const int *offsets, int c0, int c1, float *out_xyz, int *out_off,
+                   double *boxes, int *box_off, double *centroids, int &np, int &nb) {
+    const double tol[5] = {0.5, 1.1, 1.6, 2.3, 2.6f};
+    const int C = c1 - c0;
+    std::vector<std::vector<float>> ring(5 * (size_t)C);
+    for (int c = 0; c < C; ++c)
+        for (int i = offsets[c0 + c]; i < offsets[c0 + c + 1]; ++i) {
+            const float *q = xyz + 3 * (size_t)i;
+            const float x = q[0], y = q[1];
+            const float d = std::sqrt(x * x + y * y);
+            const int r = d < 15 ? 0 : (d < 30 ? 1 : (d < 45 ? 2 : (d < 60 ? 3 : 4)));
+            ring[5 * (size_t)c + r].insert(ring[5 * (size_t)c + r].end(), q, q + 3);
+        }
+    std::vector<const float *> parts;
+    std::vector<int> sizes;
+    std::vector<float> tols;
+    for (int k = 0; k < 5 * C; ++k) {
+        parts.push_back(ring[k].data());
+        sizes.push_back((int)(ring[k].size() / 3));
+        tols.push_back((float)tol[k % 5]);
+    }
+    std::vector<std::vector<int>> lab;
+    if (int rc = labels_of(h, parts, sizes, tols, lab)) return rc;  // every ring of every cloud in one pass
+    std::vector<std::vector<int>> cl;
+    for (int c = 0; c < C; ++c) {
+        out_off[c0 + c] = np;
+        box_off[c0 + c] = nb;
+        for (int r = 0; r < 5; ++r) {
+            const std::vector<float> &pts = ring[5 * (size_t)c + r];
+            if (pts.empty()) continue;
+            clusters_of(lab[5 * (size_t)c + r], 20, 100000, cl);
+            for (const std::vector<int> &idx : cl) {
+                double cen[3] = {0.0, 0.0, 0.0};
+                float lo[3] = {std::numeric_limits<float>::max(), std::numeric_limits<float>::max(),
+                               std::numeric_limits<float>::max()};
+                float hi[3] = {-lo[0], -lo[1], -lo[2]};
+                for (int i : idx) {
+                    const float *p = &pts[3 * (size_t)i];
+                    for (int k = 0; k < 3; ++k) {
+                        out_xyz[3 * (size_t)np + k] = p[k];
+                        cen[k] += p[k];
+                        if (p[k] < lo[k]) lo[k] = p[k];
+                        if (p[k] > hi[k]) hi[k] = p[k];
+                    }
+                    ++np;
+                }
+                for (int k = 0; k < 3; ++k) cen[k] /= idx.size();
+                const float l = hi[0] - lo[0], w = hi[1] - lo[1], ht = hi[2] - lo[2];
+                const double dim[3] = {l < 0 ? -1 * l : l, w < 0 ? -1 * w : w, ht < 0 ? -1 * ht : ht};
+                if (dim[0] > 0 && dim[1] > 0 && dim[2] > 0 && dim[0] < 15 && dim[1] > 0 && dim[1] < 15 &&
+                    hi[2] > -1.5 && lo[2] > -1.5 && lo[2] < 1.0) {
+                    // position, orientation (x, y, z, w; the yaw is not estimated here: identity), dimensions
+                    const double b[10] = {lo[0] + l / 2, lo[1] + w / 2, lo[2] + ht / 2, 0.0, 0.0, 0.0, 1.0,
+                                          dim[0], dim[1], dim[2]};
+                    std::memcpy(boxes + 10 * (size_t)nb, b, sizeof(b));
+                    std::memcpy(centroids + 3 * (size_t)nb, cen, sizeof(cen));
+                    ++nb;
+                }
+            }
+        }
+    }
+    out_off[c1] = np;
+    box_off[c1] = nb;
+    return NDT_OK;
+}
+}  // namespace
+
 int ndt_ec_segment(ndt_ec *h, const float *xyz, int n, float *out_xyz, int *out_n, double *boxes, int *num_boxes,
                    double *centroids, int *num_centroids) {
     if (!h || n < 0 || (n > 0 && !xyz) || !out_xyz || !out_n || !boxes || !num_boxes || !centroids ||
         !num_centroids)
         return fail(h, NDT_E_ARG, "bad argument");
     ECK(cudaSetDevice(h->device));
-    const double tol[5] = {0.5, 1.1, 1.6, 2.3, 2.6f};
-    std::vector<float> ring[5];
-    for (int i = 0; i < n; ++i) {
-        const float x = xyz[3 * (size_t)i], y = xyz[3 * (size_t)i + 1];
-        const float d = std::sqrt(x * x + y * y);
-        const int r = d < 15 ? 0 : (d < 30 ? 1 : (d < 45 ? 2 : (d < 60 ? 3 : 4)));
-        ring[r].insert(ring[r].end(), xyz + 3 * (size_t)i, xyz + 3 * (size_t)i + 3);
-    }
-    int np = 0, nb = 0, nc = 0;
-    std::vector<const float *> parts;
-    std::vector<int> sizes;
-    std::vector<float> tols;
-    for (int r = 0; r < 5; ++r) {
-        parts.push_back(ring[r].data());
-        sizes.push_back((int)(ring[r].size() / 3));
-        tols.push_back((float)tol[r]);
-    }
-    std::vector<std::vector<int>> lab;
-    if (int rc = labels_of(h, parts, sizes, tols, lab)) return rc;  // all rings in one pass
-    std::vector<std::vector<int>> cl;
-    for (int r = 0; r < 5; ++r) {
-        const std::vector<float> &c = ring[r];
-        if (sizes[r] == 0) continue;
-        clusters_of(lab[r], 20, 100000, cl);
-        for (const std::vector<int> &idx : cl) {
-            double cen[3] = {0.0, 0.0, 0.0};
-            float lo[3] = {std::numeric_limits<float>::max(), std::numeric_limits<float>::max(),
-                           std::numeric_limits<float>::max()};
-            float hi[3] = {-lo[0], -lo[1], -lo[2]};
-            for (int i : idx) {
-                const float *p = &c[3 * (size_t)i];
-                for (int k = 0; k < 3; ++k) {
-                    out_xyz[3 * (size_t)np + k] = p[k];
-                    cen[k] += p[k];
-                    if (p[k] < lo[k]) lo[k] = p[k];
-                    if (p[k] > hi[k]) hi[k] = p[k];
-                }
-                ++np;
-            }
-            for (int k = 0; k < 3; ++k) cen[k] /= idx.size();
-            const float l = hi[0] - lo[0], w = hi[1] - lo[1], ht = hi[2] - lo[2];
-            const double dim[3] = {l < 0 ? -1 * l : l, w < 0 ? -1 * w : w, ht < 0 ? -1 * ht : ht};
-            if (dim[0] > 0 && dim[1] > 0 && dim[2] > 0 && dim[0] < 15 && dim[1] > 0 && dim[1] < 15 && hi[2] > -1.5 &&
-                lo[2] > -1.5 && lo[2] < 1.0) {
-                // position, orientation (x, y, z, w; the yaw is not estimated here: identity), dimensions
-                const double b[10] = {lo[0] + l / 2, lo[1] + w / 2, lo[2] + ht / 2, 0.0, 0.0, 0.0, 1.0,
-                                      dim[0], dim[1], dim[2]};
-                std::memcpy(boxes + 10 * (size_t)nb, b, sizeof(b));
-                ++nb;
-                std::memcpy(centroids + 3 * (size_t)nc, cen, sizeof(cen));
-                ++nc;
-            }
-        }
-    }
+    const int off[2] = {0, n};
+    int oo[2], bo[2], np = 0, nb = 0;
+    if (int rc = segment_clouds(h, xyz, off, 0, 1, out_xyz, oo, boxes, bo, centroids, np, nb)) return rc;
     *out_n = np;
     *num_boxes = nb;
-    *num_centroids = nc;
+    *num_centroids = nb;
+    return NDT_OK;
+}
+
+int ndt_ec_segment_batch(ndt_ec *h, int C, const float *xyz, const int *offsets, float *out_xyz, int *out_offsets,
+                         double *boxes, int *box_offsets, double *centroids) {
+    if (!h || C <= 0 || !offsets || !out_xyz || !out_offsets || !boxes || !box_offsets || !centroids ||
+        (offsets[C] > 0 && !xyz) || offsets[0] != 0)
+        return fail(h, NDT_E_ARG, "bad argument");
+    for (int c = 0; c < C; ++c)
+        if (offsets[c + 1] < offsets[c]) return fail(h, NDT_E_ARG, "offsets must be non-decreasing");
+    ECK(cudaSetDevice(h->device));
+    int np = 0, nb = 0;
+    const int per_pass = ec::kMaxParts / 5;
+    for (int c0 = 0; c0 < C; c0 += per_pass) {
+        const int c1 = std::min(C, c0 + per_pass);
+        if (int rc = segment_clouds(h, xyz, offsets, c0, c1, out_xyz, out_offsets, boxes, box_offsets, centroids,
+                                    np, nb))
+            return rc;
+    }
     return NDT_OK;
 }
 

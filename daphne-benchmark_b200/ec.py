@@ -23,7 +23,8 @@ def _lib():
         L.ndt_ec_extract.argtypes = [p, p, C.c_int, C.c_float, C.c_int, C.c_int, C.POINTER(C.c_int), p, p]
         L.ndt_ec_segment.argtypes = [p, p, C.c_int, p, C.POINTER(C.c_int), p, C.POINTER(C.c_int), p,
                                      C.POINTER(C.c_int)]
-        for n in ("ndt_ec_create", "ndt_ec_labels", "ndt_ec_extract", "ndt_ec_segment"):
+        L.ndt_ec_segment_batch.argtypes = [p, C.c_int, p, p, p, p, p, p, p]
+        for n in ("ndt_ec_create", "ndt_ec_labels", "ndt_ec_extract", "ndt_ec_segment", "ndt_ec_segment_batch"):
             getattr(L, n).restype = C.c_int
         L._ec_ready = True
     return L
@@ -91,3 +92,21 @@ class EuclideanClusters:
         self._check(self.L.ndt_ec_segment(self.h, p.ctypes.data, n, pts.ctypes.data, C.byref(m), boxes.ctypes.data,
                                           C.byref(nb), cen.ctypes.data, C.byref(nc)), "ndt_ec_segment")
         return pts[:m.value], boxes[:nb.value], cen[:nc.value]
+
+    def segment_batch(self, clouds):
+        """segmentByDistance of several clouds, several per GPU pass: a list of (points, boxes, centroids)."""
+        clouds = [np.ascontiguousarray(c, np.float32).reshape(-1, 3) for c in clouds]
+        C_ = len(clouds)
+        off = np.zeros(C_ + 1, np.int32)
+        off[1:] = np.cumsum([len(c) for c in clouds])
+        n = int(off[-1])
+        xyz = np.concatenate(clouds) if n else np.zeros((1, 3), np.float32)
+        pts = np.zeros((max(n, 1), 3), np.float32)
+        boxes = np.zeros((max(n, 1), 10))
+        cen = np.zeros((max(n, 1), 3))
+        oo = np.zeros(C_ + 1, np.int32)
+        bo = np.zeros(C_ + 1, np.int32)
+        self._check(self.L.ndt_ec_segment_batch(self.h, C_, xyz.ctypes.data, off.ctypes.data, pts.ctypes.data,
+                                                oo.ctypes.data, boxes.ctypes.data, bo.ctypes.data, cen.ctypes.data),
+                    "ndt_ec_segment_batch")
+        return [(pts[oo[c]:oo[c + 1]], boxes[bo[c]:bo[c + 1]], cen[bo[c]:bo[c + 1]]) for c in range(C_)]

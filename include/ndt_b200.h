@@ -412,6 +412,11 @@ NDT_API int ndt_ec_extract(ndt_ec *ec, const float *xyz, int n, float tolerance,
                            int *num_clusters, int *cluster_offsets, int *cluster_indices);
 NDT_API int ndt_ec_segment(ndt_ec *ec, const float *xyz, int n, float *out_xyz, int *out_n, double *boxes,
                            int *num_boxes, double *centroids, int *num_centroids);
+/* The same for C clouds packed in xyz (offsets: C + 1 point offsets), up to 8 clouds per GPU pass: cloud c's
+ * clustered points are out_xyz[out_offsets[c] .. out_offsets[c + 1]), its boxes and centroids
+ * [box_offsets[c] .. box_offsets[c + 1]) (capacities as above with n = offsets[C]). */
+NDT_API int ndt_ec_segment_batch(ndt_ec *ec, int C, const float *xyz, const int *offsets, float *out_xyz,
+                                 int *out_offsets, double *boxes, int *box_offsets, double *centroids);
 
 #ifdef __cplusplus
 }

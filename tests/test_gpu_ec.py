@@ -65,6 +65,17 @@ def test_segment_equals_reference(ecg, gold):
         assert ok and d == 0.0, d
 
 
+def test_segment_batch_equals_single(ecg, gold):
+    clouds = [gold[f"in{i}"] for i in range(int(gold["cases"]))]
+    clouds = clouds + clouds[:4]  # 9 clouds: two passes of up to 8
+    batch = ecg.segment_batch(clouds)
+    for c, (pts, boxes, cen) in zip(clouds, batch):
+        p1, b1, c1 = ecg.segment(c)
+        assert np.array_equal(pts.view(np.uint32), p1.view(np.uint32))
+        assert np.array_equal(boxes.view(np.uint64), b1.view(np.uint64))
+        assert np.array_equal(cen.view(np.uint64), c1.view(np.uint64))
+
+
 @pytest.mark.parametrize("tol", [0.3, 0.5, 1.0])
 def test_labels_vs_brute_force(ecg, tol):
     rng = np.random.default_rng(int(tol * 10))
