@@ -152,6 +152,21 @@ struct ndt_ctx {
     ndt::SortedMap sorted{nullptr, nullptr};
     int sorted_in = -1;  // -1: in `scratch`, else the index of the buffer pair
     DevBuf sorted_keys[2], sorted_order[2], append_scratch, meta_tmp;
+    // the grid build after its bounding box, as a cached CUDA graph (the same
+    // map pointer, size, bounding box and buffers launch it again)
+    struct GridGraphKey {
+        const float4 *map;
+        int m;
+        GridMeta meta;
+        ndt::NdtGridOptions opt;
+        ndt::GridBuffers buf;
+        void *scratch;
+        int windows;
+        ndt::WindowBuffers wb;
+    } grid_key;
+    cudaGraphExec_t grid_exec = nullptr;
+    int grid_nl = 0;
+    ndt::SortedMap grid_sorted{nullptr, nullptr};
     // batch
     DevBuf chunks, chunk_begin, num_chunks, big_begin, small_begin, num_big, round_no, dev_launches;
     DevBuf points, offsets, guesses, states, tiles, tile_begin, num_tiles, partials, exc, out_T, out_conv, out_fit,
@@ -285,26 +300,40 @@ constexpr long long kMaxWindowEntries = 1LL << 28;  // window entries (16 B each
 // context's stream for the duration of the call).
 // Probe-window table of the finished dense index: W + 1 offsets and at most
 // 27 entries per usable voxel (skipped when it would not fit, or with
-// dense_probe set).
-int build_windows(ndt_ctx *c, int m) {
+// dense_probe set).  prepare_windows sizes the buffers (false: no table);
+// enqueue_windows launches the build.
+int prepare_windows(ndt_ctx *c, int m, bool &use, WindowBuffers &wb) {
     const size_t G = (size_t)c->meta_host.G;
     const long long W = (long long)window_count(c->meta_host);
     const long long ent_cap = 27LL * (long long)std::min<size_t>((size_t)m, G);
+    use = !c->prm.dense_probe && W < kMaxWindows && ent_cap < kMaxWindowEntries;
+    std::memset(&wb, 0, sizeof(wb));
+    if (!use) return NDT_OK;
+    CK(c->win_off.ensure(sizeof(int32_t) * (size_t)(W + 1)));
+    CK(c->win_ent.ensure(sizeof(float4) * (size_t)ent_cap));
+    CK(c->win_ctot.ensure(sizeof(int32_t) * (size_t)(W / 256 + 2)));
+    wb.off = c->win_off.as<int32_t>();
+    wb.ent = c->win_ent.as<float4>();
+    wb.ctot = c->win_ctot.as<int32_t>();
+    return NDT_OK;
+}
+
+int enqueue_windows(ndt_ctx *c, const WindowBuffers &wb, int *nl) {
+    int rc = grid_windows(c->meta_host, c->index.as<int32_t>(), c->mean_hi.as<float4>(), wb, c->stream, nl);
+    if (rc) return cuda_fail(c, (cudaError_t)rc, "grid_windows");
+    return NDT_OK;
+}
+
+int build_windows(ndt_ctx *c, int m) {
+    bool use = false;
+    WindowBuffers wb;
     c->have_windows = false;
-    if (!c->prm.dense_probe && W < kMaxWindows && ent_cap < kMaxWindowEntries) {
-        CK(c->win_off.ensure(sizeof(int32_t) * (size_t)(W + 1)));
-        CK(c->win_ent.ensure(sizeof(float4) * (size_t)ent_cap));
-        CK(c->win_ctot.ensure(sizeof(int32_t) * (size_t)(W / 256 + 2)));
-        WindowBuffers wb;
-        wb.off = c->win_off.as<int32_t>();
-        wb.ent = c->win_ent.as<float4>();
-        wb.ctot = c->win_ctot.as<int32_t>();
-        int nl = 0;
-        int rc = grid_windows(c->meta_host, c->index.as<int32_t>(), c->mean_hi.as<float4>(), wb, c->stream, &nl);
-        if (rc) return cuda_fail(c, (cudaError_t)rc, "grid_windows");
-        c->launches += nl;
-        c->have_windows = true;
-    }
+    if (int rc = prepare_windows(c, m, use, wb)) return rc;
+    if (!use) return NDT_OK;
+    int nl = 0;
+    if (int rc = enqueue_windows(c, wb, &nl)) return rc;
+    c->launches += nl;
+    c->have_windows = true;
     return NDT_OK;
 }
 
@@ -369,13 +398,71 @@ int build_grid(ndt_ctx *c, const float4 *d_map, int m) {
     opt.compat = c->prm.compat;
     opt.min_points = c->prm.min_points_per_voxel;
     opt.eigen_ratio = c->prm.eigen_ratio;
-    int nl = 0;
-    rc = grid_build(d_map, m, c->meta_host, c->meta.as<GridMeta>(), opt, grid_buffers(c), c->scratch.p, c->stream, &nl,
-                    &c->sorted);
-    if (rc) return cuda_fail(c, (cudaError_t)rc, "grid_build");
-    c->launches += nl;
+    bool windows = false;
+    WindowBuffers wb;
+    if (int rc0 = prepare_windows(c, m, windows, wb)) return rc0;
+    // the rest of the build (keys, sort, segments, records, windows): replayed
+    // from the cached graph when nothing it depends on has changed
+    ndt_ctx::GridGraphKey key;
+    std::memset(&key, 0, sizeof(key));
+    key.map = d_map;
+    key.m = m;
+    {  // field by field: the struct's padding bytes are not part of the key
+        const GridMeta &g = c->meta_host;
+        for (int e = 0; e < 3; ++e) {
+            key.meta.minv[e] = g.minv[e];
+            key.meta.maxv[e] = g.maxv[e];
+            key.meta.raw_min[e] = g.raw_min[e];
+            key.meta.raw_max[e] = g.raw_max[e];
+            key.meta.dim[e] = g.dim[e];
+        }
+        key.meta.res = g.res;
+        key.meta.G = g.G;
+        key.meta.occupied = g.occupied;
+        key.meta.error = g.error;
+    }
+    key.opt = opt;
+    key.buf = grid_buffers(c);
+    key.scratch = c->scratch.p;
+    key.windows = windows ? 1 : 0;
+    key.wb = wb;
+    cudaStream_t st = c->stream;
+    if (!(c->use_graphs && c->grid_exec && std::memcmp(&key, &c->grid_key, sizeof(key)) == 0)) {
+        if (c->grid_exec) cudaGraphExecDestroy(c->grid_exec);
+        c->grid_exec = nullptr;
+        int nl = 0;
+        ndt::SortedMap sorted{nullptr, nullptr};
+        if (c->use_graphs) CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        rc = grid_build(d_map, m, c->meta_host, c->meta.as<GridMeta>(), opt, key.buf, c->scratch.p, st, &nl, &sorted);
+        int rc2 = rc ? 0 : (windows ? enqueue_windows(c, wb, &nl) : 0);
+        if (c->use_graphs) {
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(st, &g);
+            if (rc || rc2 || e != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                if (rc) return cuda_fail(c, (cudaError_t)rc, "grid_build");
+                if (rc2) return rc2;
+                return cuda_fail(c, e, "grid build capture");
+            }
+            e = cudaGraphInstantiate(&c->grid_exec, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                c->grid_exec = nullptr;
+                return cuda_fail(c, e, "cudaGraphInstantiate (grid build)");
+            }
+            c->grid_key = key;
+        } else {
+            if (rc) return cuda_fail(c, (cudaError_t)rc, "grid_build");
+            if (rc2) return rc2;
+        }
+        c->grid_nl = nl;
+        c->grid_sorted = sorted;
+    }
+    if (c->grid_exec) CK(cudaGraphLaunch(c->grid_exec, st));
+    c->launches += c->grid_nl;
+    c->sorted = c->grid_sorted;
     c->sorted_in = -1;
-    if (int rc2 = build_windows(c, m)) return rc2;
+    c->have_windows = windows;
     if (c->profiling) {
         CK(cudaEventRecord(c->grid_ev[1], c->stream));
         c->grid_timed = true;
@@ -941,6 +1028,7 @@ void ndt_destroy(ndt_ctx *c) {
     for (cudaEvent_t e : c->grid_ev)
         if (e) cudaEventDestroy(e);
     for (BatchGraph &b : c->graphs) cudaGraphExecDestroy(b.exec);
+    if (c->grid_exec) cudaGraphExecDestroy(c->grid_exec);
     c->graphs.clear();
     if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
