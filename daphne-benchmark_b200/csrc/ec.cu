@@ -33,6 +33,7 @@
 #include <vector>
 
 #include "../../include/ndt_b200.h"
+#include "ec_pose.h"
 #include "grid_build.h"
 
 namespace ec {
@@ -426,6 +427,7 @@ int segment_clouds(ndt_ec *h, const float *xyz, const int *offsets, int c0, int 
     std::vector<std::vector<int>> lab;
     if (int rc = labels_of(h, parts, sizes, tols, lab)) return rc;  // every ring of every cloud in one pass
     std::vector<std::vector<int>> cl;
+    std::vector<ec::YawJob> yaw;
     for (int c = 0; c < C; ++c) {
         out_off[c0 + c] = np;
         box_off[c0 + c] = nb;
@@ -453,10 +455,13 @@ int segment_clouds(ndt_ec *h, const float *xyz, const int *offsets, int c0, int 
                 const double dim[3] = {l < 0 ? -1 * l : l, w < 0 ? -1 * w : w, ht < 0 ? -1 * ht : ht};
                 if (dim[0] > 0 && dim[1] > 0 && dim[2] > 0 && dim[0] < 15 && dim[1] > 0 && dim[1] < 15 &&
                     hi[2] > -1.5 && lo[2] > -1.5 && lo[2] < 1.0) {
-                    // position, orientation (x, y, z, w; the yaw is not estimated here: identity), dimensions
+                    // position, orientation (x, y, z, w: z and w by the yaw pass below), dimensions
                     const double b[10] = {lo[0] + l / 2, lo[1] + w / 2, lo[2] + ht / 2, 0.0, 0.0, 0.0, 1.0,
                                           dim[0], dim[1], dim[2]};
                     std::memcpy(boxes + 10 * (size_t)nb, b, sizeof(b));
+                    // the yaw only of kept boxes: the others are not output
+                    yaw.push_back({out_xyz + 3 * (size_t)(np - (int)idx.size()), (int)idx.size(), lo[0], lo[1],
+                                   boxes + 10 * (size_t)nb + 5, boxes + 10 * (size_t)nb + 6});
                     std::memcpy(centroids + 3 * (size_t)nb, cen, sizeof(cen));
                     ++nb;
                 }
@@ -465,6 +470,7 @@ int segment_clouds(ndt_ec *h, const float *xyz, const int *offsets, int c0, int 
     }
     out_off[c1] = np;
     box_off[c1] = nb;
+    ec::box_yaws(yaw.data(), (int)yaw.size());
     return NDT_OK;
 }
 }  // namespace
@@ -481,6 +487,19 @@ int ndt_ec_segment(ndt_ec *h, const float *xyz, int n, float *out_xyz, int *out_
     *out_n = np;
     *num_boxes = nb;
     *num_centroids = nb;
+    return NDT_OK;
+}
+
+int ndt_ec_box_yaw(const float *xyz, int n, double *qz, double *qw) {
+    if (n < 0 || (n > 0 && !xyz) || !qz || !qw) return NDT_E_ARG;
+    float lo[2] = {std::numeric_limits<float>::max(), std::numeric_limits<float>::max()};
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < 2; ++k) {
+            const float v = xyz[3 * (size_t)i + k];
+            if (!std::isfinite(v)) return NDT_E_ARG;
+            if (v < lo[k]) lo[k] = v;
+        }
+    ec::box_yaw(xyz, n, lo[0], lo[1], qz, qw);
     return NDT_OK;
 }
 

@@ -24,10 +24,23 @@ def _lib():
         L.ndt_ec_segment.argtypes = [p, p, C.c_int, p, C.POINTER(C.c_int), p, C.POINTER(C.c_int), p,
                                      C.POINTER(C.c_int)]
         L.ndt_ec_segment_batch.argtypes = [p, C.c_int, p, p, p, p, p, p, p]
-        for n in ("ndt_ec_create", "ndt_ec_labels", "ndt_ec_extract", "ndt_ec_segment", "ndt_ec_segment_batch"):
+        L.ndt_ec_box_yaw.argtypes = [p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        for n in ("ndt_ec_create", "ndt_ec_labels", "ndt_ec_extract", "ndt_ec_segment", "ndt_ec_segment_batch",
+                  "ndt_ec_box_yaw"):
             getattr(L, n).restype = C.c_int
         L._ec_ready = True
     return L
+
+
+def box_yaw(xyz):
+    """Yaw quaternion (z, w) of one cluster's box (host code, no GPU): ndt_ec_box_yaw."""
+    L = _lib()
+    p = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
+    qz, qw = C.c_double(), C.c_double()
+    rc = L.ndt_ec_box_yaw(p.ctypes.data, len(p), C.byref(qz), C.byref(qw))
+    if rc != 0:
+        raise _ndt.NdtError(f"ndt_ec_box_yaw: {_ndt.ERRORS.get(rc, rc)}")
+    return qz.value, qw.value
 
 
 class EuclideanClusters:

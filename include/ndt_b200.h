@@ -398,10 +398,11 @@ NDT_API int ndt_voxel_filter_device(ndt_filter *f, int B, const float *d_points,
  * points (out_xyz, capacity 3n floats; the reference colours them all
  * r, g, b = 10, 20, 30), the boxes that pass the reference's size filter (10
  * doubles each: position xyz, orientation xyzw, dimensions xyz; capacity 10n)
- * and their centroids (3 doubles each; capacity 3n).  The box yaw (the
- * reference's minimum-area-rectangle pose estimate) is not computed: the
- * orientation is the identity.  NDT_E_CAPACITY when a cloud spans more than
- * 2^28 cells of the tolerance.
+ * and their centroids (3 doubles each; capacity 3n).  The orientation is the
+ * yaw of the reference's pose estimate (:720-745): the direction of the
+ * minimum-area rectangle around the cluster's xy points (convex hull and
+ * rotating calipers), as ndt_ec_box_yaw gives it.  NDT_E_CAPACITY when a cloud
+ * spans more than 2^28 cells of the tolerance.
  */
 typedef struct ndt_ec ndt_ec;
 NDT_API int ndt_ec_create(int device, ndt_ec **out);
@@ -412,6 +413,14 @@ NDT_API int ndt_ec_extract(ndt_ec *ec, const float *xyz, int n, float tolerance,
                            int *num_clusters, int *cluster_offsets, int *cluster_indices);
 NDT_API int ndt_ec_segment(ndt_ec *ec, const float *xyz, int n, float *out_xyz, int *out_n, double *boxes,
                            int *num_boxes, double *centroids, int *num_centroids);
+/* Host only (no device work): the yaw quaternion (z, w; x = y = 0) of one
+ * cluster's box from its n points (xyz, 3 floats each), as clusterAndColor
+ * computes it (kernel.cpp:720-745, minAreaRectAngle :479-502) with one
+ * difference: the reference's minAreaRectAngle hands rotatingCalipers the
+ * cluster's point count as the hull's length and reads past the end of the
+ * hull, which makes its yaw depend on memory contents; here the hull's own
+ * length is used.  NDT_E_ARG for a non-finite x or y. */
+NDT_API int ndt_ec_box_yaw(const float *xyz, int n, double *qz, double *qw);
 /* The same for C clouds packed in xyz (offsets: C + 1 point offsets), up to 8 clouds per GPU pass: cloud c's
  * clustered points are out_xyz[out_offsets[c] .. out_offsets[c + 1]), its boxes and centroids
  * [box_offsets[c] .. box_offsets[c + 1]) (capacities as above with n = offsets[C]). */

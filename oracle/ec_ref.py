@@ -153,3 +153,22 @@ class Reference:
         k = self.L.ref_ec_segment(p.ctypes.data, n, pts.ctypes.data, n, boxes.ctypes.data, n, cen.ctypes.data, n,
                                   C.byref(nb), C.byref(nc))
         return pts[:k], boxes[:nb.value], cen[:nc.value]
+
+    def box_yaw(self, xyz):
+        """clusterAndColor's pose estimate for one cluster (kernel.cpp:720-745) through the reference's
+        convexHull and rotatingCalipers, given the hull's own length (minAreaRectAngle hands them the
+        cluster's point count and reads past the hull).  Returns (angle_deg, qz, qw)."""
+        p = np.ascontiguousarray(xyz, np.float32)
+        qz, qw = C.c_double(), C.c_double()
+        self.L.ref_ec_box_yaw.restype = C.c_float
+        self.L.ref_ec_box_yaw.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        a = self.L.ref_ec_box_yaw(p.ctypes.data, len(p), C.byref(qz), C.byref(qw))
+        return float(a), qz.value, qw.value
+
+    def convex_hull(self, xy):
+        """The reference's convexHull (kernel.cpp:376-470), clockwise, as points."""
+        p = np.ascontiguousarray(xy, np.float32)
+        out = np.zeros((max(len(p), 1), 2), np.float32)
+        self.L.ref_ec_convex_hull.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        k = self.L.ref_ec_convex_hull(p.ctypes.data, len(p), out.ctypes.data)
+        return out[:k]

@@ -85,3 +85,58 @@ REF_API int ref_ec_segment(const float *xyz, int n, float *out_xyz, int cap_pts,
     *nc = (int)ce.points.size();
     return (int)out.size();
 }
+
+// The box yaw of clusterAndColor's pose estimate (kernel.cpp:720-745) for one
+// cluster (xyz: its points), through the reference's own convexHull and
+// rotatingCalipers, with one change: minAreaRectAngle (:479-502) hands
+// rotatingCalipers the CLUSTER's point count as the hull's length and so
+// reads past the end of the hull (its result then depends on heap contents);
+// here the hull's own length is used, for both of its branches.  Writes the
+// quaternion's z and w (x = y = 0) and returns the angle in degrees.
+REF_API float ref_ec_box_yaw(const float *xyz, int n, double *qz, double *qw) {
+    float min_x = std::numeric_limits<float>::max(), min_y = std::numeric_limits<float>::max();
+    for (int i = 0; i < n; ++i) {
+        if (xyz[3 * i] < min_x) min_x = xyz[3 * i];
+        if (xyz[3 * i + 1] < min_y) min_y = xyz[3 * i + 1];
+    }
+    std::vector<Point2D> inner;
+    for (int i = 0; i < n; ++i) {  // as :724-730
+        Point2D ip;
+        ip.x = (xyz[3 * i] + fabs(min_x)) * 8;
+        ip.y = (xyz[3 * i + 1] + fabs(min_y)) * 8;
+        inner.push_back(ip);
+    }
+    float angle = 0.0f;
+    if (n > 0) {
+        std::vector<Point2D> hull;
+        convexHull(inner, hull, true, true);
+        const int h = (int)hull.size();
+        Point2D out[3];
+        if (h > 2) {
+            rotatingCalipers(hull.data(), h, (float *)out);
+            angle = (float)atan2((double)out[1].y, (double)out[1].x);
+        } else if (h == 2) {
+            double dx = hull[1].x - hull[0].x;
+            double dy = hull[1].y - hull[0].y;
+            angle = (float)atan2(dy, dx);
+        }
+        angle = (float)(angle * 180.0 / PI);
+    }
+    const double rz = n > 0 ? angle * PI / 180.0 : 0.0;
+    *qz = sin(rz * 0.5);
+    *qw = cos(rz * 0.5);
+    return angle;
+}
+
+// convexHull (kernel.cpp:376-470) of n 2-D points (clockwise, returnPoints):
+// writes the hull's points to out (capacity n) and returns their count.
+REF_API int ref_ec_convex_hull(const float *xy, int n, float *out) {
+    std::vector<Point2D> pts(n), hull;
+    for (int i = 0; i < n; ++i) pts[i] = {xy[2 * i], xy[2 * i + 1]};
+    convexHull(pts, hull, true, true);
+    for (size_t i = 0; i < hull.size(); ++i) {
+        out[2 * i] = hull[i].x;
+        out[2 * i + 1] = hull[i].y;
+    }
+    return (int)hull.size();
+}

@@ -10,7 +10,11 @@ data/ec_output.dat.gz, checks that the UNMODIFIED reference kernel
 acceptance rule (the oracle pin), and writes ec_cases.npz: per test case the
 input cloud, the reference's clusters of each distance ring (extract()'s
 output: sizes and point indices into the ring's cloud, in its order), and the
-reference's segmentByDistance boxes and centroids.
+reference's segmentByDistance boxes and centroids, and per kept box the yaw
+quaternion (z, w) of the reference's pose estimate computed with the hull's
+own length (oracle/ec_shim.cpp ref_ec_box_yaw: the reference's
+minAreaRectAngle reads past the end of the hull, so its own yaw is not
+reproducible).
 """
 from __future__ import annotations
 
@@ -36,6 +40,14 @@ def rings(xyz):
     return [xyz[r == k] for k in range(5)]
 
 
+def kept(pts):
+    """clusterAndColor's box filter (kernel.cpp:747-749) on a cluster's float extents."""
+    lo, hi = pts.min(0), pts.max(0)
+    d = hi - lo
+    return bool(d[0] > 0 and d[1] > 0 and d[2] > 0 and d[0] < 15 and d[1] < 15 and hi[2] > -1.5 and lo[2] > -1.5
+                and lo[2] < 1.0)
+
+
 def main():
     ins = ec_ref.read_input(REF_DATA / "ec_input.dat.gz")
     outs = ec_ref.read_output(REF_DATA / "ec_output.dat.gz", len(ins))
@@ -49,10 +61,16 @@ def main():
         arrays[f"boxes{i}"] = b10
         arrays[f"centroids{i}"] = cen
         arrays[f"npts{i}"] = np.array(len(pts))
+        yaw = []
         for k, cloud in enumerate(rings(xyz)):
             cl = ref.extract(cloud, RING_TOL[k])
             arrays[f"sizes{i}_{k}"] = np.array([len(c) for c in cl], np.int32)
             arrays[f"idx{i}_{k}"] = (np.concatenate(cl) if cl else np.zeros(0)).astype(np.uint16)
+            for c in cl:
+                if kept(cloud[c]):
+                    yaw.append(ref.box_yaw(cloud[c])[1:])
+        assert len(yaw) == len(b10)
+        arrays[f"yaw{i}"] = np.array(yaw, np.float64).reshape(-1, 2)
     np.savez_compressed(HERE / "ec_cases.npz", **arrays)
     print("wrote", HERE / "ec_cases.npz")
 

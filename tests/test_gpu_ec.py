@@ -2,7 +2,8 @@
 reference kernel's own results on its own data (tests/golden/ec_cases.npz,
 made by tests/golden/make_ec_fixtures.py): extract()'s clusters per distance
 ring identical (sizes, point indices, order); segmentByDistance's boxes and
-centroids identical bit for bit (the box yaw is not computed here) and the
+centroids identical bit for bit (the box yaw against the reference's pose
+estimate taken with the hull's own length) and the
 reference's acceptance rule met; labels against brute force on small clouds."""
 import pathlib
 
@@ -56,6 +57,9 @@ def test_segment_equals_reference(ecg, gold):
         assert len(boxes) == len(rb) and len(cen) == len(rc)
         # same boxes (position, dimensions) and centroids, bit for bit, in the same order
         assert np.array_equal(boxes[:, [0, 1, 2, 7, 8, 9]].view(np.uint64), rb[:, [0, 1, 2, 7, 8, 9]].copy().view(np.uint64))
+        # orientation: (0, 0, z, w) with the pose estimate's yaw (taken with the hull's own length)
+        assert np.all(boxes[:, 3:5] == 0.0)
+        assert np.array_equal(boxes[:, 5:7].copy().view(np.uint64), gold[f"yaw{i}"].view(np.uint64))
         assert np.array_equal(cen.view(np.uint64), rc.view(np.uint64))
         # the clustered points: ring by ring, cluster by cluster, as the reference appends them
         ref_pts = np.concatenate([ring[gold[f"idx{i}_{k}"].astype(np.int64)]
