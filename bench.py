@@ -233,15 +233,50 @@ def cpu_baseline(pkg, scene, aligns, mode):
         kind = "port"
         fn = lambda: orc.align_batch(prm, scans, guesses, scene.map, nthreads=cores)  # noqa: E731
         what = "FP64 restatement (oracle), shared grid"
-    fn()  # warm
+    rate, reps, t = _rate(fn, n, 3.0, 20)
+    res = {"value": rate, "unit": "aligns/s", "cores": cores, "kind": kind,
+           "sample": f"{n} alignments of the step x {reps} repetitions ({t:.1f} s wall), {what}"}
+    if mode == "compat" and kind == "reference":
+        res["variants"] = cpu_variants(binding, scene, aligns, cores)
+    return res
+
+
+def _rate(fn, n, budget_s, max_reps):
+    """Alignments per second of fn (n alignments per call): one warm call, then calls until the budget."""
+    fn()
     reps, t = 0, 0.0
-    while t < 3.0 and reps < 20:
+    while t < budget_s and reps < max_reps:
         t0 = time.perf_counter()
         fn()
         t += time.perf_counter() - t0
         reps += 1
-    return {"value": n * reps / t, "unit": "aligns/s", "cores": cores, "kind": kind,
-            "sample": f"{n} alignments of the step x {reps} repetitions ({t:.1f} s wall), {what}"}
+    return n * reps / t, reps, t
+
+
+def cpu_variants(binding, scene, aligns, cores):
+    """The other CPU arms of the same workload, each on a bounded sample (about 2 s): the serial reference on one
+    thread, the reference's OpenMP build (its own threading inside each alignment, all cores, alignments in turn)
+    and the FP64 corrected-NDT oracle (up to 30 Newton iterations with line search) on all cores."""
+    out = {}
+    n1 = min(len(aligns), 16)
+    scans = [a.scan for a in aligns[:n1]]
+    guesses = np.stack([a.guess for a in aligns[:n1]])
+    ref = binding.Reference("serial")
+    r, reps, t = _rate(lambda: ref.align_batch(scans, guesses, [scene.map] * n1, nthreads=1), n1, 2.0, 10)
+    out["reference_serial_1_thread"] = {"value": r, "cores": 1, "sample": f"{n1} alignments x {reps} ({t:.1f} s)"}
+    if binding.Reference.available("omp"):
+        omp = binding.Reference("omp")
+        r, reps, t = _rate(lambda: omp.align_batch(scans, guesses, [scene.map] * n1, nthreads=1), n1, 2.0, 10)
+        out["reference_openmp"] = {"value": r, "cores": int(os.environ.get("OMP_NUM_THREADS", cores)),
+                                   "sample": f"{n1} alignments x {reps} ({t:.1f} s), src/OpenMP/ndt_mapping"}
+    nf = min(len(aligns), max(16, 2 * cores))
+    orc = binding.Oracle()
+    prm = binding.corrected_params()
+    scans_f = [a.scan for a in aligns[:nf]]
+    guesses_f = np.stack([a.guess for a in aligns[:nf]])
+    r, reps, t = _rate(lambda: orc.align_batch(prm, scans_f, guesses_f, scene.map, nthreads=cores), nf, 2.0, 10)
+    out["corrected_fp64_oracle"] = {"value": r, "cores": cores, "sample": f"{nf} alignments x {reps} ({t:.1f} s)"}
+    return out
 
 
 def accuracy(pkg, scene, aligns, out, conv, mode, resolution):
