@@ -8,8 +8,8 @@
 // size, timer pauses around reading and checking, the acceptance rule of
 // check_next_outputs (both sides sorted, equal sizes, max |difference| of
 // points, box position / dimensions / orientation x and y, centroids,
-// <= 0.001) and exit(-3) on I/O errors.  The box yaw (orientation z, w) is not
-// estimated (the rule does not compare it).
+// <= 0.001) and exit(-3) on I/O errors.  The library computes the box yaw
+// (orientation z, w) too; the rule does not compare it.
 //
 // Environment: EC_INPUT / EC_OUTPUT override the data paths, EC_DEVICE the
 // CUDA device.
