@@ -26,6 +26,7 @@
 // Compiled with -ffp-contract=off: every product and sum rounds on its own.
 #include "ec_pose.h"
 
+#include <omp.h>
 #include <stdint.h>
 
 #include <algorithm>
@@ -242,9 +243,10 @@ void box_yaw(const float *xyz, int n, float min_x, float min_y, double *qz, doub
 }
 
 void box_yaws(const YawJob *jobs, int count) {
-    // independent clusters over the host's threads (the larger ones first would balance better; the
-    // dynamic schedule in small chunks does most of that)
-#pragma omp parallel for schedule(dynamic, 2) num_threads(kYawThreads) if (count > 4)
+    // independent clusters over the host's threads (at most kYawThreads, at most the cores there are), in a
+    // dynamic schedule of small chunks so that one large cluster does not hold up the others' threads
+    const int threads = std::max(1, std::min(kYawThreads, omp_get_num_procs()));
+#pragma omp parallel for schedule(dynamic, 2) num_threads(threads) if (count > 4 && threads > 1)
     for (int j = 0; j < count; ++j) box_yaw(jobs[j].xyz, jobs[j].n, jobs[j].min_x, jobs[j].min_y, jobs[j].qz, jobs[j].qw);
 }
 
