@@ -31,6 +31,7 @@
 
 #include "../../include/ndt_b200.h"
 #include "ctx_view.h"
+#include "nvtx_range.h"
 
 struct ndt_dat {
     int fd = -1;
@@ -250,6 +251,7 @@ int ndt_dat_map_relation(const ndt_dat *d, int i) {
 
 int ndt_dat_align(ndt_ctx *ctx, ndt_dat *d, int first, int count, float *out16, int *converged, double *fitness,
                   int *status) {
+    ndt::NvtxRange range("dat align");
     if (!ctx || !d || first < 0 || count < 0 || (long long)first + count > d->T ||
         (count > 0 && (!out16 || !converged || !fitness)))
         return d ? fail(d, NDT_E_ARG, "bad argument") : NDT_E_ARG;

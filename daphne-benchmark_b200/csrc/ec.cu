@@ -35,6 +35,7 @@
 #include "../../include/ndt_b200.h"
 #include "ec_pose.h"
 #include "grid_build.h"
+#include "nvtx_range.h"
 
 namespace ec {
 
@@ -222,6 +223,7 @@ cudaError_t ensure(void **p, size_t *cap, size_t bytes) {
 // smallest index within cloud p of point i's component (clouds never join).
 int labels_of(ndt_ec *h, const std::vector<const float *> &xyz, const std::vector<int> &n,
               const std::vector<float> &tolerance, std::vector<std::vector<int>> &labels) {
+    ndt::NvtxRange range("ec labels");
     const int np = (int)xyz.size();
     labels.assign(np, std::vector<int>());
     ec::Parts P;
@@ -470,7 +472,10 @@ int segment_clouds(ndt_ec *h, const float *xyz, const int *offsets, int c0, int 
     }
     out_off[c1] = np;
     box_off[c1] = nb;
-    ec::box_yaws(yaw.data(), (int)yaw.size());
+    {
+        ndt::NvtxRange range("ec yaw");
+        ec::box_yaws(yaw.data(), (int)yaw.size());
+    }
     return NDT_OK;
 }
 }  // namespace

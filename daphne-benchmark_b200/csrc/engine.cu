@@ -16,6 +16,7 @@
 #include "../../include/ndt_b200.h"
 #include "align.h"
 #include "ctx_view.h"
+#include "nvtx_range.h"
 #include "derivatives.h"
 #include "grid_build.h"
 #include "ndt_types.h"
@@ -366,6 +367,7 @@ int ensure_records(ndt_ctx *c, int m) {
 }
 
 int build_grid(ndt_ctx *c, const float4 *d_map, int m) {
+    NvtxRange range("grid build");
     if (m <= 0) return fail(c, NDT_E_ARG, "map must have at least one point");
     // voxel slots travel in 26 bits of a packed pair code (slot << 6 | flag << 5 | lane)
     if (m >= (1 << 25)) return fail(c, NDT_E_CAPACITY, "map larger than 2^25 points");
@@ -665,6 +667,7 @@ int get_batch_graph(ndt_ctx *c, const RunPlan &R, cudaGraphExec_t *out) {
 // call (alignment groups of one host batch).
 int run_batch(ndt_ctx *c, int B, const float4 *d_points, const int *d_offsets, int total, const float *d_guesses,
               float *d_out, int *d_conv, double *d_fit, int *d_status, bool first = true) {
+    NvtxRange range("rounds");
     if (!c->have_map) return fail(c, NDT_E_NOMAP, "no map set");
     if (B <= 0 || total < 0) return fail(c, NDT_E_ARG, "empty batch");
     const int tile = c->prm.precision == 1 ? kTile : kDerivVariants[c->variant].tile;
@@ -838,6 +841,7 @@ int staged_batch(ndt_ctx *c, int B, const int *off, const float *guesses, float 
         while (b1 < B - (G - 1 - k) && off[b1] < target) ++b1;
         bound[k + 1] = b1;
     }
+    NvtxRange range("host batch");
     if (int rc = before_copies()) return rc;
     CK(cudaMemcpyAsync(c->offsets.p, off, sizeof(int) * (size_t)(B + 1), cudaMemcpyHostToDevice, cs));
     CK(cudaMemcpyAsync(c->guesses.p, guesses, sizeof(float) * 16 * (size_t)B, cudaMemcpyHostToDevice, cs));
@@ -1066,6 +1070,7 @@ int ndt_set_map_device(ndt_ctx *c, const float *d_map, int m) {
 // bounding box, else by a full build of the grown map.  Either way the grid
 // equals ndt_set_map of the whole grown map.
 int map_append(ndt_ctx *c, const float *pts, int k, bool host) {
+    NvtxRange range("map append");
     if (!c) return NDT_E_ARG;
     if (k < 0 || (k > 0 && !pts)) return fail(c, NDT_E_ARG, "null points or negative count");
     if (int rc = set_device(c)) return rc;

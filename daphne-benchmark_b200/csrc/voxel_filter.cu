@@ -31,6 +31,7 @@
 
 #include "../../include/ndt_b200.h"
 #include "grid_build.h"
+#include "nvtx_range.h"
 
 namespace vf {
 
@@ -360,6 +361,7 @@ void *ndt_filter_stream(ndt_filter *f) { return f ? (void *)f->stream : nullptr;
 
 int ndt_voxel_filter_device(ndt_filter *f, int B, const float *d_points, const int *d_offsets, int total_points,
                             float leaf, float *d_out, int *d_out_offsets, int *out_total) {
+    ndt::NvtxRange range("voxel filter");
     if (!f || B <= 0 || total_points < 0 || !d_points || !d_offsets || !d_out || !d_out_offsets || !out_total ||
         !(leaf > 0.0f) || !std::isfinite(leaf)) {
         if (f) f->msg = "bad argument";
