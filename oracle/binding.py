@@ -104,6 +104,18 @@ class Oracle:
         L.oracle_trial_value.restype = C.c_double
         L.oracle_update_interval.argtypes = [_f64p, C.c_double, C.c_double, C.c_double]
         L.oracle_update_interval.restype = C.c_int
+        L.oracle_radius_search.argtypes = [P, _f32p, C.c_int, _f32p, _f64p, C.c_int]
+        L.oracle_radius_search.restype = C.c_int
+
+    def radius_search(self, prm, cloud, pt):
+        """Mode R voxelRadiusSearch (kernel.cpp:246-286): means of the neighbour cells of pt (x, y, z, w)."""
+        cloud = np.ascontiguousarray(cloud, np.float32)
+        means = np.zeros((64, 3))
+        k = self.lib.oracle_radius_search(C.byref(prm), cloud, cloud.shape[0],
+                                          np.ascontiguousarray(pt, np.float32).reshape(4), means, 64)
+        if k < 0:
+            raise RuntimeError(f"oracle_radius_search failed: {k}")
+        return means[:k]
 
     def gauss(self, prm):
         d1, d2 = C.c_double(), C.c_double()
@@ -277,6 +289,14 @@ class Reference:
                                      np.ascontiguousarray(trans, np.float32), scan.shape[0],
                                      np.ascontiguousarray(p6, np.float64), d1, d2, int(hessian), g, H)
         return s, g, H.reshape(6, 6)
+
+    def radius_search(self, cloud, pt):
+        """The reference's voxelRadiusSearch (kernel.cpp:246-286) on the grid of cloud."""
+        cloud = np.ascontiguousarray(cloud, np.float32)
+        means = np.zeros((64, 3))
+        k = self.lib.ref_radius_search(cloud, cloud.shape[0], np.ascontiguousarray(pt, np.float32).reshape(4),
+                                       means, 64)
+        return means[:min(k, 64)]
 
     def build_tm(self, p6, base=None):
         m = np.eye(4, dtype=np.float32).reshape(16).copy() if base is None else \

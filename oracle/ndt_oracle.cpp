@@ -851,6 +851,19 @@ ORACLE_API long long oracle_grid(const ndt_params *prm, const float *map, int m,
     return g.G;
 }
 
+// voxelRadiusSearch (kernel.cpp:246-286) of Mode R on the grid of `map`:
+// number of neighbour cells of point pt4 (their means to means3, up to cap).
+ORACLE_API int oracle_radius_search(const ndt_params *prm, const float *map, int m, const float *pt4,
+                                    double *means3, int cap) {
+    Grid g;
+    if (!prm->compat || !build_grid(*prm, g, map, m)) return NDT_E_GRID;
+    int idx[64];
+    const int k = radius_search_r(g, pt4, g.res, idx);
+    for (int i = 0; i < k && i < cap; ++i)
+        for (int e = 0; e < 3; ++e) means3[3 * i + e] = g.mean[3 * (size_t)idx[i] + e];
+    return k;
+}
+
 ORACLE_API double oracle_derivatives(const ndt_params *prm, const float *map, int m,
                                      const float *scan, const float *trans, int n, const double *p6,
                                      int hessian, double *g6, double *H36, long long *pairs) {

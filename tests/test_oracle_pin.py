@@ -217,3 +217,35 @@ def test_reference_golden_output_file(pkg):
         # the rotation block is a proper rotation (float accuracy)
         R = T[:3, :3]
         assert np.allclose(R @ R.T, np.eye(3), atol=2e-5) and abs(np.linalg.det(R) - 1) < 2e-5
+
+
+def test_radius_search_known_answers(oracle, reference, binding_mod):
+    """voxelRadiusSearch (kernel.cpp:246-286): 27 float probes p + {-r, 0, r}^3, each skipped outside the
+    bounding box; cells kept when the float distance to their mean is < r.  Oracle == reference (same cells,
+    same order) at the box's corners, edges and faces, on cell boundaries, inside and far outside."""
+    prm = binding_mod.reference_params()
+    rng = np.random.default_rng(21)
+    cloud = np.ones((3000, 4), np.float32)
+    cloud[:, :3] = rng.uniform([0, 0, 0], [9.5, 7.25, 2.5], (3000, 3)).astype(np.float32)
+    bbox = reference.grid(cloud, cells=False)[0]
+    lo, hi = bbox[:3].astype(np.float64), bbox[3:].astype(np.float64)
+    probes = []
+    for cx in (lo[0], hi[0], (lo[0] + hi[0]) / 2):
+        for cy in (lo[1], hi[1], (lo[1] + hi[1]) / 2):
+            for cz in (lo[2], hi[2], (lo[2] + hi[2]) / 2):
+                for d in (-0.6, -0.001, 0.0, 0.001, 0.6):
+                    probes.append((cx + d, cy - d, cz + d))
+    for k in range(1, 6):  # exactly on cell boundaries
+        probes.append((lo[0] + k, lo[1] + k, lo[2] + 1))
+    probes += [tuple(p) for p in rng.uniform(lo - 1.5, hi + 1.5, (200, 3))]
+    probes.append((lo[0] - 50, lo[1], lo[2]))  # far outside: every probe skipped
+    counts = []
+    for p in probes:
+        pt = np.array([p[0], p[1], p[2], 1.0], np.float32)
+        r, o = reference.radius_search(cloud, pt), oracle.radius_search(prm, cloud, pt)
+        assert np.array_equal(r.view(np.uint64), o.view(np.uint64)) or \
+            (r.shape == o.shape and np.array_equal(np.isnan(r), np.isnan(o)) and np.array_equal(r[~np.isnan(r)], o[~np.isnan(o)])), p
+        counts.append(len(o))
+        assert len(o) <= 27
+    assert counts[-1] == 0
+    assert max(counts) >= 4  # cells count only when their mean is within r, so far fewer than 27
