@@ -106,6 +106,17 @@ class Oracle:
         L.oracle_update_interval.restype = C.c_int
         L.oracle_radius_search.argtypes = [P, _f32p, C.c_int, _f32p, _f64p, C.c_int]
         L.oracle_radius_search.restype = C.c_int
+        L.oracle_update_pair.argtypes = [P, _f64p, _f64p, _f64p, _f64p, C.c_int, _f64p, _f64p]
+        L.oracle_update_pair.restype = C.c_double
+
+    def update_pair(self, prm, p6, x, xt, icov, hessian=True, g=None, H=None):
+        """One (point, cell) pair's derivative update (updateDerivatives, kernel.cpp:438-493).
+        Returns (score increment, g, H) with g / H accumulated from the given ones (zeros by default)."""
+        g = np.zeros(6) if g is None else np.array(g, np.float64)
+        H = np.zeros(36) if H is None else np.array(H, np.float64).reshape(36)
+        f = lambda a: np.ascontiguousarray(a, np.float64)  # noqa: E731
+        s = self.lib.oracle_update_pair(C.byref(prm), f(p6), f(x), f(xt), f(np.reshape(icov, 9)), int(hessian), g, H)
+        return s, g, H.reshape(6, 6)
 
     def radius_search(self, prm, cloud, pt):
         """Mode R voxelRadiusSearch (kernel.cpp:246-286): means of the neighbour cells of pt (x, y, z, w)."""
@@ -230,6 +241,8 @@ class Reference:
         L.ref_derivatives.restype = C.c_double
         L.ref_radius_search.argtypes = [_f32p, C.c_int, _f32p, _f64p, C.c_int]
         L.ref_radius_search.restype = C.c_int
+        L.ref_update_pair.argtypes = [_f64p, _f64p, _f64p, _f64p, C.c_double, C.c_double, C.c_int, _f64p, _f64p]
+        L.ref_update_pair.restype = C.c_double
         L.ref_build_tm.argtypes = [_f64p, _f32p]
         L.ref_euler.argtypes = [_f32p, _f64p]
         L.ref_solve.argtypes = [_f64p, _f64p, _f64p]
@@ -288,6 +301,14 @@ class Reference:
                                      np.ascontiguousarray(scan, np.float32),
                                      np.ascontiguousarray(trans, np.float32), scan.shape[0],
                                      np.ascontiguousarray(p6, np.float64), d1, d2, int(hessian), g, H)
+        return s, g, H.reshape(6, 6)
+
+    def update_pair(self, p6, x, xt, icov, d1, d2, hessian=True, g=None, H=None):
+        """The reference's computeAngleDerivatives + computePointDerivatives + updateDerivatives for one pair."""
+        g = np.zeros(6) if g is None else np.array(g, np.float64)
+        H = np.zeros(36) if H is None else np.array(H, np.float64).reshape(36)
+        f = lambda a: np.ascontiguousarray(a, np.float64)  # noqa: E731
+        s = self.lib.ref_update_pair(f(p6), f(x), f(xt), f(np.reshape(icov, 9)), d1, d2, int(hessian), g, H)
         return s, g, H.reshape(6, 6)
 
     def radius_search(self, cloud, pt):

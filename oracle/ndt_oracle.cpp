@@ -851,6 +851,20 @@ ORACLE_API long long oracle_grid(const ndt_params *prm, const float *map, int m,
     return g.G;
 }
 
+// One pair: angle terms of p, point terms of x, then update_pair with the
+// offset xt from the cell mean and the inverse covariance C (row major);
+// g6 / H36 accumulate in place; returns the score increment.
+ORACLE_API double oracle_update_pair(const ndt_params *prm, const double *p6, const double *x3, const double *xt3,
+                                     const double *C9, int hessian, double *g6, double *H36) {
+    Gauss gs;
+    gauss_consts(*prm, gs);
+    AngleTerms A;
+    angle_terms(p6, A);
+    PointTerms P;
+    point_terms(A, x3, P);
+    return update_pair(gs, P, xt3, C9, hessian != 0, prm->compat != 0, g6, H36);
+}
+
 // voxelRadiusSearch (kernel.cpp:246-286) of Mode R on the grid of `map`:
 // number of neighbour cells of point pt4 (their means to means3, up to cap).
 ORACLE_API int oracle_radius_search(const ndt_params *prm, const float *map, int m, const float *pt4,

@@ -160,6 +160,37 @@ REF_API double ref_derivatives(const float *map, int m, const float *scan, const
     return score;
 }
 
+// One pair through the reference's own routines: computeAngleDerivatives(p)
+// (kernel.cpp:707), computePointDerivatives(x) (:495) and updateDerivatives
+// (:438) with the scan point x, its offset from the cell mean xt and the
+// cell's inverse covariance C (row major).  g6 / H36 are accumulated in
+// place; returns the score increment (0 when the pair is rejected).
+REF_API double ref_update_pair(const double *p6, const double *x3, const double *xt3, const double *C9, double d1,
+                               double d2, int hessian, double *g6, double *H36) {
+    ndt_mapping &k = thread_instance();
+    k.gauss_d1_ = d1;
+    k.gauss_d2_ = d2;
+    std::memset(k.point_gradient_.data, 0, sizeof(k.point_gradient_.data));
+    k.point_gradient_.data[0][0] = 1.0;
+    k.point_gradient_.data[1][1] = 1.0;
+    k.point_gradient_.data[2][2] = 1.0;
+    std::memset(k.point_hessian_.data, 0, sizeof(k.point_hessian_.data));
+    Vec6 p, g;
+    Vec3 x, xt;
+    Mat33 C;
+    Mat66 H;
+    for (int i = 0; i < 6; ++i) p[i] = p6[i], g[i] = g6[i];
+    for (int i = 0; i < 3; ++i) x[i] = x3[i], xt[i] = xt3[i];
+    for (int i = 0; i < 9; ++i) C.data[i / 3][i % 3] = C9[i];
+    for (int i = 0; i < 36; ++i) H.data[i / 6][i % 6] = H36[i];
+    k.computeAngleDerivatives(p, hessian != 0);
+    k.computePointDerivatives(x, hessian != 0);
+    const double inc = k.updateDerivatives(g, H, xt, C, hessian != 0);
+    for (int i = 0; i < 6; ++i) g6[i] = g[i];
+    for (int i = 0; i < 36; ++i) H36[i] = H.data[i / 6][i % 6];
+    return inc;
+}
+
 // voxelRadiusSearch (kernel.cpp:246) on the grid of `map`: number of
 // neighbour voxels of point xyz; their means go to means3 (up to cap).
 REF_API int ref_radius_search(const float *map, int m, const float *pt4, double *means3, int cap) {

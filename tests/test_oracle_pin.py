@@ -249,3 +249,37 @@ def test_radius_search_known_answers(oracle, reference, binding_mod):
         assert len(o) <= 27
     assert counts[-1] == 0
     assert max(counts) >= 4  # cells count only when their mean is within r, so far fewer than 27
+
+
+def test_update_derivatives_known_answers(oracle, reference, binding_mod):
+    """updateDerivatives (kernel.cpp:438-493) pair by pair: oracle == reference bit for bit (score increment,
+    gradient, Hessian; with and without the Hessian; near-zero angles take the reference's exact 0 / 1 branch),
+    and the rejection branch: when d2 * exp(-d2 xCx / 2) leaves [0, 1] or is NaN the pair adds nothing."""
+    prm = binding_mod.reference_params()
+    d1, d2 = oracle.gauss(prm)
+    rng = np.random.default_rng(17)
+    for t in range(300):
+        p = rng.uniform(-0.5, 0.5, 6)
+        if t % 4 == 0:
+            p[3:] = rng.uniform(-5e-5, 5e-5, 3)  # |angle| < 1e-4: cos 1, sin 0 (kernel.cpp:710-726)
+        x = rng.uniform(-30, 30, 3)
+        xt = rng.normal(0, 0.4, 3)
+        A = rng.normal(size=(3, 3))
+        icov = A @ A.T + 0.1 * np.eye(3)
+        g0, H0 = rng.normal(size=6), rng.normal(size=36)
+        for hess in (True, False):
+            so, go, Ho = oracle.update_pair(prm, p, x, xt, icov, hess, g0, H0)
+            sr, gr, Hr = reference.update_pair(p, x, xt, icov, d1, d2, hess, g0, H0)
+            assert so == sr and np.array_equal(go, gr) and np.array_equal(Ho, Hr), (t, hess)
+    # known answer of an accepted pair: score increment -d1 exp(-d2 xCx / 2)
+    xt = np.array([0.1, -0.2, 0.05])
+    s, g, H = oracle.update_pair(prm, np.zeros(6), np.ones(3), xt, np.eye(3))
+    assert math.isclose(s, -d1 * math.exp(-d2 * float(xt @ xt) / 2), rel_tol=1e-15)
+    # rejection: an indefinite inverse covariance makes xCx < 0, e * d2 > 1 -> nothing added
+    g0, H0 = np.arange(6.0), np.arange(36.0)
+    for icov, xt in ((-np.eye(3), np.array([2.0, 2.0, 2.0])), (np.eye(3), np.array([np.nan, 0.0, 0.0]))):
+        so, go, Ho = oracle.update_pair(prm, np.full(6, 0.1), np.ones(3), xt, icov, True, g0, H0)
+        sr, gr, Hr = reference.update_pair(np.full(6, 0.1), np.ones(3), xt, icov, d1, d2, True, g0, H0)
+        assert so == 0.0 and sr == 0.0
+        assert np.array_equal(go, g0) and np.array_equal(gr, g0)
+        assert np.array_equal(Ho.reshape(36), H0) and np.array_equal(Hr.reshape(36), H0)
