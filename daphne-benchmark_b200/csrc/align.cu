@@ -24,9 +24,9 @@ constexpr double kMu = 1.e-4;     // sufficient decrease (kernel.cpp:1042)
 constexpr double kNu = 0.9;       // curvature condition (kernel.cpp:1044)
 constexpr int kMaxStepIterations = 10;  // kernel.cpp:1039
 
-__device__ void set_angles(AlignState &s, const double *pose) {
+__device__ void set_angles(AlignState &s, const double *pose, bool compat) {
     double a[kAngle];
-    angle_terms(pose, a);
+    angle_terms(pose, a, compat);
     for (int k = 0; k < kAngle; ++k) {
         s.angd[k] = a[k];
         s.angf[k] = (float)a[k];
@@ -38,7 +38,7 @@ __device__ void set_pose(AlignState &s, const StepParams &P) {
         build_tm_compat(s.T, s.x_t);
     else
         build_tm_corrected(s.T, s.x_t);
-    set_angles(s, s.x_t);
+    set_angles(s, s.x_t, P.compat);
 }
 
 __device__ __forceinline__ double dot6(const double *a, const double *b) {
@@ -238,7 +238,7 @@ __global__ void init_kernel(AlignState *__restrict__ states, const float *__rest
         s.evals = 0;
         s.status = 0;
         s.n = offsets[b + 1] - offsets[b];
-        set_angles(s, s.p);
+        set_angles(s, s.p, P.compat);
         s.eval_mode = kEvalFull;
         s.phase = kPhaseInitEval;
     }
@@ -434,12 +434,12 @@ __global__ void tile_fill_kernel(const int *__restrict__ offsets, int B, int til
 // One evaluation request at pose p (test hook: the caller supplies the
 // transformed points, so T is the identity).
 __global__ void prepare_eval_kernel(AlignState *__restrict__ s, const double *__restrict__ p6, int n,
-                                    double *__restrict__ exc) {
+                                    double *__restrict__ exc, int compat) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     for (int k = 0; k < 16; ++k) s->T[k] = (k % 5 == 0) ? 1.0f : 0.0f;
     for (int i = 0; i < 6; ++i) s->x_t[i] = s->p[i] = p6[i];
     double a[kAngle];
-    angle_terms(p6, a);
+    angle_terms(p6, a, compat != 0);
     for (int k = 0; k < kAngle; ++k) {
         s->angd[k] = a[k];
         s->angf[k] = (float)a[k];
@@ -452,8 +452,8 @@ __global__ void prepare_eval_kernel(AlignState *__restrict__ s, const double *__
 
 }  // namespace
 
-int launch_prepare_eval(AlignState *d_state, const double *d_p6, int n, double *d_exc, cudaStream_t st) {
-    prepare_eval_kernel<<<1, 32, 0, st>>>(d_state, d_p6, n, d_exc);
+int launch_prepare_eval(AlignState *d_state, const double *d_p6, int n, double *d_exc, int compat, cudaStream_t st) {
+    prepare_eval_kernel<<<1, 32, 0, st>>>(d_state, d_p6, n, d_exc, compat);
     return (int)cudaGetLastError();
 }
 

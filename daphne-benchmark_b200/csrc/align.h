@@ -26,7 +26,7 @@ int launch_init(AlignState *d_states, const float *d_guesses, const int *d_offse
                 double *d_exc, cudaStream_t st);
 int launch_step(AlignState *d_states, const double *d_partials, const int *d_chunk_begin, double *d_exc, int B,
                 const StepParams &P, int *d_active, Counters *d_counters, cudaStream_t st);
-int launch_prepare_eval(AlignState *d_state, const double *d_p6, int n, double *d_exc, cudaStream_t st);
+int launch_prepare_eval(AlignState *d_state, const double *d_p6, int n, double *d_exc, int compat, cudaStream_t st);
 int launch_score(const double *d_partials, const int *d_chunk_begin, const double *d_exc, int B, double *d_score,
                  cudaStream_t st);
 int launch_finalize(const AlignState *d_states, int B, float *d_out, int *d_conv, double *d_fit, int *d_status,

@@ -1380,7 +1380,8 @@ int ndt_derivatives(ndt_ctx *c, const float *scan, const float *trans, int n, co
     CK(cudaMemsetAsync(c->counters.p, 0, sizeof(Counters), st));
     int rc = launch_tiles(c->offsets.as<int>(), 1, tile, chunk_big(c), chunk_small(c), L, st);
     if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_tiles");
-    rc = launch_prepare_eval(c->states.as<AlignState>(), c->p6.as<double>(), n, c->exc.as<double>(), st);
+    rc = launch_prepare_eval(c->states.as<AlignState>(), c->p6.as<double>(), n, c->exc.as<double>(), c->prm.compat,
+                             st);
     if (rc) return cuda_fail(c, (cudaError_t)rc, "launch_prepare_eval");
     EvalArgs ea;
     ea.grid = grid_dev(c);

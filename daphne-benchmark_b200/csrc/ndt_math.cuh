@@ -21,8 +21,12 @@ __device__ __forceinline__ double std_max(double a, double b) { return (a < b) ?
 
 // Angle derivative terms, eq. 6.19 / 6.21 (computeAngleDerivatives,
 // kernel.cpp:707-825).  out[0..23] = j_ang a..h (3 each), out[24..68] =
-// h_ang a2 a3 b2 b3 c2 c3 d1 d2 d3 e1 e2 e3 f1 f2 f3 (3 each).
-__device__ inline void angle_terms(const double *p, double *o) {
+// h_ang a2 a3 b2 b3 c2 c3 d1 d2 d3 e1 e2 e3 f1 f2 f3 (3 each).  One term
+// differs by mode: the second derivative of the rotated x component in pitch,
+// d^2/db^2 (cy cz, -cy sz, sy) = (-cy cz, cy sz, -sy), has +sy in the
+// reference's h_ang_d1 (kernel.cpp:795-797); compat keeps it, the corrected
+// mode uses -sy.
+__device__ inline void angle_terms(const double *p, double *o, bool compat) {
     double cx, cy, cz, sx, sy, sz;
     if (fabs(p[3]) < 10e-5) { cx = 1.0; sx = 0.0; } else { cx = cos(p[3]); sx = sin(p[3]); }
     if (fabs(p[4]) < 10e-5) { cy = 1.0; sy = 0.0; } else { cy = cos(p[4]); sy = sin(p[4]); }
@@ -44,7 +48,7 @@ __device__ inline void angle_terms(const double *p, double *o) {
     h[9] = (sx * cy * cz);             h[10] = (-sx * cy * sz);           h[11] = (sx * sy);
     h[12] = (-sx * cz - cx * sy * sz); h[13] = (sx * sz - cx * sy * cz);  h[14] = 0;
     h[15] = (cx * cz - sx * sy * sz);  h[16] = (-sx * sy * cz - cx * sz); h[17] = 0;
-    h[18] = (-cy * cz);                h[19] = (cy * sz);                 h[20] = (sy);
+    h[18] = (-cy * cz);                h[19] = (cy * sz);                 h[20] = compat ? sy : -sy;
     h[21] = (-sx * sy * cz);           h[22] = (sx * sy * sz);            h[23] = (sx * cy);
     h[24] = (cx * sy * cz);            h[25] = (-cx * sy * sz);           h[26] = (-cx * cy);
     h[27] = (sy * sz);                 h[28] = (sy * cz);                 h[29] = 0;

@@ -79,7 +79,7 @@ struct Pose6 {
     double p[6];
 };
 
-__global__ void noalloc_setup_kernel(NoAllocScratch *s, Pose6 pose, int n) {
+__global__ void noalloc_setup_kernel(NoAllocScratch *s, Pose6 pose, int n, int compat) {
     const int t = threadIdx.x;
     if (t < kPartial) s->exc[t] = 0.0;
     if (t == 0) {
@@ -93,7 +93,7 @@ __global__ void noalloc_setup_kernel(NoAllocScratch *s, Pose6 pose, int n) {
         for (int k = 0; k < 16; ++k) st.T[k] = (k % 5 == 0) ? 1.0f : 0.0f;
         for (int i = 0; i < 6; ++i) st.x_t[i] = st.p[i] = pose.p[i];
         double a[kAngle];
-        angle_terms(pose.p, a);
+        angle_terms(pose.p, a, compat != 0);
         for (int k = 0; k < kAngle; ++k) {
             st.angd[k] = a[k];
             st.angf[k] = (float)a[k];
@@ -164,7 +164,7 @@ extern "C" int ndt_derivatives_noalloc(ndt_ctx *ctx, const float *d_scan, const 
     const int tile = v.precision == 1 ? kTile : kDerivVariants[v.variant].tile;
     Pose6 pose;
     for (int i = 0; i < 6; ++i) pose.p[i] = p6[i];
-    noalloc_setup_kernel<<<1, 64, 0, st>>>(s, pose, n);
+    noalloc_setup_kernel<<<1, 64, 0, st>>>(s, pose, n, v.compat);
     TileLists L;
     L.tile_begin = s->tile_begin;
     L.tiles = s->tiles;

@@ -271,7 +271,7 @@ struct AngleTerms {
     double h[15][3];
 };
 
-void angle_terms(const double *p, AngleTerms &A) {
+void angle_terms(const double *p, AngleTerms &A, bool compat) {
     double cx, cy, cz, sx, sy, sz;
     if (std::fabs(p[3]) < 10e-5) { cx = 1.0; sx = 0.0; } else { cx = std::cos(p[3]); sx = std::sin(p[3]); }
     if (std::fabs(p[4]) < 10e-5) { cy = 1.0; sy = 0.0; } else { cy = std::cos(p[4]); sy = std::sin(p[4]); }
@@ -292,7 +292,9 @@ void angle_terms(const double *p, AngleTerms &A) {
     h[3][0] = (sx * cy * cz);             h[3][1] = (-sx * cy * sz);            h[3][2] = (sx * sy);    // b3
     h[4][0] = (-sx * cz - cx * sy * sz);  h[4][1] = (sx * sz - cx * sy * cz);   h[4][2] = 0;            // c2
     h[5][0] = (cx * cz - sx * sy * sz);   h[5][1] = (-sx * sy * cz - cx * sz);  h[5][2] = 0;            // c3
-    h[6][0] = (-cy * cz);                 h[6][1] = (cy * sz);                  h[6][2] = (sy);         // d1
+    // d1: d^2/db^2 of the rotated x component is (-cy cz, cy sz, -sy); the
+    // reference has +sy (kernel.cpp:795-797), kept in compat mode only
+    h[6][0] = (-cy * cz);                 h[6][1] = (cy * sz);                  h[6][2] = compat ? sy : -sy;
     h[7][0] = (-sx * sy * cz);            h[7][1] = (sx * sy * sz);             h[7][2] = (sx * cy);    // d2
     h[8][0] = (cx * sy * cz);             h[8][1] = (-cx * sy * sz);            h[8][2] = (-cx * cy);   // d3
     h[9][0] = (sy * sz);                  h[9][1] = (sy * cz);                  h[9][2] = 0;            // e1
@@ -610,7 +612,7 @@ struct Aligner {
         double dummy_g[6];
         double *gg = hessian_only ? dummy_g : g6;
         AngleTerms A;
-        angle_terms(p, A);
+        angle_terms(p, A, prm.compat != 0);
         double score = 0.0;
         int nb[64];
         PointTerms P;
@@ -859,7 +861,7 @@ ORACLE_API double oracle_update_pair(const ndt_params *prm, const double *p6, co
     Gauss gs;
     gauss_consts(*prm, gs);
     AngleTerms A;
-    angle_terms(p6, A);
+    angle_terms(p6, A, prm->compat != 0);
     PointTerms P;
     point_terms(A, x3, P);
     return update_pair(gs, P, xt3, C9, hessian != 0, prm->compat != 0, g6, H36);
