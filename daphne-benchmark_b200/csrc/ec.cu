@@ -508,6 +508,25 @@ int ndt_ec_box_yaw(const float *xyz, int n, double *qz, double *qw) {
     return NDT_OK;
 }
 
+int ndt_ec_box_yaws(int C, const float *xyz, const int *offsets, double *qz, double *qw) {
+    if (C < 0 || (C > 0 && (!offsets || !qz || !qw)) || (C > 0 && offsets[0] != 0)) return NDT_E_ARG;
+    if (C > 0 && offsets[C] > 0 && !xyz) return NDT_E_ARG;
+    std::vector<ec::YawJob> jobs(C);
+    for (int c = 0; c < C; ++c) {
+        if (offsets[c + 1] < offsets[c]) return NDT_E_ARG;
+        float lo[2] = {std::numeric_limits<float>::max(), std::numeric_limits<float>::max()};
+        for (int i = offsets[c]; i < offsets[c + 1]; ++i)
+            for (int k = 0; k < 2; ++k) {
+                const float v = xyz[3 * (size_t)i + k];
+                if (!std::isfinite(v)) return NDT_E_ARG;
+                if (v < lo[k]) lo[k] = v;
+            }
+        jobs[c] = {xyz + 3 * (size_t)offsets[c], offsets[c + 1] - offsets[c], lo[0], lo[1], qz + c, qw + c};
+    }
+    ec::box_yaws(jobs.data(), C);
+    return NDT_OK;
+}
+
 int ndt_ec_segment_batch(ndt_ec *h, int C, const float *xyz, const int *offsets, float *out_xyz, int *out_offsets,
                          double *boxes, int *box_offsets, double *centroids) {
     if (!h || C <= 0 || !offsets || !out_xyz || !out_offsets || !boxes || !box_offsets || !centroids ||

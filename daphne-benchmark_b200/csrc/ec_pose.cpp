@@ -28,8 +28,10 @@
 
 #include <omp.h>
 #include <stdint.h>
+#include <unistd.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -242,10 +244,21 @@ void box_yaw(const float *xyz, int n, float min_x, float min_y, double *qz, doub
     *qw = std::cos(rz * 0.5);
 }
 
+// libgomp's thread pool does not survive fork(): the first process that runs
+// a parallel pass owns it, and a process forked from it after that runs its
+// passes on one thread.
+std::atomic<pid_t> g_pool_owner{0};
+
 void box_yaws(const YawJob *jobs, int count) {
     // independent clusters over the host's threads (at most kYawThreads, at most the cores there are), in a
     // dynamic schedule of small chunks so that one large cluster does not hold up the others' threads
-    const int threads = std::max(1, std::min(kYawThreads, omp_get_num_procs()));
+    int threads = std::max(1, std::min(kYawThreads, omp_get_num_procs()));
+    if (count > 4 && threads > 1) {
+        const pid_t me = getpid();
+        pid_t none = 0;
+        g_pool_owner.compare_exchange_strong(none, me);
+        if (g_pool_owner.load() != me) threads = 1;
+    }
 #pragma omp parallel for schedule(dynamic, 2) num_threads(threads) if (count > 4 && threads > 1)
     for (int j = 0; j < count; ++j) box_yaw(jobs[j].xyz, jobs[j].n, jobs[j].min_x, jobs[j].min_y, jobs[j].qz, jobs[j].qw);
 }

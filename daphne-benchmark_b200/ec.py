@@ -25,8 +25,9 @@ def _lib():
                                      C.POINTER(C.c_int)]
         L.ndt_ec_segment_batch.argtypes = [p, C.c_int, p, p, p, p, p, p, p]
         L.ndt_ec_box_yaw.argtypes = [p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.ndt_ec_box_yaws.argtypes = [C.c_int, p, p, p, p]
         for n in ("ndt_ec_create", "ndt_ec_labels", "ndt_ec_extract", "ndt_ec_segment", "ndt_ec_segment_batch",
-                  "ndt_ec_box_yaw"):
+                  "ndt_ec_box_yaw", "ndt_ec_box_yaws"):
             getattr(L, n).restype = C.c_int
         L._ec_ready = True
     return L
@@ -41,6 +42,20 @@ def box_yaw(xyz):
     if rc != 0:
         raise _ndt.NdtError(f"ndt_ec_box_yaw: {_ndt.ERRORS.get(rc, rc)}")
     return qz.value, qw.value
+
+
+def box_yaws(clusters):
+    """Yaw quaternions (C x 2: z, w) of many clusters' boxes on the host's threads: ndt_ec_box_yaws."""
+    L = _lib()
+    parts = [np.ascontiguousarray(c, np.float32).reshape(-1, 3) for c in clusters]
+    off = np.zeros(len(parts) + 1, np.int32)
+    off[1:] = np.cumsum([len(c) for c in parts])
+    xyz = np.concatenate(parts) if parts and off[-1] else np.zeros((1, 3), np.float32)
+    qz, qw = np.zeros(max(len(parts), 1)), np.zeros(max(len(parts), 1))
+    rc = L.ndt_ec_box_yaws(len(parts), xyz.ctypes.data, off.ctypes.data, qz.ctypes.data, qw.ctypes.data)
+    if rc != 0:
+        raise _ndt.NdtError(f"ndt_ec_box_yaws: {_ndt.ERRORS.get(rc, rc)}")
+    return np.stack([qz[:len(parts)], qw[:len(parts)]], axis=1)
 
 
 class EuclideanClusters:

@@ -421,6 +421,9 @@ NDT_API int ndt_ec_segment(ndt_ec *ec, const float *xyz, int n, float *out_xyz, 
  * hull, which makes its yaw depend on memory contents; here the hull's own
  * length is used.  NDT_E_ARG for a non-finite x or y. */
 NDT_API int ndt_ec_box_yaw(const float *xyz, int n, double *qz, double *qw);
+/* The same for C clusters packed in xyz (offsets: C + 1 point offsets), spread over the host's threads (up to
+ * 8; a process forked after its first parallel call runs on one thread): qz[c], qw[c] of cluster c. */
+NDT_API int ndt_ec_box_yaws(int C, const float *xyz, const int *offsets, double *qz, double *qw);
 /* The same for C clouds packed in xyz (offsets: C + 1 point offsets), up to 8 clouds per GPU pass: cloud c's
  * clustered points are out_xyz[out_offsets[c] .. out_offsets[c + 1]), its boxes and centroids
  * [box_offsets[c] .. box_offsets[c + 1]) (capacities as above with n = offsets[C]). */

@@ -115,3 +115,45 @@ def test_edge_cases(pkg):
     bad[3, 1] = np.nan
     with pytest.raises(pkg.ndt.NdtError, match="ARG"):
         pkg.ec.box_yaw(bad)
+
+
+def _golden_clusters():
+    gold = np.load(GOLDEN)
+    out = []
+    for i in range(int(gold["cases"])):
+        for k, ring in enumerate(_rings(gold[f"in{i}"])):
+            sizes, idx = gold[f"sizes{i}_{k}"], gold[f"idx{i}_{k}"].astype(np.int64)
+            out += [ring[c] for c in (np.split(idx, np.cumsum(sizes)[:-1]) if len(sizes) else [])]
+    return out
+
+
+def test_batch_equals_single(pkg):
+    clusters = _golden_clusters()
+    batch = pkg.ec.box_yaws(clusters)
+    single = np.array([pkg.ec.box_yaw(c) for c in clusters])
+    assert np.array_equal(batch.view(np.uint64), single.view(np.uint64))
+    assert pkg.ec.box_yaws([]).shape == (0, 2)
+
+
+def _child_yaws(pkg, clusters, conn):
+    conn.send(pkg.ec.box_yaws(clusters))
+    conn.close()
+
+
+def test_batch_in_forked_process(pkg):
+    """A process forked after a parallel pass (whose thread pool it does not inherit) still completes."""
+    import multiprocessing as mp
+
+    clusters = _golden_clusters()
+    parent = pkg.ec.box_yaws(clusters)  # the parallel pass that starts the pool
+    ctx = mp.get_context("fork")
+    rd, wr = ctx.Pipe(duplex=False)
+    child = ctx.Process(target=_child_yaws, args=(pkg, clusters, wr))
+    child.start()
+    got = rd.recv() if rd.poll(120) else None
+    child.join(30)
+    if child.is_alive():
+        child.kill()
+        child.join()
+    assert got is not None, "forked process did not finish"
+    assert np.array_equal(got.view(np.uint64), parent.view(np.uint64))
