@@ -243,6 +243,7 @@ class Reference:
         L.ref_radius_search.restype = C.c_int
         L.ref_update_pair.argtypes = [_f64p, _f64p, _f64p, _f64p, C.c_double, C.c_double, C.c_int, _f64p, _f64p]
         L.ref_update_pair.restype = C.c_double
+        L.ref_angle_terms.argtypes = [_f64p, _f64p]
         L.ref_build_tm.argtypes = [_f64p, _f32p]
         L.ref_euler.argtypes = [_f32p, _f64p]
         L.ref_solve.argtypes = [_f64p, _f64p, _f64p]
@@ -302,6 +303,12 @@ class Reference:
                                      np.ascontiguousarray(trans, np.float32), scan.shape[0],
                                      np.ascontiguousarray(p6, np.float64), d1, d2, int(hessian), g, H)
         return s, g, H.reshape(6, 6)
+
+    def angle_terms(self, p6):
+        """computeAngleDerivatives (kernel.cpp:707-825): j_ang a..h then h_ang a2..f3, 3 each (69 doubles)."""
+        out = np.zeros(69)
+        self.lib.ref_angle_terms(np.ascontiguousarray(p6, np.float64), out)
+        return out
 
     def update_pair(self, p6, x, xt, icov, d1, d2, hessian=True, g=None, H=None):
         """The reference's computeAngleDerivatives + computePointDerivatives + updateDerivatives for one pair."""

@@ -160,6 +160,21 @@ REF_API double ref_derivatives(const float *map, int m, const float *scan, const
     return score;
 }
 
+// computeAngleDerivatives (kernel.cpp:707-825) at pose p6: out69 = j_ang a..h,
+// then h_ang a2 a3 b2 b3 c2 c3 d1 d2 d3 e1 e2 e3 f1 f2 f3 (3 each).
+REF_API void ref_angle_terms(const double *p6, double *out69) {
+    ndt_mapping &k = thread_instance();
+    Vec6 p;
+    for (int i = 0; i < 6; ++i) p[i] = p6[i];
+    k.computeAngleDerivatives(p, true);
+    const double *terms[23] = {k.j_ang_a_, k.j_ang_b_, k.j_ang_c_, k.j_ang_d_, k.j_ang_e_, k.j_ang_f_,
+                               k.j_ang_g_, k.j_ang_h_, k.h_ang_a2_, k.h_ang_a3_, k.h_ang_b2_, k.h_ang_b3_,
+                               k.h_ang_c2_, k.h_ang_c3_, k.h_ang_d1_, k.h_ang_d2_, k.h_ang_d3_, k.h_ang_e1_,
+                               k.h_ang_e2_, k.h_ang_e3_, k.h_ang_f1_, k.h_ang_f2_, k.h_ang_f3_};
+    for (int t = 0; t < 23; ++t)
+        for (int c = 0; c < 3; ++c) out69[3 * t + c] = terms[t][c];
+}
+
 // One pair through the reference's own routines: computeAngleDerivatives(p)
 // (kernel.cpp:707), computePointDerivatives(x) (:495) and updateDerivatives
 // (:438) with the scan point x, its offset from the cell mean xt and the

@@ -1,5 +1,5 @@
 // Host build of daphne-benchmark_b200/csrc/ndt_math.cuh (the device-side
-// pose build, pose vector, 6x6 solve and More-Thuente helpers) behind a C ABI,
+// angle terms, pose build, pose vector, 6x6 solve and More-Thuente helpers) behind a C ABI,
 // for tests/test_ndt_math_host.py to compare with the reference's own routines
 // (oracle/_ref) on many random inputs.  Compiled with g++ -ffp-contract=off,
 // like the library's --fmad=false build: every product and sum rounds on its
@@ -12,6 +12,8 @@
 #include "ndt_math.cuh"
 
 #define API extern "C" __attribute__((visibility("default")))
+
+API void ndtm_angle_terms(const double *p6, int compat, double *out69) { ndt::angle_terms(p6, out69, compat != 0); }
 
 API void ndtm_build_tm_compat(const double *t6, float *m16) { ndt::build_tm_compat(m16, t6); }
 

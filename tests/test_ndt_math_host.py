@@ -1,5 +1,5 @@
-"""The device-side NDT math (daphne-benchmark_b200/csrc/ndt_math.cuh: pose
-build, pose vector, 6x6 solve, More-Thuente trial value and interval update)
+"""The device-side NDT math (daphne-benchmark_b200/csrc/ndt_math.cuh: angle
+terms, pose build, pose vector, 6x6 solve, More-Thuente trial value and interval update)
 built as host code (tests/native/ndt_math_host.cpp) and compared bit for bit
 with the reference's own routines (oracle/_ref) on many random inputs,
 including singular systems and degenerate line-search states.  The host
@@ -29,6 +29,7 @@ def ndtm(tmp_path_factory):
                     "-o", str(so)], check=True)
     L = C.CDLL(str(so))
     d, f = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS"), np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+    L.ndtm_angle_terms.argtypes = [d, C.c_int, d]
     L.ndtm_build_tm_compat.argtypes = [d, f]
     L.ndtm_pose_vector.argtypes = [C.c_int, f, d]
     L.ndtm_solve6.argtypes = [d, d, d]
@@ -93,3 +94,22 @@ def test_more_thuente_helpers(ndtm, reference):
         c1 = ndtm.ndtm_update_interval(io_ours, at, ft, gt)
         c2, io_ref = reference.update_interval(io, at, ft, gt)
         assert c1 == c2 and _same(io_ours, io_ref), t
+
+
+def test_angle_terms(ndtm, reference):
+    """compat: the reference's computeAngleDerivatives bit for bit (incl. the exact 0 / 1 of |angle| < 1e-4);
+    corrected: the same except h_ang_d1's z component, -sin(pitch) instead of +sin(pitch)."""
+    rng = np.random.default_rng(4)
+    for t in range(20000):
+        p = rng.uniform(-3.5, 3.5, 6)
+        if t % 3 == 0:
+            p[3 + rng.integers(0, 3)] = rng.uniform(-2e-4, 2e-4)
+        ref = reference.angle_terms(p)
+        ours = np.zeros(69)
+        ndtm.ndtm_angle_terms(np.ascontiguousarray(p), 1, ours)
+        assert _same(ours, ref), p
+        ndtm.ndtm_angle_terms(np.ascontiguousarray(p), 0, ours)
+        d1z = 24 + 6 * 3 + 2  # h_ang d1, z
+        assert ours[d1z] == -ref[d1z]
+        ours[d1z] = ref[d1z]
+        assert _same(ours, ref), p
