@@ -17,6 +17,8 @@ API void ndtm_angle_terms(const double *p6, int compat, double *out69) { ndt::an
 
 API void ndtm_build_tm_compat(const double *t6, float *m16) { ndt::build_tm_compat(m16, t6); }
 
+API void ndtm_build_tm_corrected(const double *p6, float *m16) { ndt::build_tm_corrected(m16, p6); }
+
 API void ndtm_pose_vector(int compat, const float *m16, double *p6) { ndt::pose_vector(compat != 0, m16, p6); }
 
 API void ndtm_solve6(const double *A36, const double *b6, double *x6) {

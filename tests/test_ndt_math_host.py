@@ -31,6 +31,7 @@ def ndtm(tmp_path_factory):
     d, f = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS"), np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
     L.ndtm_angle_terms.argtypes = [d, C.c_int, d]
     L.ndtm_build_tm_compat.argtypes = [d, f]
+    L.ndtm_build_tm_corrected.argtypes = [d, f]
     L.ndtm_pose_vector.argtypes = [C.c_int, f, d]
     L.ndtm_solve6.argtypes = [d, d, d]
     L.ndtm_trial_value.argtypes = [C.c_double] * 9
@@ -113,3 +114,19 @@ def test_angle_terms(ndtm, reference):
         assert ours[d1z] == -ref[d1z]
         ours[d1z] = ref[d1z]
         assert _same(ours, ref), p
+
+
+def test_corrected_pose_build_and_vector_equal_the_oracle(ndtm, oracle):
+    """The corrected mode's T = Trans * Rx * Ry * Rz and its inverse: the device code and the FP64 oracle agree
+    bit for bit (host libm on both sides)."""
+    rng = np.random.default_rng(5)
+    for t in range(20000):
+        p = rng.uniform(-3, 3, 6)
+        if t % 4 == 0:
+            p[3:] = rng.uniform(-1.5, 1.5, 3)
+        ours = np.zeros(16, np.float32)
+        ndtm.ndtm_build_tm_corrected(np.ascontiguousarray(p), ours)
+        assert _same(ours, oracle.build_tm(0, p)), p
+        pv = np.zeros(6)
+        ndtm.ndtm_pose_vector(0, ours, pv)
+        assert _same(pv, oracle.pose_vector(0, ours)), p
