@@ -2,7 +2,9 @@
 terms, pose build, pose vector, 6x6 solve, More-Thuente trial value and interval update)
 built as host code (tests/native/ndt_math_host.cpp) and compared bit for bit
 with the reference's own routines (oracle/_ref) on many random inputs,
-including singular systems and degenerate line-search states.  The host
+including singular systems and degenerate line-search states; the corrected
+mode's pose build and pose vector, which the reference does not have, with
+the FP64 oracle's.  The host
 build uses the same libm as the reference, so this checks each expression's
 operations and order; the device's own libm results are covered by the GPU
 parity tests."""
