@@ -140,6 +140,7 @@ def _child_yaws(pkg, clusters, conn):
     conn.close()
 
 
+@pytest.mark.filterwarnings("ignore:This process .* is multi-threaded, use of fork:DeprecationWarning")
 def test_batch_in_forked_process(pkg):
     """A process forked after a parallel pass (whose thread pool it does not inherit) still completes."""
     import multiprocessing as mp

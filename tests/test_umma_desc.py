@@ -12,11 +12,13 @@ ROOT = pathlib.Path(__file__).resolve().parent.parent
 
 
 def _cute_include():
-    try:
-        import flashinfer  # noqa: F401  (only for the location of its CUTLASS headers)
-        p = pathlib.Path(flashinfer.__file__).parent / "data" / "cutlass" / "include"
-    except Exception:
+    """CUTLASS/CuTe headers vendored in the flashinfer package, located without importing it."""
+    import importlib.util
+
+    spec = importlib.util.find_spec("flashinfer")
+    if spec is None or not spec.submodule_search_locations:
         return None
+    p = pathlib.Path(list(spec.submodule_search_locations)[0]) / "data" / "cutlass" / "include"
     return p if (p / "cute" / "arch" / "mma_sm100_desc.hpp").exists() else None
 
 
