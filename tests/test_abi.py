@@ -60,3 +60,34 @@ def test_no_cpu_fallback_without_device(pkg):
         pytest.skip("a CUDA device is present")
     with pytest.raises(pkg.ndt.NdtError):
         pkg.ndt.Context(pkg.ndt.reference_params())
+
+
+def _c_layout(tmp_path, struct, fields):
+    """sizeof and offsetof of each field of an include/ndt_b200.h struct, from the C compiler."""
+    import shutil
+    import subprocess
+
+    if not shutil.which("gcc"):
+        pytest.skip("needs gcc")
+    src = tmp_path / f"{struct}.c"
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "ndt_b200.h"', "int main(void) {",
+             f'  printf("%zu\\n", sizeof({struct}));']
+    lines += [f'  printf("%zu\\n", offsetof({struct}, {f}));' for f in fields]
+    lines += ["  return 0;", "}"]
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / struct
+    subprocess.run(["gcc", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)], check=True)
+    out = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    return out[0], out[1:]
+
+
+@pytest.mark.parametrize("mirror", ["ndt.Params", "ndt.Counters", "binding.NdtParams"])
+def test_struct_mirrors_match_the_header(pkg, binding_mod, tmp_path, mirror):
+    """Every ctypes mirror of a header struct has the C compiler's size and field offsets."""
+    mod, name = mirror.split(".")
+    cls = getattr(pkg.ndt if mod == "ndt" else binding_mod, name)
+    struct = "ndt_counters" if name == "Counters" else "ndt_params"
+    fields = [f[0] for f in cls._fields_]
+    size, offsets = _c_layout(tmp_path, struct, fields)
+    assert ctypes.sizeof(cls) == size
+    assert [getattr(cls, f).offset for f in fields] == offsets
