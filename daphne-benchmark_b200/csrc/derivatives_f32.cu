@@ -7,8 +7,9 @@
 // consecutive points per alignment, handed out to the persistent blocks in
 // chunks of consecutive tiles.  Each lane keeps its FP32 sums of the current
 // alignment in shared memory and the block reduces them once per alignment
-// run (TwoSum-compensated across lanes and warps), writing the run's FP64
-// partial to the slot of its first tile (the run's other slots get zeros).
+// run, adding the FP32 lane sums in FP64 in a fixed order (across lanes, then
+// warps), writing the run's FP64 partial to the slot of its first tile (the
+// run's other slots get zeros).
 //
 // Per point (one thread): the float transform and the reference's neighbour
 // search of probe.cuh (exact: the accepted pairs are the reference's), each

@@ -176,6 +176,7 @@ struct ndt_ctx {
     ndt_counters last{};
     long long launches = 0;
     int variant = 0;  // FP32 derivative-pass launch shape (kDerivVariants)
+    unsigned flag_cap = 1u << 20;  // FP64 side-queue capacity in pairs per derivative pass
     float s_max = 1.0f;    // radius test threshold (see radius_threshold)
     float inv_res = 0.0f;  // 1 / res when res is a power of two
     // profiling: event pairs around derivative launches and the grid build
@@ -475,15 +476,16 @@ int build_grid(ndt_ctx *c, const float4 *d_map, int m) {
     return NDT_OK;
 }
 
-constexpr unsigned kFlagCap = 1u << 20;  // queued pairs with flagged voxels per derivative pass
+constexpr unsigned kFlagCap = 1u << 20;     // default side-queue capacity (pairs per derivative pass)
+constexpr unsigned kFlagCapMax = 1u << 24;  // largest capacity ndt_set_side_queue_capacity accepts
 
 int prepare_flag_queue(ndt_ctx *c, EvalArgs &ea) {
-    CK(c->flag_q.ensure(sizeof(int4) * kFlagCap));
+    CK(c->flag_q.ensure(sizeof(int4) * c->flag_cap));
     CK(c->flag_n.ensure(sizeof(unsigned)));
     CK(c->flag_overflow.ensure(sizeof(int)));
     ea.flag_q = c->flag_q.as<int4>();
     ea.flag_n = c->flag_n.as<unsigned>();
-    ea.flag_cap = kFlagCap;
+    ea.flag_cap = c->flag_cap;
     ea.flag_overflow = c->flag_overflow.as<int>();
     CK(c->work_counter.ensure(sizeof(int)));
     ea.work_counter = c->work_counter.as<int>();
@@ -1161,7 +1163,11 @@ int ndt_align(ndt_ctx *c, const float *scan, int n, const float guess16[16], flo
     if (int rc = set_device(c)) return rc;
     const float *scans[1] = {scan};
     int ns[1] = {n};
-    return host_batch(c, 1, scans, ns, guess16, out16, converged, fitness, nullptr);
+    int status = 0;
+    if (int rc = host_batch(c, 1, scans, ns, guess16, out16, converged, fitness, &status)) return rc;
+    if (status & NDT_ST_WATCHDOG) return fail(c, NDT_E_WATCHDOG, "the evaluation watchdog stopped the alignment");
+    if (status & NDT_ST_OVERFLOW) return fail(c, NDT_E_CAPACITY, "the FP64 side queue overflowed");
+    return NDT_OK;
 }
 
 int ndt_align_with_map(ndt_ctx *c, const float *scan, int n, const float guess16[16], const float *map, int m,
@@ -1271,6 +1277,12 @@ int ndt_align_batch_device(ndt_ctx *c, int B, const float *d_points, const int *
 }
 
 int ndt_kernel_variants(void) { return kNumDerivVariants; }
+
+int ndt_set_side_queue_capacity(ndt_ctx *c, int pairs) {
+    if (!c || pairs < 0 || (unsigned)pairs > kFlagCapMax) return fail(c, NDT_E_ARG, "bad side-queue capacity");
+    c->flag_cap = pairs == 0 ? kFlagCap : (unsigned)pairs;
+    return NDT_OK;
+}
 
 int ndt_set_kernel_variant(ndt_ctx *c, int variant) {
     if (!c || variant < 0 || variant >= kNumDerivVariants) return fail(c, NDT_E_ARG, "bad kernel variant");

@@ -27,6 +27,7 @@
 // are ordered and do not overlap.
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <mutex>
 
 #include "../../include/ndt_b200.h"
@@ -116,6 +117,25 @@ __global__ void noalloc_reduce_kernel(const NoAllocScratch *s, double *out) {
     out[k] = v;
 }
 
+// Makes `device` current for its lifetime and puts the caller's current
+// device back when it ends, so that the call leaves the calling thread's
+// device selection as it found it.
+class DeviceGuard {
+public:
+    explicit DeviceGuard(int device) {
+        if (cudaGetDevice(&prev_) != cudaSuccess) prev_ = -1;
+        err_ = (prev_ == device) ? cudaSuccess : cudaSetDevice(device);
+    }
+    ~DeviceGuard() {
+        if (prev_ >= 0 && err_ == cudaSuccess) cudaSetDevice(prev_);
+    }
+    cudaError_t error() const { return err_; }
+
+private:
+    int prev_ = -1;
+    cudaError_t err_ = cudaSuccess;
+};
+
 }  // namespace
 }  // namespace ndt
 
@@ -137,11 +157,19 @@ extern "C" int ndt_derivatives_noalloc(ndt_ctx *ctx, const float *d_scan, const 
         ctx_set_error(ctx, "ndt_derivatives_noalloc: more than 65536 scan points (the static scratch limit)");
         return NDT_E_CAPACITY;
     }
+    // The kernels read the scans as float4 and write d_out as doubles: a
+    // misaligned pointer would fault on the device, so it is refused here.
+    if ((reinterpret_cast<uintptr_t>(d_scan) | reinterpret_cast<uintptr_t>(d_trans)) & 15u ||
+        reinterpret_cast<uintptr_t>(d_out) & 7u) {
+        ctx_set_error(ctx, "ndt_derivatives_noalloc: d_scan and d_trans must be 16-byte aligned, d_out 8-byte aligned");
+        return NDT_E_ARG;
+    }
     if (v.device < 0 || v.device >= kMaxDevices) {
         ctx_set_error(ctx, "ndt_derivatives_noalloc: device ordinal out of range");
         return NDT_E_ARG;
     }
-    cudaError_t e = cudaSetDevice(v.device);
+    DeviceGuard guard(v.device);
+    cudaError_t e = guard.error();
     if (e != cudaSuccess) {
         ctx_set_error(ctx, cudaGetErrorString(e));
         return NDT_E_CUDA;

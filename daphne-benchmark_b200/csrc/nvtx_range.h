@@ -1,7 +1,10 @@
 // Host-side NVTX ranges of the library's phases, in the domain "ndt_b200"
 // (NVTX3, header only: without a tool attached a range costs a pointer
-// test).  ncu selects kernels by range:
-//   ncu --nvtx --nvtx-include "ndt_b200@rounds/" ...
+// test).  ncu selects kernels by range, e.g. (always with
+// --clock-control none, so that ncu leaves the GPU clocks alone, and a small
+// capture count):
+//   ncu --nvtx --nvtx-include "ndt_b200@rounds/" --clock-control none \
+//       --metrics gpu__time_duration.sum -c 60 ...
 #pragma once
 
 #include <nvtx3/nvToolsExt.h>

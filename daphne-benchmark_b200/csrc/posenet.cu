@@ -104,6 +104,7 @@ struct PointArgs {
     Norm nm;
     int B;
     int max_points;
+    unsigned wait_limit;       // polls of the MMA barrier before the wait gives up
 };
 
 __global__ void __launch_bounds__(128, 1) point_kernel(const __grid_constant__ PointArgs a) {
@@ -198,25 +199,40 @@ __global__ void __launch_bounds__(128, 1) point_kernel(const __grid_constant__ P
                              smem_u32(sBar))
                          : "memory");
         }
-        // wait for the MMAs (bounded)
+        // wait for the MMAs (bounded).  A wait that gives up sets the error
+        // flag; the MMAs it gave up on may still be running, so the thread
+        // then waits for them with the full limit before the block leaves
+        // the tile loop and releases its TMEM.
+        bool gave_up = false;
         {
             uint32_t done = 0;
             unsigned it = 0;
             while (!done) {
+                if (it++ >= a.wait_limit) {
+                    gave_up = true;
+                    break;
+                }
                 asm volatile(
                     "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
                     "selp.b32 %0, 1, 0, p;\n\t}\n"
                     : "=r"(done)
                     : "r"(smem_u32(sBar)), "r"(phase)
                     : "memory");
-                if (!done && ++it > kWaitLimit) {
-                    if (tid == 0) atomicExch(a.err, 1);
-                    break;
-                }
+            }
+            if (gave_up) {
+                atomicExch(a.err, 1);
+                for (unsigned k = 0; k < kWaitLimit && !done; ++k)
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                        "selp.b32 %0, 1, 0, p;\n\t}\n"
+                        : "=r"(done)
+                        : "r"(smem_u32(sBar)), "r"(phase)
+                        : "memory");
             }
             phase ^= 1u;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (__syncthreads_or(gave_up)) break;  // the same decision in every thread of the block
         // this channel's 128 values: columns 32 q .. 32 q + 31 = points t * 128 + column
         const int nvalid = min(kTileRows, P - t * kTileRows);
 #pragma unroll
@@ -480,6 +496,7 @@ struct ndt_mlp {
     size_t cap_b = 0;
     int step = 0;
     pn::Norm nm{};
+    unsigned wait_limit = pn::kWaitLimit;
     std::string msg;
 };
 
@@ -526,6 +543,7 @@ int run_forward(ndt_mlp *c, int B, const float *d_points, const int *d_offsets, 
     a.w2op = c->w2op;
     a.gmax = c->gmax;
     a.err = c->err;
+    a.wait_limit = c->wait_limit;
     a.nm = c->nm;
     a.B = B;
     a.max_points = max_points;
@@ -697,7 +715,14 @@ int ndt_mlp_synchronize(ndt_mlp *c, int *tc_error) {
     MCK(cudaStreamSynchronize(c->stream));
     int e = 0;
     MCK(cudaMemcpy(&e, c->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) MCK(cudaMemset(c->err, 0, sizeof(int)));  // reported once: the flag covers the calls since the last one
     if (tc_error) *tc_error = e;
+    return NDT_OK;
+}
+
+int ndt_mlp_set_wait_limit(ndt_mlp *c, int polls) {
+    if (!c) return NDT_E_ARG;
+    c->wait_limit = polls < 0 ? pn::kWaitLimit : (unsigned)polls;
     return NDT_OK;
 }
 

@@ -2,8 +2,15 @@
 // links into the harness the same way the reference kernels do
 // (src/CPU/include/benchmark.h:11-55): an abstract `kernel` with
 // init / run(p) / check_output, a test-case count, pause/resume timer hooks,
-// and read_next_testcases.  The shape must match for the drop-in to work, so
-// the member names, signatures and meanings are the reference's.
+// and read_next_testcases.
+//
+// The class must be layout-identical to the reference's, because the
+// reference harness (src/CPU/common/main.cpp:72-80) calls init / run /
+// check_output through the vtable of the `myKernel` object that this front
+// end defines: the same virtual functions in the same order (no virtual
+// destructor: one would shift every vtable slot), the same data members in
+// the same order.  The default member initialisers only affect the
+// constructor, which runs in this front end's translation unit.
 #ifndef NDT_B200_DAPHNE_BENCHMARK_H
 #define NDT_B200_DAPHNE_BENCHMARK_H
 
@@ -11,7 +18,6 @@
 
 class kernel {
 public:
-    virtual ~kernel() {}
     // number of test cases in the input (at least 1)
     uint32_t testcases = 1;
     // pre-run set-up: opens the data files, reads the test-case count

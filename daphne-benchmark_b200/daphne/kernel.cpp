@@ -61,7 +61,7 @@ const char *env_or(const char *name, const char *dflt) {
 
 class ndt_mapping : public kernel {
 public:
-    ~ndt_mapping() override {
+    ~ndt_mapping() {
         if (ctx_) ndt_destroy(ctx_);
     }
     void init() override;

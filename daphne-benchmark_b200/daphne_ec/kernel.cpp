@@ -71,7 +71,7 @@ void read_exact(std::ifstream &f, T *p, size_t n, const char *what) {
 
 class euclidean_clustering : public kernel {
 public:
-    ~euclidean_clustering() override {
+    ~euclidean_clustering() {
         if (ec_) ndt_ec_destroy(ec_);
     }
     void init() override;

@@ -105,6 +105,7 @@ def lib():
         L.ndt_kernel_variants.argtypes = []
         L.ndt_kernel_variant_shape.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.ndt_set_kernel_variant.argtypes = [ctxp, C.c_int]
+        L.ndt_set_side_queue_capacity.argtypes = [ctxp, C.c_int]
         L.ndt_synchronize.argtypes = [ctxp]
         L.ndt_stream.argtypes = [ctxp]
         L.ndt_stream.restype = C.c_void_p
@@ -120,6 +121,7 @@ def lib():
                      "ndt_align_batch_packed_with_map",
                      "ndt_set_profiling", "ndt_kernel_variants", "ndt_kernel_variant_shape",
                      "ndt_set_kernel_variant", "ndt_window_info", "ndt_set_batch_graphs",
+                     "ndt_set_side_queue_capacity",
                      "ndt_score_batch_device"):
             getattr(L, name).restype = C.c_int
         _LIB = L
@@ -294,6 +296,10 @@ class Context:
 
     def set_kernel_variant(self, v):
         self._check(self.L.ndt_set_kernel_variant(self.h, int(v)), "ndt_set_kernel_variant")
+
+    def set_side_queue_capacity(self, pairs=0):
+        """FP64 side-queue capacity in pairs per derivative pass (0 = default 2^20)."""
+        self._check(self.L.ndt_set_side_queue_capacity(self.h, int(pairs)), "set_side_queue_capacity")
 
     def synchronize(self):
         self._check(self.L.ndt_synchronize(self.h), "ndt_synchronize")

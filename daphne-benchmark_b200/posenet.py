@@ -37,6 +37,7 @@ def _lib():
                                                 C.POINTER(C.c_float), C.POINTER(C.c_float)]
         L.ndt_mlp_maxpool_device.argtypes = [p, p, C.c_int]
         L.ndt_mlp_synchronize.argtypes = [p, C.POINTER(C.c_int)]
+        L.ndt_mlp_set_wait_limit.argtypes = [p, C.c_int]
         L.ndt_mlp_stream.argtypes = [p]
         L.ndt_mlp_stream.restype = p
         L.ndt_mlp_set_stream.argtypes = [p, p]
@@ -44,7 +45,7 @@ def _lib():
         L.ndt_mlp_judge_device.argtypes = [p, C.c_int, p, p, p, p, p, p]
         for n in ("ndt_mlp_create", "ndt_mlp_set_input_frame", "ndt_mlp_set_weights", "ndt_mlp_get_weights",
                   "ndt_mlp_forward_device", "ndt_mlp_train_step_device", "ndt_mlp_maxpool_device",
-                  "ndt_mlp_synchronize", "ndt_mlp_set_stream", "ndt_mlp_propose_device", "ndt_mlp_judge_device"):
+                  "ndt_mlp_synchronize", "ndt_mlp_set_wait_limit", "ndt_mlp_set_stream", "ndt_mlp_propose_device", "ndt_mlp_judge_device"):
             getattr(L, n).restype = C.c_int
         L._pn_ready = True
     return L
@@ -119,6 +120,16 @@ class PoseNet:
 
     def maxpool(self, d_out, B):
         self._check(self.L.ndt_mlp_maxpool_device(self.h, C.c_void_p(d_out), B), "maxpool")
+
+    def set_wait_limit(self, polls=-1):
+        """Polls of the tensor-core barrier before a wait gives up (-1 = default; 0 exercises the error path)."""
+        self._check(self.L.ndt_mlp_set_wait_limit(self.h, int(polls)), "set_wait_limit")
+
+    def synchronize_status(self):
+        """Waits for the network's stream; True when a tensor-core wait gave up since the last check."""
+        e = C.c_int()
+        self._check(self.L.ndt_mlp_synchronize(self.h, C.byref(e)), "synchronize")
+        return bool(e.value)
 
     def synchronize(self):
         e = C.c_int()

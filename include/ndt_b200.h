@@ -117,7 +117,10 @@ NDT_API int ndt_map_append_device(ndt_ctx *ctx, const float *d_points, int k);
  * One alignment with host buffers: the partial_points_callback call
  * (kernel.cpp:1405-1414) against the map set by ndt_set_map.
  * out16 = final transformation, *converged, *fitness (NDT score per point;
- * the reference never fills fitness_score).
+ * the reference never fills fitness_score).  Returns NDT_E_WATCHDOG when the
+ * evaluation budget (params.watchdog_evals) ran out and NDT_E_CAPACITY when
+ * the FP64 side queue overflowed (NDT_ST_* of the batch calls); the outputs
+ * are written in both cases.
  */
 NDT_API int ndt_align(ndt_ctx *ctx, const float *scan, int n, const float guess16[16], float out16[16],
               int *converged, double *fitness);
@@ -233,6 +236,18 @@ NDT_API int ndt_kernel_variant_shape(int variant, int *tile, int *blocks_per_sm)
 NDT_API int ndt_set_kernel_variant(ndt_ctx *ctx, int variant);
 
 /*
+ * Capacity of the FP64 side queue, in (point, voxel) pairs per derivative
+ * pass (0 = the default, 2^20; at most 2^24; 16 bytes of device memory per
+ * pair).  The queue holds the pairs whose voxel has a non-finite or huge
+ * inverse covariance (the reference's inf / NaN voxels, kept bit for bit by
+ * evaluating them in FP64).  Alignments of a pass that queued more pairs get
+ * status NDT_ST_OVERFLOW and results that leave out the pairs beyond the
+ * capacity.  No reference counterpart (the reference evaluates every pair in
+ * FP64).
+ */
+NDT_API int ndt_set_side_queue_capacity(ndt_ctx *ctx, int pairs);
+
+/*
  * Grid inspection (tests): bbox (min xyz, max xyz), dims, number of occupied
  * cells, and for each occupied cell its linear index, point count, mean[3]
  * (FP64) and inverse covariance[9] (FP64) as the reference stores them.
@@ -264,15 +279,21 @@ NDT_API int ndt_derivatives(ndt_ctx *ctx, const float *scan, const float *trans,
  * memory while they run (a real-time loop with a fixed memory budget, work
  * recorded into a CUDA graph, where cudaMalloc is not allowed): it allocates
  * nothing.  Inputs are DEVICE pointers: d_scan and d_trans (n float[4] each,
- * the original and the already transformed scan), p6 is a host array (the
- * pose vector for the angle terms); d_out receives 44 doubles: score,
- * gradient[6], Hessian[36] row major, pair count (-1 if more pairs hit
- * degenerate voxels than the side queue holds).  Scratch is one static device
- * array per GPU (at most 256 KB, held until exit), so n is limited to 65536
- * (NDT_E_CAPACITY beyond).  The first call on a device looks the array up
- * (cudaGetSymbolAddress); make it before any stream capture.  Work is
- * enqueued on the context stream (call ndt_synchronize before reading
- * d_out); calls whose work overlaps on one GPU race on the shared scratch.
+ * the original and the already transformed scan, both 16-byte aligned), p6
+ * is a host array (the pose vector for the angle terms); d_out (8-byte
+ * aligned) receives 44 doubles: score, gradient[6], Hessian[36] row major,
+ * pair count.  Misaligned pointers give NDT_E_ARG before any work.
+ * Scratch is one static device array per GPU (at most 256 KB, held until
+ * exit), which fixes two limits: n <= 65536 (NDT_E_CAPACITY beyond), and at
+ * most 2048 (point, voxel) pairs evaluated on the FP64 side path (voxels with
+ * non-finite or huge inverse covariance, points beyond ~1e6 m) per call --
+ * beyond that the pair count d_out[43] is -1 and the other outputs are not
+ * valid (ndt_derivatives holds 2^20 such pairs).  The first call on a device
+ * looks the array up (cudaGetSymbolAddress); make it before any stream
+ * capture.  The call leaves the caller's current device as it found it.
+ * Work is enqueued on the context stream (call ndt_synchronize before
+ * reading d_out); calls whose work overlaps on one GPU race on the shared
+ * scratch.
  */
 NDT_API int ndt_derivatives_noalloc(ndt_ctx *ctx, const float *d_scan, const float *d_trans, int n,
                                     const double p6[6], double *d_out);
@@ -312,7 +333,14 @@ NDT_API int ndt_mlp_train_step_device(ndt_mlp *mlp, int B, const float *d_points
                                       int update, float *h_loss, float *h_grad);
 /* Max-pool of the last forward: B x 128 packed (float bits << 32 | 0xffffffff - argmax sample). */
 NDT_API int ndt_mlp_maxpool_device(ndt_mlp *mlp, unsigned long long *d_out, int B);
+/* Waits for the network's stream; *tc_error (optional) = 1 when a tensor-core wait gave up in a call since the
+ * last ndt_mlp_synchronize (the outputs of those calls are then invalid); the flag is cleared once reported. */
 NDT_API int ndt_mlp_synchronize(ndt_mlp *mlp, int *tc_error);
+/* Polls of the tensor-core completion barrier before a wait gives up and sets the error flag (< 0: the default,
+ * 2^26, which no healthy MMA reaches; 0 gives up before the first poll, which exercises the error path).  A wait
+ * that gave up still waits, with the default limit, for the MMAs in flight before the kernel frees its tensor
+ * memory and returns. */
+NDT_API int ndt_mlp_set_wait_limit(ndt_mlp *mlp, int polls);
 NDT_API void *ndt_mlp_stream(ndt_mlp *mlp);
 /* Run the network's work on a caller's stream (e.g. ndt_stream of an NDT context, so that proposals, the
  * judge's scores and the refinement are ordered without host synchronisation); NULL = its own stream. */

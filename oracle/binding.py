@@ -18,6 +18,15 @@ import sys
 import numpy as np
 
 HERE = pathlib.Path(__file__).resolve().parent
+
+
+def reference_dir() -> pathlib.Path:
+    """The reference source tree (read-only): $NDT_REFERENCE_DIR, else the
+    directory `reference` beside this repository's checkout.  Only the
+    recipes that compile the CPU checkers and the fixture generators read
+    it; nothing run on a GPU machine needs it."""
+    env = os.environ.get("NDT_REFERENCE_DIR")
+    return pathlib.Path(env) if env else HERE.parents[1] / "reference"
 ORACLE_SO = HERE / "_build" / "libndt_oracle.so"
 REF_SO = {"serial": HERE / "_ref" / "libref_ndt_serial.so", "omp": HERE / "_ref" / "libref_ndt_omp.so"}
 
@@ -62,9 +71,9 @@ def corrected_params(resolution=1.0):
 def build(quiet=True):
     """Compile the oracle (and the reference shims when the reference is present)."""
     targets = ["oracle"]
-    if pathlib.Path(os.environ.get("NDT_REFERENCE_DIR", "/root/reference")).is_dir():
+    if (reference_dir() / "src" / "CPU" / "ndt_mapping" / "kernel.cpp").exists():
         targets.append("ref")
-    subprocess.run(["make", "-C", str(HERE), *targets], check=True,
+    subprocess.run(["make", "-C", str(HERE), f"NDT_REFERENCE_DIR={reference_dir()}", *targets], check=True,
                    stdout=subprocess.DEVNULL if quiet else None)
 
 

@@ -26,9 +26,10 @@ import numpy as np
 HERE = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE.parents[1] / "oracle"))
 
+import binding  # noqa: E402
 import ec_ref  # noqa: E402
 
-REF_DATA = pathlib.Path("/root/reference/data")
+REF_DATA = binding.reference_dir() / "data"
 RING_TOL = (0.5, 1.1, 1.6, 2.3, np.float32(2.6).item())
 
 

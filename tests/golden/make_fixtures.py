@@ -33,7 +33,7 @@ import binding  # noqa: E402
 import datfile  # noqa: E402
 import synth  # noqa: E402
 
-REF_DIR = pathlib.Path("/root/reference")
+REF_DIR = binding.reference_dir()
 
 
 def cases():

@@ -6,6 +6,7 @@ import pathlib
 import numpy as np
 import pytest
 
+import binding
 import ec_ref
 
 GOLDEN = pathlib.Path(__file__).resolve().parent / "golden" / "ec_cases.npz"
@@ -40,11 +41,14 @@ def test_fixture_shape():
         assert len(d[f"boxes{i}"]) == len(d[f"centroids{i}"])
 
 
-@pytest.mark.skipif(not (ec_ref.Reference.available() and pathlib.Path("/root/reference/data/ec_output.dat.gz").exists()),
+REF_DATA = binding.reference_dir() / "data"
+
+
+@pytest.mark.skipif(not (ec_ref.Reference.available() and (REF_DATA / "ec_output.dat.gz").exists()),
                     reason="reference tree not present")
 def test_reference_reproduces_its_shipped_output():
-    ins = ec_ref.read_input("/root/reference/data/ec_input.dat.gz")
-    outs = ec_ref.read_output("/root/reference/data/ec_output.dat.gz", len(ins))
+    ins = ec_ref.read_input(str(REF_DATA / "ec_input.dat.gz"))
+    outs = ec_ref.read_output(str(REF_DATA / "ec_output.dat.gz"), len(ins))
     ref = ec_ref.Reference()
     for xyz, out in list(zip(ins, outs))[:2]:
         pts, b10, cen = ref.segment(xyz)
