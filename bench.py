@@ -2,28 +2,37 @@
 """Throughput benchmark of the B200 NDT align path (DAPHNE ndt_mapping).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config c2] [--mode compat|corrected] [--precision 0|1]
+                    [--config c5] [--mode compat|corrected] [--precision 0|1]
 
-A step is one batch of the configuration's alignments against its map: the
-voxel grid is built from the map and every alignment runs to completion.  At
-the default configuration (c2) a step is 256 alignments of 8000-point scans
-against a 400k-point map (150 x 150 m, 120 walls), resolution 1.0 m, guesses
-+-0.5 m / +-3 deg off the ground truth, with the reference kernel's semantics
-(compat mode: the drop-in for partial_points_callback).  Inputs are seeded
-synthetic clouds (the reference's input file is not distributed).
+Default workload (c5, the metric's configuration): learned-init vs plain
+batched NDT, corrected mode.  A 2M-point map (300 x 300 m, 400 walls) at
+0.5 m; a step is 4096 alignments with scans of 2k-32k points (log-uniform)
+and guesses up to +-3 m / +-15 deg off the ground truth, all in one batch:
+  plain    the plain NDT from the raw guesses;
+  learned  network proposals from a grid of starts around each guess, the NDT
+           judge, refinement through coarse-to-fine levels ending with the
+           plain NDT (ndt_align_batch_learned_device).
+The network is trained first (untimed) on pairs the plain NDT labels on the
+same map.  `value` is the learned arm's aligns/s with inputs resident in HBM
+(L2 flushed between steps); each arm reports the fraction of its alignments
+within 2 cm / 0.1 deg of the ground truth and its aligns/s at that accuracy;
+`e2e` runs the learned arm through the C ABI with pinned host buffers; the
+roofline is the derivative pass's; the CPU baseline is the compiled reference
+kernel on the host cores, with the FP64 oracle's runs from the same starts
+as the accuracy check.  Inputs are seeded synthetic clouds.
 
-Our arm prints one JSON line with `value` (aligns/s with inputs resident in
-HBM, L2 flushed between steps), `e2e` (aligns/s through the C ABI with pinned
-host buffers, copies inside the timed region), the derivative kernel's
-roofline, the CPU baseline (the compiled reference kernel on the host cores,
-rank 0) and the SM clocks sampled during the timed region.  With torchrun
-(N > 1) every rank aligns its own batch (weak scaling; no collective on the
-data path) and the timing is the max over ranks.
+--config c2 (or c1, c3) times the plain NDT alone: c2 = 256 alignments of
+8000-point scans against a 400k-point map at 1 m, compat mode (the reference
+kernel's semantics: the drop-in for partial_points_callback), the grid built
+from the map inside every step; `e2e` through ndt_align_batch_packed_with_map.
+With torchrun (N > 1) every rank aligns its own batch (weak scaling; no
+collective on the data path) and the timing is the max over ranks.
 
 --impl reference times the reference's own CPU implementation (the compiled
 src/CPU/ndt_mapping kernel in oracle/_ref, one reference object per host
-thread on all host cores; the restated oracle when that library is absent) on
-the same workload and prints the same line with "impl": "reference".
+thread on all host cores; the restated oracle when that library is absent)
+on a bounded sample of the same workload and prints the same line with
+"impl": "reference".
 """
 from __future__ import annotations
 
@@ -172,14 +181,16 @@ def run_reference_arm(args, pkg, world, rank):
     B = len(aligns)
     npts = sum(a.scan.shape[0] for a in aligns)
     cores = os.cpu_count() or 1
-    scans = [a.scan for a in aligns]
-    guesses = np.stack([a.guess for a in aligns])
+    # each step a bounded sample of the workload: the first 4 x cores alignments (all of them when fewer)
+    n = min(B, 4 * cores)
+    scans = [a.scan for a in aligns[:n]]
+    guesses = np.stack([a.guess for a in aligns[:n]])
     if binding.Reference.available("serial"):
         ref = binding.Reference("serial")
         kind = "reference"
 
         def step():
-            ref.align_batch(scans, guesses, [scene.map] * B, nthreads=cores)
+            ref.align_batch(scans, guesses, [scene.map] * n, nthreads=cores)
     else:
         orc = binding.Oracle()
         prm = binding.reference_params(cfg.resolution) if args.mode == "compat" else \
@@ -188,7 +199,7 @@ def run_reference_arm(args, pkg, world, rank):
 
         def step():
             # the restated reference; grid rebuilt per alignment like the reference's call
-            for i in range(B):
+            for i in range(n):
                 orc.align(prm, scans[i], guesses[i], scene.map)
     for _ in range(args.warmup):
         step()
@@ -198,15 +209,16 @@ def run_reference_arm(args, pkg, world, rank):
         step()
         times.append(time.perf_counter() - t0)
     total = sum(times)
-    value = B * args.steps / total
-    sample = (f"every step: all {B} alignments of the workload, one reference object per thread "
+    value = n * args.steps / total
+    sample = (f"every step: the first {n} of the workload's {B} alignments, one reference object per thread "
               f"on {cores} host threads (grid rebuilt per alignment, as partial_points_callback does)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "aligns/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64 (reference CPU)",
         "data": "synthetic (seeded plane + walls generator)",
-        "config": config_block(cfg, args.mode, args.precision, B, npts),
+        "config": (learned_config_block(pkg, cfg, B, npts) if args.learned
+                   else config_block(cfg, args.mode, args.precision, B, npts)),
         "cpu_baseline": {"value": value, "unit": "aligns/s", "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": "aligns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -541,135 +553,366 @@ def run_ours(args, pkg, world, rank, local):
     return 0
 
 
+def learned_config_block(pkg, cfg, B, npts):
+    """The `config` of the learned-vs-plain workload (both arms print it)."""
+    lp = pkg.posenet.learned_params()
+    levels_spec = pkg.learned.refinement_levels(cfg.resolution)
+    return {"workload": f"{cfg.name}: {cfg.map_points}-point map ({cfg.area:g} x {cfg.area:g} m, {cfg.walls} walls), "
+                        f"{B} alignments per step, scans {cfg.scan_min}-{cfg.scan_max} points (log-uniform), "
+                        f"resolution {cfg.resolution:g} m, guesses +-{cfg.dt:g} m / +-{cfg.dyaw_deg:g} deg; "
+                        f"learned-init vs plain batched NDT",
+            "alignments_per_step": B, "scan_points_per_step": npts, "map_points": cfg.map_points,
+            "resolution_m": cfg.resolution, "mode": "corrected",
+            "learned": {"starts": f"{lp.grid_xy} x {lp.grid_xy} translations {lp.step_xy:g} m apart x {lp.grid_yaw} "
+                                  f"yaw", "network_passes": lp.passes,
+                        "judge": f"NDT score at {levels_spec[lp.judge_level][0]:g} m on {lp.judge_points} points per "
+                                 f"scan, raw guess kept when no proposal scores higher",
+                        "refinement_levels_m_step": levels_spec},
+            "l2": f"flushed between timed steps ({L2_FLUSH_BYTES >> 20} MiB write); scans larger than L2"}
+
+
+def learned_cpu_leg(pkg, scene, cfg, aligns, plain_out, learned_out, learned_start, levels_spec, cores):
+    """CPU baseline of the learned-vs-plain workload (bounded samples on the host cores) and, from the same CPU
+    runs, the GPU results' agreement with the FP64 oracle run from the same starts:
+      * the compiled reference kernel (src/CPU/ndt_mapping: its own parametrisation, grid rebuilt per call), all
+        cores, one object per thread -- the baseline value; its serial and OpenMP builds beside it;
+      * the FP64 corrected-NDT oracle: the plain NDT from the raw guesses (compared with the GPU's plain arm) and
+        the learned arm's refinement levels from the GPU's chosen starts (compared with the GPU's learned arm)."""
+    import binding
+    out = {}
+    n = min(len(aligns), 4 * cores)
+    scans = [a.scan for a in aligns[:n]]
+    guesses = np.stack([a.guess for a in aligns[:n]])
+    if binding.Reference.available("serial"):
+        ref = binding.Reference("serial")
+        rate, reps, t = _rate(lambda: ref.align_batch(scans, guesses, [scene.map] * n, nthreads=cores), n, 5.0, 10)
+        base = {"value": rate, "unit": "aligns/s", "cores": cores, "kind": "reference",
+                "sample": f"{n} alignments of the step x {reps} ({t:.1f} s wall), compiled reference "
+                          f"src/CPU/ndt_mapping (its own compat behaviour), one object per thread"}
+        n1 = min(len(aligns), 4)
+        r1, reps1, t1 = _rate(lambda: ref.align_batch(scans[:n1], guesses[:n1], [scene.map] * n1, nthreads=1),
+                              n1, 2.0, 5)
+        out["reference_serial_1_thread"] = {"value": r1, "cores": 1, "sample": f"{n1} alignments x {reps1} "
+                                                                                f"({t1:.1f} s)"}
+        if binding.Reference.available("omp"):
+            omp = binding.Reference("omp")
+            r2, reps2, t2 = _rate(lambda: omp.align_batch(scans[:n1], guesses[:n1], [scene.map] * n1, nthreads=1),
+                                  n1, 2.0, 5)
+            out["reference_openmp"] = {"value": r2, "cores": cores, "sample": f"{n1} alignments x {reps2} "
+                                                                               f"({t2:.1f} s), src/OpenMP/ndt_mapping"}
+    else:
+        base = None
+    orc = binding.Oracle()
+    m = min(len(aligns), 64)
+    sc = [a.scan for a in aligns[:m]]
+    prm = binding.corrected_params(cfg.resolution)
+    t0 = time.perf_counter()
+    ref_plain = orc.align_batch(prm, sc, np.stack([a.guess for a in aligns[:m]]), scene.map, nthreads=cores)[0]
+    t_plain = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    cur = learned_start[:m]
+    for res, step in levels_spec:
+        op = binding.corrected_params(res)
+        op.step_size = step
+        cur = orc.align_batch(op, sc, cur, scene.map, nthreads=cores)[0]
+    t_learned = time.perf_counter() - t0
+    out["corrected_fp64_oracle_plain"] = {"value": m / t_plain, "cores": cores,
+                                          "sample": f"{m} alignments ({t_plain:.1f} s)"}
+    out["corrected_fp64_oracle_learned_refinement"] = {
+        "value": m / t_learned, "cores": cores,
+        "sample": f"{m} alignments, the refinement levels from the GPU's chosen starts ({t_learned:.1f} s)"}
+    if base is None:
+        base = {"value": m / t_plain, "unit": "aligns/s", "cores": cores, "kind": "port",
+                "sample": out["corrected_fp64_oracle_plain"]["sample"] + ", FP64 corrected-NDT oracle"}
+    base["variants"] = out
+
+    def agree(gpu, ref):
+        dt = np.linalg.norm(gpu.reshape(-1, 4, 4)[:, :3, 3] - ref.reshape(-1, 4, 4)[:, :3, 3], axis=1)
+        dr = np.array([rot_deg(gpu[i], ref[i]) for i in range(len(ref))])
+        return {"alignments": len(ref), "within_2cm_0.1deg": int(np.sum((dt <= 0.02) & (dr <= 0.1))),
+                "max_translation_m": float(dt.max()), "max_rotation_deg": float(dr.max())}
+    acc = {"plain": agree(plain_out[:m], ref_plain), "learned": agree(learned_out[:m], cur),
+           "oracle": "FP64 corrected-NDT oracle from the same starts (learned: its refinement levels from the "
+                     "GPU's chosen starts)"}
+    return base, acc
+
+
 def run_learned(args, pkg, world, rank, local):
-    """Learned-init vs plain batched NDT (corrected NDT) on a config's
-    alignments: the network is trained first (untimed) on pairs the plain NDT
-    labels on the same map; then both pipelines run the whole batch, timed
-    with the wall clock around synchronised steps (the learned one includes
-    its proposal passes, the judge's two score passes and its host round
-    trips)."""
+    """Learned-init vs plain batched NDT (corrected NDT) on a configuration's
+    alignments (the default workload, c5).  Set-up, untimed: the network is
+    trained on the GPU on pairs that the plain NDT labels on the same map
+    (rank 0 trains; with N > 1 the weights are broadcast).  A step is the
+    whole batch through one arm, inputs resident in HBM, L2 flushed between
+    steps, timed with CUDA events from the first stream the arm uses to the
+    last:
+      plain    the plain NDT at the configuration's resolution from the raw
+               guesses (ndt_align_batch_device);
+      learned  ndt_align_batch_learned_device: network proposals from a grid of
+               starts around each guess, the NDT judge, refinement through the
+               coarse-to-fine levels (the last one is the plain NDT).
+    `value` = the learned arm's aligns/s; both arms report the fraction of
+    alignments within 2 cm / 0.1 deg of the ground truth and the aligns/s at
+    that accuracy."""
     import torch
-    import posenet_ref
     torch.cuda.set_device(local)
-    if rank != 0:
-        return 0
-    L, ndt, synth = pkg.learned, pkg.ndt, pkg.synth
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", device_id=dev, timeout=__import__("datetime").timedelta(seconds=300))
+    L, ndt, synth, PN = pkg.learned, pkg.ndt, pkg.synth, pkg.posenet
     cfg = synth.CONFIGS[args.config]
     big = cfg.map_points > 1_000_000
     args.train_scans = args.train_scans or (16000 if big else 8000)
-    args.train_epochs = args.train_epochs or (60 if big else 30)
+    args.train_epochs = args.train_epochs or (40 if big else 30)
     scene = synth.make_scene(cfg)
-    ctx = ndt.Context(ndt.corrected_params(cfg.resolution), device=local)
-    ctx.set_map(scene.map)
-    t0 = time.perf_counter()
-    pairs = L.make_pairs(cfg, scene, args.train_scans, 25, cfg.dt, cfg.dyaw_deg, seed=7, fine_frac=0.5)
-    t_pairs = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    L.label_scans(ctx, torch, pairs)
-    t_label = time.perf_counter() - t0
-    net = pkg.posenet.PoseNet(device=local, center=(0.0, 0.0, 0.0), scale=4.0)
-    net.set_weights(posenet_ref.init_weights(1))
-    t0 = time.perf_counter()
-    losses = L.train(net, torch, pairs, epochs=args.train_epochs, batch=256, lr=2e-3)
-    t_train = time.perf_counter() - t0
-    aligns = [synth.make_alignment(cfg, scene, i) for i in range(cfg.aligns)]
-    dev = L.DeviceScans(torch, [a.scan for a in aligns])
-    pts, offs, total = dev.batch(np.arange(len(aligns)))
-    guesses = np.stack([a.guess for a in aligns])
+    levels_spec = L.refinement_levels(cfg.resolution)
+    levels = L.level_contexts(ndt, scene.map, cfg.resolution, device=local, levels=levels_spec)
+    fine = levels[-1]
+    net = PN.PoseNet(device=local, center=(0.0, 0.0, 0.0), scale=4.0)
+    training = None
+    if rank == 0:
+        t0 = time.perf_counter()
+        pairs = L.make_pairs(cfg, scene, args.train_scans, 25, cfg.dt, cfg.dyaw_deg, seed=7, fine_frac=0.5)
+        t_pairs = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        L.label_scans(fine, torch, pairs)
+        t_label = time.perf_counter() - t0
+        net.set_weights(PN.init_weights(1))
+        t0 = time.perf_counter()
+        losses = L.train(net, torch, pairs, epochs=args.train_epochs, batch=256, lr=2e-3)
+        t_train = time.perf_counter() - t0
+        training = {"pairs": int(pairs.keep.sum()), "scans": args.train_scans, "epochs": args.train_epochs,
+                    "pair_generation_s": round(t_pairs, 1), "ndt_labelling_s": round(t_label, 1),
+                    "gpu_training_s": round(t_train, 1),
+                    "loss_first_last": [float(losses[:50].mean()), float(losses[-50:].mean())],
+                    "kernels": "ndt_mlp_train_step_device (forward on the tensor cores, backward and Adam on the GPU)"}
+        del pairs
+    if world > 1:
+        w = torch.from_numpy(net.get_weights() if rank == 0 else np.zeros(PN.num_weights(), np.float32)).to(dev)
+        torch.distributed.broadcast(w, 0)
+        if rank != 0:
+            net.set_weights(w.cpu().numpy())
+    B = cfg.aligns
+    aligns = [synth.make_alignment(cfg, scene, rank * B + i) for i in range(B)]
     truths = np.stack([a.truth for a in aligns])
-    B = len(aligns)
+    offs = np.zeros(B + 1, np.int32)
+    offs[1:] = np.cumsum([a.scan.shape[0] for a in aligns])
+    npts = int(offs[-1])
+    points = np.ascontiguousarray(np.concatenate([a.scan for a in aligns]))
+    guesses = np.ascontiguousarray(np.stack([a.guess for a in aligns]).astype(np.float32))
+    d_pts = torch.from_numpy(points).to(dev)
+    d_off = torch.from_numpy(offs).to(dev)
+    d_g = torch.from_numpy(guesses).to(dev)
+    outs = {k: (torch.zeros(B, 16, device=dev), torch.zeros(B, dtype=torch.int32, device=dev),
+                torch.zeros(B, dtype=torch.float64, device=dev), torch.zeros(B, dtype=torch.int32, device=dev))
+            for k in ("plain", "learned")}
+    d_choice = torch.zeros(B, dtype=torch.int32, device=dev)
+    d_start = torch.zeros(B, 16, device=dev)
+    lp = PN.learned_params()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    s_net = torch.cuda.ExternalStream(net.stream, device=dev)
+    s_fine = torch.cuda.ExternalStream(fine.stream, device=dev)
+    torch.cuda.synchronize()
 
-    def plain():
-        return L.ndt_align_device(ctx, torch, pts, offs, total, guesses)
+    def plain_step():
+        o = outs["plain"]
+        fine.align_batch_device(B, d_pts.data_ptr(), d_off.data_ptr(), npts, d_g.data_ptr(), o[0].data_ptr(),
+                                o[1].data_ptr(), o[2].data_ptr(), o[3].data_ptr())
 
-    lb = L.LearnedBatch(ctx, net, torch, pts, offs, total, guesses, passes=3)
+    def learned_step():
+        o = outs["learned"]
+        net.align_learned_device(levels, lp, B, d_pts.data_ptr(), d_off.data_ptr(), npts, d_g.data_ptr(),
+                                 o[0].data_ptr(), o[1].data_ptr(), o[2].data_ptr(), o[3].data_ptr(),
+                                 d_choice.data_ptr(), d_start.data_ptr())
 
-    class _Plain:
-        def __init__(self):
-            self.g = torch.from_numpy(np.ascontiguousarray(guesses)).cuda()
-            self.out = torch.zeros((B, 16), dtype=torch.float32, device="cuda")
-            self.conv = torch.zeros(B, dtype=torch.int32, device="cuda")
-            self.fit = torch.zeros(B, dtype=torch.float64, device="cuda")
-            self.st = torch.zeros(B, dtype=torch.int32, device="cuda")
-            torch.cuda.current_stream().synchronize()
-
-        def run(self):
-            ctx.align_batch_device(B, pts.data_ptr(), offs.data_ptr(), total, self.g.data_ptr(),
-                                   self.out.data_ptr(), self.conv.data_ptr(), self.fit.data_ptr(), self.st.data_ptr())
-            ctx.synchronize()
-            return self.out.cpu().numpy(), self.conv.cpu().numpy()
-
-    pb = _Plain()
-
-    def plain():
-        return pb.run()
-
-    def learned():
-        lb.run()
-        r = lb.results()
-        return r[0], r[1], r[2], r[3], r[4]
-
-    res = {}
-    for name, fn, step in (("plain", plain, pb.run), ("learned", learned, lb.run)):
+    arms = {"plain": (plain_step, s_fine, s_fine), "learned": (learned_step, s_net, s_fine)}
+    for name, (fn, s0, s1) in arms.items():
         for _ in range(args.warmup):
-            step()
-        times = []
+            fn()
+        torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        uuid = None
+    clocks = ClockSampler(local, uuid)
+    times = {}
+    for name, (fn, s0, s1) in arms.items():
+        ms = []
         for _ in range(args.steps):
-            _, t = L.timed(step, torch)
-            times.append(t)
-        out = fn()
-        dt, dr = L.pose_errors(out[0], truths)
+            with torch.cuda.stream(s0):
+                flush.fill_(float(np.random.random()))
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(s0)
+            fn()
+            e1.record(s1)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        times[name] = ms
+    torch.cuda.synchronize()
+    # kernels per learned step: the levels' alignment batches (each context counts its last batch, its graph's
+    # device-side round loop included), the judge's score pass (lists, initialisation, derivative pass, side
+    # pass, scores) and the pipeline's own kernels (starts, passes x (point, head, apply), subsample (3),
+    # replicate, select, status)
+    score_launches = 4 + 2 + 1
+    pipeline_launches = 1 + 3 * lp.passes + 3 + 1 + 1 + 1
+    launches = args.steps * (sum(c.counters()["launches"] for c in levels) + score_launches + pipeline_launches)
+    res = {}
+    for name in arms:
+        o = outs[name]
+        out, conv, st = o[0].cpu().numpy(), o[1].cpu().numpy(), o[3].cpu().numpy()
+        dt, dr = L.pose_errors(out, truths)
         ok = (dt <= 0.02) & (dr <= 0.1)
-        res[name] = {"aligns_per_s": B * args.steps / sum(times), "ms_per_step": 1e3 * sum(times) / args.steps,
-                     "within_2cm_0.1deg_of_truth": float(ok.mean()),
-                     "median_translation_error_m": float(np.median(dt)),
-                     "aligns_per_s_within_2cm_0.1deg_of_truth": float(ok.mean()) * B * args.steps / sum(times),
-                     "converged": float(np.mean(out[1] != 0))}
-        if name == "learned":
-            res[name]["used_proposal"] = float(np.mean(out[4]))
-    # accuracy of the refinement against the FP64 oracle from the same start
-    # poses, on a sample (the oracle is the CPU restatement)
-    import binding
-    n_acc = min(B, args.oracle_sample)
-    orc = binding.Oracle()
-    starts = lb.results()[6]
-    lb.close()
-    acc = {}
-    for name, st in (("plain", guesses), ("learned", starts)):
-        gpu = L.ndt_align_device(ctx, torch, pts, offs, total, st)[0][:n_acc]
-        ref, _, _, _ = orc.align_batch(binding.corrected_params(cfg.resolution), [a.scan for a in aligns[:n_acc]],
-                                       list(st[:n_acc]), scene.map)
-        e_t = np.linalg.norm(gpu.reshape(-1, 4, 4)[:, :3, 3] - ref.reshape(-1, 4, 4)[:, :3, 3], axis=1)
-        e_r = np.array([rot_deg(gpu[i], ref[i]) for i in range(n_acc)])
-        acc[name] = {"alignments": n_acc, "within_2cm_0.1deg": int(np.sum((e_t <= 0.02) & (e_r <= 0.1))),
-                     "max_translation_m": float(e_t.max()), "max_rotation_deg": float(e_r.max())}
-    ratio = res["learned"]["aligns_per_s"] / res["plain"]["aligns_per_s"]
-    ratio_ok = (res["learned"]["aligns_per_s_within_2cm_0.1deg_of_truth"] /
-                max(1e-9, res["plain"]["aligns_per_s_within_2cm_0.1deg_of_truth"]))
+        total_ms = sum(times[name])
+        rate = B * args.steps / (total_ms / 1e3)
+        res[name] = {"aligns_per_s": rate, "ms_per_step": total_ms / args.steps,
+                     "within_2cm_0.1deg_of_truth": float(ok.mean()), "alignments_within": int(ok.sum()),
+                     "aligns_per_s_within_2cm_0.1deg_of_truth": float(ok.mean()) * rate,
+                     "median_translation_error_m": float(np.median(dt)), "median_rotation_error_deg":
+                     float(np.median(dr)), "converged": float(np.mean(conv != 0)), "status_nonzero":
+                     int(np.count_nonzero(st))}
+    choice = d_choice.cpu().numpy()
+    K = lp.grid_xy * lp.grid_xy * lp.grid_yaw
+    res["learned"]["raw_guess_kept"] = float(np.mean(choice == K))
+    learned_out = outs["learned"][0].cpu().numpy()
+    plain_out = outs["plain"][0].cpu().numpy()
+    learned_start = d_start.cpu().numpy()
+
+    # ---- roofline: the derivative pass of the plain arm (profiling pass, every round launched from the host)
+    fine.set_profiling(True)
+    prof = {"points": 0, "probes": 0, "occupied_probes": 0, "pairs": 0, "tiles": 0, "deriv_launches": 0,
+            "deriv_ms": 0.0}
+    prof_steps = 3
+    prof_ms = []
+    for _ in range(prof_steps):
+        with torch.cuda.stream(s_fine):
+            flush.fill_(float(np.random.random()))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s_fine)
+        plain_step()
+        e1.record(s_fine)
+        e1.synchronize()
+        prof_ms.append(e0.elapsed_time(e1))
+        k = fine.counters()
+        for key in prof:
+            prof[key] += k[key]
+    fine.set_profiling(False)
+
+    # ---- end to end: the learned arm through the C ABI with pinned host buffers
+    h_pts = torch.from_numpy(points).pin_memory()
+    h_off = torch.from_numpy(offs).pin_memory()
+    h_g = torch.from_numpy(guesses).pin_memory()
+    h_out = torch.zeros(B, 16).pin_memory()
+    h_conv = torch.zeros(B, dtype=torch.int32).pin_memory()
+    h_fit = torch.zeros(B, dtype=torch.float64).pin_memory()
+    h_st = torch.zeros(B, dtype=torch.int32).pin_memory()
+
+    def host_step():
+        net.align_learned(levels, lp, B, h_pts.data_ptr(), h_off.data_ptr(), h_g.data_ptr(), h_out.data_ptr(),
+                          h_conv.data_ptr(), h_fit.data_ptr(), h_st.data_ptr())
+
+    for _ in range(args.warmup):
+        host_step()
+    e2e_ms = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(s_net):
+            flush.fill_(float(np.random.random()))
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s_net)
+        host_step()  # returns with the results on the host
+        e1.record(s_fine)
+        e1.synchronize()
+        e2e_ms.append(e0.elapsed_time(e1))
+    e2e_ok = float(np.mean(np.all(h_out.numpy().view(np.uint32) == learned_out.view(np.uint32), axis=1)))
+    clk = clocks.stop()
+
+    # ---- max over ranks
+    tot = {k: sum(v) for k, v in times.items()}
+    e2e_total = sum(e2e_ms)
+    if world > 1:
+        t = torch.tensor([tot["plain"], tot["learned"], e2e_total], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        tot["plain"], tot["learned"], e2e_total = float(t[0]), float(t[1]), float(t[2])
+    value = world * B * args.steps / (tot["learned"] / 1e3)
+    plain_value = world * B * args.steps / (tot["plain"] / 1e3)
+    e2e_value = world * B * args.steps / (e2e_total / 1e3)
+    if rank != 0:
+        net.close()
+        for c in levels:
+            c.close()
+        torch.distributed.destroy_process_group()
+        return 0
+
+    peak, peak_kind = measured_peaks()
+    n_launch = max(1, prof["deriv_launches"])
+    bytes_total = (16 * prof["points"] + 4 * prof["probes"] + 16 * prof["occupied_probes"] + 56 * prof["pairs"]
+                   + 8 * 44 * prof["tiles"])
+    bytes_per_launch = bytes_total / n_launch
+    launch_ms = prof["deriv_ms"] / n_launch
+    achieved = bytes_per_launch / (launch_ms / 1e3) / 1e9 if launch_ms > 0 else None
+    traffic = None
+    tf = ROOT / "profiles" / "derivative_traffic.json"
+    if tf.exists():
+        try:
+            td = json.loads(tf.read_text())
+            key = f"{args.config}/corrected/p0"
+            if key in td:
+                traffic = td[key]["bytes_per_launch"]
+        except Exception:
+            traffic = None
+    roofline = {"kernel": "derivative pass (derivative_f32_kernel), plain arm at the configuration's resolution",
+                "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                else "fallback 6650 GB/s",
+                "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": launch_ms,
+                "launches": prof["deriv_launches"],
+                "bytes_model": "16 B/point + 4 B/in-bounds probe + 16 B/occupied probe + 56 B/accepted pair "
+                               "+ 352 B/tile partial",
+                "share_of_step": prof["deriv_ms"] / sum(prof_ms) if prof_ms else None,
+                "measured_in": f"a profiling pass of {prof_steps} plain-arm steps (rounds launched one by one, "
+                               f"CUDA events on the library stream); profiled step {sum(prof_ms) / prof_steps:.2f} ms"}
+    cores = os.cpu_count() or 1
+    cpu, acc = learned_cpu_leg(pkg, scene, cfg, aligns, plain_out, learned_out, learned_start, levels_spec, cores) \
+        if world == 1 else (None, None)
+    r_l, r_p = res["learned"], res["plain"]
     line = {
-        "metric": METRIC, "value": res["learned"]["aligns_per_s"], "unit": "aligns/s", "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["learned"]["ms_per_step"],
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "fp32 pair terms, fp64 solve/line search; network bf16 x bf16 -> fp32 (tensor cores)",
+        "metric": METRIC, "value": value, "unit": "aligns/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": tot["learned"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32 pair terms, fp64 grid/solve/line search; network bf16 x bf16 -> fp32 (tensor cores)",
         "data": "synthetic (seeded plane + walls generator)",
-        "config": {"workload": f"{cfg.name}: {cfg.map_points}-point map ({cfg.area:.0f} x {cfg.area:.0f} m, "
-                               f"{cfg.walls} walls), {B} alignments, scans {cfg.scan_min}-{cfg.scan_max} points, "
-                               f"resolution {cfg.resolution} m, guesses +-{cfg.dt} m / +-{cfg.dyaw_deg} deg",
-                   "mode": "corrected", "learned": "3 network passes, NDT judge (score at proposal vs guess), "
-                                                  "NDT refinement"},
-        "plain": res["plain"], "learned": res["learned"],
-        "learned_vs_plain_aligns_per_s": ratio,
-        "learned_vs_plain_aligns_per_s_within_2cm_0.1deg_of_truth": ratio_ok,
+        "config": learned_config_block(pkg, cfg, B, npts),
+        "plain": r_p, "learned": r_l,
+        "learned_vs_plain_aligns_per_s": r_l["aligns_per_s"] / r_p["aligns_per_s"],
+        "learned_vs_plain_aligns_per_s_within_2cm_0.1deg_of_truth":
+            r_l["aligns_per_s_within_2cm_0.1deg_of_truth"] / max(1e-9, r_p["aligns_per_s_within_2cm_0.1deg_of_truth"]),
+        "plain_value_all_ranks": plain_value,
+        "e2e": {"value": e2e_value, "unit": "aligns/s", "h2d_bytes_per_step": int(points.nbytes + offs.nbytes +
+                                                                                   guesses.nbytes),
+                "d2h_bytes_per_step": B * (16 * 4 + 4 + 8 + 4), "ms_per_step": e2e_total / args.steps,
+                "results_equal_device_arm": e2e_ok,
+                "path": "ndt_align_batch_learned (C ABI, host buffers: pinned scans and guesses in, poses out; "
+                        "grids built in set-up)"},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
         "accuracy_vs_fp64_oracle": acc,
-        "training": {"pairs": int(pairs.keep.sum()), "scans": args.train_scans, "epochs": args.train_epochs,
-                     "pair_generation_s": t_pairs, "ndt_labelling_s": t_label, "gpu_training_s": t_train,
-                     "loss_first_last": [float(losses[:50].mean()), float(losses[-50:].mean())]},
-        "timing": "wall clock around synchronised steps (the learned pipeline: proposal passes, two score passes, "
-                  "judge and refinement enqueued on one stream, one synchronisation)",
+        "clocks": clk,
+        "gpu_launches": int(launches),
+        "training": training,
     }
-    print(json.dumps(line))
+    print(json.dumps(line), flush=True)
     net.close()
-    ctx.close()
+    for c in levels:
+        c.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
     return 0
 
 
@@ -1011,8 +1254,10 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", default="c2")
-    ap.add_argument("--mode", choices=["compat", "corrected"], default="compat")
+    ap.add_argument("--config", default="c5",
+                    help="c5 (default) / c4: learned-init vs plain (corrected NDT); c1-c3: the plain NDT alone")
+    ap.add_argument("--mode", choices=["compat", "corrected"], default=None,
+                    help="plain-NDT workloads: compat (reference behaviour; default for c1, c2) or corrected")
     ap.add_argument("--precision", type=int, choices=[0, 1], default=0)
     ap.add_argument("--variant", default="auto",
                     help="derivative-pass launch shape: an index, or 'auto' (autotuned on the workload)")
@@ -1025,9 +1270,10 @@ def main(argv=None):
     ap.add_argument("--posenet", action="store_true", help="time the network kernels alone")
     ap.add_argument("--posenet-scans", type=int, default=4096)
     ap.add_argument("--learned", action="store_true",
-                    help="learned-init vs plain batched NDT (trains the network first; use --config c4 or c5)")
+                    help="learned-init vs plain batched NDT on any configuration (default for c4 and c5)")
+    ap.add_argument("--no-learned", action="store_true", help="c4 / c5: the plain NDT line instead")
     ap.add_argument("--train-scans", type=int, default=0, help="0: 8000 (c4), 16000 (c5)")
-    ap.add_argument("--train-epochs", type=int, default=0, help="0: 30 (c4), 60 (c5)")
+    ap.add_argument("--train-epochs", type=int, default=0, help="0: 30 (c4), 40 (c5)")
     ap.add_argument("--oracle-sample", type=int, default=64)
     ap.add_argument("--filter", action="store_true", help="time the scan pre-filter (voxel-grid downsampling)")
     ap.add_argument("--append", action="store_true", help="time map growth (ndt_map_append) against rebuilds")
@@ -1042,6 +1288,12 @@ def main(argv=None):
         ap.error("--warmup must be >= 3")
     pkg = load_pkg()
     world, rank, local = dist_setup()
+    if args.config not in pkg.synth.CONFIGS:
+        ap.error(f"unknown config {args.config}")
+    if args.config in ("c4", "c5") and not args.no_learned:
+        args.learned = True
+    if args.mode is None:
+        args.mode = "compat" if args.config in ("c1", "c2") else "corrected"
     if args.posenet and args.impl != "reference":
         return run_posenet(args, pkg, local)
     if args.learned and args.impl != "reference":

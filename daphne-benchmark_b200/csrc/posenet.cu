@@ -38,6 +38,7 @@
 #include <string>
 
 #include "../../include/ndt_b200.h"
+#include "mlp_internal.h"
 #include "umma_desc.h"
 
 namespace pn {
@@ -49,12 +50,6 @@ constexpr int oW1 = 0, oB1 = oW1 + kH1 * 3, oW2 = oB1 + kH1, oB2 = oW2 + kH2 * k
 constexpr int kTileRows = 128;                  // points per tensor-core tile (MMA M)
 constexpr int kOperandBytes = kTileRows * kH1 * 2;  // 16 KB per BF16 operand
 constexpr uint32_t kTmemCols = 128;             // FP32 accumulator columns (MMA N)
-constexpr unsigned kWaitLimit = 1u << 26;       // bounded mbarrier wait (error flag when exceeded)
-
-struct Norm {
-    float cx, cy, cz, inv_s;   // input centring and scale
-    float dscale[6];           // pose-correction units
-};
 
 // Byte offset of element (r, k) in an interleaved K-major operand (64 K).
 __host__ __device__ __forceinline__ uint32_t op_offset(int r, int k) {
@@ -103,6 +98,7 @@ struct PointArgs {
     int *err;
     Norm nm;
     int B;
+    int scans;                 // candidate b reads scan b % scans (several starts of one scan)
     int max_points;
     unsigned wait_limit;       // polls of the MMA barrier before the wait gives up
 };
@@ -121,7 +117,8 @@ __global__ void __launch_bounds__(128, 1) point_kernel(const __grid_constant__ P
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int b = blockIdx.x;
     if (b >= a.B) return;  // (grid = B: never taken)
-    const int start = a.offsets[b], n = a.offsets[b + 1] - start;
+    const int sb = b % a.scans;
+    const int start = a.offsets[sb], n = a.offsets[sb + 1] - start;
     const int P = n < a.max_points ? n : a.max_points;
 
     // operands and small weights into shared memory
@@ -426,37 +423,6 @@ __global__ void reduce_adam_kernel(const __grid_constant__ AdamArgs a) {
     a.w[i] -= a.lr * (m / a.bc1) / (sqrtf(v / a.bc2) + a.eps);
 }
 
-// Pose vector (x, y, z, roll, pitch, yaw) of T = Trans Rx Ry Rz and back, FP64.
-__device__ __forceinline__ void pose_of(const float *T, double p[6]) {
-    p[0] = T[3];
-    p[1] = T[7];
-    p[2] = T[11];
-    p[3] = atan2(-(double)T[6], (double)T[10]);
-    p[4] = asin(fmin(1.0, fmax(-1.0, (double)T[2])));
-    p[5] = atan2(-(double)T[1], (double)T[0]);
-}
-
-__device__ __forceinline__ void matrix_of(const double p[6], float *T) {
-    double sa, ca, sb, cb, sc, cc;
-    sincos(p[3], &sa, &ca);
-    sincos(p[4], &sb, &cb);
-    sincos(p[5], &sc, &cc);
-    T[0] = (float)(cb * cc);
-    T[1] = (float)(-cb * sc);
-    T[2] = (float)sb;
-    T[3] = (float)p[0];
-    T[4] = (float)(ca * sc + sa * sb * cc);
-    T[5] = (float)(ca * cc - sa * sb * sc);
-    T[6] = (float)(-sa * cb);
-    T[7] = (float)p[1];
-    T[8] = (float)(sa * sc - ca * sb * cc);
-    T[9] = (float)(sa * cc + ca * sb * sc);
-    T[10] = (float)(ca * cb);
-    T[11] = (float)p[2];
-    T[12] = T[13] = T[14] = 0.0f;
-    T[15] = 1.0f;
-}
-
 // proposal = T(pose(guess) + y * dscale)
 __global__ void apply_kernel(const float *__restrict__ guesses, const float *__restrict__ y, Norm nm, int B,
                              float *__restrict__ out) {
@@ -483,22 +449,7 @@ __global__ void judge_kernel(const float *__restrict__ prop, const float *__rest
 }  // namespace pn
 
 // ---------------------------------------------------------------------------
-// C ABI
-struct ndt_mlp {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    cudaStream_t own_stream = nullptr;  // created with the network; `stream` may be a caller's
-    float *w = nullptr, *m = nullptr, *v = nullptr, *grad = nullptr, *loss = nullptr;
-    uint8_t *w2op = nullptr;
-    int *err = nullptr;
-    unsigned long long *gmax = nullptr;
-    float *grad_scan = nullptr, *loss_scan = nullptr;
-    size_t cap_b = 0;
-    int step = 0;
-    pn::Norm nm{};
-    unsigned wait_limit = pn::kWaitLimit;
-    std::string msg;
-};
+// C ABI (struct ndt_mlp: mlp_internal.h)
 
 namespace {
 
@@ -533,7 +484,7 @@ int ensure_batch(ndt_mlp *c, int B) {
 }
 
 int run_forward(ndt_mlp *c, int B, const float *d_points, const int *d_offsets, const float *d_guesses,
-                int max_points) {
+                int max_points, int scans) {
     if (int rc = ensure_batch(c, B)) return rc;
     pn::PointArgs a;
     a.points = reinterpret_cast<const float4 *>(d_points);
@@ -546,6 +497,7 @@ int run_forward(ndt_mlp *c, int B, const float *d_points, const int *d_offsets, 
     a.wait_limit = c->wait_limit;
     a.nm = c->nm;
     a.B = B;
+    a.scans = scans;
     a.max_points = max_points;
     pn::point_kernel<<<B, 128, kPointSmemAlloc, c->stream>>>(a);
     MCK(cudaGetLastError());
@@ -595,6 +547,9 @@ void ndt_mlp_destroy(ndt_mlp *c) {
     void *bufs[] = {c->w, c->m, c->v, c->grad, c->loss, c->w2op, c->err, c->gmax, c->grad_scan, c->loss_scan};
     for (void *p : bufs)
         if (p) cudaFree(p);
+    learned_buffers_free(c->lb);
+    for (cudaEvent_t e : c->ev)
+        if (e) cudaEventDestroy(e);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
 }
@@ -636,7 +591,14 @@ int ndt_mlp_forward_device(ndt_mlp *c, int B, const float *d_points, const int *
                            int max_points, float *d_y6) {
     if (!c || B <= 0 || !d_points || !d_offsets || !d_guesses || !d_y6 || max_points <= 0) return NDT_E_ARG;
     MCK(cudaSetDevice(c->device));
-    if (int rc = run_forward(c, B, d_points, d_offsets, d_guesses, max_points)) return rc;
+    return mlp_forward(c, B, B, d_points, d_offsets, d_guesses, max_points, d_y6);
+}
+
+}  // extern "C"
+
+int mlp_forward(ndt_mlp *c, int B, int scans, const float *d_points, const int *d_offsets, const float *d_guesses,
+                int max_points, float *d_y6) {
+    if (int rc = run_forward(c, B, d_points, d_offsets, d_guesses, max_points, scans)) return rc;
     pn::HeadArgs h;
     std::memset(&h, 0, sizeof(h));
     h.points = reinterpret_cast<const float4 *>(d_points);
@@ -653,12 +615,26 @@ int ndt_mlp_forward_device(ndt_mlp *c, int B, const float *d_points, const int *
     return NDT_OK;
 }
 
+int mlp_propose(ndt_mlp *c, int B, int scans, const float *d_points, const int *d_offsets, const float *d_guesses,
+                int max_points, int passes, float *d_y6, float *d_prop16) {
+    const float *g = d_guesses;
+    for (int k = 0; k < passes; ++k) {
+        if (int rc = mlp_forward(c, B, scans, d_points, d_offsets, g, max_points, d_y6)) return rc;
+        pn::apply_kernel<<<(B + 127) / 128, 128, 0, c->stream>>>(g, d_y6, c->nm, B, d_prop16);
+        MCK(cudaGetLastError());
+        g = d_prop16;  // the next pass reads the previous proposal (in place: each thread reads its own row first)
+    }
+    return NDT_OK;
+}
+
+extern "C" {
+
 int ndt_mlp_train_step_device(ndt_mlp *c, int B, const float *d_points, const int *d_offsets, const float *d_guesses,
                               const float *d_target6, int max_points, float lr, int update, float *h_loss,
                               float *h_grad) {
     if (!c || B <= 0 || !d_points || !d_offsets || !d_guesses || !d_target6 || max_points <= 0) return NDT_E_ARG;
     MCK(cudaSetDevice(c->device));
-    if (int rc = run_forward(c, B, d_points, d_offsets, d_guesses, max_points)) return rc;
+    if (int rc = run_forward(c, B, d_points, d_offsets, d_guesses, max_points, B)) return rc;
     pn::HeadArgs h;
     std::memset(&h, 0, sizeof(h));
     h.points = reinterpret_cast<const float4 *>(d_points);
@@ -740,14 +716,7 @@ int ndt_mlp_propose_device(ndt_mlp *c, int B, const float *d_points, const int *
     if (!c || B <= 0 || !d_points || !d_offsets || !d_guesses || !d_y6 || !d_prop16 || max_points <= 0 || passes < 1)
         return NDT_E_ARG;
     MCK(cudaSetDevice(c->device));
-    const float *g = d_guesses;
-    for (int k = 0; k < passes; ++k) {
-        if (int rc = ndt_mlp_forward_device(c, B, d_points, d_offsets, g, max_points, d_y6)) return rc;
-        pn::apply_kernel<<<(B + 127) / 128, 128, 0, c->stream>>>(g, d_y6, c->nm, B, d_prop16);
-        MCK(cudaGetLastError());
-        g = d_prop16;  // the next pass reads the previous proposal (in place: each thread reads its own row first)
-    }
-    return NDT_OK;
+    return mlp_propose(c, B, B, d_points, d_offsets, d_guesses, max_points, passes, d_y6, d_prop16);
 }
 
 int ndt_mlp_judge_device(ndt_mlp *c, int B, const float *d_prop16, const float *d_guesses, const double *d_score_prop,

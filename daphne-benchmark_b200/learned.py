@@ -2,14 +2,19 @@
 plain GPU NDT, training of the point-feature network on the GPU, and the
 proposal -> judge -> refine pipeline.
 
-Pipeline for a batch of (scan, guess):
-  1. the network proposes a corrected pose from the scan seen at its guess
-     (`PoseNet.forward`, tensor-core kernels);
-  2. the NDT judges: the score of the scan at the proposal and at the raw
-     guess (`Context.score_batch_device`, one derivative pass each); the
-     start pose is the proposal where its score is at least the guess's, the
-     raw guess otherwise (the fallback);
-  3. the plain NDT refines every alignment from its start pose (one batch).
+Pipeline for a batch of (scan, guess) (`LearnedBatch`, one call of the C
+entry point ndt_align_batch_learned_device; `learned_align` restates it step
+by step through the single-purpose entry points):
+  1. the network proposes corrected poses from K starts around the guess (a
+     grid of translations and yaw offsets; `PoseNet`, tensor-core kernels),
+     each start refined by `passes` network passes;
+  2. the NDT judges: the score of every proposal and of the raw guess at a
+     coarse level (`Context.score_batch_device` on a strided subsample of the
+     scan); the start pose is the best-scoring candidate, the raw guess when
+     no proposal scores higher (the fallback);
+  3. the plain NDT refines every alignment from its start pose through the
+     levels (coarse to fine resolution; `refinement_levels`), the last level
+     being the plain NDT of the configuration.
 
 Training pairs: (scan, perturbed guess -> converged pose), generated on the
 GPU by the same library: the converged pose is where the plain NDT settles
@@ -207,66 +212,135 @@ def score(ctx, torch, pts, offs, total, poses_np):
     return s.cpu().numpy()
 
 
-class LearnedBatch:
-    """Device buffers of the learned pipeline for one batch; run() enqueues
-    proposal passes, the two score passes, the judge and the refinement on the
-    NDT context's stream (the network is put on that stream), with one
-    synchronisation at the end."""
+def refinement_levels(resolution, step=0.1):
+    """(resolution, step_size) of the refinement levels, coarse to fine: 4 r,
+    2 r and the plain NDT's own r with its step (the coarse levels take longer
+    steps: the step limits how far one Newton iteration moves the pose)."""
+    return [(4.0 * resolution, 1.0 * resolution), (2.0 * resolution, 0.4 * resolution), (resolution, step)]
 
-    def __init__(self, ctx, net, torch, pts, offs, total, guesses_np, max_points=512, passes=3):
+
+def level_contexts(ndt, cloud, resolution, device=0, levels=None):
+    """Corrected-NDT contexts holding `cloud` at every refinement level."""
+    out = []
+    for res, step in (levels or refinement_levels(resolution)):
+        p = ndt.corrected_params(res)
+        p.step_size = step
+        c = ndt.Context(p, device=device)
+        c.set_map(cloud)
+        out.append(c)
+    return out
+
+
+class LearnedBatch:
+    """Device buffers of the learned pipeline for one batch; run() enqueues the
+    whole pipeline (ndt_align_batch_learned_device: proposals from the starts,
+    the judge's score pass, refinement through the levels) and waits for the
+    last level."""
+
+    def __init__(self, levels, net, torch, pts, offs, total, guesses_np, params=None):
         B = len(guesses_np)
-        self.ctx, self.net, self.torch = ctx, net, torch
+        self.levels, self.net, self.torch = levels, net, torch
         self.pts, self.offs, self.total, self.B = pts, offs, total, B
-        self.max_points, self.passes = max_points, passes
-        f32 = dict(dtype=torch.float32, device="cuda")
+        self.params = params if params is not None else posenet.learned_params()
         self.g = torch.from_numpy(np.ascontiguousarray(guesses_np, np.float32)).cuda()
-        self.y = torch.zeros((B, 6), **f32)
-        self.prop = torch.zeros((B, 16), **f32)
-        self.start = torch.zeros((B, 16), **f32)
-        self.s_p = torch.zeros(B, dtype=torch.float64, device="cuda")
-        self.s_g = torch.zeros(B, dtype=torch.float64, device="cuda")
-        self.used = torch.zeros(B, dtype=torch.int32, device="cuda")
-        self.out = torch.zeros((B, 16), **f32)
+        self.out = torch.zeros((B, 16), dtype=torch.float32, device="cuda")
         self.conv = torch.zeros(B, dtype=torch.int32, device="cuda")
         self.fit = torch.zeros(B, dtype=torch.float64, device="cuda")
         self.st = torch.zeros(B, dtype=torch.int32, device="cuda")
+        self.choice = torch.zeros(B, dtype=torch.int32, device="cuda")
+        self.start = torch.zeros((B, 16), dtype=torch.float32, device="cuda")
         torch.cuda.current_stream().synchronize()
-        net.set_stream(ctx.stream)
 
     def run(self):
-        n, c, B = self.net, self.ctx, self.B
-        n.propose_device(B, self.pts.data_ptr(), self.offs.data_ptr(), self.g.data_ptr(), self.y.data_ptr(),
-                         self.prop.data_ptr(), self.passes, self.max_points)
-        c.score_batch_device(B, self.pts.data_ptr(), self.offs.data_ptr(), self.total, self.prop.data_ptr(),
-                             self.s_p.data_ptr())
-        c.score_batch_device(B, self.pts.data_ptr(), self.offs.data_ptr(), self.total, self.g.data_ptr(),
-                             self.s_g.data_ptr())
-        n.judge_device(B, self.prop.data_ptr(), self.g.data_ptr(), self.s_p.data_ptr(), self.s_g.data_ptr(),
-                       self.start.data_ptr(), self.used.data_ptr())
-        c.align_batch_device(B, self.pts.data_ptr(), self.offs.data_ptr(), self.total, self.start.data_ptr(),
-                             self.out.data_ptr(), self.conv.data_ptr(), self.fit.data_ptr(), self.st.data_ptr())
-        c.synchronize()
+        self.net.align_learned_device(self.levels, self.params, self.B, self.pts.data_ptr(), self.offs.data_ptr(),
+                                      self.total, self.g.data_ptr(), self.out.data_ptr(), self.conv.data_ptr(),
+                                      self.fit.data_ptr(), self.st.data_ptr(), self.choice.data_ptr(),
+                                      self.start.data_ptr())
+        self.levels[-1].synchronize()
+        if self.net.synchronize_status():
+            raise RuntimeError("tensor-core wait gave up in the network's kernels")
 
     def results(self):
+        """(out, conv, fit, status, choice, start): choice = K for the raw guess (the fallback), start = the
+        pose the refinement started from."""
         return (self.out.cpu().numpy(), self.conv.cpu().numpy(), self.fit.cpu().numpy(), self.st.cpu().numpy(),
-                self.used.cpu().numpy() != 0, self.prop.cpu().numpy(), self.start.cpu().numpy())
+                self.choice.cpu().numpy(), self.start.cpu().numpy())
 
     def close(self):
-        self.net.set_stream(None)
+        pass
 
 
-def learned_align(ctx, net, torch, pts, offs, total, guesses_np, max_points=512, passes=1):
-    """Proposal (the network applied `passes` times, each pass to the previous
-    proposal) -> judge -> refine.  Returns (out, conv, fit, status, used_proposal)."""
-    prop = guesses_np
-    for _ in range(passes):
-        prop, _ = propose(net, torch, pts, offs, prop, max_points)
-    s_prop = score(ctx, torch, pts, offs, total, prop)
-    s_guess = score(ctx, torch, pts, offs, total, guesses_np)
-    use = s_prop >= s_guess
-    start = np.where(use[:, None], prop, guesses_np).astype(np.float32)
-    out, conv, fit, st = ndt_align_device(ctx, torch, pts, offs, total, start)
-    return out, conv, fit, st, use
+def start_offsets(params):
+    """(dx, dy, dyaw_rad) of the K starts in the order of the C pipeline (start_kernel)."""
+    gxy, gyaw = params.grid_xy, params.grid_yaw
+    out = []
+    for k in range(gxy * gxy * gyaw):
+        iyaw, ixy = k % gyaw, k // gyaw
+        ix, iy = ixy % gxy, ixy // gxy
+        out.append(((ix - 0.5 * (gxy - 1)) * params.step_xy, (iy - 0.5 * (gxy - 1)) * params.step_xy,
+                    math.radians((iyaw - 0.5 * (gyaw - 1)) * params.step_yaw_deg)))
+    return out
+
+
+def learned_align(levels, net, torch, scans, guesses_np, params=None):
+    """The learned pipeline step by step through the single-purpose entry
+    points (network proposals, score pass, plain NDT per level), with the
+    judge's choice made here on the host.  Same arithmetic as LearnedBatch:
+    returns (out, conv, fit, status, choice)."""
+    params = params if params is not None else posenet.learned_params()
+    B = len(guesses_np)
+    dev = DeviceScans(torch, scans)
+    pts, offs, total = dev.batch(np.arange(B))
+    cands = []
+    for dx, dy, dyaw in start_offsets(params):
+        p = posenet.poses_from_matrices(guesses_np)
+        c, s_ = np.cos(p[:, 5]), np.sin(p[:, 5])
+        p[:, 0] += c * dx - s_ * dy
+        p[:, 1] += s_ * dx + c * dy
+        p[:, 5] += dyaw
+        g = posenet.matrices_from_poses(p)
+        if params.passes > 0:
+            g = propose_passes(net, torch, pts, offs, g, params.passes, params.max_points)
+        cands.append(g)
+    cands.append(np.asarray(guesses_np, np.float32))
+    judge = levels[params.judge_level]
+    sub = DeviceScans(torch, scans, max_points=params.judge_points or None)
+    sp, so, st = sub.batch(np.arange(B))
+    scores = np.stack([score(judge, torch, sp, so, st, g) for g in cands])
+    K = len(cands) - 1
+    choice = np.full(B, K, np.int64)
+    best = scores[K].copy()
+    for k in range(K):
+        win = (scores[k] > best) | (np.isnan(best) & ~np.isnan(scores[k]))
+        choice[win] = k
+        best[win] = scores[k][win]
+    cur = np.stack(cands)[choice, np.arange(B)]
+    status = np.zeros(B, np.int32)
+    out = conv = fit = None
+    for l, ctx in enumerate(levels):
+        cap = params.level_points[l]
+        if cap > 0:
+            lv = DeviceScans(torch, scans, max_points=cap)
+            lp_, lo_, lt_ = lv.batch(np.arange(B))
+        else:
+            lp_, lo_, lt_ = pts, offs, total
+        out, conv, fit, st_l = ndt_align_device(ctx, torch, lp_, lo_, lt_, cur)
+        status |= st_l
+        cur = out
+    return out, conv, fit, status, choice.astype(np.int32)
+
+
+def propose_passes(net, torch, pts, offs, guesses_np, passes, max_points=512):
+    """The network's proposals after `passes` passes (device-side application, ndt_mlp_propose_device)."""
+    B = len(guesses_np)
+    g = torch.from_numpy(np.ascontiguousarray(guesses_np, np.float32)).cuda()
+    y = torch.zeros((B, 6), dtype=torch.float32, device="cuda")
+    prop = torch.zeros((B, 16), dtype=torch.float32, device="cuda")
+    torch.cuda.current_stream().synchronize()
+    net.propose_device(B, pts.data_ptr(), offs.data_ptr(), g.data_ptr(), y.data_ptr(), prop.data_ptr(), passes,
+                       max_points)
+    net.synchronize()
+    return prop.cpu().numpy()
 
 
 def pose_errors(out, truths):

@@ -17,6 +17,41 @@ from . import ndt as _ndt
 
 H1, H2, H3, OUT = 64, 128, 64, 6
 DELTA_SCALE = np.array([1.0, 1.0, 0.1, 0.02, 0.02, 0.1], np.float32)  # m, m, m, rad, rad, rad
+MAX_LEVELS = 8  # NDT_LEARNED_MAX_LEVELS
+# FP32 weight blob layout (ndt_mlp_num_weights values): W1[64][3], b1, W2[128][64], b2, W3[64][128], b3, W4[6][64], b4
+_OFF = np.cumsum([0, H1 * 3, H1, H2 * H1, H2, H3 * H2, H3, OUT * H3, OUT])
+
+
+def init_weights(seed=0):
+    """He-style initialisation: normal weights with variance 2 / fan-in (the output layer scaled by 0.1 of
+    1 / fan-in, so the first proposals stay near the guess), zero biases."""
+    rng = np.random.default_rng(seed)
+    w = np.zeros(int(_OFF[-1]), np.float32)
+    w[_OFF[0]:_OFF[1]] = rng.normal(0, np.sqrt(2.0 / 3), H1 * 3)
+    w[_OFF[2]:_OFF[3]] = rng.normal(0, np.sqrt(2.0 / H1), H2 * H1)
+    w[_OFF[4]:_OFF[5]] = rng.normal(0, np.sqrt(2.0 / H2), H3 * H2)
+    w[_OFF[6]:_OFF[7]] = rng.normal(0, np.sqrt(1.0 / H3) * 0.1, OUT * H3)
+    return w
+
+
+class LearnedParams(C.Structure):
+    """ndt_learned_params (include/ndt_b200.h): the learned-init pipeline's set-up."""
+    _fields_ = [("max_points", C.c_int32), ("passes", C.c_int32), ("grid_xy", C.c_int32), ("grid_yaw", C.c_int32),
+                ("step_xy", C.c_float), ("step_yaw_deg", C.c_float), ("judge_level", C.c_int32),
+                ("judge_points", C.c_int32), ("level_points", C.c_int32 * MAX_LEVELS)]
+
+
+def learned_params(**kw):
+    """The library's defaults (ndt_learned_params_default), overridden by keyword."""
+    p = LearnedParams()
+    _lib().ndt_learned_params_default(C.byref(p))
+    for k, v in kw.items():
+        if k == "level_points":
+            for i, n in enumerate(v):
+                p.level_points[i] = int(n)
+        else:
+            setattr(p, k, v)
+    return p
 
 
 def _lib():
@@ -43,6 +78,14 @@ def _lib():
         L.ndt_mlp_set_stream.argtypes = [p, p]
         L.ndt_mlp_propose_device.argtypes = [p, C.c_int, p, p, p, C.c_int, C.c_int, p, p]
         L.ndt_mlp_judge_device.argtypes = [p, C.c_int, p, p, p, p, p, p]
+        L.ndt_learned_params_default.argtypes = [C.POINTER(LearnedParams)]
+        L.ndt_learned_params_default.restype = None
+        L.ndt_align_batch_learned_device.argtypes = [p, C.POINTER(C.c_void_p), C.c_int, C.POINTER(LearnedParams),
+                                                     C.c_int, p, p, C.c_int, p, p, p, p, p, p, p]
+        L.ndt_align_batch_learned_device.restype = C.c_int
+        L.ndt_align_batch_learned.argtypes = [p, C.POINTER(C.c_void_p), C.c_int, C.POINTER(LearnedParams),
+                                              C.c_int, p, p, p, p, p, p, p, p, p]
+        L.ndt_align_batch_learned.restype = C.c_int
         for n in ("ndt_mlp_create", "ndt_mlp_set_input_frame", "ndt_mlp_set_weights", "ndt_mlp_get_weights",
                   "ndt_mlp_forward_device", "ndt_mlp_train_step_device", "ndt_mlp_maxpool_device",
                   "ndt_mlp_synchronize", "ndt_mlp_set_wait_limit", "ndt_mlp_set_stream", "ndt_mlp_propose_device", "ndt_mlp_judge_device"):
@@ -145,6 +188,33 @@ class PoseNet:
         self._check(self.L.ndt_mlp_propose_device(self.h, B, C.c_void_p(d_points), C.c_void_p(d_offsets),
                                                   C.c_void_p(d_guesses), max_points, passes, C.c_void_p(d_y),
                                                   C.c_void_p(d_prop)), "propose")
+
+    def align_learned_device(self, levels, lp, B, d_points, d_offsets, total, d_guesses, d_out, d_conv, d_fit,
+                             d_status=0, d_choice=0, d_start=0):
+        """ndt_align_batch_learned_device: proposals from lp's starts, the NDT judge, refinement through
+        `levels` (ndt.Context objects, coarse to fine).  Device pointers as ints; enqueued, ready after
+        levels[-1].synchronize()."""
+        arr = (C.c_void_p * len(levels))(*[c.h.value if isinstance(c.h, C.c_void_p) else c.h for c in levels])
+        rc = self.L.ndt_align_batch_learned_device(self.h, arr, len(levels), C.byref(lp), B, C.c_void_p(d_points),
+                                                   C.c_void_p(d_offsets), int(total), C.c_void_p(d_guesses),
+                                                   C.c_void_p(d_out), C.c_void_p(d_conv), C.c_void_p(d_fit),
+                                                   C.c_void_p(d_status or None), C.c_void_p(d_choice or None),
+                                                   C.c_void_p(d_start or None))
+        if rc != 0:
+            raise _ndt.NdtError(f"ndt_align_batch_learned_device ({_ndt.ERRORS.get(rc, rc)}): "
+                                f"{self.L.ndt_mlp_last_error(self.h).decode()}")
+
+    def align_learned(self, levels, lp, B, points, offsets, guesses, out, conv, fit, status=0, choice=0, start=0):
+        """ndt_align_batch_learned: the same with host buffers (addresses as ints, e.g. of pinned tensors);
+        returns when the results are on the host."""
+        arr = (C.c_void_p * len(levels))(*[c.h.value if isinstance(c.h, C.c_void_p) else c.h for c in levels])
+        rc = self.L.ndt_align_batch_learned(self.h, arr, len(levels), C.byref(lp), B, C.c_void_p(points),
+                                            C.c_void_p(offsets), C.c_void_p(guesses), C.c_void_p(out),
+                                            C.c_void_p(conv), C.c_void_p(fit), C.c_void_p(status or None),
+                                            C.c_void_p(choice or None), C.c_void_p(start or None))
+        if rc != 0:
+            raise _ndt.NdtError(f"ndt_align_batch_learned ({_ndt.ERRORS.get(rc, rc)}): "
+                                f"{self.L.ndt_mlp_last_error(self.h).decode()}")
 
     def judge_device(self, B, d_prop, d_guesses, d_s_prop, d_s_guess, d_start, d_used=0):
         self._check(self.L.ndt_mlp_judge_device(self.h, B, C.c_void_p(d_prop), C.c_void_p(d_guesses),

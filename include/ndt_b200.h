@@ -357,6 +357,59 @@ NDT_API int ndt_mlp_judge_device(ndt_mlp *mlp, int B, const float *d_prop16, con
                                  int *d_used);
 
 /*
+ * Learned-init batched alignment (no counterpart in the reference, whose align
+ * call starts the NDT at the caller's guess: partial_points_callback,
+ * src/CPU/ndt_mapping/kernel.cpp:1405-1414).  For B scans (d_points,
+ * d_offsets: B + 1 prefix offsets) with guesses (B x 16), against contexts
+ * levels[0 .. n_levels) that hold the same map at coarse-to-fine resolutions
+ * (compat = 0):
+ *   1. starts: each guess moved by a fixed pattern of K = grid_xy^2 x grid_yaw
+ *      offsets (translations step_xy apart in the guess's heading frame, yaw
+ *      offsets step_yaw_deg apart, centred on the guess);
+ *   2. proposals: the network runs `passes` times from every start, each pass
+ *      from the previous proposal (max_points points per scan);
+ *   3. the judge: the NDT score of the K proposals and of the raw guess, on
+ *      judge_points evenly strided points of the scan (0 = all), with the map
+ *      of levels[judge_level]; each scan starts from its best-scoring
+ *      candidate, the raw guess whenever no proposal scores higher;
+ *   4. refinement: the plain NDT from that start through every level in order
+ *      (level l reads level_points[l] evenly strided points per scan, 0 =
+ *      all); the last level's result is the output.
+ * Outputs (device): d_out (B x 16), d_conv, d_fit as ndt_align_batch_device;
+ * d_status (optional) = OR of the levels' NDT_ST_* bits; d_choice (optional)
+ * = the winning candidate per scan: k < K for the proposal from start k, K
+ * for the raw guess; d_start16 (optional, B x 16) = the winning candidate's
+ * pose, where the refinement started.  Work is enqueued on the network's and the contexts'
+ * streams, ordered by events; the results are ready after
+ * ndt_synchronize(levels[n_levels - 1]).  Inputs must be ready when called.
+ */
+#define NDT_LEARNED_MAX_LEVELS 8
+typedef struct ndt_learned_params {
+    int32_t max_points;    /* network: points read per scan */
+    int32_t passes;        /* network passes per start (0: the starts themselves are the candidates) */
+    int32_t grid_xy;       /* starts: grid_xy x grid_xy translations ... */
+    int32_t grid_yaw;      /* ... times grid_yaw yaw offsets */
+    float step_xy;         /* translation spacing of the starts [m] */
+    float step_yaw_deg;    /* yaw spacing of the starts [deg] */
+    int32_t judge_level;   /* index of the level whose map scores the candidates */
+    int32_t judge_points;  /* points per scan in the score pass (0 = all) */
+    int32_t level_points[NDT_LEARNED_MAX_LEVELS];  /* points per scan at each refinement level (0 = all) */
+} ndt_learned_params;
+/* Defaults: 512 points, 3 passes, a 3 x 3 grid of starts 1.5 m apart, judge at level 0 on 2048 points. */
+NDT_API void ndt_learned_params_default(ndt_learned_params *p);
+NDT_API int ndt_align_batch_learned_device(ndt_mlp *mlp, ndt_ctx *const *levels, int n_levels,
+                                           const ndt_learned_params *lp, int B, const float *d_points,
+                                           const int *d_offsets, int total_points, const float *d_guesses,
+                                           float *d_out, int *d_conv, double *d_fit, int *d_status, int *d_choice,
+                                           float *d_start16);
+/* The same with HOST buffers (the scans packed as ndt_align_batch_packed takes them: points = sum(ns)
+ * float[4], offsets = B + 1 prefix offsets): copies in, the pipeline, copies out; returns when the results
+ * are in out, converged, fitness, status, choice and start16 (the last three may be NULL). */
+NDT_API int ndt_align_batch_learned(ndt_mlp *mlp, ndt_ctx *const *levels, int n_levels, const ndt_learned_params *lp,
+                                    int B, const float *points, const int *offsets, const float *guesses, float *out,
+                                    int *converged, double *fitness, int *status, int *choice, float *start16);
+
+/*
  * The input file on the fast path (replaces the reference's one-value-at-a-
  * time reads of ndt_input.dat, parseInitGuess / parseFilteredScan,
  * kernel.cpp:143-173, read_next_testcases :192-229; same format).

