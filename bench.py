@@ -555,8 +555,8 @@ def run_ours(args, pkg, world, rank, local):
 
 def learned_config_block(pkg, cfg, B, npts):
     """The `config` of the learned-vs-plain workload (both arms print it)."""
-    lp = pkg.posenet.learned_params()
     levels_spec = pkg.learned.refinement_levels(cfg.resolution)
+    lp = pkg.learned.pipeline_params(levels_spec)
     return {"workload": f"{cfg.name}: {cfg.map_points}-point map ({cfg.area:g} x {cfg.area:g} m, {cfg.walls} walls), "
                         f"{B} alignments per step, scans {cfg.scan_min}-{cfg.scan_max} points (log-uniform), "
                         f"resolution {cfg.resolution:g} m, guesses +-{cfg.dt:g} m / +-{cfg.dyaw_deg:g} deg; "
@@ -565,9 +565,9 @@ def learned_config_block(pkg, cfg, B, npts):
             "resolution_m": cfg.resolution, "mode": "corrected",
             "learned": {"starts": f"{lp.grid_xy} x {lp.grid_xy} translations {lp.step_xy:g} m apart x {lp.grid_yaw} "
                                   f"yaw", "network_passes": lp.passes,
-                        "judge": f"NDT score at {levels_spec[lp.judge_level][0]:g} m on {lp.judge_points} points per "
-                                 f"scan, raw guess kept when no proposal scores higher",
-                        "refinement_levels_m_step": levels_spec},
+                        "judge": f"NDT score at {levels_spec[lp.judge_level]['resolution']:g} m on {lp.judge_points} "
+                                 f"points per scan, raw guess kept when no proposal scores higher",
+                        "refinement_levels": levels_spec},
             "l2": f"flushed between timed steps ({L2_FLUSH_BYTES >> 20} MiB write); scans larger than L2"}
 
 
@@ -611,9 +611,8 @@ def learned_cpu_leg(pkg, scene, cfg, aligns, plain_out, learned_out, learned_sta
     t_plain = time.perf_counter() - t0
     t0 = time.perf_counter()
     cur = learned_start[:m]
-    for res, step in levels_spec:
-        op = binding.corrected_params(res)
-        op.step_size = step
+    for lvl in levels_spec:
+        op = pkg.learned.level_params(binding.corrected_params(lvl["resolution"]), lvl)
         cur = orc.align_batch(op, sc, cur, scene.map, nthreads=cores)[0]
     t_learned = time.perf_counter() - t0
     out["corrected_fp64_oracle_plain"] = {"value": m / t_plain, "cores": cores,
@@ -626,14 +625,44 @@ def learned_cpu_leg(pkg, scene, cfg, aligns, plain_out, learned_out, learned_sta
                 "sample": out["corrected_fp64_oracle_plain"]["sample"] + ", FP64 corrected-NDT oracle"}
     base["variants"] = out
 
-    def agree(gpu, ref):
+    def plain_run(i, g):
+        return orc.align(prm, sc[i], g, scene.map)[0]
+
+    def learned_run(i, g):
+        for lvl in levels_spec:
+            op = pkg.learned.level_params(binding.corrected_params(lvl["resolution"]), lvl)
+            g = orc.align(op, sc[i], g, scene.map)[0]
+        return g
+
+    def unstable(run, i, start):
+        # the oracle itself: does a one-ulp change of one entry of its float start move its result by > 2 cm?
+        base = run(i, np.asarray(start, np.float32))
+        for j in (3, 7, 11, 0, 1, 4):
+            for d in (np.inf, -np.inf):
+                g = np.array(start, np.float32).reshape(16)
+                g[j] = np.nextafter(g[j], np.float32(d))
+                o = run(i, g)
+                if np.linalg.norm(o.reshape(4, 4)[:3, 3] - base.reshape(4, 4)[:3, 3]) > 0.02 or \
+                        rot_deg(o, base) > 0.1:
+                    return True
+        return False
+
+    def agree(gpu, ref, run, starts):
         dt = np.linalg.norm(gpu.reshape(-1, 4, 4)[:, :3, 3] - ref.reshape(-1, 4, 4)[:, :3, 3], axis=1)
         dr = np.array([rot_deg(gpu[i], ref[i]) for i in range(len(ref))])
-        return {"alignments": len(ref), "within_2cm_0.1deg": int(np.sum((dt <= 0.02) & (dr <= 0.1))),
-                "max_translation_m": float(dt.max()), "max_rotation_deg": float(dr.max())}
-    acc = {"plain": agree(plain_out[:m], ref_plain), "learned": agree(learned_out[:m], cur),
+        ok = (dt <= 0.02) & (dr <= 0.1)
+        exc = np.flatnonzero(~ok)
+        return {"alignments": len(ref), "within_2cm_0.1deg": int(ok.sum()),
+                "max_translation_m_within": float(dt[ok].max()) if ok.any() else None,
+                "max_rotation_deg_within": float(dr[ok].max()) if ok.any() else None,
+                "exceptions": int(len(exc)),
+                "exceptions_where_the_oracle_is_not_reproducible": int(sum(unstable(run, i, starts[i])
+                                                                           for i in exc))}
+    acc = {"plain": agree(plain_out[:m], ref_plain, plain_run, [a.guess for a in aligns[:m]]),
+           "learned": agree(learned_out[:m], cur, learned_run, learned_start[:m]),
            "oracle": "FP64 corrected-NDT oracle from the same starts (learned: its refinement levels from the "
-                     "GPU's chosen starts)"}
+                     "GPU's chosen starts); an exception is not reproducible by the oracle when a one-ulp change "
+                     "of one entry of its float start moves its own result by more than 2 cm / 0.1 deg"}
     return base, acc
 
 
@@ -708,7 +737,7 @@ def run_learned(args, pkg, world, rank, local):
             for k in ("plain", "learned")}
     d_choice = torch.zeros(B, dtype=torch.int32, device=dev)
     d_start = torch.zeros(B, 16, device=dev)
-    lp = PN.learned_params()
+    lp = L.pipeline_params(levels_spec)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     s_net = torch.cuda.ExternalStream(net.stream, device=dev)
     s_fine = torch.cuda.ExternalStream(fine.stream, device=dev)

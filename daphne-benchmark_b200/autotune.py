@@ -4,7 +4,12 @@ The derivative kernel is compiled in several shapes (points per tile =
 threads per block, resident blocks per SM; see ndt.kernel_variants()).  The
 best shape depends on the workload (scan sizes, neighbour counts, map
 density), so tune() runs the caller's step once per shape, times it with CUDA
-events on the context's stream and selects the fastest on the context.
+events on the context's stream and selects the fastest on the context.  The
+step may be anything enqueued on the context's stream (the benchmark's step
+builds the grid and aligns a batch).  C and C++ callers tune an alignment
+batch with the library's own ndt_autotune_batch / ndt_autotune_batch_device
+(Context.autotune_device here), which the DAPHNE harness front end calls on
+its first batch.
 """
 from __future__ import annotations
 

@@ -43,6 +43,10 @@ struct DerivVariant {
     int min_blocks;
 };
 constexpr int kNumDerivVariants = 7;
+// The shape a new context starts with: 128 threads x 5 blocks per SM, the one
+// the autotuner picked on B200 for the benchmark's workloads (c2 compat, c3
+// and c5 corrected).
+constexpr int kDefaultDerivVariant = 5;
 extern const DerivVariant kDerivVariants[kNumDerivVariants];
 
 // precision 0 = FP32 pair arithmetic (launch shape `variant`), 1 = FP64

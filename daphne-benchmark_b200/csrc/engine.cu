@@ -175,7 +175,7 @@ struct ndt_ctx {
     HostBuf h_offsets, h_active, h_counters, h_out;
     ndt_counters last{};
     long long launches = 0;
-    int variant = 0;  // FP32 derivative-pass launch shape (kDerivVariants)
+    int variant = kDefaultDerivVariant;  // FP32 derivative-pass launch shape (kDerivVariants)
     unsigned flag_cap = 1u << 20;  // FP64 side-queue capacity in pairs per derivative pass
     float s_max = 1.0f;    // radius test threshold (see radius_threshold)
     float inv_res = 0.0f;  // 1 / res when res is a power of two
@@ -1282,6 +1282,88 @@ int ndt_set_side_queue_capacity(ndt_ctx *c, int pairs) {
     if (!c || pairs < 0 || (unsigned)pairs > kFlagCapMax) return fail(c, NDT_E_ARG, "bad side-queue capacity");
     c->flag_cap = pairs == 0 ? kFlagCap : (unsigned)pairs;
     return NDT_OK;
+}
+
+int ndt_get_kernel_variant(ndt_ctx *c) { return c ? c->variant : NDT_E_ARG; }
+
+// Times a device batch with every launch shape of the FP32 derivative pass
+// (one untimed warm call each, then `repeats` calls timed with CUDA events on
+// the context stream; the minimum counts) and selects the fastest.  Results
+// go to the context's own output buffers.
+int ndt_autotune_batch_device(ndt_ctx *c, int B, const float *d_points, const int *d_offsets, int total_points,
+                              const float *d_guesses, int repeats, int *best, float *ms_per_variant) {
+    if (!c || !d_points || !d_offsets || !d_guesses || B <= 0 || repeats < 1)
+        return fail(c, NDT_E_ARG, "ndt_autotune_batch_device: bad argument");
+    if (int rc = set_device(c)) return rc;
+    if (!c->have_map) return fail(c, NDT_E_NOMAP, "no map set");
+    if (c->prm.precision == 1) {  // one launch shape only
+        if (best) *best = c->variant;
+        return NDT_OK;
+    }
+    CK(c->out_T.ensure(sizeof(float) * 16 * (size_t)B));
+    CK(c->out_conv.ensure(sizeof(int) * (size_t)B));
+    CK(c->out_fit.ensure(sizeof(double) * (size_t)B));
+    CK(c->out_status.ensure(sizeof(int) * (size_t)B));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(cudaEventCreate(&e0));
+    cudaError_t ee = cudaEventCreate(&e1);
+    if (ee != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return cuda_fail(c, ee, "cudaEventCreate");
+    }
+    const int keep = c->variant;
+    int winner = keep, rc = NDT_OK;
+    float winner_ms = 0.0f;
+    for (int v = 0; v < kNumDerivVariants && rc == NDT_OK; ++v) {
+        c->variant = v;
+        float best_ms = -1.0f;
+        for (int r = 0; r <= repeats && rc == NDT_OK; ++r) {
+            if (r > 0 && (ee = cudaEventRecord(e0, c->stream)) != cudaSuccess) {
+                rc = cuda_fail(c, ee, "cudaEventRecord");
+                break;
+            }
+            rc = run_batch(c, B, (const float4 *)d_points, d_offsets, total_points, d_guesses, c->out_T.as<float>(),
+                           c->out_conv.as<int>(), c->out_fit.as<double>(), c->out_status.as<int>());
+            if (rc || r == 0) continue;
+            float ms = 0.0f;
+            if ((ee = cudaEventRecord(e1, c->stream)) != cudaSuccess || (ee = cudaEventSynchronize(e1)) != cudaSuccess ||
+                (ee = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess) {
+                rc = cuda_fail(c, ee, "autotune timing");
+                break;
+            }
+            if (best_ms < 0.0f || ms < best_ms) best_ms = ms;
+        }
+        if (rc) break;
+        if (ms_per_variant) ms_per_variant[v] = best_ms;
+        if (v == 0 || best_ms < winner_ms) {
+            winner = v;
+            winner_ms = best_ms;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->variant = rc ? keep : winner;
+    if (rc) return rc;
+    if (best) *best = winner;
+    return NDT_OK;
+}
+
+// The same from host buffers (packed scans as ndt_align_batch_packed takes
+// them): the batch is uploaded once, then tuned on the device.
+int ndt_autotune_batch(ndt_ctx *c, int B, const float *points, const int *offsets, const float *guesses,
+                       int repeats, int *best, float *ms_per_variant) {
+    if (!c || !points || !offsets || !guesses || B <= 0) return fail(c, NDT_E_ARG, "ndt_autotune_batch: bad argument");
+    if (int rc = set_device(c)) return rc;
+    const long long total = offsets[B];
+    if (total < 0 || offsets[0] != 0) return fail(c, NDT_E_ARG, "ndt_autotune_batch: bad offsets");
+    CK(c->points.ensure(sizeof(float4) * (size_t)std::max<long long>(1, total)));
+    CK(c->offsets.ensure(sizeof(int) * (size_t)(B + 1)));
+    CK(c->guesses.ensure(sizeof(float) * 16 * (size_t)B));
+    CK(cudaMemcpyAsync(c->points.p, points, sizeof(float4) * (size_t)total, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->offsets.p, offsets, sizeof(int) * (size_t)(B + 1), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->guesses.p, guesses, sizeof(float) * 16 * (size_t)B, cudaMemcpyHostToDevice, c->stream));
+    return ndt_autotune_batch_device(c, B, c->points.as<float>(), c->offsets.as<int>(), (int)total,
+                                     c->guesses.as<float>(), repeats, best, ms_per_variant);
 }
 
 int ndt_set_kernel_variant(ndt_ctx *c, int variant) {

@@ -67,6 +67,8 @@ struct ndt_mlp {
     int *err = nullptr;
     unsigned long long *gmax = nullptr;
     float *grad_scan = nullptr, *loss_scan = nullptr;
+    float *dg = nullptr;         // B x 128: the head's gradient at the max-pooled features
+    float *head_part = nullptr;  // per 128-scan tile: the head's weight and bias gradient sums
     size_t cap_b = 0;
     int step = 0;
     pn::Norm nm{};

@@ -212,20 +212,41 @@ def score(ctx, torch, pts, offs, total, poses_np):
     return s.cpu().numpy()
 
 
-def refinement_levels(resolution, step=0.1):
-    """(resolution, step_size) of the refinement levels, coarse to fine: 4 r,
-    2 r and the plain NDT's own r with its step (the coarse levels take longer
-    steps: the step limits how far one Newton iteration moves the pose)."""
-    return [(4.0 * resolution, 1.0 * resolution), (2.0 * resolution, 0.4 * resolution), (resolution, step)]
+def refinement_levels(resolution, step=0.1, max_iterations=30, eps=0.01):
+    """The refinement levels, coarse to fine: dicts of the corrected-NDT
+    parameters that differ per level, and the points per scan each level
+    reads (an evenly strided subsample; 0 = all).  4 r and 2 r take longer
+    steps (the step limits how far one Newton iteration moves the pose) on
+    4096 and 8192 points; the last level is the plain NDT of the configuration
+    (its own r, step, iterations and epsilon) on every point."""
+    return [dict(resolution=4.0 * resolution, step_size=1.0 * resolution, max_iterations=max_iterations,
+                 transformation_epsilon=eps, points_per_scan=4096),
+            dict(resolution=2.0 * resolution, step_size=0.4 * resolution, max_iterations=max_iterations,
+                 transformation_epsilon=eps, points_per_scan=8192),
+            dict(resolution=resolution, step_size=step, max_iterations=max_iterations, transformation_epsilon=eps,
+                 points_per_scan=0)]
+
+
+def pipeline_params(levels, **kw):
+    """ndt_learned_params for `levels` (refinement_levels): the library defaults with each level's point
+    count, overridden by keyword."""
+    kw.setdefault("level_points", [lvl.get("points_per_scan", 0) for lvl in levels])
+    return posenet.learned_params(**kw)
+
+
+def level_params(prm, level):
+    """Sets a level's NDT fields on a corrected-NDT parameter struct (ndt.Params or the oracle's); returns it."""
+    for k, v in level.items():
+        if k != "points_per_scan":
+            setattr(prm, k, v)
+    return prm
 
 
 def level_contexts(ndt, cloud, resolution, device=0, levels=None):
     """Corrected-NDT contexts holding `cloud` at every refinement level."""
     out = []
-    for res, step in (levels or refinement_levels(resolution)):
-        p = ndt.corrected_params(res)
-        p.step_size = step
-        c = ndt.Context(p, device=device)
+    for lvl in (levels or refinement_levels(resolution)):
+        c = ndt.Context(level_params(ndt.corrected_params(lvl["resolution"]), lvl), device=device)
         c.set_map(cloud)
         out.append(c)
     return out
@@ -241,7 +262,7 @@ class LearnedBatch:
         B = len(guesses_np)
         self.levels, self.net, self.torch = levels, net, torch
         self.pts, self.offs, self.total, self.B = pts, offs, total, B
-        self.params = params if params is not None else posenet.learned_params()
+        self.params = params if params is not None else pipeline_params(refinement_levels(1.0))
         self.g = torch.from_numpy(np.ascontiguousarray(guesses_np, np.float32)).cuda()
         self.out = torch.zeros((B, 16), dtype=torch.float32, device="cuda")
         self.conv = torch.zeros(B, dtype=torch.int32, device="cuda")
@@ -287,7 +308,7 @@ def learned_align(levels, net, torch, scans, guesses_np, params=None):
     points (network proposals, score pass, plain NDT per level), with the
     judge's choice made here on the host.  Same arithmetic as LearnedBatch:
     returns (out, conv, fit, status, choice)."""
-    params = params if params is not None else posenet.learned_params()
+    params = params if params is not None else pipeline_params(refinement_levels(1.0))
     B = len(guesses_np)
     dev = DeviceScans(torch, scans)
     pts, offs, total = dev.batch(np.arange(B))

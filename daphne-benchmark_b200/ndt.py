@@ -106,6 +106,9 @@ def lib():
         L.ndt_kernel_variant_shape.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.ndt_set_kernel_variant.argtypes = [ctxp, C.c_int]
         L.ndt_set_side_queue_capacity.argtypes = [ctxp, C.c_int]
+        L.ndt_get_kernel_variant.argtypes = [ctxp]
+        L.ndt_autotune_batch_device.argtypes = [ctxp, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                                                C.POINTER(C.c_int), _f32p]
         L.ndt_synchronize.argtypes = [ctxp]
         L.ndt_stream.argtypes = [ctxp]
         L.ndt_stream.restype = C.c_void_p
@@ -121,7 +124,7 @@ def lib():
                      "ndt_align_batch_packed_with_map",
                      "ndt_set_profiling", "ndt_kernel_variants", "ndt_kernel_variant_shape",
                      "ndt_set_kernel_variant", "ndt_window_info", "ndt_set_batch_graphs",
-                     "ndt_set_side_queue_capacity",
+                     "ndt_set_side_queue_capacity", "ndt_get_kernel_variant", "ndt_autotune_batch_device",
                      "ndt_score_batch_device"):
             getattr(L, name).restype = C.c_int
         _LIB = L
@@ -300,6 +303,19 @@ class Context:
     def set_side_queue_capacity(self, pairs=0):
         """FP64 side-queue capacity in pairs per derivative pass (0 = default 2^20)."""
         self._check(self.L.ndt_set_side_queue_capacity(self.h, int(pairs)), "set_side_queue_capacity")
+
+    def kernel_variant(self):
+        return self._check(self.L.ndt_get_kernel_variant(self.h), "ndt_get_kernel_variant")
+
+    def autotune_device(self, B, d_points, d_offsets, total, d_guesses, repeats=2):
+        """ndt_autotune_batch_device: times the batch with every launch shape, selects the fastest;
+        returns (best, ms per variant)."""
+        best = C.c_int()
+        ms = np.zeros(self.L.ndt_kernel_variants(), np.float32)
+        self._check(self.L.ndt_autotune_batch_device(self.h, B, C.c_void_p(d_points), C.c_void_p(d_offsets), total,
+                                                     C.c_void_p(d_guesses), repeats, C.byref(best), ms),
+                    "ndt_autotune_batch_device")
+        return best.value, ms
 
     def synchronize(self):
         self._check(self.L.ndt_synchronize(self.h), "ndt_synchronize")

@@ -227,13 +227,26 @@ NDT_API int ndt_score_batch_device(ndt_ctx *ctx, int B, const float *d_points, c
 
 /*
  * Launch shape of the FP32 derivative pass (points per tile = threads per
- * block, resident blocks per SM).  The autotuner (daphne-benchmark_b200/
- * autotune.py) times every variant on a sample batch and selects one.
- * No reference counterpart (the reference has no GPU derivative pass).
+ * block, resident blocks per SM).  A new context starts with variant 5
+ * (128 x 5), the shape the autotuner picked on B200 for the benchmark's
+ * workloads.  ndt_autotune_batch_device times a caller's batch with every
+ * variant (one warm call, then `repeats` timed calls each, CUDA events on the
+ * context stream, minimum taken), selects the fastest on the context and
+ * returns it in *best, with the times in ms_per_variant (optional,
+ * ndt_kernel_variants() entries); ndt_autotune_batch takes the batch in host
+ * buffers (packed as ndt_align_batch_packed).  The variant changes only the
+ * FP32 summation order, never which pairs are evaluated.  No reference
+ * counterpart (the reference has no GPU derivative pass).
  */
 NDT_API int ndt_kernel_variants(void);
 NDT_API int ndt_kernel_variant_shape(int variant, int *tile, int *blocks_per_sm);
 NDT_API int ndt_set_kernel_variant(ndt_ctx *ctx, int variant);
+NDT_API int ndt_get_kernel_variant(ndt_ctx *ctx);
+NDT_API int ndt_autotune_batch_device(ndt_ctx *ctx, int B, const float *d_points, const int *d_offsets,
+                                      int total_points, const float *d_guesses, int repeats, int *best,
+                                      float *ms_per_variant);
+NDT_API int ndt_autotune_batch(ndt_ctx *ctx, int B, const float *points, const int *offsets, const float *guesses,
+                               int repeats, int *best, float *ms_per_variant);
 
 /*
  * Capacity of the FP64 side queue, in (point, voxel) pairs per derivative
@@ -304,7 +317,8 @@ NDT_API int ndt_derivatives_noalloc(ndt_ctx *ctx, const float *d_scan, const flo
  * correction for the NDT to refine.  Per point u (3) -> 64 -> 128 (shared
  * layers, ReLU; the 64 -> 128 layer in BF16 on the tensor cores with FP32
  * accumulation), max-pool over up to max_points evenly strided points of the
- * scan, then 128 -> 64 -> 6.  u = (T_guess x - center) / scale; the output y
+ * scan, then 128 -> 64 -> 6 (both head layers, and in training every GEMM of
+ * the head's backward, in BF16 on the tensor cores over tiles of 128 scans).  u = (T_guess x - center) / scale; the output y
  * is the correction of the pose vector (x, y, z, roll, pitch, yaw of the
  * corrected parametrisation T = Trans Rx Ry Rz) in units of delta_scale6.
  * Weights: ndt_mlp_num_weights() FP32 values (W1[64][3], b1[64], W2[128][64],

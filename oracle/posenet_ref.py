@@ -4,7 +4,10 @@ Restates daphne-benchmark_b200/csrc/posenet.cu in numpy: the point feature
 u = (T x - c) / s in float32 (each operation rounded, the library's order),
 layer 1 with the kernel's fused multiply-adds (emulated in float64 and rounded
 to float32 after each), layer 2 on BF16-rounded operands with an exact sum,
-ReLU, max-pool with the smallest index among ties, the head, the loss
+ReLU, max-pool with the smallest index among ties, the head (its products
+on BF16-rounded operands, as the tensor-core head kernel computes them: W3 g,
+W4 h3, and in the backward W4^T dy, W3^T dh3, dy h3^T and dh3 g^T, the
+per-scan dy = 2 (y - t) / 6 rounded before the batch mean), the loss
 mean((y - t)^2) over outputs and scans, and its gradient (the straight-through
 gradient of the BF16 roundings, as the kernels take it).  With bf16=False
 every rounding is dropped and the arithmetic is float64: the form used for
@@ -108,9 +111,18 @@ def forward_scan(w, scan, guess16, center, scale, max_points=1024, bf16_mode=Tru
         g = np.zeros(H2)
     W3, b3 = P["W3"].astype(np.float64), P["b3"].astype(np.float64)
     W4, b4 = P["W4"].astype(np.float64), P["b4"].astype(np.float64)
-    h3 = np.maximum(W3 @ g + b3, 0.0)
-    y = W4 @ h3 + b4
+    if bf16_mode:  # the head's products run on the tensor cores: BF16 operands, FP32 sums
+        h3 = np.maximum(_b(W3) @ _b(g) + b3, 0.0)
+        y = _b(W4) @ _b(h3) + b4
+    else:
+        h3 = np.maximum(W3 @ g + b3, 0.0)
+        y = W4 @ h3 + b4
     return dict(u=u, h1=h1, a=a, W2=W2, g=g, arg=arg, h3=h3, y=y)
+
+
+def _b(x):
+    """float64 values rounded to float32, then to BF16 (a tensor-core operand)."""
+    return bf16(np.asarray(x, np.float64).astype(np.float32)).astype(np.float64)
 
 
 def loss_and_grad(w, scans, guesses, targets, center, scale, max_points=1024, bf16_mode=True, argmaxes=None):
@@ -127,13 +139,23 @@ def loss_and_grad(w, scans, guesses, targets, center, scale, max_points=1024, bf
                          None if argmaxes is None else argmaxes[b])
         dy = f["y"] - np.asarray(targets[b], np.float64)
         loss += float(np.mean(dy ** 2))
-        dy = dy * (2.0 / OUT) / B
-        G["W4"] += np.outer(dy, f["h3"])
-        G["b4"] += dy
-        dh3 = (W4.T @ dy) * (f["h3"] > 0)
-        G["W3"] += np.outer(dh3, f["g"])
-        G["b3"] += dh3
-        dg = (W3.T @ dh3) * (f["g"] > 0)
+        if bf16_mode:
+            # per-scan head gradient on the tensor cores (BF16 operands), the batch mean taken at the end
+            dy = dy * (2.0 / OUT)
+            G["W4"] += np.outer(_b(dy), _b(f["h3"])) / B
+            G["b4"] += dy / B
+            dh3 = (_b(W4).T @ _b(dy)) * (f["h3"] > 0)
+            G["W3"] += np.outer(_b(dh3), _b(f["g"])) / B
+            G["b3"] += dh3 / B
+            dg = (_b(W3).T @ _b(dh3)) * (f["g"] > 0) / B
+        else:
+            dy = dy * (2.0 / OUT) / B
+            G["W4"] += np.outer(dy, f["h3"])
+            G["b4"] += dy
+            dh3 = (W4.T @ dy) * (f["h3"] > 0)
+            G["W3"] += np.outer(dh3, f["g"])
+            G["b3"] += dh3
+            dg = (W3.T @ dh3) * (f["g"] > 0)
         if len(f["u"]) == 0:
             continue
         rows = f["arg"]

@@ -24,6 +24,8 @@ import math
 import numpy as np
 import pytest
 
+from test_gpu_parity import check_fp32_against_oracle
+
 pytestmark = pytest.mark.gpu
 
 
@@ -102,11 +104,12 @@ def test_learned_refinement_vs_fp64_oracle(pkg, trained, binding_mod, oracle):
     """The refinement levels from the judge's chosen starts (the pipeline's
     d_start16 output), run by the FP64 oracle level by level (same
     resolutions and step sizes), against the device pipeline's result:
-    <= 2 cm / 0.1 deg on a sample."""
+    <= 2 cm / 0.1 deg on a sample, except where the oracle's own chain is
+    not reproducible at that start (check_fp32_against_oracle)."""
     torch = pytest.importorskip("torch")
     L = pkg.learned
     cfg, scene, levels, net, aligns = trained
-    sample = aligns[:24]
+    sample = aligns[:32]
     scans = [a.scan for a in sample]
     guesses = np.stack([a.guess for a in sample])
     prm = pkg.posenet.learned_params(grid_xy=3, step_xy=0.5, judge_points=1024)
@@ -115,14 +118,18 @@ def test_learned_refinement_vs_fp64_oracle(pkg, trained, binding_mod, oracle):
     lb = L.LearnedBatch(levels, net, torch, pts, offs, total, guesses, prm)
     lb.run()
     out, conv, _, st, choice, cur = lb.results()
-    for res, step in L.refinement_levels(cfg.resolution):
-        op = binding_mod.corrected_params(res)
-        op.step_size = step
-        cur = oracle.align_batch(op, scans, cur, scene.map)[0]
-    worst = (0.0, 0.0)
-    for i in range(len(sample)):
-        dt = float(np.linalg.norm(out[i].reshape(4, 4)[:3, 3] - cur[i].reshape(4, 4)[:3, 3]))
-        dr = _rot_deg(out[i], cur[i])
-        worst = (max(worst[0], dt), max(worst[1], dr))
-        assert dt <= 0.02 and dr <= 0.1, (i, dt, dr)
-    print(f"learned refinement vs FP64 oracle: worst {worst[0]:.2e} m, {worst[1]:.2e} deg")
+    starts = cur.copy()
+    prms = []
+    for lvl in L.refinement_levels(cfg.resolution):
+        prms.append(L.level_params(binding_mod.corrected_params(lvl["resolution"]), lvl))
+
+    def chain(i, g):
+        for op in prms:
+            g = oracle.align(op, scans[i], g, scene.map)[0]
+        return g
+
+    ref = np.stack([chain(i, starts[i]) for i in range(len(sample))])
+    runs = [lambda g, i=i: chain(i, g) for i in range(len(sample))]
+    bad, worst = check_fp32_against_oracle(out, ref, conv, conv, st, runs, starts, max_frac=0.1)
+    print(f"learned refinement vs FP64 oracle: {len(sample) - len(bad)}/{len(sample)} within 2 cm / 0.1 deg, "
+          f"worst {worst[0]:.2e} m, {worst[1]:.2e} deg")

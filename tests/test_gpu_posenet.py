@@ -1,6 +1,9 @@
-"""The learned-initial-pose network's kernels (csrc/posenet.cu, BF16 tensor
-cores via tcgen05 for the shared 64 -> 128 layer) against the CPU reference
-(oracle/posenet_ref.py) through the C ABI.
+"""The learned-initial-pose network's kernels (csrc/posenet.cu: BF16 tensor
+cores via tcgen05 for the shared 64 -> 128 layer, for the head's forward
+and for its backward products -- dY W4, dH3 W3 and the weight gradients
+dH3^T G, dY^T H3 summed over 128-scan tiles) against the CPU reference
+(oracle/posenet_ref.py, which rounds the same operands to BF16) through the
+C ABI, on one partial head tile (8 scans) and on three tiles (300 scans).
 
 Tolerances: the max-pool values within 1e-4 relative (the reference sums the
 BF16 products exactly, the tensor cores in FP32); the outputs y within 1e-3
@@ -49,9 +52,13 @@ def _close(a, b, tol):
     return np.max(np.abs(a - b)) <= tol * max(1.0, float(np.max(np.abs(b))))
 
 
-def test_posenet_forward_and_gradient_match_reference(pkg):
+SMALL = [3000, 128, 1, 777, 0, 2048, 129, 64]
+TILES = [int(n) for n in np.random.default_rng(9).integers(0, 700, 300)]
+
+
+@pytest.mark.parametrize("sizes", [SMALL, TILES], ids=["8_scans", "300_scans"])
+def test_posenet_forward_and_gradient_match_reference(pkg, sizes):
     torch = pytest.importorskip("torch")
-    sizes = [3000, 128, 1, 777, 0, 2048, 129, 64]
     scans, guesses, targets = _batch(11, sizes)
     center, scale, maxp = (0.0, 0.0, 0.0), 50.0, 1024
     w = R.init_weights(5)
