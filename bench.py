@@ -635,34 +635,49 @@ def learned_cpu_leg(pkg, scene, cfg, aligns, plain_out, learned_out, learned_sta
         return g
 
     def unstable(run, i, start):
-        # the oracle itself: does a one-ulp change of one entry of its float start move its result by > 2 cm?
+        # the oracle itself: does moving one entry of its float start by 1 to 64 ulps (below a millimetre here)
+        # move its own result by more than 2 cm / 0.1 deg?
         base = run(i, np.asarray(start, np.float32))
-        for j in (3, 7, 11, 0, 1, 4):
-            for d in (np.inf, -np.inf):
-                g = np.array(start, np.float32).reshape(16)
-                g[j] = np.nextafter(g[j], np.float32(d))
-                o = run(i, g)
-                if np.linalg.norm(o.reshape(4, 4)[:3, 3] - base.reshape(4, 4)[:3, 3]) > 0.02 or \
-                        rot_deg(o, base) > 0.1:
-                    return True
+        for k in (1, 4, 16, 64):
+            for j in range(12):
+                for up in (np.inf, -np.inf):
+                    g = np.array(start, np.float32).reshape(16)
+                    for _ in range(k):
+                        g[j] = np.nextafter(g[j], np.float32(up))
+                    o = run(i, g)
+                    if np.linalg.norm(o.reshape(4, 4)[:3, 3] - base.reshape(4, 4)[:3, 3]) > 0.02 or \
+                            rot_deg(o, base) > 0.1:
+                        return True
         return False
 
-    def agree(gpu, ref, run, starts):
+    truths = np.stack([a.truth for a in aligns[:m]])
+
+    def near_truth(poses):
+        dt = np.linalg.norm(poses.reshape(-1, 4, 4)[:, :3, 3] - truths[:, :3, 3], axis=1)
+        dr = np.array([rot_deg(poses[i], truths[i].astype(np.float32)) for i in range(m)])
+        return (dt <= 0.02) & (dr <= 0.1)
+
+    def agree(gpu, ref, run, starts, check=4):
         dt = np.linalg.norm(gpu.reshape(-1, 4, 4)[:, :3, 3] - ref.reshape(-1, 4, 4)[:, :3, 3], axis=1)
         dr = np.array([rot_deg(gpu[i], ref[i]) for i in range(len(ref))])
         ok = (dt <= 0.02) & (dr <= 0.1)
         exc = np.flatnonzero(~ok)
+        checked = exc[:check]
         return {"alignments": len(ref), "within_2cm_0.1deg": int(ok.sum()),
                 "max_translation_m_within": float(dt[ok].max()) if ok.any() else None,
                 "max_rotation_deg_within": float(dr[ok].max()) if ok.any() else None,
-                "exceptions": int(len(exc)),
-                "exceptions_where_the_oracle_is_not_reproducible": int(sum(unstable(run, i, starts[i])
-                                                                           for i in exc))}
+                "exceptions": int(len(exc)), "exceptions_checked": int(len(checked)),
+                "checked_exceptions_where_the_oracle_is_not_reproducible":
+                    int(sum(unstable(run, i, starts[i]) for i in checked)),
+                "gpu_within_2cm_0.1deg_of_truth": int(near_truth(gpu).sum()),
+                "oracle_within_2cm_0.1deg_of_truth": int(near_truth(ref).sum())}
     acc = {"plain": agree(plain_out[:m], ref_plain, plain_run, [a.guess for a in aligns[:m]]),
            "learned": agree(learned_out[:m], cur, learned_run, learned_start[:m]),
            "oracle": "FP64 corrected-NDT oracle from the same starts (learned: its refinement levels from the "
-                     "GPU's chosen starts); an exception is not reproducible by the oracle when a one-ulp change "
-                     "of one entry of its float start moves its own result by more than 2 cm / 0.1 deg"}
+                     "GPU's chosen starts).  An exception is not reproducible by the oracle when moving one entry "
+                     "of its float start by 1 to 64 ulps moves its own result by more than 2 cm / 0.1 deg; "
+                     "*_within_2cm_0.1deg_of_truth compares how often the GPU and the oracle reach the ground "
+                     "truth on the same sample (equal accuracy)"}
     return base, acc
 
 

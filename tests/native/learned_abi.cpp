@@ -2,7 +2,7 @@
 // only, no CUDA headers): the way a C++ host of the align call would use it.
 //
 // Input file (little endian): int32 M, M x float[4] map; int32 L, L x
-// (float resolution, step, max iterations, epsilon); int32 W, W floats of network weights;
+// (double resolution, step, max iterations, epsilon); int32 W, W floats of network weights;
 // float[3] centre, float scale, float[6] delta scale; int32 B, (B + 1) int32
 // offsets, offsets[B] x float[4] points, B x float[16] guesses.
 // Output file: B x float[16] poses, B int32 converged, B double fitness,
@@ -42,7 +42,7 @@ int main(int argc, char **argv) {
     std::vector<float> map(4 * (size_t)M);
     get(in, map.data(), map.size());
     get(in, &L, 1);
-    std::vector<float> lv(4 * (size_t)L);
+    std::vector<double> lv(4 * (size_t)L);
     get(in, lv.data(), lv.size());
     get(in, &W, 1);
     std::vector<float> w(W);
@@ -63,7 +63,7 @@ int main(int argc, char **argv) {
     for (int l = 0; l < L; ++l) {
         ndt_params p;
         ndt_params_corrected(&p);
-        p.resolution = lv[4 * l];
+        p.resolution = (float)lv[4 * l];
         p.step_size = lv[4 * l + 1];
         p.max_iterations = (int)lv[4 * l + 2];
         p.transformation_epsilon = lv[4 * l + 3];

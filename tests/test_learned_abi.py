@@ -55,7 +55,7 @@ def test_cpp_learned_batch_equals_python(pkg, exe, tmp_path):
     with open(tmp_path / "in.bin", "wb") as f:
         f.write(struct.pack("<i", len(scene.map)) + np.ascontiguousarray(scene.map, np.float32).tobytes())
         lv = [[lvl["resolution"], lvl["step_size"], lvl["max_iterations"], lvl["transformation_epsilon"]] for lvl in spec]
-        f.write(struct.pack("<i", len(spec)) + np.asarray(lv, np.float32).tobytes())
+        f.write(struct.pack("<i", len(spec)) + np.asarray(lv, np.float64).tobytes())
         f.write(struct.pack("<i", len(w)) + w.tobytes())
         f.write(np.zeros(3, np.float32).tobytes() + struct.pack("<f", 4.0) + PN.DELTA_SCALE.tobytes())
         f.write(struct.pack("<i", B) + offsets.tobytes())
