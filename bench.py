@@ -785,6 +785,7 @@ def run_learned(args, pkg, world, rank, local):
     times = {}
     for name, (fn, s0, s1) in arms.items():
         ms = []
+        torch.cuda.nvtx.range_push(f"timed {name}")  # a profiler can keep to the timed steps (ncu --nvtx)
         for _ in range(args.steps):
             with torch.cuda.stream(s0):
                 flush.fill_(float(np.random.random()))
@@ -795,6 +796,7 @@ def run_learned(args, pkg, world, rank, local):
             e1.record(s1)
             e1.synchronize()
             ms.append(e0.elapsed_time(e1))
+        torch.cuda.nvtx.range_pop()
         times[name] = ms
     torch.cuda.synchronize()
     # kernels per learned step: the levels' alignment batches (each context counts its last batch, its graph's
@@ -966,7 +968,6 @@ def run_posenet(args, pkg, local):
     events on the network's stream; the shared 64 -> 128 layer's FLOPs
     against the measured dense BF16 peak."""
     import torch
-    import posenet_ref
     torch.cuda.set_device(local)
     B, P = args.posenet_scans, 512
     rng = np.random.default_rng(0)
@@ -979,7 +980,7 @@ def run_posenet(args, pkg, local):
     y = torch.zeros((B, 6), dtype=torch.float32, device="cuda")
     torch.cuda.synchronize()
     net = pkg.posenet.PoseNet(device=local, scale=4.0)
-    net.set_weights(posenet_ref.init_weights(1))
+    net.set_weights(pkg.posenet.init_weights(1))
     st = torch.cuda.ExternalStream(net.stream)
     out = {}
     for name, fn in (("forward", lambda: net.forward(B, d["p"].data_ptr(), d["o"].data_ptr(), d["g"].data_ptr(),
@@ -998,7 +999,7 @@ def run_posenet(args, pkg, local):
         e1.synchronize()
         net.synchronize()
         out[name] = e0.elapsed_time(e1) / args.steps
-    flops = 2.0 * B * P * 128 * 64
+    flops = 2.0 * B * P * 128 * 64 + 2.0 * B * (128 * 64 + 64 * 16)  # shared layer + head (N padded to 16)
     peak = None
     pk = ROOT / "MEASURED_PEAKS.json"
     if pk.exists():
@@ -1006,9 +1007,35 @@ def run_posenet(args, pkg, local):
     tf = flops / (out["forward"] / 1e3) / 1e12
     print(json.dumps({"workload": f"point network: {B} scans x {P} points", "forward_ms": out["forward"],
                       "train_step_256_ms": out["train_step_256"],
-                      "shared_layer_tflops": tf, "bf16_peak_tflops": peak,
+                      "tensor_core_tflops": tf, "bf16_peak_tflops": peak,
                       "frac_of_bf16_peak": (tf / peak) if peak else None}))
     net.close()
+    return 0
+
+
+def run_profile_case(args, pkg, local):
+    """A short run for profilers: the configuration's map and its first
+    --prof-aligns alignments (corrected mode unless --mode compat), one batch
+    through the plain NDT (every round launched from the host, so a profiler
+    sees each derivative pass), after the grid build.  Prints the batch's work
+    counters and its derivative-pass launches in order."""
+    import torch
+    torch.cuda.set_device(local)
+    cfg = pkg.synth.CONFIGS[args.config]
+    scene = pkg.synth.make_scene(cfg)
+    aligns = [pkg.synth.make_alignment(cfg, scene, i) for i in range(min(cfg.aligns, args.prof_aligns))]
+    ndt = pkg.ndt
+    prm = ndt.reference_params(cfg.resolution) if args.mode == "compat" else ndt.corrected_params(cfg.resolution)
+    with ndt.Context(prm, device=local) as ctx:
+        if args.variant != "auto":
+            ctx.set_kernel_variant(int(args.variant))
+        ctx.set_map(scene.map)
+        ctx.set_profiling(True)
+        ctx.align_batch([a.scan for a in aligns], [a.guess for a in aligns])
+        k = ctx.counters()
+    print(json.dumps({"workload": f"{cfg.name} map, first {len(aligns)} alignments, {args.mode}",
+                      "scan_points": int(sum(len(a.scan) for a in aligns)), "variant": args.variant,
+                      "counters": k}))
     return 0
 
 
@@ -1319,6 +1346,9 @@ def main(argv=None):
     ap.add_argument("--train-scans", type=int, default=0, help="0: 8000 (c4), 16000 (c5)")
     ap.add_argument("--train-epochs", type=int, default=0, help="0: 30 (c4), 40 (c5)")
     ap.add_argument("--oracle-sample", type=int, default=64)
+    ap.add_argument("--prof", action="store_true",
+                    help="a short run for profilers (one plain batch of --prof-aligns alignments, rounds from the host)")
+    ap.add_argument("--prof-aligns", type=int, default=1024)
     ap.add_argument("--filter", action="store_true", help="time the scan pre-filter (voxel-grid downsampling)")
     ap.add_argument("--append", action="store_true", help="time map growth (ndt_map_append) against rebuilds")
     ap.add_argument("--append-scans", type=int, default=32)
@@ -1340,6 +1370,8 @@ def main(argv=None):
         args.mode = "compat" if args.config in ("c1", "c2") else "corrected"
     if args.posenet and args.impl != "reference":
         return run_posenet(args, pkg, local)
+    if args.prof and args.impl != "reference":
+        return run_profile_case(args, pkg, local)
     if args.learned and args.impl != "reference":
         return run_learned(args, pkg, world, rank, local)
     if args.filter and args.impl != "reference":

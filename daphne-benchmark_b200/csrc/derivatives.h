@@ -27,6 +27,12 @@ struct EvalArgs {  // (GridDev is in ndt_types.h)
     unsigned flag_cap;     // queue capacity
     int *flag_overflow;    // set when the queue overflowed
     int *work_counter;     // FP32 pass: next chunk (reset by launch_derivatives)
+    // FP32 pass, optional: the pass first compacts the chunks whose alignment
+    // asks for an evaluation into active_chunks (capacity: the chunk count)
+    // and hands out only those (batches whose alignments finish at different
+    // rounds); null: every chunk is handed out and inactive ones skipped.
+    int *active_chunks = nullptr;
+    int *num_active = nullptr;
 };
 
 constexpr int kOwn = 27;        // accepted pairs of one point per collect call, at most (3 x 3 x 3 probes)

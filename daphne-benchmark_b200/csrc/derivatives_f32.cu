@@ -395,6 +395,23 @@ __device__ __forceinline__ void eval_deferred(const WarpPairs &P, const uint2 *r
     contract_add(F, x.x, x.y, x.z, P.ang, P.acc, P.stride, P.d2, P.hess, P.compat);
 }
 
+// The chunks of the alignments that ask for an evaluation, in a list the FP32
+// pass hands out (warp-aggregated appends; the order of the list does not
+// change any result, since each chunk writes its own partial slot).
+__global__ void active_chunks_kernel(const __grid_constant__ EvalArgs args) {
+    const int nc = *args.num_chunks;
+    const int lane = threadIdx.x & 31;
+    for (int base = blockIdx.x * blockDim.x; base < nc; base += gridDim.x * blockDim.x) {
+        const int c = base + threadIdx.x;
+        const bool act = c < nc && args.states[args.chunks[c].align].eval_mode != kEvalNone;
+        const unsigned bal = __ballot_sync(0xffffffffu, act);
+        int at = 0;
+        if (lane == 0 && bal) at = atomicAdd(args.num_active, __popc(bal));
+        at = __shfl_sync(0xffffffffu, at, 0);
+        if (act) args.active_chunks[at + __popc(bal & ((1u << lane) - 1u))] = c;
+    }
+}
+
 template <int TILE, int MINB>
 __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(const __grid_constant__ EvalArgs args) {
     constexpr int kW = TILE / 32;
@@ -426,7 +443,7 @@ __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(const __grid
     P.d2 = (float)args.d2;
     P.compat = compat;
 
-    const int nc = *args.num_chunks;
+    const int nc = args.num_active ? *args.num_active : *args.num_chunks;
     for (int k = 0; k < kAcc; ++k) P.acc[k * TILE] = 0.0f;
     if (lane == 0) s_cnt[warp][0] = s_cnt[warp][1] = s_cnt[warp][2] = 0;
     unsigned long long blk_probe = 0, blk_occ = 0, blk_pair = 0, blk_pts = 0, blk_tiles = 0;
@@ -439,11 +456,14 @@ __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(const __grid
     // block takes which chunk.  (No block takes more than nc chunks; the
     // bound only guards against a corrupted counter.)
     for (int it = 0; it <= nc; ++it) {
-        if (threadIdx.x == 0) s_chunk[parity] = atomicAdd(args.work_counter, 1);
+        if (threadIdx.x == 0) {
+            const int k = atomicAdd(args.work_counter, 1);
+            s_chunk[parity] = k < nc ? (args.active_chunks ? args.active_chunks[k] : k) : -1;
+        }
         __syncthreads();
         const int chunk = s_chunk[parity];
         parity ^= 1;
-        if (chunk >= nc) break;
+        if (chunk < 0) break;
         const Chunk ck = args.chunks[chunk];
         const AlignState *st = args.states + ck.align;
         if (threadIdx.x == 0) s_mode = st->eval_mode;
@@ -587,6 +607,10 @@ int launch_derivatives(const EvalArgs &args, int precision, int variant, int sms
     int blocks = (int)(want < args.max_tiles ? want : args.max_tiles);
     cudaMemsetAsync(args.flag_n, 0, sizeof(unsigned), st);
     cudaMemsetAsync(args.work_counter, 0, sizeof(int), st);
+    if (args.active_chunks) {
+        cudaMemsetAsync(args.num_active, 0, sizeof(int), st);
+        active_chunks_kernel<<<sms * 4, 256, 0, st>>>(args);
+    }
     switch (variant) {
         case 0: launch_one<256, 2>(args, blocks, st); break;
         case 1: launch_one<256, 1>(args, blocks, st); break;

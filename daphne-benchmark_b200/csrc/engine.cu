@@ -171,7 +171,7 @@ struct ndt_ctx {
     // batch
     DevBuf chunks, chunk_begin, num_chunks, big_begin, small_begin, num_big, round_no, dev_launches;
     DevBuf points, offsets, guesses, states, tiles, tile_begin, num_tiles, partials, exc, out_T, out_conv, out_fit,
-        out_status, active, counters, p6, trans, flag_q, flag_n, flag_overflow, work_counter;
+        out_status, active, counters, p6, trans, flag_q, flag_n, flag_overflow, work_counter, active_chunks, num_active;
     HostBuf h_offsets, h_active, h_counters, h_out;
     ndt_counters last{};
     long long launches = 0;
@@ -563,7 +563,9 @@ int enqueue_epilogue(ndt_ctx *c, const RunPlan &R, cudaStream_t st) {
 }
 
 // Kernel launches of one round (derivative pass + step kernel).
-int round_launches(const RunPlan &R) { return 1 + (R.precision == 1 ? 1 : kDerivLaunchesFP32); }
+int round_launches(const RunPlan &R) {
+    return 1 + (R.precision == 1 ? 1 : kDerivLaunchesFP32 + (R.ea.active_chunks ? 1 : 0));
+}
 
 // The batch as one CUDA graph: prologue, a conditional WHILE node whose body
 // is one round plus round_cond_kernel, epilogue.  Built by stream capture
@@ -729,6 +731,13 @@ int run_batch(ndt_ctx *c, int B, const float4 *d_points, const int *d_offsets, i
     // is fixed.
     R.fixed = R.P.compat && (R.P.step_max - R.P.step_min) > 0;
     R.max_rounds = R.fixed ? R.P.max_iterations + 3 : R.P.watchdog_evals + 1;
+    if (!R.fixed && R.precision == 0) {
+        // alignments finish at different rounds: each FP32 pass hands out only the chunks of active ones
+        CK(c->active_chunks.ensure(sizeof(int) * (size_t)max_tiles));
+        CK(c->num_active.ensure(sizeof(int)));
+        ea.active_chunks = c->active_chunks.as<int>();
+        ea.num_active = c->num_active.as<int>();
+    }
 
     if (c->use_graphs && !c->profiling) {
         // one graph launch: the rounds run on the device until no alignment
@@ -1025,7 +1034,8 @@ void ndt_destroy(ndt_ctx *c) {
                       &c->big_begin, &c->small_begin, &c->num_big, &c->round_no, &c->dev_launches,
                       &c->partials, &c->exc, &c->out_T, &c->out_conv,
                       &c->out_fit, &c->out_status, &c->active, &c->counters, &c->p6, &c->trans,
-                      &c->flag_q, &c->flag_n, &c->flag_overflow, &c->work_counter};
+                      &c->flag_q, &c->flag_n, &c->flag_overflow, &c->work_counter, &c->active_chunks,
+                      &c->num_active};
     for (DevBuf *b : bufs) b->release();
     HostBuf *hb[] = {&c->h_offsets, &c->h_active, &c->h_counters, &c->h_out};
     for (HostBuf *b : hb) b->release();
