@@ -711,6 +711,8 @@ def run_learned(args, pkg, world, rank, local):
     scene = synth.make_scene(cfg)
     levels_spec = L.refinement_levels(cfg.resolution)
     levels = L.level_contexts(ndt, scene.map, cfg.resolution, device=local, levels=levels_spec)
+    for c in levels:
+        c.set_batch_graphs(bool(args.graphs))  # --graphs 0: every round launched from the host (for profilers)
     fine = levels[-1]
     net = PN.PoseNet(device=local, center=(0.0, 0.0, 0.0), scale=4.0)
     training = None
@@ -902,19 +904,24 @@ def run_learned(args, pkg, world, rank, local):
     bytes_per_launch = bytes_total / n_launch
     launch_ms = prof["deriv_ms"] / n_launch
     achieved = bytes_per_launch / (launch_ms / 1e3) / 1e9 if launch_ms > 0 else None
+    # DRAM traffic from the committed ncu capture of this kernel on a smaller case of the same map (every
+    # alignment active), scaled to this run's launches by the scan points they process
     traffic = None
     tf = ROOT / "profiles" / "derivative_traffic.json"
     if tf.exists():
         try:
             td = json.loads(tf.read_text())
             key = f"{args.config}/corrected/p0"
-            if key in td:
-                traffic = td[key]["bytes_per_launch"]
+            if key in td and "bytes_per_point" in td[key]:
+                traffic = td[key]["bytes_per_point"] * prof["points"] / n_launch
         except Exception:
             traffic = None
     roofline = {"kernel": "derivative pass (derivative_f32_kernel), plain arm at the configuration's resolution",
                 "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "traffic_source": "profiles/derivative_f32_c5_corrected.md: ncu DRAM bytes per scan point of the "
+                                  "same kernel and launch shape on 1024 alignments of this map, times this run's "
+                                  "points per launch",
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                 else "fallback 6650 GB/s",
                 "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": launch_ms,
