@@ -4,11 +4,10 @@
 //
 // Who needs it: callers that must not allocate device memory while they
 // run -- a real-time control loop with a fixed memory budget (cudaMalloc can
-// block, synchronise the device and take unbounded time), code that runs
-// while another component holds the device's memory pool, or a pipeline that
-// records its work into a CUDA graph (cudaMalloc is not allowed during stream
-// capture).  They set up a context and its map beforehand, then call this as
-// often as they like.
+// block, synchronise the device and take unbounded time), or code that runs
+// while another component owns the device's memory and has handed out all of
+// it.  They set up a context and its map beforehand, then call this as often
+// as they like.
 //
 // Its scratch memory (tile and chunk lists, one alignment state, per-chunk
 // partial sums, the FP64 side queue, counters) is the file-scope array

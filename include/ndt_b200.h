@@ -289,9 +289,9 @@ NDT_API int ndt_derivatives(ndt_ctx *ctx, const float *scan, const float *trans,
 /*
  * ndt_derivatives_noalloc -- no counterpart in the reference.  The same
  * evaluation as ndt_derivatives, for callers that cannot allocate device
- * memory while they run (a real-time loop with a fixed memory budget, work
- * recorded into a CUDA graph, where cudaMalloc is not allowed): it allocates
- * nothing.  Inputs are DEVICE pointers: d_scan and d_trans (n float[4] each,
+ * memory while they run (a real-time loop with a fixed memory budget, where
+ * cudaMalloc can block and take unbounded time, or code running while
+ * another component owns all of the device's memory): it allocates nothing.  Inputs are DEVICE pointers: d_scan and d_trans (n float[4] each,
  * the original and the already transformed scan, both 16-byte aligned), p6
  * is a host array (the pose vector for the angle terms); d_out (8-byte
  * aligned) receives 44 doubles: score, gradient[6], Hessian[36] row major,

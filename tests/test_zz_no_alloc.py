@@ -1,8 +1,10 @@
 """ndt_derivatives_noalloc: the evaluation entry point that allocates no
 device memory at call time (for callers such as real-time loops with a fixed
-memory budget, or work recorded into a CUDA graph, which cannot call
-cudaMalloc while they run).  Its scratch is one static device array shared by
-every call, so the test calls it twice in a row, on two different scans, and
+memory budget, where cudaMalloc can block and take unbounded time, or code
+running while another component owns all of the device's memory: they cannot
+call cudaMalloc while they run).  Its scratch is one static device array
+shared by every call, so the test calls it twice in a row, on two different
+scans, and
 checks each result against the allocating entry point ndt_derivatives
 through the C ABI, with the derivative tolerance of the parity tests (FP32
 pairs: 2e-3 relative to the largest entry; FP64 pairs: 1e-9).
