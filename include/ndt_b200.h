@@ -396,6 +396,9 @@ NDT_API int ndt_mlp_judge_device(ndt_mlp *mlp, int B, const float *d_prop16, con
  * pose, where the refinement started.  Work is enqueued on the network's and the contexts'
  * streams, ordered by events; the results are ready after
  * ndt_synchronize(levels[n_levels - 1]).  Inputs must be ready when called.
+ * The pipeline's buffers belong to the network object: consecutive calls on
+ * one network are ordered by the events, but one network must not be used
+ * from two host threads at once (as a context must not).
  */
 #define NDT_LEARNED_MAX_LEVELS 8
 typedef struct ndt_learned_params {

@@ -133,3 +133,52 @@ def test_learned_refinement_vs_fp64_oracle(pkg, trained, binding_mod, oracle):
     bad, worst = check_fp32_against_oracle(out, ref, conv, conv, st, runs, starts, max_frac=0.1)
     print(f"learned refinement vs FP64 oracle: {len(sample) - len(bad)}/{len(sample)} within 2 cm / 0.1 deg, "
           f"worst {worst[0]:.2e} m, {worst[1]:.2e} deg")
+
+
+def test_learned_pipeline_edge_cases(pkg, trained):
+    """Ragged and empty scans, a batch of one, the same call twice (bit-identical),
+    and bad arguments (NDT_E_ARG, nothing enqueued)."""
+    torch = pytest.importorskip("torch")
+    import ctypes as C
+    L = pkg.learned
+    cfg, scene, levels, net, aligns = trained
+    sizes = [0, 1, 5, 3000, 64, 0, 700]
+    scans = []
+    for k, n in enumerate(sizes):
+        s = aligns[k].scan
+        scans.append(np.ascontiguousarray(s[(np.arange(n) * len(s)) // max(n, 1)]) if n else np.zeros((0, 4), np.float32))
+    guesses = np.stack([aligns[k].guess for k in range(len(sizes))])
+    dev = L.DeviceScans(torch, scans)
+    pts, offs, total = dev.batch(np.arange(len(sizes)))
+    prm = pkg.posenet.learned_params(grid_xy=2, grid_yaw=2, step_xy=0.5, step_yaw_deg=3.0, judge_points=512,
+                                     level_points=[256, 512, 0])
+    lb = L.LearnedBatch(levels, net, torch, pts, offs, total, guesses, prm)
+    lb.run()
+    r1 = lb.results()
+    lb.run()
+    r2 = lb.results()
+    for a, b in zip(r1, r2):
+        assert np.array_equal(np.asarray(a).view(np.uint8), np.asarray(b).view(np.uint8))
+    out, conv, fit, st, choice, start = r1
+    assert np.isfinite(out).all() and (st == 0).all()
+    assert choice.min() >= 0 and choice.max() <= 8
+    for k, n in enumerate(sizes):
+        if n == 0:
+            assert fit[k] == 0.0
+    one = L.LearnedBatch(levels, net, torch, *dev.batch(np.array([3])), guesses[3:4], prm)
+    one.run()
+    assert np.array_equal(one.results()[0].view(np.uint32), out[3:4].view(np.uint32))  # batch-independent
+    # argument errors
+    arr = (C.c_void_p * len(levels))(*[c.h.value for c in levels])
+    f = net.L.ndt_align_batch_learned_device
+    bad = [pkg.posenet.learned_params(grid_xy=0), pkg.posenet.learned_params(judge_level=3),
+           pkg.posenet.learned_params(max_points=0)]
+    for p in bad:
+        rc = f(net.h, arr, len(levels), C.byref(p), len(sizes), C.c_void_p(pts.data_ptr()),
+               C.c_void_p(offs.data_ptr()), total, C.c_void_p(lb.g.data_ptr()), C.c_void_p(lb.out.data_ptr()),
+               C.c_void_p(lb.conv.data_ptr()), C.c_void_p(lb.fit.data_ptr()), None, None, None)
+        assert rc == -1  # NDT_E_ARG
+    rc = f(net.h, arr, 0, C.byref(prm), len(sizes), C.c_void_p(pts.data_ptr()), C.c_void_p(offs.data_ptr()), total,
+           C.c_void_p(lb.g.data_ptr()), C.c_void_p(lb.out.data_ptr()), C.c_void_p(lb.conv.data_ptr()),
+           C.c_void_p(lb.fit.data_ptr()), None, None, None)
+    assert rc == -1
