@@ -49,3 +49,27 @@ def test_dat_align_equals_batches(pkg, tmp_path, n_same, scan_pts):
         # a sub-range starting inside a run of equal maps
         o2, c2, f2, s2 = f.align(ctx, first=3, count=5)
         assert np.array_equal(o2.view(np.uint32), out[3:8].view(np.uint32))
+
+
+def test_dat_align_vs_fp64_oracle(pkg, oracle, binding_mod, tmp_path):
+    """The file path against the FP64 oracle (the restated reference, pinned
+    to it bit for bit) on every case of a small file with a shared, a grown
+    and a new map: translation column bit-exact, converged equal, rotation
+    within 0.05 deg, and the reference's own acceptance rule."""
+    import math
+    cfg = pkg.synth.small_config("dat_o", 20000, 40.0, 16, 1500, seed=72)
+    scene = pkg.synth.make_scene(cfg)
+    path, cases = _write(pkg, tmp_path, cfg, scene, 4, grow_pts=2000)
+    prm = binding_mod.reference_params(cfg.resolution)
+    with pkg.ndt.DatFile(path) as f, pkg.ndt.Context(pkg.ndt.reference_params(cfg.resolution)) as ctx:
+        out, conv, _, status = f.align(ctx)
+    assert (status == 0).all()
+    for i, (g, s, m) in enumerate(cases):
+        ref, rconv, _, _ = oracle.align(prm, s, g, m)
+        T, R = out[i].reshape(4, 4), np.asarray(ref, np.float32).reshape(4, 4)
+        assert np.array_equal(T[:, 3].view(np.uint32), R[:, 3].view(np.uint32)), i
+        assert int(conv[i]) == int(rconv), i
+        d = T[:3, :3].astype(np.float64) - R[:3, :3].astype(np.float64)
+        assert math.degrees(2 * math.asin(min(1.0, float(np.linalg.norm(d)) / math.sqrt(8)))) <= 0.05, i
+        ok, _ = pkg.datfile.reference_check(out[i], conv[i], R.reshape(16), rconv)
+        assert ok, i
