@@ -386,3 +386,28 @@ def test_library_autotune(pkg, oracle, binding_mod):
         assert np.array_equal(T[:, 3].view(np.uint32), R[:, 3].view(np.uint32))
         assert int(conv[i]) == int(rconv[i]) and status[i] == 0
         assert _rot_err_deg(out[i], ref[i]) <= ROT_TOL_DEG_FP32
+
+
+def test_c3_batched_corrected_vs_fp64_oracle(pkg, oracle, binding_mod):
+    """The batched configuration (c3: the c2 map at 1 m, scans of 1k-16k points,
+    guesses up to 1 m / 5 deg off) as one batch of 256 alignments through the
+    batch graph (per-alignment early exit, active-chunk hand-out), FP32 pairs,
+    against the FP64 oracle from the same guesses on a sample of 64
+    (check_fp32_against_oracle); every alignment of the batch has status 0."""
+    cfg = pkg.synth.CONFIGS["c3"]
+    scene = pkg.synth.make_scene(cfg)
+    aligns = [pkg.synth.make_alignment(cfg, scene, i) for i in range(256)]
+    scans, guesses = [a.scan for a in aligns], [a.guess for a in aligns]
+    with pkg.ndt.Context(pkg.ndt.corrected_params(cfg.resolution)) as ctx:
+        ctx.set_map(scene.map)
+        out, conv, _, status = ctx.align_batch(scans, guesses)
+        k = ctx.counters()
+    assert (status == 0).all()
+    assert k["rounds"] < k["evaluations"] / 4  # alignments left the loop at different rounds
+    prm = binding_mod.corrected_params(cfg.resolution)
+    n = 64
+    ref, rconv, _, _ = oracle.align_batch(prm, scans[:n], guesses[:n], scene.map)
+    runs = [lambda g, i=i: oracle.align(prm, scans[i], g, scene.map)[0] for i in range(n)]
+    bad, worst = check_fp32_against_oracle(out[:n], ref, conv[:n], rconv, status[:n], runs, guesses[:n])
+    print(f"c3 batch: {n - len(bad)}/{n} within 2 cm / 0.1 deg (worst {worst[0]:.2e} m, {worst[1]:.2e} deg), "
+          f"{k['rounds']} rounds, {k['evaluations'] / len(aligns):.1f} evaluations per alignment")
