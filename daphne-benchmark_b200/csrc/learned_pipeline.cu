@@ -250,7 +250,7 @@ extern "C" {
 void ndt_learned_params_default(ndt_learned_params *p) {
     if (!p) return;
     std::memset(p, 0, sizeof(*p));
-    p->max_points = 512;
+    p->max_points = 1024;
     p->passes = 3;
     p->grid_xy = 3;
     p->grid_yaw = 1;

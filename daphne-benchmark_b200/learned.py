@@ -35,6 +35,12 @@ import numpy as np
 
 from . import posenet, synth
 
+# Points the network reads per scan (evenly strided), in training and in the
+# pipeline: the library's default (ndt_learned_params_default).  On the 16 m
+# noiseless-wall scans of the c5 workload 1024 points reach the truth more
+# often than 512 at the same batch time (31.7% against 27.5%).
+NET_POINTS = 1024
+
 
 @dataclasses.dataclass
 class Pairs:
@@ -159,7 +165,7 @@ def label_pairs(ctx, torch, pairs: Pairs, chunk=4096):
     return pairs
 
 
-def train(net, torch, pairs: Pairs, epochs=4, batch=512, lr=2e-3, max_points=512, seed=0, log=None):
+def train(net, torch, pairs: Pairs, epochs=4, batch=512, lr=2e-3, max_points=NET_POINTS, seed=0, log=None):
     """Trains the network on the kept pairs (points subsampled to max_points,
     the same points its forward samples at inference)."""
     dev = DeviceScans(torch, pairs.scans, max_points=max_points)
@@ -190,7 +196,7 @@ def train(net, torch, pairs: Pairs, epochs=4, batch=512, lr=2e-3, max_points=512
     return np.asarray(losses)
 
 
-def propose(net, torch, pts, offs, guesses_np, max_points=512):
+def propose(net, torch, pts, offs, guesses_np, max_points=NET_POINTS):
     """Network proposals (B x 16 float32) for scans at their guesses."""
     B = len(guesses_np)
     g = torch.from_numpy(np.ascontiguousarray(guesses_np, np.float32)).cuda()
@@ -351,7 +357,7 @@ def learned_align(levels, net, torch, scans, guesses_np, params=None):
     return out, conv, fit, status, choice.astype(np.int32)
 
 
-def propose_passes(net, torch, pts, offs, guesses_np, passes, max_points=512):
+def propose_passes(net, torch, pts, offs, guesses_np, passes, max_points=NET_POINTS):
     """The network's proposals after `passes` passes (device-side application, ndt_mlp_propose_device)."""
     B = len(guesses_np)
     g = torch.from_numpy(np.ascontiguousarray(guesses_np, np.float32)).cuda()

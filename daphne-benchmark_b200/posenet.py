@@ -184,7 +184,7 @@ class PoseNet:
         """Run on a caller's stream (an int handle, e.g. Context.stream), or its own (None)."""
         self._check(self.L.ndt_mlp_set_stream(self.h, C.c_void_p(stream) if stream else None), "set_stream")
 
-    def propose_device(self, B, d_points, d_offsets, d_guesses, d_y, d_prop, passes=3, max_points=512):
+    def propose_device(self, B, d_points, d_offsets, d_guesses, d_y, d_prop, passes=3, max_points=1024):
         self._check(self.L.ndt_mlp_propose_device(self.h, B, C.c_void_p(d_points), C.c_void_p(d_offsets),
                                                   C.c_void_p(d_guesses), max_points, passes, C.c_void_p(d_y),
                                                   C.c_void_p(d_prop)), "propose")
