@@ -49,10 +49,11 @@ struct DerivVariant {
     int min_blocks;
 };
 constexpr int kNumDerivVariants = 7;
-// The shape a new context starts with: 128 threads x 5 blocks per SM, the one
-// the autotuner picked on B200 for the benchmark's workloads (c2 compat, c3
-// and c5 corrected).
-constexpr int kDefaultDerivVariant = 5;
+// The shape a new context starts with: 128 threads x 6 blocks per SM (80
+// registers, 35.7 KB of shared memory per block), the fastest on B200 for the
+// corrected-mode workloads (c5: 2M-point map at 0.5 m); on c2 compat 128 x 5
+// is within 1 %.
+constexpr int kDefaultDerivVariant = 6;
 extern const DerivVariant kDerivVariants[kNumDerivVariants];
 
 // precision 0 = FP32 pair arithmetic (launch shape `variant`), 1 = FP64

@@ -14,12 +14,17 @@
 // Per point (one thread): the float transform and the reference's neighbour
 // search of probe.cuh (exact: the accepted pairs are the reference's), each
 // lane's pairs in its own column of shared memory.  Then, per warp:
-//   dense  (more than 40 pairs in the warp): each lane sums its own pairs
+//   dense  (more than 32 pairs in the warp): each lane sums its own pairs
 //          into 16 FP32 point sums and contracts them with its point's
 //          Jacobian and Hessian terms once (factored form below);
 //   sparse: the pairs are appended to a per-warp ring and evaluated 32 at a
 //          time, one pair per lane, each contracted on its own; the ring is
 //          emptied at the end of the alignment run.
+// Both kinds go through one evaluation loop (eval_steps), so the pair sums
+// and the contraction appear once in the kernel; compat and corrected mode,
+// and maps with and without a probe-window table, are separate
+// instantiations.  The kernel's instruction footprint is what this buys:
+// each instantiation carries only the code it runs.
 // Voxels flagged by the grid build (inverse-covariance entries non-finite or
 // beyond 1e30) are queued and evaluated in FP64 by flagged_kernel, so that
 // infinities and NaNs propagate as in the reference.
@@ -79,10 +84,13 @@ __device__ __forceinline__ void pair_sums(PairSums &F, float p0, float p1, float
     if (!(e2 <= 1.0f && e2 >= 0.0f)) return;  // kernel.cpp:456 (also rejects NaN)
     const float w = d1 * e2;
     F.s = fmaf(-d1, e, F.s);
-    const float wq0 = w * q0, wq1 = w * q1, wq2 = w * q2;
-    F.u0 += wq0;
-    F.u1 += wq1;
-    F.u2 += wq2;
+    // every multiply-add is written as fmaf or as separately rounded
+    // operations, so the FP32 results do not depend on the compiler's
+    // contraction choices (which can change with the surrounding code)
+    const float wq0 = __fmul_rn(w, q0), wq1 = __fmul_rn(w, q1), wq2 = __fmul_rn(w, q2);
+    F.u0 = fmaf(w, q0, F.u0);
+    F.u1 = fmaf(w, q1, F.u1);
+    F.u2 = fmaf(w, q2, F.u2);
     if (!hess) return;
     F.q00 = fmaf(wq0, q0, F.q00);
     F.q01 = fmaf(wq0, q1, F.q01);
@@ -277,8 +285,14 @@ __global__ void flagged_kernel(const __grid_constant__ EvalArgs args) {
 }
 
 // Dynamic shared memory of the FP32 kernel (W warps).
-constexpr int kDefer = 128;           // per-warp ring of deferred pairs (power of two)
-constexpr int kDenseThreshold = 40;   // a warp with more pairs than this evaluates them per point
+// A warp with more pairs than kDenseThreshold in one collect call evaluates
+// them per point; fewer go to its ring of deferred pairs.  The ring holds
+// fewer than 32 pairs between calls and receives at most kDenseThreshold, so
+// kDefer >= 31 + kDenseThreshold; 64 keeps the 128-thread block at 35.5 KB of
+// shared memory, so that 6 blocks fit on an SM.
+constexpr int kDefer = 64;            // per-warp ring of deferred pairs (power of two)
+constexpr int kDenseThreshold = 32;
+static_assert(kDefer >= 31 + kDenseThreshold, "the deferred ring must hold a collect call's pairs");
 
 template <int W>
 struct F32Smem {
@@ -307,6 +321,9 @@ __device__ void reduce_run(F32Smem<W> &sm, double *s_tot, const unsigned (*s_cnt
         if (threadIdx.x < kPartial) out[threadIdx.x] = 0.0;
         return;
     }
+    // (not unrolled: the unrolled loop adds ~11 KB of code to a kernel whose hot
+    // loop is already larger than the instruction cache)
+#pragma unroll 1
     for (int k = warp; k < kAcc; k += W) {
         double sum = 0.0;
 #pragma unroll
@@ -343,7 +360,7 @@ struct WarpPairs {
     int stride;
     int align;
     float d1, d2;
-    bool hess, compat;
+    bool hess;
 };
 
 // Queues a pair with a flagged voxel for flagged_kernel (FP64).
@@ -366,33 +383,68 @@ __device__ __forceinline__ void add_pair(const WarpPairs &P, PairSums &F, int sl
     pair_sums(F, p0, p1, p2, ca, cb, P.d1, P.d2, P.hess);
 }
 
-// Evaluates deferred pairs [head, head + cnt) of the warp's ring (cnt <= 32),
-// one per lane: the lane reloads the pair's point, transforms it again (the
-// same float operations) and contracts the single pair.
-__device__ __forceinline__ void eval_deferred(const WarpPairs &P, const uint2 *ring, unsigned head, int cnt) {
+// The evaluation steps after one collect call of a warp: first the dense
+// step (dense: each lane sums its own pairs own[0..c) and contracts them once
+// with its point), then full rounds of 32 deferred pairs from the warp's ring
+// (one pair per lane: the lane reloads the pair's point, transforms it again
+// with the same float operations and contracts the single pair), and, when
+// `flush` is set (the chunk's last collect call), the ring's remainder.  Both
+// kinds share this one loop, so the pair sums and the contraction are inlined
+// once in the kernel (a smaller instruction footprint).  Pairs with a flagged
+// voxel are queued for flagged_kernel instead.
+template <bool COMPAT>
+__device__ __forceinline__ void eval_steps(const WarpPairs &P, const unsigned (*own)[32], const uint2 *ring,
+                                           unsigned &head, unsigned tail, bool dense, bool flush, int c, int i,
+                                           float4 x, float px, float py, float pz) {
     const int lane = threadIdx.x & 31;
-    if (lane >= cnt) return;
-    const uint2 d = ring[(head + lane) & (kDefer - 1)];
-    const int slot = (int)(d.x >> 6);
-    const int pi = (int)d.y;
-    if (d.x & 32u) {
-        queue_flagged(*P.args, P.align, pi, slot);
-        return;
+    for (;;) {
+        int cnt = 0, pi = i;
+        float4 xe = x;
+        float ex = px, ey = py, ez = pz;
+        bool from_ring = false;
+        unsigned rcode = 0;
+        if (dense) {
+            dense = false;
+            cnt = c;
+        } else {
+            const unsigned avail = tail - head;
+            if (avail == 0u || (avail < 32u && !flush)) break;
+            const int take = avail < 32u ? (int)avail : 32;
+            __syncwarp();
+            from_ring = true;
+            if (lane < take) {
+                const uint2 d = ring[(head + lane) & (kDefer - 1)];
+                rcode = d.x;
+                pi = (int)d.y;
+                cnt = 1;
+                xe = __ldg(P.args->points + pi);
+                if (P.args->trans) {
+                    const float4 y = __ldg(P.args->trans + pi);
+                    ex = y.x; ey = y.y; ez = y.z;
+                } else {
+                    ex = transform_row(P.T, xe.x, xe.y, xe.z);
+                    ey = transform_row(P.T + 4, xe.x, xe.y, xe.z);
+                    ez = transform_row(P.T + 8, xe.x, xe.y, xe.z);
+                }
+            }
+            head += (unsigned)take;
+        }
+        PairSums F;
+        zero(F);
+        const int maxc = __reduce_max_sync(kFull, cnt);
+        for (int k = 0; k < maxc; ++k) {
+            if (k < cnt) {
+                const unsigned code = from_ring ? rcode : own[k][lane];
+                const int slot = (int)(code >> 6);
+                if (code & 32u)
+                    queue_flagged(*P.args, P.align, pi, slot);
+                else
+                    add_pair(P, F, slot, ex, ey, ez);
+            }
+        }
+        if (cnt > 0 && !(from_ring && (rcode & 32u)))
+            contract_add(F, xe.x, xe.y, xe.z, P.ang, P.acc, P.stride, P.d2, P.hess, COMPAT);
     }
-    const float4 x = __ldg(P.args->points + pi);
-    float px, py, pz;
-    if (P.args->trans) {
-        const float4 y = __ldg(P.args->trans + pi);
-        px = y.x; py = y.y; pz = y.z;
-    } else {
-        px = transform_row(P.T, x.x, x.y, x.z);
-        py = transform_row(P.T + 4, x.x, x.y, x.z);
-        pz = transform_row(P.T + 8, x.x, x.y, x.z);
-    }
-    PairSums F;
-    zero(F);
-    add_pair(P, F, slot, px, py, pz);
-    contract_add(F, x.x, x.y, x.z, P.ang, P.acc, P.stride, P.d2, P.hess, P.compat);
 }
 
 // The chunks of the alignments that ask for an evaluation, in a list the FP32
@@ -412,7 +464,10 @@ __global__ void active_chunks_kernel(const __grid_constant__ EvalArgs args) {
     }
 }
 
-template <int TILE, int MINB>
+// COMPAT: the reference's Hessian form and pose build (else corrected); WIN: the
+// map has a probe-window table (the neighbour search compiles only the paths it
+// can take, a smaller instruction footprint).
+template <int TILE, int MINB, bool COMPAT, bool WIN>
 __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(const __grid_constant__ EvalArgs args) {
     constexpr int kW = TILE / 32;
     static_assert(TILE >= kPartial, "the partial is written by one thread per entry");
@@ -422,12 +477,14 @@ __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(const __grid
     __shared__ double s_tot[kAcc];
     __shared__ unsigned s_cnt[kW][3];
     __shared__ int s_chunk[2];
+    // per-warp work counters (points, tiles, probes, occupied probes, pairs), kept
+    // only when the caller asked for counters (in shared memory: no registers)
+    __shared__ unsigned long long s_work[kW][5];
     extern __shared__ __align__(16) unsigned char s_dyn[];
     F32Smem<kW> &sm = *reinterpret_cast<F32Smem<kW> *>(s_dyn);
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const bool compat = args.compat != 0;
-    const double kR = compat ? -args.d2 : 1.0;
+    constexpr bool compat = COMPAT;
     const GridDev &grid = args.grid;
     unsigned (*own)[32] = sm.own[warp];
     uint2 *ring = sm.defer[warp];
@@ -441,12 +498,12 @@ __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(const __grid
     P.stride = TILE;
     P.d1 = (float)args.d1;
     P.d2 = (float)args.d2;
-    P.compat = compat;
 
     const int nc = args.num_active ? *args.num_active : *args.num_chunks;
     for (int k = 0; k < kAcc; ++k) P.acc[k * TILE] = 0.0f;
     if (lane == 0) s_cnt[warp][0] = s_cnt[warp][1] = s_cnt[warp][2] = 0;
-    unsigned long long blk_probe = 0, blk_occ = 0, blk_pair = 0, blk_pts = 0, blk_tiles = 0;
+    if (lane == 0)
+        for (int q = 0; q < 5; ++q) s_work[warp][q] = 0;
     unsigned head = 0, tail = 0;  // deferred ring of this warp (warp-uniform)
     int parity = 0;
 
@@ -494,29 +551,16 @@ __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(const __grid
             do {
                 __syncwarp();
                 OwnSink sink{own, 0};
-                collect_pairs(grid, px, py, pz, valid, sink, n_probe, n_occ, resume);
+                collect_pairs<OwnSink, WIN ? kProbeWindows : kProbeDenseIndex>(grid, px, py, pz, valid, sink, n_probe,
+                                                                               n_occ, resume);
                 __syncwarp();
                 const int c = sink.c;
                 n_pair += c;
                 const int n = __reduce_add_sync(kFull, c);
-                if (n > kDenseThreshold) {
-                    // dense: each lane sums its own pairs, then one contraction
-                    PairSums F;
-                    zero(F);
-                    const int maxc = __reduce_max_sync(kFull, c);
-                    for (int k = 0; k < maxc; ++k) {
-                        if (k < c) {
-                            const unsigned code = own[k][lane];
-                            const int slot = (int)(code >> 6);
-                            if (code & 32u)
-                                queue_flagged(args, ck.align, i, slot);
-                            else
-                                add_pair(P, F, slot, px, py, pz);
-                        }
-                    }
-                    if (c > 0) contract_add(F, x.x, x.y, x.z, s_ang, P.acc, TILE, P.d2, P.hess, compat);
-                } else if (n > 0) {
-                    // sparse: defer into the ring, evaluate full rounds of 32
+                // dense (more than kDenseThreshold pairs in the warp): per point;
+                // sparse: into the ring, evaluated in rounds of 32
+                const bool dense = n > kDenseThreshold;
+                if (!dense && n > 0) {
                     int pre = c;
 #pragma unroll
                     for (int o = 1; o < 32; o <<= 1) {
@@ -527,56 +571,74 @@ __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(const __grid
                     for (int k = 0; k < c; ++k)
                         ring[(tail + pre + k) & (kDefer - 1)] = make_uint2(own[k][lane] & ~31u, (unsigned)i);
                     tail += n;
-                    while (tail - head >= 32) {
-                        __syncwarp();
-                        eval_deferred(P, ring, head, 32);
-                        head += 32;
-                    }
                 }
+                // the chunk's last collect call also empties the ring
+                const bool flush = resume < 0 && ti + 1 == ck.end;
+                eval_steps<COMPAT>(P, own, ring, head, tail, dense, flush, c, i, x, px, py, pz);
             } while (resume >= 0);
-            // per-warp work counters (pairs feed the partial's count)
-            n_probe = __reduce_add_sync(kFull, n_probe);
-            n_occ = __reduce_add_sync(kFull, n_occ);
+            // per-warp work counters: the pairs feed the partial's count; the
+            // others only when the caller asked for counters
             n_pair = __reduce_add_sync(kFull, n_pair);
             if (lane == 0) s_cnt[warp][2] += n_pair;
-            blk_probe += n_probe;
-            blk_occ += n_occ;
-            blk_pair += n_pair;
-            blk_pts += (unsigned long long)(tile.end - tile.start);
-            blk_tiles += 1;
+            if (args.counters) {
+                const unsigned probes = __reduce_add_sync(kFull, n_probe);
+                const unsigned occupied = __reduce_add_sync(kFull, n_occ);
+                if (lane == 0) {
+                    s_work[warp][0] += (unsigned)(tile.end - tile.start);
+                    s_work[warp][1] += 1;
+                    s_work[warp][2] += probes;
+                    s_work[warp][3] += occupied;
+                    s_work[warp][4] += n_pair;
+                }
+            }
         }
-        // end of the chunk: the deferred pairs, then the block's sums
-        while (tail != head) {
-            const int c = (int)min(32u, tail - head);
-            __syncwarp();
-            eval_deferred(P, ring, head, c);
-            head += c;
-        }
+        // end of the chunk (the last collect call emptied the ring): the block's sums
         head = tail = 0;
-        reduce_run<kW>(sm, s_tot, s_cnt, args.partials + (size_t)ck.slot * kPartial, kR, compat);
+        reduce_run<kW>(sm, s_tot, s_cnt, args.partials + (size_t)ck.slot * kPartial, compat ? -args.d2 : 1.0, compat);
         __syncthreads();
         if (lane == 0) s_cnt[warp][0] = s_cnt[warp][1] = s_cnt[warp][2] = 0;
     }
-    if (args.counters && lane == 0 && blk_tiles) {
-        if (warp == 0) {
-            atomicAdd(&args.counters->points, blk_pts);
-            atomicAdd(&args.counters->tiles, blk_tiles);
+    if (args.counters && lane == 0 && s_work[warp][1]) {
+        if (warp == 0) {  // every warp of the block saw the same tiles
+            atomicAdd(&args.counters->points, s_work[warp][0]);
+            atomicAdd(&args.counters->tiles, s_work[warp][1]);
         }
-        atomicAdd(&args.counters->probes, blk_probe);
-        atomicAdd(&args.counters->occupied_probes, blk_occ);
-        atomicAdd(&args.counters->pairs, blk_pair);
+        atomicAdd(&args.counters->probes, s_work[warp][2]);
+        atomicAdd(&args.counters->occupied_probes, s_work[warp][3]);
+        atomicAdd(&args.counters->pairs, s_work[warp][4]);
     }
 }
 
 template <int TILE, int MINB>
 cudaError_t prepare_one() {
-    return cudaFuncSetAttribute(derivative_f32_kernel<TILE, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sizeof(F32Smem<TILE / 32>));
+    const int bytes = (int)sizeof(F32Smem<TILE / 32>);
+    const void *k[4] = {(const void *)derivative_f32_kernel<TILE, MINB, true, true>,
+                        (const void *)derivative_f32_kernel<TILE, MINB, true, false>,
+                        (const void *)derivative_f32_kernel<TILE, MINB, false, true>,
+                        (const void *)derivative_f32_kernel<TILE, MINB, false, false>};
+    cudaError_t e = cudaSuccess;
+    for (const void *f : k) {
+        const cudaError_t r = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (r != cudaSuccess) e = r;
+    }
+    return e;
 }
 
 template <int TILE, int MINB>
 void launch_one(const EvalArgs &args, int blocks, cudaStream_t st) {
-    derivative_f32_kernel<TILE, MINB><<<blocks, TILE, sizeof(F32Smem<TILE / 32>), st>>>(args);
+    const size_t smem = sizeof(F32Smem<TILE / 32>);
+    const bool win = args.grid.win_off != nullptr;
+    if (args.compat) {
+        if (win)
+            derivative_f32_kernel<TILE, MINB, true, true><<<blocks, TILE, smem, st>>>(args);
+        else
+            derivative_f32_kernel<TILE, MINB, true, false><<<blocks, TILE, smem, st>>>(args);
+    } else {
+        if (win)
+            derivative_f32_kernel<TILE, MINB, false, true><<<blocks, TILE, smem, st>>>(args);
+        else
+            derivative_f32_kernel<TILE, MINB, false, false><<<blocks, TILE, smem, st>>>(args);
+    }
 }
 
 }  // namespace

@@ -171,6 +171,12 @@ struct OwnSink {
     __device__ __forceinline__ bool full() const { return __any_sync(kFull, c >= kOwn); }
 };
 
+// The neighbour-search paths a caller compiles in (bit mask; the generic path
+// is always there): kProbeWindows needs the probe-window table.
+constexpr int kProbeWindows = 1;
+constexpr int kProbeDenseIndex = 2;
+constexpr int kProbeAll = kProbeWindows | kProbeDenseIndex;
+
 // Collects the accepted (point, voxel) pairs of every lane's point into
 // `sink`.  `resume` is 0 on the first call; it comes back -1 when the point's
 // probes are done, or, on the generic path (trip counts up to 4: coordinates
@@ -184,7 +190,10 @@ struct OwnSink {
 //            the appends of probes no lane accepted;
 //   generic  one probe at a time, the reference's loop as written.
 // The pairs are the reference's on every path; only their order differs.
-template <class Sink>
+// kPaths selects the compiled paths: without kProbeDenseIndex the warps the
+// window path cannot take use the generic one; without kProbeWindows the
+// table is not read.
+template <class Sink, int kPaths = kProbeAll>
 __device__ __forceinline__ void collect_pairs(const GridDev &grid, float px, float py, float pz, bool valid, Sink &sink,
                                               unsigned &n_probe, unsigned &n_occ, int &resume) {
     const int lane = threadIdx.x & 31;
@@ -202,7 +211,7 @@ __device__ __forceinline__ void collect_pairs(const GridDev &grid, float px, flo
               mz = __reduce_max_sync(kFull, az.n);
     const float tol = radius_margin(px, py, pz, res);
     const bool small = mx <= 3 && my <= 3 && mz <= 3;
-    if (small && grid.win_off) {
+    if ((kPaths & kProbeWindows) && small && grid.win_off) {
         bool ok = true;
         const int bx = window_base(ax, g.dim[0], ok);
         const int by = window_base(ay, g.dim[1], ok);
@@ -240,7 +249,7 @@ __device__ __forceinline__ void collect_pairs(const GridDev &grid, float px, flo
             return;
         }
     }
-    if (small) {
+    if ((kPaths & kProbeDenseIndex) && small) {
 #pragma unroll 1
         for (int a = 0; a < 3; ++a) {
             const bool za = any_in && ((az.in >> a) & 1u);
@@ -329,7 +338,7 @@ __device__ __forceinline__ double h_entry(const double *tot, int i, int j, doubl
     if (i >= 3 && j >= 3) {
         int a = i - 3, b = j - 3;
         double r = compat ? tot[28 + 3 * a + b] : tot[28 + 3 * (a < b ? a : b) + (a < b ? b : a)];
-        v += kR * r;
+        v = fma(kR, r, v);  // explicit, so the result does not depend on contraction choices
     }
     return v;
 }

@@ -227,9 +227,8 @@ NDT_API int ndt_score_batch_device(ndt_ctx *ctx, int B, const float *d_points, c
 
 /*
  * Launch shape of the FP32 derivative pass (points per tile = threads per
- * block, resident blocks per SM).  A new context starts with variant 5
- * (128 x 5), the shape the autotuner picked on B200 for the benchmark's
- * workloads.  ndt_autotune_batch_device times a caller's batch with every
+ * block, resident blocks per SM).  A new context starts with variant 6
+ * (128 x 6), the fastest on B200 for the corrected-mode benchmark workload.  ndt_autotune_batch_device times a caller's batch with every
  * variant (one warm call, then `repeats` timed calls each, CUDA events on the
  * context stream, minimum taken), selects the fastest on the context and
  * returns it in *best, with the times in ms_per_variant (optional,

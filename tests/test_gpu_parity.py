@@ -372,7 +372,7 @@ def test_library_autotune(pkg, oracle, binding_mod):
     pts, offs, total = dev.batch(np.arange(len(aligns)))
     g = torch.from_numpy(np.stack([a.guess for a in aligns]).astype(np.float32)).cuda()
     with pkg.ndt.Context(pkg.ndt.reference_params()) as ctx:
-        assert ctx.kernel_variant() == 5  # the default shape
+        assert ctx.kernel_variant() == 6  # the default shape
         ctx.set_map(scene.map)
         torch.cuda.synchronize()
         best, ms = ctx.autotune_device(len(aligns), pts.data_ptr(), offs.data_ptr(), total, g.data_ptr())

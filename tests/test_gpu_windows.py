@@ -103,6 +103,13 @@ def test_window_align_equals_dense(pkg):
             out, conv, fit, status = ctx.align_batch([a.scan for a in aligns], [a.guess for a in aligns])
             k = ctx.counters()
             outs.append((out, conv, status, k["probes"], k["occupied_probes"], k["pairs"]))
+            # every derivative pass covers each point and tile of its alignment once
+            n = {len(a.scan) for a in aligns}
+            assert len(n) == 1
+            n = n.pop()
+            tile = pkg.ndt.kernel_variants()[ctx.kernel_variant()][0]
+            assert k["points"] == n * k["evaluations"], (k["points"], n, k["evaluations"])
+            assert k["tiles"] == -(-n // tile) * k["evaluations"]
     (o0, c0, s0, *k0), (o1, c1, s1, *k1) = outs
     assert k0 == k1
     assert np.array_equal(c0, c1) and (s0 == 0).all() and (s1 == 0).all()
