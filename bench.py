@@ -758,6 +758,24 @@ def run_learned(args, pkg, world, rank, local):
     d_choice = torch.zeros(B, dtype=torch.int32, device=dev)
     d_start = torch.zeros(B, 16, device=dev)
     lp = L.pipeline_params(levels_spec)
+    # the derivative pass's launch shape per level context, autotuned once (untimed) on this step's scans and
+    # raw guesses at the level's resolution and point budget (ndt_autotune_batch_device): the fastest shape
+    # depends on the voxel size (0.5 m: 128 x 6, 1-2 m: 128 x 5 on B200)
+    tuned_shapes = {}
+    if args.variant == "auto":
+        for c, spec in zip(levels, levels_spec):
+            cap = spec.get("points_per_scan", 0)
+            sub = L.DeviceScans(torch, [a.scan for a in aligns], max_points=cap) if cap else None
+            sp, so, st = sub.batch(np.arange(B)) if cap else (d_pts, d_off, npts)
+            best, ms = c.autotune_device(B, sp.data_ptr(), so.data_ptr(), st, d_g.data_ptr())
+            tuned_shapes[f"{spec['resolution']} m"] = {"variant": int(best),
+                                                       "shape": list(ndt.kernel_variants()[best]),
+                                                       "batch_ms_by_variant": [round(float(x), 3) for x in ms]}
+            del sub, sp, so
+        torch.cuda.synchronize()
+    else:
+        for c in levels:
+            c.set_kernel_variant(int(args.variant))
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     s_net = torch.cuda.ExternalStream(net.stream, device=dev)
     s_fine = torch.cuda.ExternalStream(fine.stream, device=dev)
@@ -968,6 +986,7 @@ def run_learned(args, pkg, world, rank, local):
         "accuracy_vs_fp64_oracle": acc,
         "clocks": clk,
         "gpu_launches": int(launches),
+        "kernel_variants": tuned_shapes or {"all levels": args.variant},
         "training": training,
     }
     print(json.dumps(line), flush=True)
