@@ -72,9 +72,8 @@ __device__ __forceinline__ void zero(PairSums &F) {
     F.w00 = F.w01 = F.w02 = F.w11 = F.w12 = F.w22 = 0.0f;
 }
 
-__device__ __forceinline__ void pair_sums(PairSums &F, float p0, float p1, float p2, float4 ca, float4 cb, float d1,
-                                          float d2, bool hess) {
-    const float c00 = ca.x, c01 = ca.y, c02 = ca.z, c11 = ca.w, c12 = cb.x, c22 = cb.y;
+__device__ __forceinline__ void pair_sums(PairSums &F, float p0, float p1, float p2, float c00, float c01, float c02,
+                                          float c11, float c12, float c22, float d1, float d2, bool hess) {
     const float q0 = fmaf(c00, p0, fmaf(c01, p1, c02 * p2));
     const float q1 = fmaf(c01, p0, fmaf(c11, p1, c12 * p2));
     const float q2 = fmaf(c02, p0, fmaf(c12, p1, c22 * p2));
@@ -275,8 +274,8 @@ __global__ void flagged_kernel(const __grid_constant__ EvalArgs args) {
         float t[kTerms];
         for (int k = 0; k < 8; ++k) t[k] = dot3f(x.x, x.y, x.z, st.angf + 3 * k);
         for (int k = 0; k < 15; ++k) t[8 + k] = dot3f(x.x, x.y, x.z, st.angf + 24 + 3 * k);
-        const float4 hi = args.grid.mean_hi[e.z];
-        const float4 lo = args.grid.mean_lo[e.z];
+        const float4 hi = args.grid.vox32[3 * (size_t)e.z];
+        const float4 lo = args.grid.vox32[3 * (size_t)e.z + 1];
         pair_fp64_flagged(args.exc + (size_t)e.x * kPartial, t, __fsub_rn(__fsub_rn(px, hi.x), lo.x),
                           __fsub_rn(__fsub_rn(py, hi.y), lo.y), __fsub_rn(__fsub_rn(pz, hi.z), lo.z),
                           args.grid.icov64 + 9 * (size_t)e.z, args.d1, args.d2, hess, args.compat != 0);
@@ -373,14 +372,12 @@ __device__ __forceinline__ void queue_flagged(const EvalArgs &args, int align, i
 // the FP64 mean, and the pair's sums.
 __device__ __forceinline__ void add_pair(const WarpPairs &P, PairSums &F, int slot, float px, float py, float pz) {
     const GridDev &g = *P.grid;
-    const float4 hi = __ldg(g.mean_hi + slot);
-    const float4 lo = __ldg(g.mean_lo + slot);
-    const float4 ca = __ldg(g.icov32 + 2 * slot);
-    const float4 cb = __ldg(g.icov32 + 2 * slot + 1);
+    const float4 *r = g.vox32 + 3 * slot;  // one 48-byte record
+    const float4 hi = __ldg(r), lo = __ldg(r + 1), cc = __ldg(r + 2);
     const float p0 = __fsub_rn(__fsub_rn(px, hi.x), lo.x);
     const float p1 = __fsub_rn(__fsub_rn(py, hi.y), lo.y);
     const float p2 = __fsub_rn(__fsub_rn(pz, hi.z), lo.z);
-    pair_sums(F, p0, p1, p2, ca, cb, P.d1, P.d2, P.hess);
+    pair_sums(F, p0, p1, p2, hi.w, lo.w, cc.x, cc.y, cc.z, cc.w, P.d1, P.d2, P.hess);
 }
 
 // The evaluation steps after one collect call of a warp: first the dense

@@ -139,7 +139,7 @@ struct ndt_ctx {
     std::string err;
     double d1 = 0, d2 = 0;
     // grid
-    DevBuf map, index, slot_of, mean, mean_hi, mean_lo, icov32, icov64, count, cell, seg_start, seg_cell, scratch, meta;
+    DevBuf map, index, slot_of, mean, vox32, icov64, count, cell, seg_start, seg_cell, scratch, meta;
     DevBuf win_off, win_ent, win_ctot;
     GridMeta meta_host{};
     bool have_map = false;
@@ -250,9 +250,7 @@ GridBuffers grid_buffers(ndt_ctx *c) {
     GridBuffers b;
     b.index = c->index.as<int32_t>();
     b.mean = c->mean.as<double4>();
-    b.mean_hi = c->mean_hi.as<float4>();
-    b.mean_lo = c->mean_lo.as<float4>();
-    b.icov32 = c->icov32.as<float4>();
+    b.vox32 = c->vox32.as<float4>();
     b.icov64 = c->icov64.as<double>();
     b.count = c->count.as<int32_t>();
     b.cell = c->cell.as<int32_t>();
@@ -267,12 +265,10 @@ GridDev grid_dev(ndt_ctx *c) {
     g.meta = c->meta_host;
     g.index = c->index.as<int32_t>();
     g.mean = c->mean.as<double4>();
-    g.mean_hi = c->mean_hi.as<float4>();
-    g.mean_lo = c->mean_lo.as<float4>();
+    g.vox32 = c->vox32.as<float4>();
     g.s_max = c->s_max;
     g.inv_res = c->inv_res;
     g.radius_final = (float)((double)c->prm.resolution + (double)0.001f);
-    g.icov32 = c->icov32.as<float4>();
     g.icov64 = c->icov64.as<double>();
     g.win_off = c->have_windows ? c->win_off.as<int32_t>() : nullptr;
     g.win_ent = c->have_windows ? c->win_ent.as<float4>() : nullptr;
@@ -321,7 +317,7 @@ int prepare_windows(ndt_ctx *c, int m, bool &use, WindowBuffers &wb) {
 }
 
 int enqueue_windows(ndt_ctx *c, const WindowBuffers &wb, int *nl) {
-    int rc = grid_windows(c->meta_host, c->index.as<int32_t>(), c->mean_hi.as<float4>(), wb, c->stream, nl);
+    int rc = grid_windows(c->meta_host, c->index.as<int32_t>(), c->vox32.as<float4>(), wb, c->stream, nl);
     if (rc) return cuda_fail(c, (cudaError_t)rc, "grid_windows");
     return NDT_OK;
 }
@@ -344,9 +340,7 @@ int grow_records(ndt_ctx *c, int m, int keep) {
     cudaStream_t st = c->stream;
     const size_t n = (size_t)m, k = (size_t)keep;
     CK(c->mean.grow_keep(sizeof(double4) * n, sizeof(double4) * k, st));
-    CK(c->mean_hi.grow_keep(sizeof(float4) * n, sizeof(float4) * k, st));
-    CK(c->mean_lo.grow_keep(sizeof(float4) * n, sizeof(float4) * k, st));
-    CK(c->icov32.grow_keep(2 * sizeof(float4) * n, 2 * sizeof(float4) * k, st));
+    CK(c->vox32.grow_keep(3 * sizeof(float4) * n, 3 * sizeof(float4) * k, st));
     CK(c->icov64.grow_keep(9 * sizeof(double) * n, 9 * sizeof(double) * k, st));
     CK(c->count.grow_keep(sizeof(int32_t) * n, sizeof(int32_t) * k, st));
     CK(c->cell.grow_keep(sizeof(int32_t) * n, sizeof(int32_t) * k, st));
@@ -356,9 +350,7 @@ int grow_records(ndt_ctx *c, int m, int keep) {
 // Per-voxel record buffers for a map of m points.
 int ensure_records(ndt_ctx *c, int m) {
     CK(c->mean.ensure(sizeof(double4) * (size_t)m));
-    CK(c->mean_hi.ensure(sizeof(float4) * (size_t)m));
-    CK(c->mean_lo.ensure(sizeof(float4) * (size_t)m));
-    CK(c->icov32.ensure(2 * sizeof(float4) * (size_t)m));
+    CK(c->vox32.ensure(3 * sizeof(float4) * (size_t)m));
     CK(c->icov64.ensure(9 * sizeof(double) * (size_t)m));
     CK(c->count.ensure(sizeof(int32_t) * (size_t)m));
     CK(c->cell.ensure(sizeof(int32_t) * (size_t)m));
@@ -1027,8 +1019,8 @@ void ndt_destroy(ndt_ctx *c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
-    DevBuf *bufs[] = {&c->win_off, &c->win_ent, &c->win_ctot, &c->map, &c->index, &c->mean, &c->mean_hi,
-                      &c->mean_lo, &c->icov32, &c->icov64, &c->count, &c->cell, &c->seg_start, &c->seg_cell,
+    DevBuf *bufs[] = {&c->win_off, &c->win_ent, &c->win_ctot, &c->map, &c->index, &c->mean, &c->vox32,
+                      &c->icov64, &c->count, &c->cell, &c->seg_start, &c->seg_cell,
                       &c->scratch, &c->meta, &c->points, &c->offsets, &c->guesses, &c->states,
                       &c->tiles, &c->tile_begin, &c->num_tiles, &c->chunks, &c->chunk_begin, &c->num_chunks,
                       &c->big_begin, &c->small_begin, &c->num_big, &c->round_no, &c->dev_launches,

@@ -436,13 +436,12 @@ __device__ bool write_records(int s, const double *mu, const double *C, GridBuff
         if (!isfinite(mu[k])) bad = true;
     buf.mean[s] = make_double4(mu[0], mu[1], mu[2], bad ? 1.0 : 0.0);
     const float h0 = (float)mu[0], h1 = (float)mu[1], h2 = (float)mu[2];
-    buf.mean_hi[s] = make_float4(h0, h1, h2, 0.0f);
-    buf.mean_lo[s] = make_float4((float)(mu[0] - (double)h0), (float)(mu[1] - (double)h1), (float)(mu[2] - (double)h2),
-                                 0.0f);
     float c00 = (float)C[0], c11 = (float)C[4], c22 = (float)C[8];
     float c01 = (float)((C[1] + C[3]) * 0.5), c02 = (float)((C[2] + C[6]) * 0.5), c12 = (float)((C[5] + C[7]) * 0.5);
-    buf.icov32[2 * s] = make_float4(c00, c01, c02, c11);
-    buf.icov32[2 * s + 1] = make_float4(c12, c22, 0.0f, 0.0f);
+    float4 *r = buf.vox32 + 3 * (size_t)s;  // the FP32 pair record (GridDev::vox32)
+    r[0] = make_float4(h0, h1, h2, c00);
+    r[1] = make_float4((float)(mu[0] - (double)h0), (float)(mu[1] - (double)h1), (float)(mu[2] - (double)h2), c01);
+    r[2] = make_float4(c02, c11, c12, c22);
     for (int k = 0; k < 9; ++k) buf.icov64[9 * (size_t)s + k] = C[k];
     return bad;
 }
@@ -727,7 +726,7 @@ __global__ void window_count_kernel(const int32_t *__restrict__ index, WinGeom g
 }
 
 // ctot holds the exclusive block offsets here.
-__global__ void window_fill_kernel(const int32_t *__restrict__ index, const float4 *__restrict__ mean_hi, WinGeom g,
+__global__ void window_fill_kernel(const int32_t *__restrict__ index, const float4 *__restrict__ vox32, WinGeom g,
                                    const int *__restrict__ ctot, int32_t *__restrict__ off, float4 *__restrict__ ent) {
     const int w = blockIdx.x * kThreads + threadIdx.x;
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
@@ -748,7 +747,7 @@ __global__ void window_fill_kernel(const int32_t *__restrict__ index, const floa
     if (w == g.W - 1) off[g.W] = pos + c;
     visit_window(index, g, w, [&](int v, int o) {
         const int slot = v & kSlotMask;
-        const float4 h = __ldg(mean_hi + slot);
+        const float4 h = __ldg(vox32 + 3 * (size_t)slot);
         const unsigned code = ((unsigned)slot << 6) | ((v & kSlotFlag) ? 32u : 0u) | (unsigned)o;
         ent[pos++] = make_float4(h.x, h.y, h.z, __uint_as_float(code));
     });
@@ -782,7 +781,7 @@ int64_t window_count(const GridMeta &g) {
     return (int64_t)(g.dim[0] + 2) * (int64_t)(g.dim[1] + 2) * (int64_t)(g.dim[2] + 2);
 }
 
-int grid_windows(const GridMeta &meta_host, const int32_t *index, const float4 *mean_hi, WindowBuffers wb,
+int grid_windows(const GridMeta &meta_host, const int32_t *index, const float4 *vox32, WindowBuffers wb,
                  cudaStream_t st, int *launches) {
     WinGeom g;
     for (int e = 0; e < 3; ++e) {
@@ -793,7 +792,7 @@ int grid_windows(const GridMeta &meta_host, const int32_t *index, const float4 *
     const int nb = div_up(g.W, kThreads);
     window_count_kernel<<<nb, kThreads, 0, st>>>(index, g, wb.ctot);
     scan_single_block_kernel<<<1, 1024, 0, st>>>(wb.ctot, nb, nullptr);
-    window_fill_kernel<<<nb, kThreads, 0, st>>>(index, mean_hi, g, wb.ctot, wb.off, wb.ent);
+    window_fill_kernel<<<nb, kThreads, 0, st>>>(index, vox32, g, wb.ctot, wb.off, wb.ent);
     if (launches) *launches += 3;
     return (int)cudaGetLastError();
 }

@@ -12,9 +12,7 @@ namespace ndt {
 struct GridBuffers {
     int32_t *index;      // G dense cell -> voxel slot (-1 = no usable voxel)
     double4 *mean;       // slot -> mean xyz, w = 1 if the FP32 pair path must not be used
-    float4 *mean_hi;     // slot -> float(mean) xyz
-    float4 *mean_lo;     // slot -> float(mean - float(mean)) xyz
-    float4 *icov32;      // slot -> 2 float4 (symmetrised FP32 inverse covariance)
+    float4 *vox32;       // slot -> 3 float4, the FP32 pair record (GridDev::vox32)
     double *icov64;      // slot -> 9 doubles
     int32_t *count;      // slot -> points in the cell
     int32_t *cell;       // slot -> dense cell id
@@ -46,7 +44,7 @@ struct WindowBuffers {
 int64_t window_count(const GridMeta &g);  // W = (dim_x + 2)(dim_y + 2)(dim_z + 2)
 
 // Builds the table from the finished dense index (after grid_build).
-int grid_windows(const GridMeta &meta_host, const int32_t *index, const float4 *mean_hi, WindowBuffers wb,
+int grid_windows(const GridMeta &meta_host, const int32_t *index, const float4 *vox32, WindowBuffers wb,
                  cudaStream_t st, int *launches);
 
 // Stable LSD radix sort of n (key, value) pairs on the low `bits` key bits,

@@ -50,12 +50,14 @@ struct GridDev {
     GridMeta meta;
     const int32_t *index;    // G: dense cell -> voxel slot | kSlotFlag, -1 = none
     const double4 *mean;     // K: mean xyz (FP64), w = 1 when the FP32 path must not be used
-    const float4 *mean_hi;   // K: float(mean) xyz (the probe's first, conservative distance test)
-    const float4 *mean_lo;   // K: float(mean - float(mean)) xyz (x' = (x - hi) - lo)
+    // 3K: a voxel's FP32 pair record, one 48-byte gather: {float(mean) xyz, c00},
+    // {float(mean - float(mean)) xyz, c01}, {c02 c11 c12 c22} (the symmetrised
+    // inverse covariance); x' = (x - hi) - lo, and hi is the probe's first,
+    // conservative distance test
+    const float4 *vox32;
     float s_max;             // largest float s with sqrtf(s) < res (the radius test without sqrt)
     float inv_res;           // 1 / res when res is a power of two (exact), else 0 (divide)
     float radius_final;      // (float)(res + 0.001f): the probe loop bound of kernel.cpp:254
-    const float4 *icov32;    // 2K: {c00 c01 c02 c11}, {c12 c22 0 0} (symmetrised, FP32)
     const double *icov64;    // 9K: inverse covariance as the reference stores it (row major)
     // probe-window table (grid_build.h), nullptr when not built
     const int32_t *win_off;  // W + 1

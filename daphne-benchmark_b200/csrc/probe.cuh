@@ -281,7 +281,7 @@ __device__ __forceinline__ void collect_pairs(const GridDev &grid, float px, flo
                 float4 hi[3];
 #pragma unroll
                 for (int c = 0; c < 3; ++c)
-                    if ((row >> c) & 1u) hi[c] = __ldg(grid.mean_hi + (v[3 * b + c] & kSlotMask));
+                    if ((row >> c) & 1u) hi[c] = __ldg(grid.vox32 + 3 * (v[3 * b + c] & kSlotMask));
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
                     if (!__any_sync(kFull, (row >> c) & 1u)) continue;
@@ -318,7 +318,7 @@ __device__ __forceinline__ void collect_pairs(const GridDev &grid, float px, flo
         bool ok = false;
         if (v >= 0) {
             ++n_occ;
-            ok = accept(grid, v & kSlotMask, __ldg(grid.mean_hi + (v & kSlotMask)), px, py, pz, tol);
+            ok = accept(grid, v & kSlotMask, __ldg(grid.vox32 + 3 * (v & kSlotMask)), px, py, pz, tol);
         }
         sink.add_far(ok, pair_code(v, lane));
     }
