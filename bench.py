@@ -770,6 +770,7 @@ def run_learned(args, pkg, world, rank, local):
             best, ms = c.autotune_device(B, sp.data_ptr(), so.data_ptr(), st, d_g.data_ptr())
             tuned_shapes[f"{spec['resolution']} m"] = {"variant": int(best),
                                                        "shape": list(ndt.kernel_variants()[best]),
+                                                       "chunk_tiles": c.chunk_tiles(),
                                                        "batch_ms_by_variant": [round(float(x), 3) for x in ms]}
             del sub, sp, so
         torch.cuda.synchronize()

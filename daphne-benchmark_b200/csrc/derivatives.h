@@ -36,7 +36,12 @@ struct EvalArgs {  // (GridDev is in ndt_types.h)
 };
 
 constexpr int kOwn = 27;        // accepted pairs of one point per collect call, at most (3 x 3 x 3 probes)
-constexpr int kChunkBig = 8;    // tiles per large chunk of the FP32 pass (the FP64 pass: 1)
+constexpr int kChunkBig = 8;    // tiles per large chunk of the FP32 pass by default (the FP64 pass: 1)
+constexpr int kMaxChunkTiles = 64;
+// the chunk sizes the autotuner times (8 suits batches of many large scans,
+// c5: 21k chunks per pass; 4 the smaller c3 / c4 batches, where the end of
+// the pass is a larger share)
+constexpr int kChunkChoices[] = {4, 6, 8};
 constexpr int kChunkSmall = 2;  // tiles per small chunk of the FP32 pass (the FP64 pass: 1)
 
 // Per-device set-up (dynamic shared memory opt-in); call with the device current.

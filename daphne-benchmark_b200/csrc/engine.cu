@@ -176,6 +176,7 @@ struct ndt_ctx {
     ndt_counters last{};
     long long launches = 0;
     int variant = kDefaultDerivVariant;  // FP32 derivative-pass launch shape (kDerivVariants)
+    int chunk_tiles = kChunkBig;         // FP32 derivative pass: tiles per large chunk
     unsigned flag_cap = 1u << 20;  // FP64 side-queue capacity in pairs per derivative pass
     float s_max = 1.0f;    // radius test threshold (see radius_threshold)
     float inv_res = 0.0f;  // 1 / res when res is a power of two
@@ -509,7 +510,7 @@ int prepare_lists(ndt_ctx *c, int B, int max_tiles, TileLists &L) {
     return NDT_OK;
 }
 
-int chunk_big(const ndt_ctx *c) { return c->prm.precision == 1 ? 1 : kChunkBig; }
+int chunk_big(const ndt_ctx *c) { return c->prm.precision == 1 ? 1 : c->chunk_tiles; }
 int chunk_small(const ndt_ctx *c) { return c->prm.precision == 1 ? 1 : kChunkSmall; }
 
 // Device-side batch: everything already on the device.
@@ -1290,8 +1291,9 @@ int ndt_get_kernel_variant(ndt_ctx *c) { return c ? c->variant : NDT_E_ARG; }
 
 // Times a device batch with every launch shape of the FP32 derivative pass
 // (one untimed warm call each, then `repeats` calls timed with CUDA events on
-// the context stream; the minimum counts) and selects the fastest.  Results
-// go to the context's own output buffers.
+// the context stream; the minimum counts) and selects the fastest; then, with
+// that shape, every chunk size of kChunkChoices, and selects the fastest.
+// Results go to the context's own output buffers.
 int ndt_autotune_batch_device(ndt_ctx *c, int B, const float *d_points, const int *d_offsets, int total_points,
                               const float *d_guesses, int repeats, int *best, float *ms_per_variant) {
     if (!c || !d_points || !d_offsets || !d_guesses || B <= 0 || repeats < 1)
@@ -1313,38 +1315,55 @@ int ndt_autotune_batch_device(ndt_ctx *c, int B, const float *d_points, const in
         cudaEventDestroy(e0);
         return cuda_fail(c, ee, "cudaEventCreate");
     }
-    const int keep = c->variant;
+    // the fastest of `repeats` timed calls of the current configuration, after one warm call
+    auto time_config = [&](float &best_ms) -> int {
+        best_ms = -1.0f;
+        for (int r = 0; r <= repeats; ++r) {
+            if (r > 0 && (ee = cudaEventRecord(e0, c->stream)) != cudaSuccess) return cuda_fail(c, ee, "cudaEventRecord");
+            if (int rc = run_batch(c, B, (const float4 *)d_points, d_offsets, total_points, d_guesses,
+                                   c->out_T.as<float>(), c->out_conv.as<int>(), c->out_fit.as<double>(),
+                                   c->out_status.as<int>()))
+                return rc;
+            if (r == 0) continue;
+            float ms = 0.0f;
+            if ((ee = cudaEventRecord(e1, c->stream)) != cudaSuccess || (ee = cudaEventSynchronize(e1)) != cudaSuccess ||
+                (ee = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess)
+                return cuda_fail(c, ee, "autotune timing");
+            if (best_ms < 0.0f || ms < best_ms) best_ms = ms;
+        }
+        return NDT_OK;
+    };
+    const int keep = c->variant, keep_chunk = c->chunk_tiles;
     int winner = keep, rc = NDT_OK;
     float winner_ms = 0.0f;
     for (int v = 0; v < kNumDerivVariants && rc == NDT_OK; ++v) {
         c->variant = v;
-        float best_ms = -1.0f;
-        for (int r = 0; r <= repeats && rc == NDT_OK; ++r) {
-            if (r > 0 && (ee = cudaEventRecord(e0, c->stream)) != cudaSuccess) {
-                rc = cuda_fail(c, ee, "cudaEventRecord");
-                break;
-            }
-            rc = run_batch(c, B, (const float4 *)d_points, d_offsets, total_points, d_guesses, c->out_T.as<float>(),
-                           c->out_conv.as<int>(), c->out_fit.as<double>(), c->out_status.as<int>());
-            if (rc || r == 0) continue;
-            float ms = 0.0f;
-            if ((ee = cudaEventRecord(e1, c->stream)) != cudaSuccess || (ee = cudaEventSynchronize(e1)) != cudaSuccess ||
-                (ee = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess) {
-                rc = cuda_fail(c, ee, "autotune timing");
-                break;
-            }
-            if (best_ms < 0.0f || ms < best_ms) best_ms = ms;
-        }
-        if (rc) break;
-        if (ms_per_variant) ms_per_variant[v] = best_ms;
-        if (v == 0 || best_ms < winner_ms) {
+        float ms = 0.0f;
+        if ((rc = time_config(ms)) != NDT_OK) break;
+        if (ms_per_variant) ms_per_variant[v] = ms;
+        if (v == 0 || ms < winner_ms) {
             winner = v;
-            winner_ms = best_ms;
+            winner_ms = ms;
+        }
+    }
+    int chunk = keep_chunk;
+    if (rc == NDT_OK) {
+        c->variant = winner;
+        for (int k : kChunkChoices) {
+            if (k == keep_chunk) continue;  // timed above with the winning shape
+            c->chunk_tiles = k;
+            float ms = 0.0f;
+            if ((rc = time_config(ms)) != NDT_OK) break;
+            if (ms < winner_ms) {
+                chunk = k;
+                winner_ms = ms;
+            }
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     c->variant = rc ? keep : winner;
+    c->chunk_tiles = rc ? keep_chunk : chunk;
     if (rc) return rc;
     if (best) *best = winner;
     return NDT_OK;
@@ -1373,6 +1392,14 @@ int ndt_set_kernel_variant(ndt_ctx *c, int variant) {
     c->variant = variant;
     return NDT_OK;
 }
+
+int ndt_set_chunk_tiles(ndt_ctx *c, int tiles) {
+    if (!c || tiles < 1 || tiles > kMaxChunkTiles) return fail(c, NDT_E_ARG, "chunk tiles out of range");
+    c->chunk_tiles = tiles;
+    return NDT_OK;
+}
+
+int ndt_get_chunk_tiles(ndt_ctx *c) { return c ? c->chunk_tiles : NDT_E_ARG; }
 
 int ndt_kernel_variant_shape(int variant, int *tile, int *blocks_per_sm) {
     if (variant < 0 || variant >= kNumDerivVariants || !tile || !blocks_per_sm) return NDT_E_ARG;

@@ -107,6 +107,8 @@ def lib():
         L.ndt_set_kernel_variant.argtypes = [ctxp, C.c_int]
         L.ndt_set_side_queue_capacity.argtypes = [ctxp, C.c_int]
         L.ndt_get_kernel_variant.argtypes = [ctxp]
+        L.ndt_set_chunk_tiles.argtypes = [ctxp, C.c_int]
+        L.ndt_get_chunk_tiles.argtypes = [ctxp]
         L.ndt_autotune_batch_device.argtypes = [ctxp, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
                                                 C.POINTER(C.c_int), _f32p]
         L.ndt_synchronize.argtypes = [ctxp]
@@ -125,7 +127,7 @@ def lib():
                      "ndt_set_profiling", "ndt_kernel_variants", "ndt_kernel_variant_shape",
                      "ndt_set_kernel_variant", "ndt_window_info", "ndt_set_batch_graphs",
                      "ndt_set_side_queue_capacity", "ndt_get_kernel_variant", "ndt_autotune_batch_device",
-                     "ndt_score_batch_device"):
+                     "ndt_score_batch_device", "ndt_set_chunk_tiles", "ndt_get_chunk_tiles"):
             getattr(L, name).restype = C.c_int
         _LIB = L
     return _LIB
@@ -307,9 +309,16 @@ class Context:
     def kernel_variant(self):
         return self._check(self.L.ndt_get_kernel_variant(self.h), "ndt_get_kernel_variant")
 
+    def set_chunk_tiles(self, tiles):
+        """Tiles per large chunk of the FP32 derivative pass (1..64; default 8)."""
+        self._check(self.L.ndt_set_chunk_tiles(self.h, int(tiles)), "ndt_set_chunk_tiles")
+
+    def chunk_tiles(self):
+        return self._check(self.L.ndt_get_chunk_tiles(self.h), "ndt_get_chunk_tiles")
+
     def autotune_device(self, B, d_points, d_offsets, total, d_guesses, repeats=2):
-        """ndt_autotune_batch_device: times the batch with every launch shape, selects the fastest;
-        returns (best, ms per variant)."""
+        """ndt_autotune_batch_device: times the batch with every launch shape, selects the fastest, then
+        the chunk size (chunk_tiles()); returns (best, ms per variant)."""
         best = C.c_int()
         ms = np.zeros(self.L.ndt_kernel_variants(), np.float32)
         self._check(self.L.ndt_autotune_batch_device(self.h, B, C.c_void_p(d_points), C.c_void_p(d_offsets), total,

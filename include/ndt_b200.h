@@ -232,15 +232,25 @@ NDT_API int ndt_score_batch_device(ndt_ctx *ctx, int B, const float *d_points, c
  * variant (one warm call, then `repeats` timed calls each, CUDA events on the
  * context stream, minimum taken), selects the fastest on the context and
  * returns it in *best, with the times in ms_per_variant (optional,
- * ndt_kernel_variants() entries); ndt_autotune_batch takes the batch in host
- * buffers (packed as ndt_align_batch_packed).  The variant changes only the
- * FP32 summation order, never which pairs are evaluated.  No reference
+ * ndt_kernel_variants() entries), then times the chosen shape with 4, 6 and 8
+ * tiles per chunk and keeps the fastest (ndt_get_chunk_tiles reads it);
+ * ndt_autotune_batch takes the batch in host buffers (packed as
+ * ndt_align_batch_packed).  The variant and the chunk size change only the
+ * FP32 summation order, never which pairs are evaluated; with both fixed, an
+ * alignment's result does not depend on the rest of its batch.  No reference
  * counterpart (the reference has no GPU derivative pass).
+ *
+ * ndt_set_chunk_tiles: tiles of consecutive points per unit of work the FP32
+ * pass hands out (1..64; default 8).  Larger chunks pay the per-chunk hand-out
+ * and block reduction less often; smaller ones balance the end of a pass over
+ * fewer tiles better.
  */
 NDT_API int ndt_kernel_variants(void);
 NDT_API int ndt_kernel_variant_shape(int variant, int *tile, int *blocks_per_sm);
 NDT_API int ndt_set_kernel_variant(ndt_ctx *ctx, int variant);
 NDT_API int ndt_get_kernel_variant(ndt_ctx *ctx);
+NDT_API int ndt_set_chunk_tiles(ndt_ctx *ctx, int tiles);
+NDT_API int ndt_get_chunk_tiles(ndt_ctx *ctx);
 NDT_API int ndt_autotune_batch_device(ndt_ctx *ctx, int B, const float *d_points, const int *d_offsets,
                                       int total_points, const float *d_guesses, int repeats, int *best,
                                       float *ms_per_variant);

@@ -378,6 +378,7 @@ def test_library_autotune(pkg, oracle, binding_mod):
         best, ms = ctx.autotune_device(len(aligns), pts.data_ptr(), offs.data_ptr(), total, g.data_ptr())
         assert ctx.kernel_variant() == best and 0 <= best < N_VARIANTS
         assert (ms > 0).all() and ms[best] == ms.min()
+        assert ctx.chunk_tiles() in (4, 6, 8)  # the chunk size is tuned after the shape
         out, conv, _, status = ctx.align_batch([a.scan for a in aligns], [a.guess for a in aligns])
     ref, rconv, _, _ = oracle.align_batch(binding_mod.reference_params(), [a.scan for a in aligns],
                                           [a.guess for a in aligns], scene.map)
@@ -411,3 +412,31 @@ def test_c3_batched_corrected_vs_fp64_oracle(pkg, oracle, binding_mod):
     bad, worst = check_fp32_against_oracle(out[:n], ref, conv[:n], rconv, status[:n], runs, guesses[:n])
     print(f"c3 batch: {n - len(bad)}/{n} within 2 cm / 0.1 deg (worst {worst[0]:.2e} m, {worst[1]:.2e} deg), "
           f"{k['rounds']} rounds, {k['evaluations'] / len(aligns):.1f} evaluations per alignment")
+
+
+@pytest.mark.parametrize("chunk", [1, 3, 4, 16])
+def test_chunk_sizes_corrected_vs_fp64_oracle(pkg, oracle, binding_mod, chunk):
+    """Chunk sizes of the FP32 pass (ndt_set_chunk_tiles) change only the FP32
+    summation order: corrected alignments against the FP64 oracle from the
+    same guesses (check_fp32_against_oracle), and out-of-range sizes are
+    rejected."""
+    cfg = pkg.synth.small_config("ck", 30000, 50.0, 20, 3000, seed=63)
+    scene = pkg.synth.make_scene(cfg)
+    aligns = [pkg.synth.make_alignment(cfg, scene, i, n_points=600 + 700 * (i % 5)) for i in range(12)]
+    scans, guesses = [a.scan for a in aligns], np.stack([a.guess for a in aligns])
+    with pkg.ndt.Context(pkg.ndt.corrected_params(cfg.resolution)) as ctx:
+        ctx.set_chunk_tiles(chunk)
+        assert ctx.chunk_tiles() == chunk
+        for bad in (0, 65):
+            with pytest.raises(pkg.ndt.NdtError):
+                ctx.set_chunk_tiles(bad)
+        assert ctx.chunk_tiles() == chunk
+        ctx.set_map(scene.map)
+        out, conv, _, status = ctx.align_batch(scans, guesses)
+        # an alignment's result does not depend on the rest of its batch
+        one = ctx.align_batch(scans[3:4], guesses[3:4])[0]
+        assert np.array_equal(one.view(np.uint32), out[3:4].view(np.uint32))
+    prm = binding_mod.corrected_params(cfg.resolution)
+    ref, rconv, _, _ = oracle.align_batch(prm, scans, guesses, scene.map)
+    runs = [lambda g, i=i: oracle.align(prm, scans[i], g, scene.map)[0] for i in range(len(aligns))]
+    check_fp32_against_oracle(out, ref, conv, rconv, status, runs, guesses)
