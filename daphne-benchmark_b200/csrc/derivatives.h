@@ -42,7 +42,7 @@ constexpr int kMaxChunkTiles = 64;
 // c5: 21k chunks per pass; 4 the smaller c3 / c4 batches, where the end of
 // the pass is a larger share)
 constexpr int kChunkChoices[] = {4, 6, 8};
-constexpr int kChunkSmall = 2;  // tiles per small chunk of the FP32 pass (the FP64 pass: 1)
+constexpr int kChunkSmall = 4;  // tiles per small chunk of the FP32 pass, at most the large size (the FP64 pass: 1)
 
 // Per-device set-up (dynamic shared memory opt-in); call with the device current.
 int prepare_derivatives();

@@ -511,7 +511,7 @@ int prepare_lists(ndt_ctx *c, int B, int max_tiles, TileLists &L) {
 }
 
 int chunk_big(const ndt_ctx *c) { return c->prm.precision == 1 ? 1 : c->chunk_tiles; }
-int chunk_small(const ndt_ctx *c) { return c->prm.precision == 1 ? 1 : kChunkSmall; }
+int chunk_small(const ndt_ctx *c) { return c->prm.precision == 1 ? 1 : std::min(kChunkSmall, c->chunk_tiles); }
 
 // Device-side batch: everything already on the device.
 // Round-loop condition of a batch graph: another round while an alignment
