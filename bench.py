@@ -604,7 +604,9 @@ def learned_cpu_leg(pkg, scene, cfg, aligns, plain_out, learned_out, learned_sta
     else:
         base = None
     orc = binding.Oracle()
-    m = min(len(aligns), 64)
+    # 256 alignments: the population comparison (how often each reaches the truth) of chaotic refinement chains
+    # needs more than 64 to separate a real difference from sampling noise
+    m = min(len(aligns), 256)
     sc = [a.scan for a in aligns[:m]]
     prm = binding.corrected_params(cfg.resolution)
     t0 = time.perf_counter()
