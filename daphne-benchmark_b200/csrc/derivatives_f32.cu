@@ -287,7 +287,7 @@ __global__ void flagged_kernel(const __grid_constant__ EvalArgs args) {
 // A warp with more pairs than kDenseThreshold in one collect call evaluates
 // them per point; fewer go to its ring of deferred pairs.  The ring holds
 // fewer than 32 pairs between calls and receives at most kDenseThreshold, so
-// kDefer >= 31 + kDenseThreshold; 64 keeps the 128-thread block at 35.5 KB of
+// kDefer >= 31 + kDenseThreshold; 64 keeps the 128-thread block at 35.7 KB of
 // shared memory, so that 6 blocks fit on an SM.
 constexpr int kDefer = 64;            // per-warp ring of deferred pairs (power of two)
 constexpr int kDenseThreshold = 32;
@@ -309,13 +309,13 @@ struct F32Smem {
 // result does not depend on timing.  A chunk in which no warp found a pair
 // writes its zeros directly.
 template <int W>
-__device__ void reduce_run(F32Smem<W> &sm, double *s_tot, const unsigned (*s_cnt)[3], double *out, double kR,
+__device__ void reduce_run(F32Smem<W> &sm, double *s_tot, const unsigned *s_pairs, double *out, double kR,
                            bool compat) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     __syncthreads();
     unsigned np = 0;
 #pragma unroll
-    for (int w = 0; w < W; ++w) np += s_cnt[w][2];
+    for (int w = 0; w < W; ++w) np += s_pairs[w];
     if (np == 0) {  // block-uniform
         if (threadIdx.x < kPartial) out[threadIdx.x] = 0.0;
         return;
@@ -472,7 +472,7 @@ __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(const __grid
     __shared__ float s_ang[kAngle];
     __shared__ int s_mode;
     __shared__ double s_tot[kAcc];
-    __shared__ unsigned s_cnt[kW][3];
+    __shared__ unsigned s_pairs[kW];  // pairs each warp found in the current chunk
     __shared__ int s_chunk[2];
     // per-warp work counters (points, tiles, probes, occupied probes, pairs), kept
     // only when the caller asked for counters (in shared memory: no registers)
@@ -498,7 +498,7 @@ __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(const __grid
 
     const int nc = args.num_active ? *args.num_active : *args.num_chunks;
     for (int k = 0; k < kAcc; ++k) P.acc[k * TILE] = 0.0f;
-    if (lane == 0) s_cnt[warp][0] = s_cnt[warp][1] = s_cnt[warp][2] = 0;
+    if (lane == 0) s_pairs[warp] = 0;
     if (lane == 0)
         for (int q = 0; q < 5; ++q) s_work[warp][q] = 0;
     unsigned head = 0, tail = 0;  // deferred ring of this warp (warp-uniform)
@@ -576,7 +576,7 @@ __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(const __grid
             // per-warp work counters: the pairs feed the partial's count; the
             // others only when the caller asked for counters
             n_pair = __reduce_add_sync(kFull, n_pair);
-            if (lane == 0) s_cnt[warp][2] += n_pair;
+            if (lane == 0) s_pairs[warp] += n_pair;
             if (args.counters) {
                 const unsigned probes = __reduce_add_sync(kFull, n_probe);
                 const unsigned occupied = __reduce_add_sync(kFull, n_occ);
@@ -591,9 +591,9 @@ __global__ void __launch_bounds__(TILE, MINB) derivative_f32_kernel(const __grid
         }
         // end of the chunk (the last collect call emptied the ring): the block's sums
         head = tail = 0;
-        reduce_run<kW>(sm, s_tot, s_cnt, args.partials + (size_t)ck.slot * kPartial, compat ? -args.d2 : 1.0, compat);
+        reduce_run<kW>(sm, s_tot, s_pairs, args.partials + (size_t)ck.slot * kPartial, compat ? -args.d2 : 1.0, compat);
         __syncthreads();
-        if (lane == 0) s_cnt[warp][0] = s_cnt[warp][1] = s_cnt[warp][2] = 0;
+        if (lane == 0) s_pairs[warp] = 0;
     }
     if (args.counters && lane == 0 && s_work[warp][1]) {
         if (warp == 0) {  // every warp of the block saw the same tiles
