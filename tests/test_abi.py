@@ -52,6 +52,10 @@ def test_bad_arguments_rejected(pkg):
     p = pkg.ndt.reference_params()
     p.precision = 7
     assert L.ndt_create(ctypes.byref(p), 0, ctypes.byref(h)) == -1
+    # context setters reject a null context before touching a device
+    assert L.ndt_set_chunk_tiles(None, 8) == -1
+    assert L.ndt_get_chunk_tiles(None) == -1
+    assert L.ndt_set_kernel_variant(None, 0) == -1
 
 
 def test_no_cpu_fallback_without_device(pkg):
