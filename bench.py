@@ -614,9 +614,10 @@ def learned_cpu_leg(pkg, scene, cfg, aligns, plain_out, learned_out, learned_sta
     t_plain = time.perf_counter() - t0
     t0 = time.perf_counter()
     cur = learned_start[:m]
-    for lvl in levels_spec:
+    for lvl in levels_spec:  # each level on the points the pipeline gives it (an evenly strided subsample)
         op = pkg.learned.level_params(binding.corrected_params(lvl["resolution"]), lvl)
-        cur = orc.align_batch(op, sc, cur, scene.map, nthreads=cores)[0]
+        lsc = [pkg.learned.subsample(s, lvl.get("points_per_scan", 0)) for s in sc]
+        cur = orc.align_batch(op, lsc, cur, scene.map, nthreads=cores)[0]
     t_learned = time.perf_counter() - t0
     out["corrected_fp64_oracle_plain"] = {"value": m / t_plain, "cores": cores,
                                           "sample": f"{m} alignments ({t_plain:.1f} s)"}
@@ -634,7 +635,7 @@ def learned_cpu_leg(pkg, scene, cfg, aligns, plain_out, learned_out, learned_sta
     def learned_run(i, g):
         for lvl in levels_spec:
             op = pkg.learned.level_params(binding.corrected_params(lvl["resolution"]), lvl)
-            g = orc.align(op, sc[i], g, scene.map)[0]
+            g = orc.align(op, pkg.learned.subsample(sc[i], lvl.get("points_per_scan", 0)), g, scene.map)[0]
         return g
 
     def unstable(run, i, start):

@@ -85,6 +85,16 @@ def make_pairs(cfg, scene, n_scans, per_scan, dt, dyaw_deg, seed, first_index=10
     return Pairs(scans, np.stack(truths), np.asarray(pair_scan, np.int64), np.stack(guesses))
 
 
+def subsample(scan, max_points):
+    """The evenly strided subsample a pipeline level reads (the library's
+    subsample_kernel): point (j n) / m of the scan for j < m = min(n,
+    max_points); the whole scan when max_points is 0 or None."""
+    n = len(scan)
+    if not max_points or n <= max_points:
+        return scan
+    return np.ascontiguousarray(scan[(np.arange(max_points) * n) // max_points])
+
+
 class DeviceScans:
     """Scans resident on the device (concatenated), with helpers that build
     packed batches of pairs by gathering on the device."""
@@ -92,8 +102,7 @@ class DeviceScans:
     def __init__(self, torch, scans, max_points=None):
         self.torch = torch
         if max_points:
-            scans = [s[(np.arange(min(len(s), max_points)) * len(s)) // max(1, min(len(s), max_points))]
-                     for s in scans]
+            scans = [subsample(s, max_points) for s in scans]
         self.sizes = np.array([len(s) for s in scans], np.int64)
         self.starts = np.zeros(len(scans) + 1, np.int64)
         self.starts[1:] = np.cumsum(self.sizes)

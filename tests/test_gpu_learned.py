@@ -121,11 +121,11 @@ def test_learned_refinement_vs_fp64_oracle(pkg, trained, binding_mod, oracle):
     starts = cur.copy()
     prms = []
     for lvl in L.refinement_levels(cfg.resolution):
-        prms.append(L.level_params(binding_mod.corrected_params(lvl["resolution"]), lvl))
+        prms.append((L.level_params(binding_mod.corrected_params(lvl["resolution"]), lvl), lvl["points_per_scan"]))
 
     def chain(i, g):
-        for op in prms:
-            g = oracle.align(op, scans[i], g, scene.map)[0]
+        for op, cap in prms:  # each level on the points the pipeline gives it
+            g = oracle.align(op, L.subsample(scans[i], cap), g, scene.map)[0]
         return g
 
     ref = np.stack([chain(i, starts[i]) for i in range(len(sample))])
