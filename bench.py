@@ -553,18 +553,27 @@ def run_ours(args, pkg, world, rank, local):
     return 0
 
 
+# Start grid of the learned pipeline per workload, measured on B200 (one trained network each, 4096 / 1024
+# alignments): c5 (guesses +-3 m / +-15 deg) runs the library's default, 3 x 3 x 3 starts 2.5 m and 10 deg apart
+# with 2 network passes: 45 % reach the truth, 13.2k accurate aligns/s, against 32 % and 10.9k with 3 x 3 starts
+# 1.5 m apart and 3 passes.  c4 (+-2 m / +-10 deg, a network trained on half the scans) is the other way round:
+# 3 x 3 starts 1.5 m apart with 3 passes reach 57 % (23.8k/s), 3 x 3 x 3 starts 1.67 m / 6.7 deg apart with
+# 2 passes 49 % (17.3k/s).
+LEARNED_STARTS = {"c4": dict(grid_yaw=1, passes=3, step_xy=1.5)}
+
+
 def learned_config_block(pkg, cfg, B, npts):
     """The `config` of the learned-vs-plain workload (both arms print it)."""
     levels_spec = pkg.learned.refinement_levels(cfg.resolution)
-    lp = pkg.learned.pipeline_params(levels_spec)
+    lp = pkg.learned.pipeline_params(levels_spec, **LEARNED_STARTS.get(cfg.name, {}))
     return {"workload": f"{cfg.name}: {cfg.map_points}-point map ({cfg.area:g} x {cfg.area:g} m, {cfg.walls} walls), "
                         f"{B} alignments per step, scans {cfg.scan_min}-{cfg.scan_max} points (log-uniform), "
                         f"resolution {cfg.resolution:g} m, guesses +-{cfg.dt:g} m / +-{cfg.dyaw_deg:g} deg; "
                         f"learned-init vs plain batched NDT",
             "alignments_per_step": B, "scan_points_per_step": npts, "map_points": cfg.map_points,
             "resolution_m": cfg.resolution, "mode": "corrected",
-            "learned": {"starts": f"{lp.grid_xy} x {lp.grid_xy} translations {lp.step_xy:g} m apart x {lp.grid_yaw} "
-                                  f"yaw", "network_passes": lp.passes,
+            "learned": {"starts": f"{lp.grid_xy} x {lp.grid_xy} translations {lp.step_xy:.3g} m apart x {lp.grid_yaw} "
+                                  f"yaws {lp.step_yaw_deg:.3g} deg apart", "network_passes": lp.passes,
                         "judge": f"NDT score at {levels_spec[lp.judge_level]['resolution']:g} m on {lp.judge_points} "
                                  f"points per scan, raw guess kept when no proposal scores higher",
                         "refinement_levels": levels_spec},
@@ -760,7 +769,7 @@ def run_learned(args, pkg, world, rank, local):
             for k in ("plain", "learned")}
     d_choice = torch.zeros(B, dtype=torch.int32, device=dev)
     d_start = torch.zeros(B, 16, device=dev)
-    lp = L.pipeline_params(levels_spec)
+    lp = L.pipeline_params(levels_spec, **LEARNED_STARTS.get(cfg.name, {}))
     # the derivative pass's launch shape per level context, autotuned once (untimed) on this step's scans and
     # raw guesses at the level's resolution and point budget (ndt_autotune_batch_device): the fastest shape
     # depends on the voxel size (0.5 m: 128 x 6, 1-2 m: 128 x 5 on B200)

@@ -251,11 +251,11 @@ void ndt_learned_params_default(ndt_learned_params *p) {
     if (!p) return;
     std::memset(p, 0, sizeof(*p));
     p->max_points = 1024;
-    p->passes = 3;
+    p->passes = 2;
     p->grid_xy = 3;
-    p->grid_yaw = 1;
-    p->step_xy = 1.5f;
-    p->step_yaw_deg = 7.5f;
+    p->grid_yaw = 3;
+    p->step_xy = 2.5f;
+    p->step_yaw_deg = 10.0f;
     p->judge_level = 0;
     p->judge_points = 2048;
 }

@@ -421,7 +421,8 @@ typedef struct ndt_learned_params {
     int32_t judge_points;  /* points per scan in the score pass (0 = all) */
     int32_t level_points[NDT_LEARNED_MAX_LEVELS];  /* points per scan at each refinement level (0 = all) */
 } ndt_learned_params;
-/* Defaults: 1024 points, 3 passes, a 3 x 3 grid of starts 1.5 m apart, judge at level 0 on 2048 points. */
+/* Defaults: 1024 points, 2 passes, a 3 x 3 x 3 grid of starts 2.5 m and 10 deg apart (for guesses within
+ * +-3 m / +-15 deg), judge at level 0 on 2048 points. */
 NDT_API void ndt_learned_params_default(ndt_learned_params *p);
 NDT_API int ndt_align_batch_learned_device(ndt_mlp *mlp, ndt_ctx *const *levels, int n_levels,
                                            const ndt_learned_params *lp, int B, const float *d_points,

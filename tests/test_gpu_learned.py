@@ -74,12 +74,12 @@ def test_learned_pipeline_gain(pkg, trained):
     assert np.median(p_dt) < 0.6 * np.median(g_dt)
 
     plain = L.ndt_align_device(levels[-1], torch, pts, offs, total, guesses)
-    prm = pkg.posenet.learned_params(grid_xy=3, step_xy=0.5, judge_points=1024)
+    prm = pkg.posenet.learned_params(grid_xy=3, grid_yaw=1, passes=3, step_xy=0.5, judge_points=1024)
     lb = L.LearnedBatch(levels, net, torch, pts, offs, total, guesses, prm)
     lb.run()
     out, conv, fit, st, choice, _ = lb.results()
     nonet = L.LearnedBatch(levels, net, torch, pts, offs, total, guesses,
-                           pkg.posenet.learned_params(grid_xy=3, step_xy=0.5, judge_points=1024, passes=0))
+                           pkg.posenet.learned_params(grid_xy=3, grid_yaw=1, step_xy=0.5, judge_points=1024, passes=0))
     nonet.run()
     out0 = nonet.results()[0]
     ok_plain, ok_learned, ok_nonet = (float(_ok(L, o, truths).mean()) for o in (plain[0], out, out0))
@@ -112,7 +112,7 @@ def test_learned_refinement_vs_fp64_oracle(pkg, trained, binding_mod, oracle):
     sample = aligns[:32]
     scans = [a.scan for a in sample]
     guesses = np.stack([a.guess for a in sample])
-    prm = pkg.posenet.learned_params(grid_xy=3, step_xy=0.5, judge_points=1024)
+    prm = pkg.posenet.learned_params(grid_xy=3, grid_yaw=1, passes=3, step_xy=0.5, judge_points=1024)
     dev = L.DeviceScans(torch, scans)
     pts, offs, total = dev.batch(np.arange(len(sample)))
     lb = L.LearnedBatch(levels, net, torch, pts, offs, total, guesses, prm)
