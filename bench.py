@@ -572,8 +572,9 @@ def learned_config_block(pkg, cfg, B, npts):
                         f"learned-init vs plain batched NDT",
             "alignments_per_step": B, "scan_points_per_step": npts, "map_points": cfg.map_points,
             "resolution_m": cfg.resolution, "mode": "corrected",
-            "learned": {"starts": f"{lp.grid_xy} x {lp.grid_xy} translations {lp.step_xy:.3g} m apart x {lp.grid_yaw} "
-                                  f"yaws {lp.step_yaw_deg:.3g} deg apart", "network_passes": lp.passes,
+            "learned": {"starts": f"{lp.grid_xy} x {lp.grid_xy} translations {lp.step_xy:.3g} m apart x "
+                                  + (f"{lp.grid_yaw} yaws {lp.step_yaw_deg:.3g} deg apart" if lp.grid_yaw > 1
+                                     else "1 yaw"), "network_passes": lp.passes,
                         "judge": f"NDT score at {levels_spec[lp.judge_level]['resolution']:g} m on {lp.judge_points} "
                                  f"points per scan, raw guess kept when no proposal scores higher",
                         "refinement_levels": levels_spec},
